@@ -1,0 +1,164 @@
+/*
+ * skgemm — C ABI of the B200 (sm_100a) FP64 Stream-K GEMM / SYRK / rotation
+ * library for the dense subspace steps of a real-space DFT eigensolver
+ * (S = Psi^T Psi, Hs = Psi^T (H Psi), Psi' = Psi Q).
+ *
+ * The entry points mirror the static C++ entry points of the reference
+ * (shriramch/stream-k-gemm), which are host-side, blocking, FP64 and operate
+ * on caller-owned buffers in the reference's packed layouts:
+ *
+ *   packed16 (band-tile, "A" of GEMM/SYRK):  X[(m/16)*K*16 + k*16 + m%16] = X(k, m)
+ *   packed32 (band-tile, "B" of GEMM):       X[(n/32)*K*32 + k*32 + n%32] = X(k, n)
+ *   grid-packed (rotation input):            A[(g/16)*nb*16 + b*16 + g%16]
+ *   band-packed (rotation output):           D[(b/16)*Nd*16 + g*16 + b%16]
+ *
+ * Differences from the reference, all deliberate:
+ *   - Remainders are computed. A packed16 buffer holds ceil(M/16) tiles and a
+ *     packed32 buffer ceil(N/32) tiles (padding rows may hold any finite or
+ *     non-finite value: they only feed output rows/columns that are not
+ *     stored). The reference drops M%16 rows and N%32 columns of the GEMM
+ *     (gemm_opt.cpp:318, :249) and its SYRK stores past C when M%16 != 0
+ *     (syrk_crsp.cpp:152-165); here every stored element is in bounds.
+ *   - SYRK applies alpha and beta exactly once: C = alpha*A^T*A + beta*C on the
+ *     upper triangle. The reference scales only the last K chunk by alpha when
+ *     K > 256 (sme_syrk.hpp:123-133); both agree for alpha = 1.
+ *   - Sizes are int64_t (the reference uses int).
+ *   - Every call returns a status (the reference has none).
+ *
+ * Host-pointer entry points are blocking: they stage inputs into device memory
+ * (pinned or pageable host memory both work), run, copy the result back and
+ * synchronise. The *_dev entry points take device pointers and a CUDA stream
+ * (cudaStream_t passed as void*, NULL = legacy default stream) and are
+ * asynchronous; device-side failures of an asynchronous call (a bounded wait
+ * that ran out) are reported by skgemm_stream_status().
+ */
+#ifndef SKGEMM_H
+#define SKGEMM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SKGEMM_OK 0
+#define SKGEMM_ERR_INVALID_ARG (-1)    /* bad shape, NULL pointer, bad option */
+#define SKGEMM_ERR_OOM (-2)            /* device memory or HBM budget exhausted */
+#define SKGEMM_ERR_CUDA (-3)           /* CUDA runtime / driver error */
+#define SKGEMM_ERR_DEVICE_TIMEOUT (-4) /* a bounded device-side wait expired */
+#define SKGEMM_ERR_NO_DEVICE (-5)      /* no sm_100 device visible */
+#define SKGEMM_ERR_UNSUPPORTED (-6)    /* valid request this build cannot serve */
+
+/* ------------------------------------------------------------- precision */
+/* SKGEMM_PREC_NATIVE: FP64 DMMA tensor cores, Stream-K. The plain method and
+ * the drop-in for the reference call.
+ * SKGEMM_PREC_OZAKI_I8: Ozaki scheme II (Chinese-remainder reconstruction) —
+ * operands scaled to integers, reduced modulo `slices` pairwise-coprime
+ * moduli <= 256, INT8 x INT8 -> INT32 products on tcgen05 tensor cores,
+ * FP64 reconstruction. */
+#define SKGEMM_PREC_NATIVE 0
+#define SKGEMM_PREC_OZAKI_I8 1
+
+typedef struct skgemm_options {
+  int precision;        /* SKGEMM_PREC_* */
+  int slices;           /* Ozaki: number of moduli; 0 = choose automatically */
+  double err_bound_out; /* out: a-priori bound of the relative Frobenius error
+                           contributed by the split (0 for native) */
+  int slices_used_out;  /* out: moduli actually used */
+} skgemm_options_t;
+
+/* -------------------------------------------------- library / diagnostics */
+const char* skgemm_version(void);
+/* Message of the most recent failing call on this host thread. */
+const char* skgemm_last_error(void);
+/* Synchronise `stream` and report (then clear) device-side failures of the
+ * asynchronous calls issued on it since the last check. */
+int skgemm_stream_status(void* stream);
+/* Measured FP64 tensor-core (DMMA m16n8k8) throughput of the current device,
+ * TFLOP/s, from a register-resident peak loop; the analogue of the
+ * reference's FMOPA peak probe (sme_peak_microbench.cpp:16-61). */
+int skgemm_probe_fp64_peak(double* tflops_out);
+
+/* --------------------------------------------------------------- GEMM */
+/* D = alpha * A * B + gamma (gamma added to every element).
+ * A column-major M x K (A[i + k*M]), B row-major K x N (B[k*N + j]),
+ * D row-major M x N (D[i*N + j]). Host pointers.
+ * Replaces gemm<double>::compute_test (gemm_opt.cpp:376-392) and the Stream-K
+ * check's gemm<double>::compute_test (gemm_crsp.cpp:369-385). */
+int skgemm_dgemm(int64_t M, int64_t N, int64_t K, const double* A_colmajor,
+                 const double* B_rowmajor, double* D_rowmajor, double alpha,
+                 double gamma);
+
+/* Same contract on packed operands: A packed16 (ceil(M/16) tiles), B packed32
+ * (ceil(N/32) tiles), D row-major. Host pointers.
+ * Replaces gemm<double>::compute_packed (gemm_opt.cpp:314-337) and
+ * gemm<double>::compute_streamk_packed (gemm_crsp.cpp:316-337). */
+int skgemm_dgemm_packed(int64_t M, int64_t N, int64_t K, const double* A_packed16,
+                        const double* B_packed32, double* D_rowmajor, double alpha,
+                        double gamma);
+
+/* Device-pointer, stream-ordered forms of the two calls above.
+ * ldd = row stride of D (>= N). */
+int skgemm_dgemm_dev(int64_t M, int64_t N, int64_t K, const double* A_colmajor,
+                     int64_t lda, const double* B_rowmajor, int64_t ldb, double* D,
+                     int64_t ldd, double alpha, double gamma, void* stream);
+int skgemm_dgemm_packed_dev(int64_t M, int64_t N, int64_t K, const double* A_packed16,
+                            const double* B_packed32, double* D, int64_t ldd,
+                            double alpha, double gamma, void* stream);
+/* Packed GEMM with a precision selector (native or Ozaki). */
+int skgemm_dgemm_packed_dev_opt(int64_t M, int64_t N, int64_t K,
+                                const double* A_packed16, const double* B_packed32,
+                                double* D, int64_t ldd, double alpha, double gamma,
+                                skgemm_options_t* opts, void* stream);
+
+/* --------------------------------------------------------------- SYRK */
+/* C = alpha * A^T * A + beta * C on the upper triangle (m1 <= m2) of the
+ * column-major M x M matrix C (C[m1 + m2*M]); A packed16 K x M. The strict
+ * lower triangle of C is not touched. beta == 0 does not read C.
+ * Replaces sme_syrk<double>::compute (include/sme_syrk.hpp:137-149) and the
+ * 8-ZA check sme_syrk<double>::compute (syrk_crsp.cpp:306-348). Host pointers. */
+int skgemm_dsyrk_packed(int64_t K, int64_t M, const double* A_packed16,
+                        double* C_colmajor, double alpha, double beta);
+/* Device-pointer form; ldc = column stride of C (>= M). */
+int skgemm_dsyrk_packed_dev(int64_t K, int64_t M, const double* A_packed16, double* C,
+                            int64_t ldc, double alpha, double beta, void* stream);
+int skgemm_dsyrk_packed_dev_opt(int64_t K, int64_t M, const double* A_packed16,
+                                double* C, int64_t ldc, double alpha, double beta,
+                                skgemm_options_t* opts, void* stream);
+
+/* ----------------------------------------------------- subspace rotation */
+/* D = A * Q: Psi' = Psi Q. A grid-packed Nd x nb, Q row-major nb x nb,
+ * D band-packed Nd x nb. No scaling (the CheFSI rotation never needs it).
+ * Host pointers. Nd % 16 == 0 and nb % 16 == 0 are required by the packed
+ * layouts themselves (the reference further requires nb % 32 == 0,
+ * sme_trp_3d.hpp:108-109).
+ * Replaces sme_gemm_trp_3d<double>::compute (include/sme_trp_3d.hpp:194-215). */
+int skgemm_drot(int64_t Nd, int64_t nb, const double* A_gridpacked,
+                const double* Q_rowmajor, double* D_bandpacked);
+int skgemm_drot_dev(int64_t Nd, int64_t nb, const double* A_gridpacked,
+                    const double* Q_rowmajor, double* D_bandpacked, void* stream);
+int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A_gridpacked,
+                        const double* Q_rowmajor, double* D_bandpacked,
+                        skgemm_options_t* opts, void* stream);
+
+/* ------------------------------------------------------ layout converters */
+/* Device-side packing, the B200 counterpart of gemm<double>::pack_A / pack_B
+ * (gemm_opt.cpp:342-371): strided dense X(r, k) = X[r*sr + k*sk] ->
+ * packed-T panels X[(r/T)*K*T + k*T + r%T], T in {16, 32}, zero padding for
+ * r >= R. */
+int skgemm_pack_dev(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk,
+                    int T, double* X_packed, void* stream);
+/* Band-packed <-> grid-packed conversion of an Nd x nb block of states
+ * (sme_pack<double>::band_to_grid_tile / grid_to_band_tile,
+ * include/sme_pack.hpp:232-313). */
+int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src_band,
+                            double* dst_grid, void* stream);
+int skgemm_grid_to_band_dev(int64_t Nd, int64_t nb, const double* src_grid,
+                            double* dst_band, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SKGEMM_H */

@@ -1,0 +1,193 @@
+"""CPU oracle — TEST INFRASTRUCTURE.
+
+Used only by tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg, as the checker (never as the thing measured on the GPU, never shipped):
+
+* ``liboracle.so`` (oracle.c): restatements of the reference's portable
+  reference loops (gemm_opt.cpp:467-475, syrk_crsp.cpp:355-373,
+  trp_3d_test.cpp:55-66) and a double-double (Dot2) accurate oracle;
+* ``_ref/libref_*.so``: the reference's own kernel files compiled in place
+  with a host emulation of the SME intrinsics they use (ref_shim/arm_sme.h),
+  built by ``make ref`` where the reference tree exists and carried as built
+  files elsewhere.
+
+Parity status: pinned — the emulated reference passes all of its own
+known-answer tests (gemm_opt 4/4, gemm_crsp 4/4, syrk_crsp 5/5, trp_3d 6/6),
+and the restatements are checked against it in tests/test_oracle.py.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i64 = ctypes.c_int64
+_lib: Optional[ctypes.CDLL] = None
+_refs: dict = {}
+
+
+def build(reference_root: str = "/root/reference") -> None:
+    """make liboracle.so, and oracle/_ref when the reference tree is present."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    if os.path.isdir(reference_root):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}"], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.oracle_gemm_naive.argtypes = [_i64, _i64, _i64, _f64p, _f64p, _f64p,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.oracle_syrk_naive.argtypes = [_i64, _i64, _f64p, _f64p, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int]
+        L.oracle_rot_naive.argtypes = [_i64, _i64, _f64p, _f64p, _f64p, ctypes.c_int]
+        L.oracle_dot2_gemm.argtypes = [_i64, _i64, _i64, _f64p, _i64, _i64, _f64p, _i64, _i64,
+                                       _f64p, _i64, _i64, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int]
+        L.oracle_dot2_sampled.argtypes = [_i64, ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.POINTER(ctypes.c_int64), _i64, _f64p, _i64,
+                                          _i64, _f64p, _i64, _i64, _f64p, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int]
+        L.oracle_pack.argtypes = [_i64, _i64, _f64p, _i64, _i64, ctypes.c_int, _f64p]
+        L.oracle_init_A_packed_rand.argtypes = [_i64, _i64, _f64p, ctypes.c_int]
+        for f in ("oracle_gemm_naive", "oracle_syrk_naive", "oracle_rot_naive",
+                  "oracle_dot2_gemm", "oracle_dot2_sampled", "oracle_pack",
+                  "oracle_init_A_packed_rand"):
+            getattr(L, f).restype = None
+        _lib = L
+    return _lib
+
+
+def ref(name: str) -> ctypes.CDLL:
+    """The reference's own kernel file ``name`` built in place (oracle/_ref)."""
+    if name not in _refs:
+        path = os.path.join(REF_DIR, f"libref_{name}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+        _refs[name] = ctypes.CDLL(path)
+    return _refs[name]
+
+
+def have_ref() -> bool:
+    return all(os.path.exists(os.path.join(REF_DIR, f"libref_{n}.so"))
+               for n in ("gemm_opt", "gemm_crsp", "sme_syrk", "syrk_crsp", "trp_3d"))
+
+
+def ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_f64p)
+
+
+def nthreads() -> int:
+    return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------- layouts
+def pack(X: np.ndarray, T: int) -> np.ndarray:
+    """(R, K) matrix -> packed-T panels [ceil(R/T)][K][T], zero padded."""
+    R, K = X.shape
+    tiles = (R + T - 1) // T
+    P = np.zeros((tiles * T, K))
+    P[:R] = X
+    return np.ascontiguousarray(P.reshape(tiles, T, K).transpose(0, 2, 1))
+
+
+def unpack(P: np.ndarray, R: int) -> np.ndarray:
+    """packed-T panels [tiles][K][T] -> (R, K) matrix."""
+    tiles, K, T = P.shape
+    return np.ascontiguousarray(P.transpose(0, 2, 1).reshape(tiles * T, K)[:R])
+
+
+def grid_pack(A: np.ndarray) -> np.ndarray:
+    """(Nd, nb) states -> grid-packed [Nd/16][nb][16] (trp_3d_test.cpp:31-39)."""
+    return pack(A, 16)
+
+
+def band_pack(A: np.ndarray) -> np.ndarray:
+    """(Nd, nb) states -> band-packed [nb/16][Nd][16] (trp_3d_test.cpp:41-49)."""
+    return pack(np.ascontiguousarray(A.T), 16)
+
+
+def band_unpack(P: np.ndarray, Nd: int) -> np.ndarray:
+    tiles, Nd_, T = P.shape
+    return np.ascontiguousarray(unpack(P, tiles * T).T[:Nd])
+
+
+# ----------------------------------------------------------------- oracles
+def gemm_naive(A_col: np.ndarray, B_row: np.ndarray, M, N, K, alpha=1.0, gamma=0.0,
+               threads: int = 1) -> np.ndarray:
+    D = np.zeros(M * N)
+    lib().oracle_gemm_naive(M, N, K, ptr(A_col), ptr(B_row), ptr(D), alpha, gamma, threads)
+    return D.reshape(M, N)
+
+
+def syrk_naive(Ap: np.ndarray, K, M, C: np.ndarray, alpha=1.0, beta=0.0,
+               threads: int = 1) -> np.ndarray:
+    C = np.array(C, dtype=np.float64, order="C", copy=True)
+    lib().oracle_syrk_naive(K, M, ptr(Ap), ptr(C), alpha, beta, threads)
+    return C
+
+
+def rot_naive(A_grid: np.ndarray, Q: np.ndarray, Nd, nb, threads: int = 1) -> np.ndarray:
+    D = np.zeros(Nd * nb)
+    lib().oracle_rot_naive(Nd, nb, ptr(A_grid), ptr(Q), ptr(D), threads)
+    return D
+
+
+def dot2_matmul(X: np.ndarray, Y: np.ndarray, alpha=1.0, gamma=0.0) -> np.ndarray:
+    """alpha * X @ Y + gamma, every dot product in double-double (Dot2)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    M, K = X.shape
+    K2, N = Y.shape
+    assert K == K2
+    out = np.zeros((M, N))
+    lib().oracle_dot2_gemm(M, N, K, ptr(X), K, 1, ptr(Y), N, 1, ptr(out), N, 1, alpha, gamma,
+                           nthreads())
+    return out
+
+
+def dot2_sampled(X: np.ndarray, Y: np.ndarray, ii: np.ndarray, jj: np.ndarray,
+                 alpha=1.0, gamma=0.0, x_strides=None, y_strides=None, K=None) -> np.ndarray:
+    """Entries (ii[t], jj[t]) of alpha * X @ Y + gamma in double-double.
+
+    X is indexed X.flat[i*sxi + k*sxk] and Y Y.flat[k*syk + j*syj]; the default
+    strides are those of C-contiguous (M, K) and (K, N) matrices."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    if K is None:
+        K = X.shape[1]
+    sxi, sxk = x_strides if x_strides else (X.shape[1], 1)
+    syk, syj = y_strides if y_strides else (Y.shape[1], 1)
+    ii = np.ascontiguousarray(ii, dtype=np.int64)
+    jj = np.ascontiguousarray(jj, dtype=np.int64)
+    out = np.zeros(len(ii))
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    lib().oracle_dot2_sampled(len(ii), ii.ctypes.data_as(i64p), jj.ctypes.data_as(i64p), K,
+                              ptr(X), sxi, sxk, ptr(Y), syk, syj, ptr(out), alpha, gamma,
+                              nthreads())
+    return out
+
+
+def init_A_packed_rand(K: int, M: int, seed: int) -> np.ndarray:
+    """syrk_crsp.cpp:379-395 seeded init (host C library rand())."""
+    A = np.zeros(((M + 15) // 16) * K * 16)
+    lib().oracle_init_A_packed_rand(K, M, ptr(A), seed)
+    return A
+
+
+def rel_frobenius(x: np.ndarray, ref: np.ndarray) -> float:
+    ref = np.asarray(ref, dtype=np.float64).ravel()
+    d = np.linalg.norm(np.asarray(x, dtype=np.float64).ravel() - ref)
+    n = np.linalg.norm(ref.ravel())
+    return float(d / n) if n > 0 else float(d)

@@ -1,0 +1,137 @@
+/*
+ * CPU oracle for the FP64 GEMM / SYRK / rotation path — TEST INFRASTRUCTURE
+ * (see oracle.h). Parity of these loops with the reference is pinned by
+ * tests/test_oracle.py against the reference's own kernels built from its
+ * sources (oracle/_ref) and against the committed golden vectors.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+
+static int clamp_threads(int n) { return n < 1 ? 1 : n; }
+
+/* ------------------------------------------------------------ naive loops */
+void oracle_gemm_naive(int64_t M, int64_t N, int64_t K, const double* A, const double* B,
+                       double* D, double alpha, double gamma, int nthreads) {
+  /* gemm_opt.cpp:467-475: i outer, j, then k; sum += A[i + k*M] * B[k*N + j]. */
+#pragma omp parallel for schedule(static) num_threads(clamp_threads(nthreads))
+  for (int64_t i = 0; i < M; ++i) {
+    for (int64_t j = 0; j < N; ++j) {
+      double sum = 0.0;
+      for (int64_t k = 0; k < K; ++k) sum += A[i + k * M] * B[k * N + j];
+      D[i * N + j] = alpha * sum + gamma;
+    }
+  }
+}
+
+void oracle_syrk_naive(int64_t K, int64_t M, const double* A, double* C, double alpha,
+                       double beta, int nthreads) {
+  /* syrk_crsp.cpp:360-372: m1 outer, m2 >= m1, k inner. */
+#pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(nthreads))
+  for (int64_t m1 = 0; m1 < M; ++m1) {
+    for (int64_t m2 = m1; m2 < M; ++m2) {
+      double sum = 0.0;
+      const double* a1 = A + (m1 / 16) * K * 16 + m1 % 16;
+      const double* a2 = A + (m2 / 16) * K * 16 + m2 % 16;
+      for (int64_t k = 0; k < K; ++k) sum += a1[k * 16] * a2[k * 16];
+      C[m1 + m2 * M] = alpha * sum + beta * C[m1 + m2 * M];
+    }
+  }
+}
+
+void oracle_rot_naive(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
+                      int nthreads) {
+  /* trp_3d_test.cpp:57-65: g outer, bp, then b; grid_packed_get / band_packed_set
+   * index maps of trp_3d_test.cpp:31-49. */
+#pragma omp parallel for schedule(static) num_threads(clamp_threads(nthreads))
+  for (int64_t g = 0; g < Nd; ++g) {
+    for (int64_t bp = 0; bp < nb; ++bp) {
+      double sum = 0.0;
+      const double* arow = A + (g / 16) * nb * 16 + g % 16;
+      for (int64_t b = 0; b < nb; ++b) sum += arow[b * 16] * Q[b * nb + bp];
+      D[(bp / 16) * Nd * 16 + g * 16 + bp % 16] = sum;
+    }
+  }
+}
+
+/* ------------------------------------------------------- double-double */
+/* TwoSum (Knuth): s + e = a + b exactly. */
+static inline void two_sum(double a, double b, double* s, double* e) {
+  double x = a + b;
+  double z = x - a;
+  *e = (a - (x - z)) + (b - z);
+  *s = x;
+}
+
+/* TwoProduct via fma: p + e = a * b exactly. */
+static inline void two_prod(double a, double b, double* p, double* e) {
+  double x = a * b;
+  *e = fma(a, b, -x);
+  *p = x;
+}
+
+/* Dot2 over K terms, then alpha * (s + c) + gamma in double-double. */
+static double dot2_elem(int64_t K, const double* x, int64_t sx, const double* y, int64_t sy,
+                        double alpha, double gamma) {
+  double s = 0.0, c = 0.0;
+  for (int64_t k = 0; k < K; ++k) {
+    double p, ep, es;
+    two_prod(x[k * sx], y[k * sy], &p, &ep);
+    two_sum(s, p, &s, &es);
+    c += es + ep;
+  }
+  /* Normalise (s, c), multiply by alpha, add gamma. */
+  double hi, lo;
+  two_sum(s, c, &hi, &lo);
+  double ph, pl;
+  two_prod(alpha, hi, &ph, &pl);
+  pl += alpha * lo;
+  double sh, sl;
+  two_sum(ph, gamma, &sh, &sl);
+  sl += pl;
+  return sh + sl;
+}
+
+void oracle_dot2_gemm(int64_t M, int64_t N, int64_t K, const double* X, int64_t sxi,
+                      int64_t sxk, const double* Y, int64_t syk, int64_t syj, double* out,
+                      int64_t soi, int64_t soj, double alpha, double gamma, int nthreads) {
+#pragma omp parallel for collapse(2) schedule(static) num_threads(clamp_threads(nthreads))
+  for (int64_t i = 0; i < M; ++i)
+    for (int64_t j = 0; j < N; ++j)
+      out[i * soi + j * soj] = dot2_elem(K, X + i * sxi, sxk, Y + j * syj, syk, alpha, gamma);
+}
+
+void oracle_dot2_sampled(int64_t npos, const int64_t* ii, const int64_t* jj, int64_t K,
+                         const double* X, int64_t sxi, int64_t sxk, const double* Y,
+                         int64_t syk, int64_t syj, double* out, double alpha, double gamma,
+                         int nthreads) {
+#pragma omp parallel for schedule(dynamic, 4) num_threads(clamp_threads(nthreads))
+  for (int64_t t = 0; t < npos; ++t)
+    out[t] = dot2_elem(K, X + ii[t] * sxi, sxk, Y + jj[t] * syj, syk, alpha, gamma);
+}
+
+/* ---------------------------------------------------------- layouts */
+void oracle_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, int T,
+                 double* Xp) {
+  int64_t tiles = (R + T - 1) / T;
+  for (int64_t t = 0; t < tiles; ++t)
+    for (int64_t k = 0; k < K; ++k)
+      for (int64_t i = 0; i < T; ++i) {
+        int64_t r = t * T + i;
+        Xp[(t * K + k) * T + i] = r < R ? X[r * sr + k * sk] : 0.0;
+      }
+}
+
+void oracle_init_A_packed_rand(int64_t K, int64_t M, double* A, int seed) {
+  /* syrk_crsp.cpp:381-394: one rand() per live entry, in [tm][k][ml] order. */
+  srand(seed);
+  int64_t tiles = (M + 15) / 16;
+  for (int64_t tm = 0; tm < tiles; ++tm)
+    for (int64_t k = 0; k < K; ++k)
+      for (int ml = 0; ml < 16; ++ml) {
+        int64_t m = tm * 16 + ml;
+        A[(tm * K + k) * 16 + ml] = m < M ? (double)(rand() % 100) / 100.0 : 0.0;
+      }
+}

@@ -1,0 +1,507 @@
+// C ABI of libskgemm (declared in include/skgemm.h) and the host runtime it
+// rests on: per-device state, per-stream Stream-K workspaces, staging of the
+// blocking host-pointer entry points, TMA descriptor encoding, status strings.
+#include <cudaTypedefs.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "skg_common.cuh"
+#include "skg_fp64_types.h"
+#include "skg_ozaki.h"
+#include "skg_runtime.h"
+
+namespace skg {
+
+// ------------------------------------------------------------------ status
+static thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return fail(SKGEMM_ERR_OOM, m);
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+    return fail(SKGEMM_ERR_NO_DEVICE, m);
+  return fail(SKGEMM_ERR_CUDA, m);
+}
+
+// ----------------------------------------------------------------- buffers
+int DeviceBuffer::ensure(size_t need) {
+  if (need <= bytes) return SKGEMM_OK;
+  release();
+  SKG_CUDA(cudaMalloc(&ptr, need));
+  bytes = need;
+  return SKGEMM_OK;
+}
+
+void DeviceBuffer::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+int StreamWorkspace::ensure(int slots) {
+  if ((size_t)slots <= partial_slots && err) return SKGEMM_OK;
+  if (partials) cudaFree(partials);
+  if (flags) cudaFree(flags);
+  partials = nullptr;
+  flags = nullptr;
+  partial_slots = 0;
+  SKG_CUDA(cudaMalloc(&partials, (size_t)slots * kBM * kBN * sizeof(double)));
+  SKG_CUDA(cudaMalloc(&flags, (size_t)slots * sizeof(uint32_t)));
+  SKG_CUDA(cudaMemset(flags, 0, (size_t)slots * sizeof(uint32_t)));
+  if (!err) {
+    SKG_CUDA(cudaMalloc(&err, sizeof(uint32_t)));
+    SKG_CUDA(cudaMemset(err, 0, sizeof(uint32_t)));
+  }
+  partial_slots = slots;
+  epoch = 0;
+  return SKGEMM_OK;
+}
+
+// ------------------------------------------------------------------ device
+static DeviceState g_dev[64];
+static std::mutex g_dev_mu;
+
+DeviceState* current_device(int* status) {
+  int d = -1;
+  cudaError_t e = cudaGetDevice(&d);
+  if (e != cudaSuccess || d < 0 || d >= 64) {
+    *status = cuda_fail(e == cudaSuccess ? cudaErrorNoDevice : e, "cudaGetDevice");
+    return nullptr;
+  }
+  DeviceState* dev = &g_dev[d];
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (dev->device < 0) {
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, d);
+    if (e != cudaSuccess) {
+      *status = cuda_fail(e, "cudaGetDeviceProperties");
+      return nullptr;
+    }
+    if (prop.major != 10) {
+      *status = fail(SKGEMM_ERR_NO_DEVICE, "skgemm requires an sm_100 (B200-class) device");
+      return nullptr;
+    }
+    dev->num_sms = prop.multiProcessorCount;
+    dev->cc_major = prop.major;
+    dev->cc_minor = prop.minor;
+    dev->device = d;
+  }
+  *status = SKGEMM_OK;
+  return dev;
+}
+
+StreamWorkspace* stream_workspace(DeviceState* dev, cudaStream_t s, int slots, int* status) {
+  std::lock_guard<std::mutex> lk(dev->mu);
+  StreamWorkspace*& ws = dev->ws[s];
+  if (!ws) ws = new StreamWorkspace();
+  *status = ws->ensure(slots);
+  return *status == SKGEMM_OK ? ws : nullptr;
+}
+
+int consume_device_error(StreamWorkspace* ws, cudaStream_t s) {
+  SKG_CUDA(cudaStreamSynchronize(s));
+  if (!ws || !ws->err) return SKGEMM_OK;
+  uint32_t word = 0;
+  SKG_CUDA(cudaMemcpy(&word, ws->err, sizeof(word), cudaMemcpyDeviceToHost));
+  if (word == 0) return SKGEMM_OK;
+  SKG_CUDA(cudaMemset(ws->err, 0, sizeof(uint32_t)));
+  char buf[160];
+  snprintf(buf, sizeof(buf), "device-side wait ran past its budget (error word 0x%x)", word);
+  return fail(SKGEMM_ERR_DEVICE_TIMEOUT, buf);
+}
+
+// ------------------------------------------------------------------- TMA
+int encode_tiled(CUtensorMap* map, int rank, const void* base, const uint64_t* dims,
+                 const uint64_t* strides_bytes, const uint32_t* box, CUtensorMapDataType dtype,
+                 CUtensorMapSwizzle swizzle) {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+      return fail(SKGEMM_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  CUresult r = fn(map, dtype, (cuuint32_t)rank, const_cast<void*>(base),
+                  reinterpret_cast<const cuuint64_t*>(dims),
+                  reinterpret_cast<const cuuint64_t*>(strides_bytes),
+                  reinterpret_cast<const cuuint32_t*>(box), estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char buf[128];
+    snprintf(buf, sizeof(buf), "cuTensorMapEncodeTiled failed (CUresult %d, rank %d)", (int)r,
+             rank);
+    return fail(SKGEMM_ERR_INVALID_ARG, buf);
+  }
+  return SKGEMM_OK;
+}
+
+// ------------------------------------------------------- K == 0 epilogues
+namespace {
+
+__global__ void k0_kernel(int mode, int64_t M, int64_t N, double* D, int64_t ld, double gamma,
+                          int beta_zero) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= M * N) return;
+  int64_t m = idx / N, n = idx % N;
+  if (mode == kOutRowMajor) {
+    D[m * ld + n] = gamma;  // alpha * 0 + gamma
+  } else if (mode == kOutSyrkUpper) {
+    if (m <= n) {
+      double* c = D + m + n * ld;
+      *c = beta_zero ? 0.0 : gamma * (*c);
+    }
+  }
+}
+
+int run_k0(int mode, int64_t M, int64_t N, double* D, int64_t ld, double gamma, bool beta_zero,
+           cudaStream_t s) {
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  int64_t n = M * N;
+  k0_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(mode, M, N, D, ld, gamma,
+                                                        beta_zero ? 1 : 0);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+// Native FP64 entry shared by the C ABI functions below.
+int run_native(const Fp64Problem& prob, cudaStream_t s) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  if (prob.M == 0 || prob.N == 0) return SKGEMM_OK;
+  if (prob.K == 0)
+    return run_k0(prob.out_kind, prob.M, prob.N, prob.D, prob.ldd, prob.gamma, prob.beta_zero,
+                  s);
+  return launch_fp64(dev, prob, s);
+}
+
+Fp64Problem gemm_packed_problem(int64_t M, int64_t N, int64_t K, const double* Ap,
+                                const double* Bp, double* D, int64_t ldd, double alpha,
+                                double gamma) {
+  Fp64Problem p;
+  p.a = {Ap, kOpPacked16, M, 0};
+  p.b = {Bp, kOpPacked32, N, 0};
+  p.M = M;
+  p.N = N;
+  p.K = K;
+  p.tile_order = kTilesAll;
+  p.out_kind = kOutRowMajor;
+  p.D = D;
+  p.ldd = ldd;
+  p.alpha = alpha;
+  p.gamma = gamma;
+  p.beta_zero = false;
+  return p;
+}
+
+Fp64Problem syrk_problem(int64_t K, int64_t M, const double* Ap, double* C, int64_t ldc,
+                         double alpha, double beta) {
+  Fp64Problem p;
+  p.a = {Ap, kOpPacked16, M, 0};
+  p.b = {Ap, kOpPacked16, M, 0};
+  p.M = M;
+  p.N = M;
+  p.K = K;
+  p.tile_order = kTilesUpper;
+  p.out_kind = kOutSyrkUpper;
+  p.D = C;
+  p.ldd = ldc;
+  p.alpha = alpha;
+  p.gamma = beta;
+  p.beta_zero = (beta == 0.0);
+  return p;
+}
+
+Fp64Problem rot_problem(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D) {
+  Fp64Problem p;
+  p.a = {A, kOpPacked16, Nd, 0};
+  p.b = {Q, kOpDense, nb, nb};
+  p.M = Nd;
+  p.N = nb;
+  p.K = nb;
+  p.tile_order = kTilesAll;
+  p.out_kind = kOutBand16;
+  p.D = D;
+  p.ldd = 0;
+  p.alpha = 1.0;
+  p.gamma = 0.0;
+  p.beta_zero = true;
+  return p;
+}
+
+int check_dims(int64_t a, int64_t b, int64_t c) {
+  if (a < 0 || b < 0 || c < 0) return fail(SKGEMM_ERR_INVALID_ARG, "negative dimension");
+  return SKGEMM_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Blocking host-pointer execution: copies `nin` inputs to device staging
+// buffers, runs `body` with the device pointers, copies `out` back.
+struct HostIO {
+  const void* src;
+  size_t bytes;
+};
+
+template <typename Body>
+int run_host(int nin, const HostIO* in, void* out_host, size_t out_bytes, bool out_is_input,
+             Body body) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  std::lock_guard<std::mutex> lk(dev->host_mu);
+  if (!dev->host_stream) SKG_CUDA(cudaStreamCreateWithFlags(&dev->host_stream, cudaStreamNonBlocking));
+  cudaStream_t s = dev->host_stream;
+  void* dptr[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (int i = 0; i < nin; ++i) {
+    if ((st = dev->stage[i].ensure(in[i].bytes ? in[i].bytes : 16)) != SKGEMM_OK) return st;
+    dptr[i] = dev->stage[i].ptr;
+    if (in[i].bytes) SKG_CUDA(cudaMemcpyAsync(dptr[i], in[i].src, in[i].bytes, cudaMemcpyHostToDevice, s));
+  }
+  if ((st = dev->stage[3].ensure(out_bytes ? out_bytes : 16)) != SKGEMM_OK) return st;
+  dptr[3] = dev->stage[3].ptr;
+  if (out_is_input && out_bytes)
+    SKG_CUDA(cudaMemcpyAsync(dptr[3], out_host, out_bytes, cudaMemcpyHostToDevice, s));
+  if ((st = body(dptr, s)) != SKGEMM_OK) {
+    cudaStreamSynchronize(s);
+    return st;
+  }
+  if (out_bytes) SKG_CUDA(cudaMemcpyAsync(out_host, dptr[3], out_bytes, cudaMemcpyDeviceToHost, s));
+  StreamWorkspace* ws = nullptr;
+  {
+    std::lock_guard<std::mutex> lk2(dev->mu);
+    auto it = dev->ws.find(s);
+    if (it != dev->ws.end()) ws = it->second;
+  }
+  return consume_device_error(ws, s);
+}
+
+}  // namespace
+}  // namespace skg
+
+using namespace skg;
+
+#define SKG_EXPORT extern "C" __attribute__((visibility("default")))
+
+SKG_EXPORT const char* skgemm_version(void) { return "skgemm 0.1.0 (sm_100a)"; }
+
+SKG_EXPORT const char* skgemm_last_error(void) { return g_last_error.c_str(); }
+
+SKG_EXPORT int skgemm_stream_status(void* stream) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  StreamWorkspace* ws = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(dev->mu);
+    auto it = dev->ws.find(s);
+    if (it != dev->ws.end()) ws = it->second;
+  }
+  int e = consume_device_error(ws, s);
+  if (e != SKGEMM_OK) return e;
+  return ozaki_consume_error(dev, s);
+}
+
+SKG_EXPORT int skgemm_probe_fp64_peak(double* tflops_out) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  return probe_fp64_peak(dev, tflops_out);
+}
+
+// ------------------------------------------------------------------- GEMM
+SKG_EXPORT int skgemm_dgemm_packed_dev(int64_t M, int64_t N, int64_t K, const double* Ap,
+                                       const double* Bp, double* D, int64_t ldd, double alpha,
+                                       double gamma, void* stream) {
+  int st = check_dims(M, N, K);
+  if (st) return st;
+  if (ldd < N) return fail(SKGEMM_ERR_INVALID_ARG, "ldd < N");
+  return run_native(gemm_packed_problem(M, N, K, Ap, Bp, D, ldd, alpha, gamma),
+                    reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_dgemm_dev(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
+                                const double* B, int64_t ldb, double* D, int64_t ldd,
+                                double alpha, double gamma, void* stream) {
+  int st = check_dims(M, N, K);
+  if (st) return st;
+  if (lda < M || ldb < N || ldd < N) return fail(SKGEMM_ERR_INVALID_ARG, "leading dimension too small");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  Fp64Problem p = gemm_packed_problem(M, N, K, nullptr, nullptr, D, ldd, alpha, gamma);
+  // Operands whose columns are 16-byte aligned are read in place through 2-D
+  // TMA maps; others are first packed on the device (HBM-bound, O(MK + KN)).
+  double* scratch[2] = {nullptr, nullptr};
+  if (K > 0 && (lda % 2 == 0) && aligned16(A)) {
+    p.a = {A, kOpDense, M, lda};
+  } else if (K > 0) {
+    SKG_CUDA(cudaMallocAsync(&scratch[0], (size_t)((M + 15) / 16 * 16) * K * 8, s));
+    if ((st = launch_pack(M, K, A, 1, lda, 16, scratch[0], s))) return st;
+    p.a = {scratch[0], kOpPacked16, M, 0};
+  }
+  if (K > 0 && (ldb % 2 == 0) && aligned16(B)) {
+    p.b = {B, kOpDense, N, ldb};
+  } else if (K > 0) {
+    SKG_CUDA(cudaMallocAsync(&scratch[1], (size_t)((N + 31) / 32 * 32) * K * 8, s));
+    if ((st = launch_pack(N, K, B, 1, ldb, 32, scratch[1], s))) return st;
+    p.b = {scratch[1], kOpPacked32, N, 0};
+  }
+  st = run_native(p, s);
+  for (double* x : scratch)
+    if (x) cudaFreeAsync(x, s);
+  return st;
+}
+
+SKG_EXPORT int skgemm_dgemm_packed_dev_opt(int64_t M, int64_t N, int64_t K, const double* Ap,
+                                           const double* Bp, double* D, int64_t ldd,
+                                           double alpha, double gamma, skgemm_options_t* opts,
+                                           void* stream) {
+  if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
+    if (opts) {
+      opts->err_bound_out = 0.0;
+      opts->slices_used_out = 0;
+    }
+    return skgemm_dgemm_packed_dev(M, N, K, Ap, Bp, D, ldd, alpha, gamma, stream);
+  }
+  int st = check_dims(M, N, K);
+  if (st) return st;
+  if (ldd < N) return fail(SKGEMM_ERR_INVALID_ARG, "ldd < N");
+  return ozaki_gemm_packed(M, N, K, Ap, Bp, D, ldd, alpha, gamma, opts,
+                           reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_dgemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap,
+                                   const double* Bp, double* D, double alpha, double gamma) {
+  int st = check_dims(M, N, K);
+  if (st) return st;
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  if (!Ap || !Bp || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  HostIO in[2] = {{Ap, (size_t)((M + 15) / 16) * 16 * K * 8},
+                  {Bp, (size_t)((N + 31) / 32) * 32 * K * 8}};
+  return run_host(2, in, D, (size_t)M * N * 8, false, [&](void** d, cudaStream_t s) {
+    return skgemm_dgemm_packed_dev(M, N, K, (const double*)d[0], (const double*)d[1],
+                                   (double*)d[3], N, alpha, gamma, s);
+  });
+}
+
+SKG_EXPORT int skgemm_dgemm(int64_t M, int64_t N, int64_t K, const double* A, const double* B,
+                            double* D, double alpha, double gamma) {
+  int st = check_dims(M, N, K);
+  if (st) return st;
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  if (!A || !B || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  HostIO in[2] = {{A, (size_t)M * K * 8}, {B, (size_t)K * N * 8}};
+  return run_host(2, in, D, (size_t)M * N * 8, false, [&](void** d, cudaStream_t s) {
+    return skgemm_dgemm_dev(M, N, K, (const double*)d[0], M, (const double*)d[1], N,
+                            (double*)d[3], N, alpha, gamma, s);
+  });
+}
+
+// ------------------------------------------------------------------- SYRK
+SKG_EXPORT int skgemm_dsyrk_packed_dev(int64_t K, int64_t M, const double* Ap, double* C,
+                                       int64_t ldc, double alpha, double beta, void* stream) {
+  int st = check_dims(K, M, 0);
+  if (st) return st;
+  if (ldc < M) return fail(SKGEMM_ERR_INVALID_ARG, "ldc < M");
+  return run_native(syrk_problem(K, M, Ap, C, ldc, alpha, beta),
+                    reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_dsyrk_packed_dev_opt(int64_t K, int64_t M, const double* Ap, double* C,
+                                           int64_t ldc, double alpha, double beta,
+                                           skgemm_options_t* opts, void* stream) {
+  if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
+    if (opts) {
+      opts->err_bound_out = 0.0;
+      opts->slices_used_out = 0;
+    }
+    return skgemm_dsyrk_packed_dev(K, M, Ap, C, ldc, alpha, beta, stream);
+  }
+  int st = check_dims(K, M, 0);
+  if (st) return st;
+  if (ldc < M) return fail(SKGEMM_ERR_INVALID_ARG, "ldc < M");
+  return ozaki_syrk_packed(K, M, Ap, C, ldc, alpha, beta, opts,
+                           reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_dsyrk_packed(int64_t K, int64_t M, const double* Ap, double* C,
+                                   double alpha, double beta) {
+  int st = check_dims(K, M, 0);
+  if (st) return st;
+  if (M == 0) return SKGEMM_OK;
+  if (!Ap || !C) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  HostIO in[1] = {{Ap, (size_t)((M + 15) / 16) * 16 * K * 8}};
+  // C is copied in and out whole: the strict lower triangle is returned as the
+  // caller passed it, and beta != 0 reads the upper triangle.
+  return run_host(1, in, C, (size_t)M * M * 8, true, [&](void** d, cudaStream_t s) {
+    return skgemm_dsyrk_packed_dev(K, M, (const double*)d[0], (double*)d[3], M, alpha, beta, s);
+  });
+}
+
+// --------------------------------------------------------------- rotation
+static int check_rot(int64_t Nd, int64_t nb) {
+  if (Nd < 0 || nb < 0) return fail(SKGEMM_ERR_INVALID_ARG, "negative dimension");
+  if (Nd % 16 || nb % 16)
+    return fail(SKGEMM_ERR_INVALID_ARG, "rotation layouts need Nd and nb multiples of 16");
+  return SKGEMM_OK;
+}
+
+SKG_EXPORT int skgemm_drot_dev(int64_t Nd, int64_t nb, const double* A, const double* Q,
+                               double* D, void* stream) {
+  int st = check_rot(Nd, nb);
+  if (st) return st;
+  return run_native(rot_problem(Nd, nb, A, Q, D), reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A, const double* Q,
+                                   double* D, skgemm_options_t* opts, void* stream) {
+  if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
+    if (opts) {
+      opts->err_bound_out = 0.0;
+      opts->slices_used_out = 0;
+    }
+    return skgemm_drot_dev(Nd, nb, A, Q, D, stream);
+  }
+  int st = check_rot(Nd, nb);
+  if (st) return st;
+  return ozaki_rot(Nd, nb, A, Q, D, opts, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double* Q,
+                           double* D) {
+  int st = check_rot(Nd, nb);
+  if (st) return st;
+  if (Nd == 0 || nb == 0) return SKGEMM_OK;
+  if (!A || !Q || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  HostIO in[2] = {{A, (size_t)Nd * nb * 8}, {Q, (size_t)nb * nb * 8}};
+  return run_host(2, in, D, (size_t)Nd * nb * 8, false, [&](void** d, cudaStream_t s) {
+    return skgemm_drot_dev(Nd, nb, (const double*)d[0], (const double*)d[1], (double*)d[3], s);
+  });
+}
+
+// ------------------------------------------------------ layout converters
+SKG_EXPORT int skgemm_pack_dev(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk,
+                               int T, double* Xp, void* stream) {
+  return launch_pack(R, K, X, sr, sk, T, Xp, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
+                                       void* stream) {
+  return launch_band_to_grid(Nd, nb, src, dst, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_grid_to_band_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
+                                       void* stream) {
+  return launch_grid_to_band(Nd, nb, src, dst, reinterpret_cast<cudaStream_t>(stream));
+}

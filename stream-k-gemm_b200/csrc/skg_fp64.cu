@@ -1,0 +1,140 @@
+// Host launcher of the native FP64 Stream-K kernel: operand descriptors ->
+// TMA tensor maps, Stream-K schedule, cooperative persistent launch.
+#include <algorithm>
+
+#include "skg_fp64_kernel.cuh"
+#include "skg_runtime.h"
+
+namespace skg {
+
+namespace {
+
+int make_operand_map(CUtensorMap* map, const Fp64Operand& op, int64_t K, int rows_per_tile) {
+  if (op.ptr == nullptr) return fail(SKGEMM_ERR_INVALID_ARG, "null operand pointer");
+  if ((reinterpret_cast<uintptr_t>(op.ptr) & 15) != 0)
+    return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
+  const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const CUtensorMapSwizzle sw = CU_TENSOR_MAP_SWIZZLE_128B;
+  if (op.kind == kOpPacked16) {
+    uint64_t dims[3] = {16, (uint64_t)K, (uint64_t)((op.rows + 15) / 16)};
+    uint64_t strides[2] = {16 * 8, (uint64_t)K * 16 * 8};
+    uint32_t box[3] = {16, (uint32_t)kBK, (uint32_t)(rows_per_tile / 16)};
+    return encode_tiled(map, 3, op.ptr, dims, strides, box, dt, sw);
+  }
+  if (op.kind == kOpPacked32) {
+    uint64_t dims[3] = {32, (uint64_t)K, (uint64_t)((op.rows + 31) / 32)};
+    uint64_t strides[2] = {32 * 8, (uint64_t)K * 32 * 8};
+    uint32_t box[3] = {16, (uint32_t)kBK, (uint32_t)(rows_per_tile / 32)};
+    return encode_tiled(map, 3, op.ptr, dims, strides, box, dt, sw);
+  }
+  if (op.kind == kOpDense) {
+    if (op.ld < op.rows || ((op.ld * 8) % 16) != 0)
+      return fail(SKGEMM_ERR_INVALID_ARG, "dense operand leading dimension must be even and >= rows");
+    uint64_t dims[2] = {(uint64_t)op.rows, (uint64_t)K};
+    uint64_t strides[1] = {(uint64_t)op.ld * 8};
+    uint32_t box[2] = {16, (uint32_t)kBK};
+    return encode_tiled(map, 2, op.ptr, dims, strides, box, dt, sw);
+  }
+  return fail(SKGEMM_ERR_INVALID_ARG, "unknown operand kind");
+}
+
+struct Schedule {
+  int tiles_m, tiles_n, num_tiles, ipt;
+  int64_t total;
+  int grid;
+};
+
+Schedule make_schedule(DeviceState* dev, const Fp64Problem& prob) {
+  Schedule sc;
+  sc.tiles_m = (int)((prob.M + kBM - 1) / kBM);
+  sc.tiles_n = (int)((prob.N + kBN - 1) / kBN);
+  sc.num_tiles = prob.tile_order == kTilesUpper ? sc.tiles_n * (sc.tiles_n + 1) / 2
+                                                : sc.tiles_m * sc.tiles_n;
+  sc.ipt = (int)((prob.K + kBK - 1) / kBK);
+  sc.total = (int64_t)sc.num_tiles * sc.ipt;
+  sc.grid = (int)std::min<int64_t>(dev->num_sms, sc.total);
+  return sc;
+}
+
+}  // namespace
+
+int fp64_grid_for(DeviceState* dev, const Fp64Problem& prob) {
+  if (prob.M <= 0 || prob.N <= 0 || prob.K <= 0) return 0;
+  return make_schedule(dev, prob).grid;
+}
+
+int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
+                StreamWorkspace* ws_override) {
+  if (prob.M < 0 || prob.N < 0 || prob.K < 0)
+    return fail(SKGEMM_ERR_INVALID_ARG, "negative dimension");
+  if (prob.tile_order == kTilesUpper && prob.M != prob.N)
+    return fail(SKGEMM_ERR_INVALID_ARG, "SYRK tiles need a square output");
+  if (prob.K > (int64_t)INT32_MAX - kBK || prob.M > ((int64_t)1 << 31) ||
+      prob.N > ((int64_t)1 << 31))
+    return fail(SKGEMM_ERR_INVALID_ARG, "dimension too large");
+  if (prob.M == 0 || prob.N == 0) return SKGEMM_OK;
+  if (prob.D == nullptr) return fail(SKGEMM_ERR_INVALID_ARG, "null output pointer");
+  if (prob.K == 0) {
+    // Empty reduction: D = gamma (GEMM), C = beta*C (SYRK), D = 0 (rotation).
+    return fail(SKGEMM_ERR_UNSUPPORTED, "K == 0 is handled by the caller");
+  }
+  Schedule sc = make_schedule(dev, prob);
+  if ((int64_t)sc.num_tiles * sc.ipt > ((int64_t)1 << 40))
+    return fail(SKGEMM_ERR_INVALID_ARG, "problem too large");
+
+  int st = SKGEMM_OK;
+  StreamWorkspace* ws = ws_override ? ws_override : stream_workspace(dev, s, sc.grid, &st);
+  if (!ws) return st;
+  if ((int)ws->partial_slots < sc.grid)
+    return fail(SKGEMM_ERR_INVALID_ARG, "workspace has fewer partial slots than the grid");
+
+  CUtensorMap mapA, mapB;
+  if ((st = make_operand_map(&mapA, prob.a, prob.K, kBM)) != SKGEMM_OK) return st;
+  if ((st = make_operand_map(&mapB, prob.b, prob.K, kBN)) != SKGEMM_OK) return st;
+
+  Fp64Params p;
+  p.M = prob.M;
+  p.N = prob.N;
+  p.K = prob.K;
+  p.tiles_m = sc.tiles_m;
+  p.tiles_n = sc.tiles_n;
+  p.num_tiles = sc.num_tiles;
+  p.iters_per_tile = sc.ipt;
+  p.total_iters = sc.total;
+  p.grid = sc.grid;
+  p.a_kind = prob.a.kind;
+  p.b_kind = prob.b.kind;
+  p.tile_order = prob.tile_order;
+  p.out_kind = prob.out_kind;
+  p.D = prob.D;
+  p.ldd = prob.ldd;
+  p.alpha = prob.alpha;
+  p.gamma = prob.gamma;
+  p.beta_zero = prob.beta_zero ? 1 : 0;
+  p.workspace = ws->partials;
+  p.flags = ws->flags;
+  p.epoch = ++ws->epoch;
+  if (p.epoch == 0) p.epoch = ++ws->epoch;  // 0 is the value of a fresh flag
+  p.err = ws->err;
+
+  static bool attr_done[64] = {false};
+  if (dev->device < 64 && !attr_done[dev->device]) {
+    SKG_CUDA(cudaFuncSetAttribute(fp64_streamk_kernel,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    attr_done[dev->device] = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sc.grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmemBytes;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  SKG_CUDA(cudaLaunchKernelEx(&cfg, fp64_streamk_kernel, mapA, mapB, p));
+  return SKGEMM_OK;
+}
+
+}  // namespace skg

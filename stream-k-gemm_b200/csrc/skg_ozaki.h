@@ -1,0 +1,20 @@
+// Ozaki split-precision path (declarations used by the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "skg_runtime.h"
+
+namespace skg {
+
+int ozaki_gemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp,
+                      double* D, int64_t ldd, double alpha, double gamma,
+                      skgemm_options_t* opts, cudaStream_t s);
+int ozaki_syrk_packed(int64_t K, int64_t M, const double* Ap, double* C, int64_t ldc,
+                      double alpha, double beta, skgemm_options_t* opts, cudaStream_t s);
+int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
+              skgemm_options_t* opts, cudaStream_t s);
+int ozaki_consume_error(DeviceState* dev, cudaStream_t s);
+
+}  // namespace skg

@@ -1,0 +1,111 @@
+// Internal host-side runtime shared by the C ABI and the kernels' launchers:
+// per-device state, per-stream Stream-K workspaces, device buffers and the
+// status plumbing. Not part of the public ABI (include/skgemm.h is).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "skgemm.h"
+
+namespace skg {
+
+// Records a message for skgemm_last_error() and returns `code`.
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define SKG_CUDA(call)                                        \
+  do {                                                        \
+    cudaError_t skg_e_ = (call);                              \
+    if (skg_e_ != cudaSuccess) return ::skg::cuda_fail(skg_e_, #call); \
+  } while (0)
+
+// Grow-only device buffer.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need);
+  void release();
+};
+
+// State of one stream's Stream-K launches: partial-tile slots, flags, the
+// epoch the flags of the next launch will carry, and the device error word.
+struct StreamWorkspace {
+  double* partials = nullptr;
+  size_t partial_slots = 0;
+  uint32_t* flags = nullptr;
+  uint32_t* err = nullptr;  // device error word
+  uint32_t epoch = 0;
+  int ensure(int slots);
+};
+
+struct DeviceState {
+  int device = -1;
+  int num_sms = 0;
+  int cc_major = 0, cc_minor = 0;
+  std::mutex mu;
+  std::map<cudaStream_t, StreamWorkspace*> ws;
+  // Staging buffers of the blocking host-pointer entry points (guarded by
+  // host_mu: host-pointer calls on one device are serialised).
+  std::mutex host_mu;
+  DeviceBuffer stage[4];
+  cudaStream_t host_stream = nullptr;
+};
+
+// Current device's state (initialises on first use). Returns nullptr and
+// records an error when no sm_100 device is usable.
+DeviceState* current_device(int* status);
+StreamWorkspace* stream_workspace(DeviceState* dev, cudaStream_t s, int slots, int* status);
+
+// Encodes a tiled TMA descriptor through the driver entry point.
+int encode_tiled(CUtensorMap* map, int rank, const void* base, const uint64_t* dims,
+                 const uint64_t* strides_bytes /*rank-1*/, const uint32_t* box,
+                 CUtensorMapDataType dtype, CUtensorMapSwizzle swizzle);
+
+// ----------------------------------------------------------------- FP64
+struct Fp64Operand {
+  const double* ptr;
+  int kind;    // skg::OperandKind
+  int64_t rows;  // extent of the M (or N) dimension
+  int64_t ld;    // k stride for kOpDense
+};
+
+struct Fp64Problem {
+  Fp64Operand a, b;
+  int64_t M, N, K;
+  int tile_order;  // skg::TileOrder
+  int out_kind;    // skg::OutKind
+  double* D;
+  int64_t ldd;
+  double alpha;
+  double gamma;  // GEMM gamma / SYRK beta
+  bool beta_zero;
+};
+
+// Enqueues the native FP64 Stream-K kernel on `s`. `ws_override` (optional)
+// supplies caller-owned partial slots/flags/err instead of the stream cache.
+int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
+                StreamWorkspace* ws_override = nullptr);
+// Number of Stream-K partial slots the launch of `prob` uses (= its grid).
+int fp64_grid_for(DeviceState* dev, const Fp64Problem& prob);
+
+// Layout kernels.
+int launch_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, int T,
+                double* Xp, cudaStream_t s);
+int launch_band_to_grid(int64_t Nd, int64_t nb, const double* src, double* dst,
+                        cudaStream_t s);
+int launch_grid_to_band(int64_t Nd, int64_t nb, const double* src, double* dst,
+                        cudaStream_t s);
+
+// Peak probe.
+int probe_fp64_peak(DeviceState* dev, double* tflops);
+
+// Reads and clears the error word of `ws` (synchronises `s`).
+int consume_device_error(StreamWorkspace* ws, cudaStream_t s);
+
+}  // namespace skg

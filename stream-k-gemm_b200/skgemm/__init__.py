@@ -1,0 +1,254 @@
+"""Python binding of libskgemm (the C ABI in include/skgemm.h) over ctypes.
+
+The host-side classes mirror the reference's static C++ entry points, with the
+same names, argument order and meaning, so that checks read like the
+reference's own drivers:
+
+* ``gemm.compute_test(M, N, K, A, B, D, alpha, gamma)``     gemm_opt.cpp:376
+* ``gemm.compute_packed(M, N, K, Ap, Bp, D, alpha, gamma)`` gemm_opt.cpp:314
+* ``gemm.compute_streamk_packed(...)``                      gemm_crsp.cpp:316
+* ``sme_syrk.compute(K, M, Ap, C, alpha, beta)``            sme_syrk.hpp:137
+* ``sme_gemm_trp_3d.compute(Nd, nb, A, B, D)``              sme_trp_3d.hpp:194
+
+They take host numpy float64 arrays and block, like the reference. Where the
+reference silently returns (bad shapes, no error channel) these raise
+``SkgemmError`` carrying the C status code.
+
+The ``*_dev`` functions take CUDA device pointers (or torch tensors) and a
+stream, and are asynchronous. There is no CPU fallback: without the built
+library or an sm_100 device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "libskgemm.so")
+
+OK = 0
+ERR_INVALID_ARG = -1
+ERR_OOM = -2
+ERR_CUDA = -3
+ERR_DEVICE_TIMEOUT = -4
+ERR_NO_DEVICE = -5
+ERR_UNSUPPORTED = -6
+
+PREC_NATIVE = 0
+PREC_OZAKI_I8 = 1
+
+
+class SkgemmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"skgemm status {code}: {msg}")
+        self.code = code
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("slices", ctypes.c_int),
+                ("err_bound_out", ctypes.c_double), ("slices_used_out", ctypes.c_int)]
+
+
+_i64 = ctypes.c_int64
+_vp = ctypes.c_void_p
+_d = ctypes.c_double
+_lib: Optional[ctypes.CDLL] = None
+
+# name -> argtypes (all return int status except the two string getters)
+_SIGS = {
+    "skgemm_stream_status": [_vp],
+    "skgemm_probe_fp64_peak": [ctypes.POINTER(ctypes.c_double)],
+    "skgemm_dgemm": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d],
+    "skgemm_dgemm_packed": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d],
+    "skgemm_dgemm_dev": [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _d, _d, _vp],
+    "skgemm_dgemm_packed_dev": [_i64, _i64, _i64, _vp, _vp, _vp, _i64, _d, _d, _vp],
+    "skgemm_dgemm_packed_dev_opt": [_i64, _i64, _i64, _vp, _vp, _vp, _i64, _d, _d,
+                                    ctypes.POINTER(Options), _vp],
+    "skgemm_dsyrk_packed": [_i64, _i64, _vp, _vp, _d, _d],
+    "skgemm_dsyrk_packed_dev": [_i64, _i64, _vp, _vp, _i64, _d, _d, _vp],
+    "skgemm_dsyrk_packed_dev_opt": [_i64, _i64, _vp, _vp, _i64, _d, _d,
+                                    ctypes.POINTER(Options), _vp],
+    "skgemm_drot": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_drot_dev": [_i64, _i64, _vp, _vp, _vp, _vp],
+    "skgemm_drot_dev_opt": [_i64, _i64, _vp, _vp, _vp, ctypes.POINTER(Options), _vp],
+    "skgemm_pack_dev": [_i64, _i64, _vp, _i64, _i64, ctypes.c_int, _vp, _vp],
+    "skgemm_band_to_grid_dev": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_grid_to_band_dev": [_i64, _i64, _vp, _vp, _vp],
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libskgemm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SkgemmError(ERR_UNSUPPORTED,
+                              f"{LIB_PATH} not built (python stream-k-gemm_b200/build.py)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        L.skgemm_version.restype = ctypes.c_char_p
+        L.skgemm_version.argtypes = []
+        L.skgemm_last_error.restype = ctypes.c_char_p
+        L.skgemm_last_error.argtypes = []
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> list:
+    return ["skgemm_version", "skgemm_last_error"] + list(_SIGS)
+
+
+def version() -> str:
+    return lib().skgemm_version().decode()
+
+
+def _check(code: int) -> int:
+    if code != OK:
+        msg = lib().skgemm_last_error().decode(errors="replace")
+        raise SkgemmError(code, msg)
+    return code
+
+
+def _hptr(a: np.ndarray, writable: bool = False):
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise SkgemmError(ERR_INVALID_ARG, "host arrays must be C-contiguous float64 numpy arrays")
+    if writable and not a.flags.writeable:
+        raise SkgemmError(ERR_INVALID_ARG, "output array is read-only")
+    return a.ctypes.data
+
+
+def _dptr(x) -> int:
+    """Device address of a torch tensor, or an int address as given."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    return int(x.data_ptr())
+
+
+def _stream(s) -> int:
+    if s is None:
+        return 0
+    if isinstance(s, int):
+        return s
+    return int(s.cuda_stream)  # torch.cuda.Stream
+
+
+# ------------------------------------------------------- reference mirror
+class gemm:
+    """Mirror of the reference's ``gemm<double>`` (gemm_opt.cpp:55 /
+    gemm_crsp.cpp:57): D = alpha*A*B + gamma."""
+
+    @staticmethod
+    def compute_test(M, N, K, A_colmajor, B_rowmajor, D, alpha=1.0, gamma=0.0):
+        _check(lib().skgemm_dgemm(M, N, K, _hptr(A_colmajor), _hptr(B_rowmajor),
+                                  _hptr(D, True), alpha, gamma))
+
+    @staticmethod
+    def compute_packed(M, N, K, A_packed, B_packed, D, alpha=1.0, gamma=0.0):
+        _check(lib().skgemm_dgemm_packed(M, N, K, _hptr(A_packed), _hptr(B_packed),
+                                         _hptr(D, True), alpha, gamma))
+
+    compute_streamk_packed = compute_packed
+
+
+class sme_syrk:
+    """Mirror of ``sme_syrk<double>`` (include/sme_syrk.hpp:22, syrk_crsp.cpp:51):
+    C = alpha*A^T*A + beta*C, upper triangle, column-major C."""
+
+    @staticmethod
+    def compute(K, M, A_packed, C, alpha=1.0, beta=0.0):
+        _check(lib().skgemm_dsyrk_packed(K, M, _hptr(A_packed), _hptr(C, True), alpha, beta))
+
+
+class sme_gemm_trp_3d:
+    """Mirror of ``sme_gemm_trp_3d<double>`` (include/sme_trp_3d.hpp:48): D = A*B
+    with A grid-packed, B row-major, D band-packed."""
+
+    @staticmethod
+    def compute(Nd, nb, A_grid, B, D_band):
+        _check(lib().skgemm_drot(Nd, nb, _hptr(A_grid), _hptr(B), _hptr(D_band, True)))
+
+
+sme_gemm_trp = sme_gemm_trp_3d
+
+
+# --------------------------------------------------------- device entries
+def _opts(precision, slices):
+    if precision is None or precision == PREC_NATIVE:
+        return None
+    o = Options()
+    o.precision = precision
+    o.slices = slices or 0
+    return o
+
+
+def dgemm_packed_dev(M, N, K, A_packed, B_packed, D, ldd=None, alpha=1.0, gamma=0.0,
+                     stream=None, precision=None, slices=0):
+    o = _opts(precision, slices)
+    if o is None:
+        _check(lib().skgemm_dgemm_packed_dev(M, N, K, _dptr(A_packed), _dptr(B_packed),
+                                             _dptr(D), ldd or N, alpha, gamma, _stream(stream)))
+        return None
+    _check(lib().skgemm_dgemm_packed_dev_opt(M, N, K, _dptr(A_packed), _dptr(B_packed),
+                                             _dptr(D), ldd or N, alpha, gamma,
+                                             ctypes.byref(o), _stream(stream)))
+    return o
+
+
+def dgemm_dev(M, N, K, A_colmajor, lda, B_rowmajor, ldb, D, ldd, alpha=1.0, gamma=0.0,
+              stream=None):
+    _check(lib().skgemm_dgemm_dev(M, N, K, _dptr(A_colmajor), lda, _dptr(B_rowmajor), ldb,
+                                  _dptr(D), ldd, alpha, gamma, _stream(stream)))
+
+
+def dsyrk_packed_dev(K, M, A_packed, C, ldc=None, alpha=1.0, beta=0.0, stream=None,
+                     precision=None, slices=0):
+    o = _opts(precision, slices)
+    if o is None:
+        _check(lib().skgemm_dsyrk_packed_dev(K, M, _dptr(A_packed), _dptr(C), ldc or M, alpha,
+                                             beta, _stream(stream)))
+        return None
+    _check(lib().skgemm_dsyrk_packed_dev_opt(K, M, _dptr(A_packed), _dptr(C), ldc or M, alpha,
+                                             beta, ctypes.byref(o), _stream(stream)))
+    return o
+
+
+def drot_dev(Nd, nb, A_grid, Q, D_band, stream=None, precision=None, slices=0):
+    o = _opts(precision, slices)
+    if o is None:
+        _check(lib().skgemm_drot_dev(Nd, nb, _dptr(A_grid), _dptr(Q), _dptr(D_band),
+                                     _stream(stream)))
+        return None
+    _check(lib().skgemm_drot_dev_opt(Nd, nb, _dptr(A_grid), _dptr(Q), _dptr(D_band),
+                                     ctypes.byref(o), _stream(stream)))
+    return o
+
+
+def pack_dev(R, K, X, sr, sk, T, X_packed, stream=None):
+    _check(lib().skgemm_pack_dev(R, K, _dptr(X), sr, sk, T, _dptr(X_packed), _stream(stream)))
+
+
+def band_to_grid_dev(Nd, nb, src, dst, stream=None):
+    _check(lib().skgemm_band_to_grid_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
+
+
+def grid_to_band_dev(Nd, nb, src, dst, stream=None):
+    _check(lib().skgemm_grid_to_band_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
+
+
+def stream_status(stream=None) -> None:
+    """Synchronise ``stream``; raise if a device-side wait ran out of budget."""
+    _check(lib().skgemm_stream_status(_stream(stream)))
+
+
+def probe_fp64_peak() -> float:
+    v = ctypes.c_double(0.0)
+    _check(lib().skgemm_probe_fp64_peak(ctypes.byref(v)))
+    return v.value
