@@ -1,0 +1,412 @@
+"""Benchmark of the DFT subspace step on B200 (and the reference CPU arm).
+
+Workload (one "step"): the three subspace operations of one CheFSI iteration
+on Psi = 110592 x 512 (48^3 grid points x 512 states, N(0,1)/sqrt(Nd)
+entries), H*Psi an independent matrix of the same shape and distribution, and
+Q = 512 x 512 U[-1,1]:
+    S   = Psi^T Psi        (SYRK, upper triangle)   M(M+1)K   = 2.905e10 flop
+    Hs  = Psi^T (H Psi)    (GEMM)                   2 M^2 K   = 5.798e10 flop
+    Psi'= Psi Q            (rotation)               2 Nd nb^2 = 5.798e10 flop
+in the reference's packed layouts (band-packed Psi for SYRK/GEMM, 32-band-
+packed H*Psi, grid-packed Psi for the rotation, band-packed Psi').
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision native|ozaki]
+    python bench.py --impl reference ...     # the reference's CPU kernels
+
+Timing: K steps bracketed by a barrier and a device synchronise, CUDA events on
+the launching stream, max over ranks. Every input is larger than L2 (126 MB),
+so no flush is needed between steps. N > 1 runs independent replicas (the path
+has no exchange step on one node): value = all ranks' flops / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "stream-k-gemm_b200"))
+
+ND, NB = 110592, 512
+FLOP_SYRK = NB * (NB + 1) * ND
+FLOP_GEMM = 2 * NB * NB * ND
+FLOP_ROT = 2 * ND * NB * NB
+FLOP_STEP = FLOP_SYRK + FLOP_GEMM + FLOP_ROT
+METRIC = "FP64-accurate TFLOP/s (Ozaki vs native Stream-K) and p50/p99 solve latency"
+WORKLOAD = "dft_subspace_step_psi110592x512"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="skgemm", choices=["skgemm", "reference"])
+    ap.add_argument("--precision", default="native", choices=["native", "ozaki"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[4:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        peak = max(r[0] for r in rows)
+        load = [r for r in rows if r[0] >= 0.5 * peak] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i in range(4)
+                          if r[2][i + 1].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[0] for r in load),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_setup(n):
+    import torch
+    if n <= 1 or "RANK" not in os.environ:
+        return 0, 1, None
+    import datetime
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    return dist.get_rank(), dist.get_world_size(), dist
+
+
+def max_over_ranks(x, dist):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    import torch
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+# ------------------------------------------------------------------ inputs
+def make_inputs(device):
+    """Seeded synthetic inputs of the workload, generated on the device."""
+    import torch
+    import skgemm
+    g = torch.Generator(device=device).manual_seed(20240611)
+    scale = 1.0 / ND ** 0.5
+    psi = torch.randn(ND, NB, generator=g, dtype=torch.float64, device=device) * scale
+    hpsi = torch.randn(ND, NB, generator=g, dtype=torch.float64, device=device) * scale
+    q = torch.rand(NB, NB, generator=g, dtype=torch.float64, device=device) * 2 - 1
+    band = torch.empty(ND * NB, dtype=torch.float64, device=device)
+    h32 = torch.empty_like(band)
+    grid = torch.empty_like(band)
+    skgemm.pack_dev(NB, ND, psi, 1, NB, 16, band)   # band-packed Psi
+    skgemm.pack_dev(NB, ND, hpsi, 1, NB, 32, h32)   # 32-band-packed H Psi
+    skgemm.pack_dev(ND, NB, psi, NB, 1, 16, grid)   # grid-packed Psi
+    torch.cuda.synchronize()
+    del psi, hpsi
+    return band, h32, grid, q
+
+
+# ----------------------------------------------------------- GPU arm
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import skgemm
+
+    rank, world, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    prec = skgemm.PREC_OZAKI_I8 if args.precision == "ozaki" else None
+    band, h32, grid, q = make_inputs(dev)
+    S = torch.zeros(NB, NB, dtype=torch.float64, device=dev)
+    Hs = torch.zeros_like(S)
+    Pn = torch.empty_like(band)
+    stream = torch.cuda.current_stream()
+    peak = skgemm.probe_fp64_peak()
+
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+
+    def step(evs=None):
+        if evs:
+            evs[0].record(stream)
+        skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, 1.0, 0.0, stream=stream, precision=prec)
+        if evs:
+            evs[1].record(stream)
+        skgemm.dgemm_packed_dev(NB, NB, ND, band, h32, Hs, NB, 1.0, 0.0, stream=stream,
+                                precision=prec)
+        if evs:
+            evs[2].record(stream)
+        skgemm.drot_dev(ND, NB, grid, q, Pn, stream=stream, precision=prec)
+        if evs:
+            evs[3].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    skgemm.stream_status(stream)
+    clocks = ClockSampler(torch.cuda.current_device())
+    barrier(dist)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(args.steps):
+        step(ev[i])
+    t1.record(stream)
+    barrier(dist)
+    clk = clocks.stop()
+    skgemm.stream_status(stream)
+    total_ms = max_over_ranks(t0.elapsed_time(t1), dist)
+    per_op = np.array([[ev[i][j].elapsed_time(ev[i][j + 1]) for j in range(3)]
+                       for i in range(args.steps)])
+    step_ms = per_op.sum(axis=1)
+    kernel_ms = float(per_op.sum())
+    achieved = FLOP_STEP * args.steps / (kernel_ms * 1e-3) / 1e12
+
+    line = {
+        "metric": METRIC, "value": round(FLOP_STEP * args.steps * world / (total_ms * 1e-3) / 1e12, 3),
+        "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "Nd": ND, "nb": NB, "ops": ["syrk", "gemm", "rotation"],
+                   "precision": args.precision, "parallelism": f"replicas{world}",
+                   "flop_per_step": FLOP_STEP, "l2": "inputs larger than L2 (453 MB each)"},
+        "latency_ms": {"p50": round(float(np.percentile(step_ms, 50)), 4),
+                       "p99": round(float(np.percentile(step_ms, 99)), 4),
+                       "syrk": round(float(per_op[:, 0].mean()), 4),
+                       "gemm": round(float(per_op[:, 1].mean()), 4),
+                       "rotation": round(float(per_op[:, 2].mean()), 4)},
+        "op_tflops": {"syrk": round(FLOP_SYRK / per_op[:, 0].mean() / 1e9, 3),
+                      "gemm": round(FLOP_GEMM / per_op[:, 1].mean() / 1e9, 3),
+                      "rotation": round(FLOP_ROT / per_op[:, 2].mean() / 1e9, 3)},
+        "roofline": {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
+                     "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                     "peak_source": "measured FP64 DMMA peak (skgemm_probe_fp64_peak, this run)",
+                     "kernel": "fp64_streamk_kernel",
+                     "traffic": read_profile_traffic()},
+        "clocks": clk,
+        "gpu_launches": 3 * args.steps,
+    }
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(args, band, h32, grid, q, dist)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def read_profile_traffic():
+    """DRAM bytes (read + write) per launch of the dominant kernel, from the
+    committed ncu summary of the same workload (mean of its three launches)."""
+    path = os.path.join(REPO, "profiles", "fp64_streamk_kernel_dft_subspace.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_e2e(args, band, h32, grid, q, dist):
+    """Same step through the blocking host-pointer C ABI (the reference-facing
+    call): inputs copied from pinned host memory and results read back every step."""
+    import torch
+    import skgemm
+    hb = band.cpu().pin_memory().numpy()
+    hh = h32.cpu().pin_memory().numpy()
+    hg = grid.cpu().pin_memory().numpy()
+    hq = q.cpu().pin_memory().numpy().ravel()
+    S = torch.zeros(NB * NB, dtype=torch.float64).pin_memory().numpy()
+    Hs = torch.zeros(NB * NB, dtype=torch.float64).pin_memory().numpy()
+    Pn = torch.zeros(ND * NB, dtype=torch.float64).pin_memory().numpy()
+
+    def step():
+        skgemm.sme_syrk.compute(ND, NB, hb, S, 1.0, 0.0)
+        skgemm.gemm.compute_packed(NB, NB, ND, hb, hh, Hs, 1.0, 0.0)
+        skgemm.sme_gemm_trp_3d.compute(ND, NB, hg, hq, Pn)
+
+    steps = max(2, min(args.steps, 5))
+    for _ in range(2):
+        step()
+    barrier(dist)
+    t = time.perf_counter()
+    for _ in range(steps):
+        step()
+    el = max_over_ranks(time.perf_counter() - t, dist)
+    h2d = hb.nbytes * 2 + hh.nbytes + hg.nbytes + hq.nbytes + S.nbytes
+    d2h = S.nbytes + Hs.nbytes + Pn.nbytes
+    world = 1 if dist is None else dist.get_world_size()
+    return {"value": round(FLOP_STEP * steps * world / el / 1e12, 4), "unit": "TFLOP/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": round(el / steps * 1e3, 3), "steps": steps,
+            "api": "skgemm_dsyrk_packed + skgemm_dgemm_packed + skgemm_drot (host pointers)"}
+
+
+# ------------------------------------------------------------- CPU arm
+def _ref_sample(kslice: int):
+    """Inputs for a K-sliced sample of the workload: the first `kslice` grid
+    points of Psi / H Psi (SYRK, GEMM) and `kslice` grid rows (rotation)."""
+    import numpy as np
+    rng = np.random.default_rng(20240611)
+    scale = 1.0 / ND ** 0.5
+    psi = rng.standard_normal((kslice, NB)) * scale
+    hpsi = rng.standard_normal((kslice, NB)) * scale
+    q = rng.uniform(-1, 1, (NB, NB))
+    import oracle
+    band = oracle.pack(np.ascontiguousarray(psi.T), 16).ravel()
+    h32 = oracle.pack(np.ascontiguousarray(hpsi.T), 32).ravel()
+    grid = oracle.grid_pack(psi).ravel()
+    return band, h32, grid, np.ascontiguousarray(q).ravel()
+
+
+def cpu_step_reference(kslice, inputs):
+    """One sample step on the reference's own kernels (oracle/_ref, all cores):
+    sme_syrk<double>::compute, gemm<double>::compute_packed, sme_gemm_trp_3d."""
+    import ctypes
+    import numpy as np
+    import oracle
+    band, h32, grid, q = inputs
+    dp = ctypes.POINTER(ctypes.c_double)
+    sy = oracle.ref("sme_syrk").ref_sme_syrk_compute
+    sy.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_double]
+    gm = oracle.ref("gemm_opt").ref_gemm_opt_compute_packed
+    gm.argtypes = [ctypes.c_int] * 3 + [dp] * 3 + [ctypes.c_double] * 2
+    rt = oracle.ref("trp_3d").ref_trp_3d_compute
+    rt.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
+    S = np.zeros(NB * NB)
+    Hs = np.zeros(NB * NB)
+    P = np.zeros(kslice * NB)
+    t = time.perf_counter()
+    sy(kslice, NB, oracle.ptr(band), oracle.ptr(S), 1.0, 0.0)
+    gm(NB, NB, kslice, oracle.ptr(band), oracle.ptr(h32), oracle.ptr(Hs), 1.0, 0.0)
+    rt(kslice, NB, oracle.ptr(grid), oracle.ptr(q), oracle.ptr(P))
+    return time.perf_counter() - t
+
+
+def cpu_baseline(sample_seconds=10.0, kslice=ND):
+    """The reference's own kernels (oracle/_ref) on the host cores, on the full
+    workload (or a K-slice of it), repeated until about `sample_seconds`."""
+    import oracle
+    if not oracle.have_ref():
+        return None
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    inputs = _ref_sample(kslice)
+    times = [cpu_step_reference(kslice, inputs)]
+    while sum(times) < sample_seconds and len(times) < 20:
+        times.append(cpu_step_reference(kslice, inputs))
+    flops = (NB * (NB + 1) + 2 * NB * NB) * kslice + 2 * kslice * NB * NB
+    return {"value": round(flops * len(times) / sum(times) / 1e12, 6), "unit": "TFLOP/s",
+            "cores": cores, "kind": "reference",
+            "sample": f"{len(times)} passes of the three ops on {kslice} of {ND} grid points; "
+                      f"reference kernels sme_syrk.hpp / gemm_opt.cpp / sme_trp_3d.hpp built "
+                      f"-O3 (AVX2) with the host SME-intrinsic emulation, OpenMP {cores} threads",
+            "seconds": round(sum(times), 3)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+        return
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    # Each step is the full workload unless steps * (one step) would exceed
+    # about 150 s; then each step is the same K-slice of it.
+    ks = ND
+    inputs = _ref_sample(ks)
+    t1 = cpu_step_reference(ks, inputs)
+    if (args.steps + args.warmup) * t1 > 150.0:
+        ks = max(1024, int(ND * 150.0 / ((args.steps + args.warmup) * t1)) // 16 * 16)
+        inputs = _ref_sample(ks)
+    for _ in range(max(0, args.warmup - 1)):
+        cpu_step_reference(ks, inputs)
+    times = [cpu_step_reference(ks, inputs) for _ in range(args.steps)]
+    flops = (NB * (NB + 1) + 2 * NB * NB) * ks + 2 * ks * NB * NB
+    tot = sum(times)
+    v = flops * len(times) / tot / 1e12
+    sample = (f"each step: the three ops on {ks} of {ND} grid points, reference kernels "
+              f"(oracle/_ref) with {cores} OpenMP threads")
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "TFLOP/s",
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(tot / len(times) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "Nd": ND, "nb": NB,
+                       "ops": ["syrk", "gemm", "rotation"], "sample_grid_points": ks},
+            "cpu_baseline": {"value": round(v, 6), "unit": "TFLOP/s", "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(v, 6), "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()
