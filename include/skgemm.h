@@ -106,6 +106,26 @@ int skgemm_dgemm_dev(int64_t M, int64_t N, int64_t K, const double* A_colmajor,
 int skgemm_dgemm_packed_dev(int64_t M, int64_t N, int64_t K, const double* A_packed16,
                             const double* B_packed32, double* D, int64_t ldd,
                             double alpha, double gamma, void* stream);
+/* Allocation-free form of skgemm_dgemm_packed_dev, for callers that cannot
+ * allocate device memory at call time: applications that reserve the device's
+ * memory in their own pool up front, code whose device footprint must stay
+ * fixed after start-up, or loops that cannot take the synchronisation of
+ * cudaMalloc / cudaFree. No counterpart in the reference (whose drivers
+ * allocate every buffer themselves).
+ * Same contract and result as skgemm_dgemm_packed_dev (native FP64). Its
+ * Stream-K scratch is a static device array of 148 partial-tile slots
+ * (19.4 MB) that exists on every GPU that loads the library until the process
+ * exits; a launch that needs more slots (a device with more than 148 SMs) is
+ * rejected with SKGEMM_ERR_INVALID_ARG. The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device current,
+ * so make that first call before any stream capture. Every call shares the
+ * array, so calls are serialised by a process-wide lock and each call returns
+ * only after its kernel has finished (it synchronises `stream`); a device-side
+ * wait that ran out is reported as SKGEMM_ERR_DEVICE_TIMEOUT. */
+int skgemm_dgemm_packed_dev_noalloc(int64_t M, int64_t N, int64_t K,
+                                    const double* A_packed16, const double* B_packed32,
+                                    double* D, int64_t ldd, double alpha, double gamma,
+                                    void* stream);
 /* Packed GEMM with a precision selector (native or Ozaki). */
 int skgemm_dgemm_packed_dev_opt(int64_t M, int64_t N, int64_t K,
                                 const double* A_packed16, const double* B_packed32,

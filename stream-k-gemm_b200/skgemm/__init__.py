@@ -65,6 +65,7 @@ _SIGS = {
     "skgemm_dgemm_packed": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d],
     "skgemm_dgemm_dev": [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _d, _d, _vp],
     "skgemm_dgemm_packed_dev": [_i64, _i64, _i64, _vp, _vp, _vp, _i64, _d, _d, _vp],
+    "skgemm_dgemm_packed_dev_noalloc": [_i64, _i64, _i64, _vp, _vp, _vp, _i64, _d, _d, _vp],
     "skgemm_dgemm_packed_dev_opt": [_i64, _i64, _i64, _vp, _vp, _vp, _i64, _d, _d,
                                     ctypes.POINTER(Options), _vp],
     "skgemm_dsyrk_packed": [_i64, _i64, _vp, _vp, _d, _d],
@@ -200,6 +201,14 @@ def dgemm_packed_dev(M, N, K, A_packed, B_packed, D, ldd=None, alpha=1.0, gamma=
                                              _dptr(D), ldd or N, alpha, gamma,
                                              ctypes.byref(o), _stream(stream)))
     return o
+
+
+def dgemm_packed_dev_noalloc(M, N, K, A_packed, B_packed, D, ldd=None, alpha=1.0, gamma=0.0,
+                             stream=None):
+    """Allocation-free packed GEMM (static device scratch; blocks until done)."""
+    _check(lib().skgemm_dgemm_packed_dev_noalloc(M, N, K, _dptr(A_packed), _dptr(B_packed),
+                                                 _dptr(D), ldd or N, alpha, gamma,
+                                                 _stream(stream)))
 
 
 def dgemm_dev(M, N, K, A_colmajor, lda, B_rowmajor, ldb, D, ldd, alpha=1.0, gamma=0.0,
