@@ -79,6 +79,17 @@ int skgemm_stream_status(void* stream);
  * TFLOP/s, from a register-resident peak loop; the analogue of the
  * reference's FMOPA peak probe (sme_peak_microbench.cpp:16-61). */
 int skgemm_probe_fp64_peak(double* tflops_out);
+/* Measured INT8 tensor-core (tcgen05.mma kind::i8, 128x256x32) throughput of
+ * the current device, TOP/s; the roofline denominator of the Ozaki path. */
+int skgemm_probe_i8_peak(double* tops_out);
+
+/* Exact INT8 GEMM on tcgen05 tensor cores: C[i*ldc + j] = sum_k A[i*lda + k] *
+ * B[j*ldb + k] in int32 (both operands K-major int8; device pointers). The
+ * engine of the Ozaki path, exposed for callers with integer data. Requires
+ * |result| < 2^31 (guaranteed for K <= 131072). No counterpart in the
+ * reference (which is FP64 only). */
+int skgemm_igemm_s8_dev(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda,
+                        const int8_t* B, int64_t ldb, int32_t* C, int64_t ldc, void* stream);
 
 /* --------------------------------------------------------------- GEMM */
 /* D = alpha * A * B + gamma (gamma added to every element).

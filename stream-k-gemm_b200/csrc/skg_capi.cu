@@ -320,6 +320,20 @@ SKG_EXPORT int skgemm_probe_fp64_peak(double* tflops_out) {
   return probe_fp64_peak(dev, tflops_out);
 }
 
+SKG_EXPORT int skgemm_probe_i8_peak(double* tops_out) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  if (!tops_out) return fail(SKGEMM_ERR_INVALID_ARG, "null output");
+  return probe_i8_peak(dev, tops_out);
+}
+
+SKG_EXPORT int skgemm_igemm_s8_dev(int64_t M, int64_t N, int64_t K, const int8_t* A,
+                                   int64_t lda, const int8_t* B, int64_t ldb, int32_t* C,
+                                   int64_t ldc, void* stream) {
+  return igemm_s8(M, N, K, A, lda, B, ldb, C, ldc, reinterpret_cast<cudaStream_t>(stream));
+}
+
 // ------------------------------------------------------------------- GEMM
 SKG_EXPORT int skgemm_dgemm_packed_dev(int64_t M, int64_t N, int64_t K, const double* Ap,
                                        const double* Bp, double* D, int64_t ldd, double alpha,

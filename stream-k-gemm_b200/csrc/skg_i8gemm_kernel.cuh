@@ -1,0 +1,389 @@
+// INT8 x INT8 -> INT32 GEMM on tcgen05 tensor cores (sm_100a), the engine of
+// the Ozaki split-precision path. Exact: every partial product of two int8
+// residues is at most 2^14 in magnitude, so a 32-bit accumulator is exact for
+// up to 2^31 / 2^14 = 131072 products, and work is split into k-segments of
+// at most `seg_kb_cap` 128-wide k-blocks.
+//
+// Operands are per-modulus residue matrices, K-major bytes:
+//   A_res[l][RA][KP], B_res[l][RB][KP]   (row r, k contiguous; zero padding)
+// loaded by TMA boxes {128 B of k, 128 (A) / 256 (B) rows, 1 modulus} with the
+// 128-byte swizzle, which is the canonical K-major SW128 UMMA layout.
+//
+// CTA: 192 threads = warp 0 TMA producer, warp 1 MMA issuer (one thread) and
+// TMEM owner, warps 2-5 epilogue (warp w reads TMEM lanes 32*(w%4)..+31).
+// Tile 128 x 256 (UMMA M=128, N=256, K=32), 4-stage smem ring (48 KB/stage),
+// two 256-column TMEM accumulators so the epilogue of one work item overlaps
+// the MMAs of the next.
+//
+// Schedules:
+//  kSchedLanes   (huge K, small M x N: S = Psi^T Psi, Hs = Psi^T H Psi)
+//     CTA c -> tile t = c % T, lane q = c / T. Lane q owns a contiguous range
+//     of the (modulus, k-block) space; all T CTAs of a lane walk the same
+//     range in lockstep, so each (modulus, k-range) panel of A and B is read
+//     from HBM about once and served to the other tiles from L2. Each
+//     segment (one modulus, <= seg_kb_cap k-blocks) ends in an int32 partial
+//     slab written to `partials[seg_slot][t]` (plan-built slot table).
+//  kSchedUnits   (huge M, small K: Psi' = Psi Q)
+//     work units (tm, l, tn) with the full K, round-robin over CTAs; the
+//     epilogue writes (acc mod m_l) as one byte per element to
+//     `residues[l][row][col]`.
+#pragma once
+
+#include "skg_common.cuh"
+#include "skg_tcgen05.cuh"
+
+namespace skg {
+
+constexpr int kI8BM = 128;
+constexpr int kI8BN = 256;
+constexpr int kI8BK = 128;  // bytes of k per stage
+constexpr int kI8UmmaK = 32;
+constexpr int kI8Stages = 4;
+constexpr int kI8Threads = 192;
+constexpr int kI8TileABytes = kI8BM * kI8BK;  // 16 KB
+constexpr int kI8TileBBytes = kI8BN * kI8BK;  // 32 KB
+constexpr int kI8StageBytes = kI8TileABytes + kI8TileBBytes;
+constexpr int kI8SmemBytes = kI8Stages * kI8StageBytes + 1024 + 256;
+constexpr int kI8TmemCols = 512;
+constexpr int kI8MaxModuli = 16;
+
+enum I8Sched : int { kSchedLanes = 0, kSchedUnits = 1 };
+
+// One k-segment of a lane: modulus l, k-blocks [kb0, kb1), partial slot.
+struct I8Segment {
+  int l, kb0, kb1, slot;
+};
+
+struct I8Params {
+  int sched;
+  int L;             // moduli
+  int KB;            // k-blocks of the padded K (KP / 128)
+  int M, N;          // output extent (bounds of stores)
+  // kSchedLanes
+  int T;             // tiles
+  int Q;             // lanes
+  const int2* tiles;            // [T] (tm, tn)
+  const int* lane_seg_off;      // [Q+1] offsets into segs
+  const I8Segment* segs;        // segments of all lanes
+  int32_t* partials;            // [slots][T][128][256]
+  // kSchedUnits
+  int tiles_m, tiles_n;
+  uint8_t* residues;            // [L][M][ldr]
+  int64_t ldr;
+  uint32_t* err;
+};
+
+// Moduli and the constants of an unsigned remainder by multiply-high:
+// for 0 <= u < 2^26, q = umulhi(u, magic) is floor(u/m) or one more.
+struct I8ModConsts {
+  uint32_t m[kI8MaxModuli];
+  uint32_t magic[kI8MaxModuli];   // ceil(2^32 / m)
+  uint32_t offset[kI8MaxModuli];  // multiple of m >= 2^25 (makes |acc| < 2^25 positive)
+};
+
+__device__ __forceinline__ uint32_t i8_mod_u(uint32_t u, uint32_t m, uint32_t magic) {
+  uint32_t q = __umulhi(u, magic);
+  int32_t r = (int32_t)(u - q * m);
+  return (uint32_t)(r < 0 ? r + (int32_t)m : r);
+}
+
+// Work item seen by all roles.
+struct I8Item {
+  int l, tm, tn, kb0, kb1, slot;
+};
+
+__device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cursor,
+                                             I8Item& it) {
+  if (p.sched == kSchedLanes) {
+    const int q = cta / p.T, t = cta - q * p.T;
+    if (q >= p.Q) return false;
+    const int idx = p.lane_seg_off[q] + cursor;
+    if (idx >= p.lane_seg_off[q + 1]) return false;
+    const I8Segment s = p.segs[idx];
+    const int2 tt = p.tiles[t];
+    it.l = s.l;
+    it.kb0 = s.kb0;
+    it.kb1 = s.kb1;
+    it.slot = s.slot * p.T + t;
+    it.tm = tt.x;
+    it.tn = tt.y;
+    ++cursor;
+    return true;
+  }
+  // kSchedUnits: u = cta + cursor * grid, order (tm, l, tn)
+  const int64_t u = (int64_t)cta + (int64_t)cursor * gridDim.x;
+  const int64_t total = (int64_t)p.tiles_m * p.L * p.tiles_n;
+  if (u >= total) return false;
+  const int tn = (int)(u % p.tiles_n);
+  const int64_t r = u / p.tiles_n;
+  it.l = (int)(r % p.L);
+  it.tm = (int)(r / p.L);
+  it.tn = tn;
+  it.kb0 = 0;
+  it.kb1 = p.KB;
+  it.slot = 0;
+  ++cursor;
+  return true;
+}
+
+__global__ void __launch_bounds__(kI8Threads, 1)
+    i8_gemm_kernel(const __grid_constant__ CUtensorMap mapA,
+                   const __grid_constant__ CUtensorMap mapB, const I8Params p,
+                   const I8ModConsts mc) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + kI8Stages * kI8StageBytes);
+  uint64_t* empty_bar = full_bar + kI8Stages;
+  uint64_t* tfull_bar = empty_bar + kI8Stages;
+  uint64_t* tempty_bar = tfull_bar + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty_bar + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int cta = blockIdx.x;
+
+  // Idle CTAs (no work at all) leave before touching TMEM.
+  {
+    int cur = 0;
+    I8Item probe;
+    if (!i8_next_item(p, cta, cur, probe)) return;
+  }
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kI8Stages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull_bar[a], 1);
+      mbar_init(&tempty_bar[a], 4);  // one arrival per epilogue warp
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, kI8TmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    if (lane == 0) {
+      tma_prefetch_desc(&mapA);
+      tma_prefetch_desc(&mapB);
+      int stage = 0;
+      uint32_t phase = 0;
+      int cur = 0;
+      int64_t issued = 0;
+      I8Item it;
+      while (!*abort_flag && i8_next_item(p, cta, cur, it)) {
+        for (int kb = it.kb0; kb < it.kb1; ++kb) {
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1, p.err)) {
+            *abort_flag = 1;
+            break;
+          }
+          ++issued;
+          uint8_t* sa = smem + stage * kI8StageBytes;
+          mbar_arrive_expect_tx(&full_bar[stage], kI8StageBytes);
+          tma_load_3d(sa, &mapA, &full_bar[stage], kb * kI8BK, it.tm * kI8BM, it.l);
+          tma_load_3d(sa + kI8TileABytes, &mapB, &full_bar[stage], kb * kI8BK, it.tn * kI8BN,
+                      it.l);
+          if (++stage == kI8Stages) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+      }
+      // Drain: the last (up to kI8Stages) loads issued have landed before the
+      // CTA may exit (immediate on the normal path, where the MMA issuer has
+      // already consumed them; bounded on an abort path).
+      for (int j = 1; j <= kI8Stages && j <= issued; ++j) {
+        int s2 = stage - j;
+        uint32_t ph = phase;
+        if (s2 < 0) {
+          s2 += kI8Stages;
+          ph ^= 1;
+        }
+        mbar_wait(&full_bar[s2], ph, p.err);
+      }
+    }
+  } else if (warp == 1) {
+    // --------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN);
+      const uint32_t smem_base = smem_u32(smem);
+      int stage = 0;
+      uint32_t phase = 0;
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      int cur = 0;
+      I8Item it;
+      while (!*abort_flag && i8_next_item(p, cta, cur, it)) {
+        if (!mbar_wait(&tempty_bar[acc], acc_phase ^ 1, p.err)) {
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tmem_d = tmem_base + (uint32_t)(acc * kI8BN);
+        for (int kb = it.kb0; kb < it.kb1; ++kb) {
+          if (!mbar_wait(&full_bar[stage], phase, p.err)) {
+            *abort_flag = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_base + stage * kI8StageBytes;
+          const uint64_t adesc = umma_desc_kmajor_sw128(sa);
+          const uint64_t bdesc = umma_desc_kmajor_sw128(sa + kI8TileABytes);
+#pragma unroll
+          for (int kk = 0; kk < kI8BK / kI8UmmaK; ++kk) {
+            // advance 32 bytes of k inside the 128-byte swizzle atom
+            umma_i8(tmem_d, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
+                    (kb > it.kb0 || kk > 0) ? 1u : 0u);
+          }
+          umma_commit(&empty_bar[stage]);  // frees the smem stage when these MMAs finish
+          if (++stage == kI8Stages) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+        umma_commit(&tfull_bar[acc]);  // accumulator ready for the epilogue
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1;
+        }
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
+    const int row_in_tile = quarter * 32 + lane;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    int cur = 0;
+    I8Item it;
+    while (i8_next_item(p, cta, cur, it)) {
+      if (*abort_flag || !mbar_wait(&tfull_bar[acc], acc_phase, p.err)) {
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kI8BN);
+      const int row = it.tm * kI8BM + row_in_tile;
+      if (p.sched == kSchedLanes) {
+        int32_t* dst = p.partials + ((int64_t)it.slot * kI8BM + row_in_tile) * kI8BN;
+#pragma unroll 1
+        for (int c = 0; c < kI8BN / 32; ++c) {
+          uint32_t v[32];
+          tmem_ld_32x32b_x32(taddr + c * 32, v);
+          tmem_ld_wait();
+          int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            d4[j] = make_int4((int)v[4 * j], (int)v[4 * j + 1], (int)v[4 * j + 2], (int)v[4 * j + 3]);
+        }
+      } else {
+        const uint32_t m = mc.m[it.l], magic = mc.magic[it.l], off = mc.offset[it.l];
+        const bool row_ok = row < p.M;
+        uint8_t* dst = p.residues + ((int64_t)it.l * p.M + row) * p.ldr;
+#pragma unroll 1
+        for (int c = 0; c < kI8BN / 32; ++c) {
+          uint32_t v[32];
+          tmem_ld_32x32b_x32(taddr + c * 32, v);
+          tmem_ld_wait();
+          const int col0 = it.tn * kI8BN + c * 32;
+          if (row_ok && col0 < p.N) {
+            uint32_t w[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              uint32_t b0 = i8_mod_u(v[4 * j] + off, m, magic);
+              uint32_t b1 = i8_mod_u(v[4 * j + 1] + off, m, magic);
+              uint32_t b2 = i8_mod_u(v[4 * j + 2] + off, m, magic);
+              uint32_t b3 = i8_mod_u(v[4 * j + 3] + off, m, magic);
+              w[j] = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+            }
+            if (col0 + 32 <= p.N) {
+              uint4* d4 = reinterpret_cast<uint4*>(dst + col0);
+              d4[0] = make_uint4(w[0], w[1], w[2], w[3]);
+              d4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            } else {
+              for (int j = 0; j < 32 && col0 + j < p.N; ++j)
+                dst[col0 + j] = (uint8_t)(w[j >> 2] >> (8 * (j & 3)));
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty_bar[acc]);
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+  }
+
+  // Teardown: every role's loop is bounded, so all threads arrive here.
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem_base, kI8TmemCols);
+}
+
+// INT8 tensor-core peak probe: MMAs on one resident smem stage (no TMA),
+// accumulating into TMEM; used only to measure the kind::i8 throughput.
+__global__ void __launch_bounds__(128, 1) i8_peak_kernel(int iters, uint32_t* sink) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint64_t* done = reinterpret_cast<uint64_t*>(smem + kI8StageBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  for (int i = threadIdx.x; i < kI8StageBytes / 4; i += blockDim.x)
+    reinterpret_cast<uint32_t*>(smem)[i] = 0x01010101u * (uint32_t)(i & 3);
+  if (threadIdx.x == 0) {
+    mbar_init(done, 1);
+    fence_mbar_init();
+  }
+  fence_proxy_async_smem();
+  if ((threadIdx.x >> 5) == 0) {
+    tmem_alloc(tmem_slot, kI8TmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  if (threadIdx.x == 0) {
+    const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN);
+    const uint32_t sa = smem_u32(smem);
+    const uint64_t adesc = umma_desc_kmajor_sw128(sa);
+    const uint64_t bdesc = umma_desc_kmajor_sw128(sa + kI8TileABytes);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        umma_i8(tmem_base + (uint32_t)((it & 1) * kI8BN), adesc + kk * 2, bdesc + kk * 2, idesc,
+                it > 1 ? 1u : 0u);
+    }
+    umma_commit(done);
+  }
+  __syncwarp();
+  if (threadIdx.x < 32) {  // warp 0, converged: tcgen05.ld is warp-collective
+    const bool ok = mbar_wait(done, 0, sink + 1);
+    tc_fence_after();
+    uint32_t v[32];
+    tmem_ld_32x32b_x32(tmem_base, v);
+    tmem_ld_wait();
+    if (ok && v[0] == 0xFFFFFFFFu) sink[0] = v[1];  // keeps the MMAs live
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(tmem_base, kI8TmemCols);
+}
+
+}  // namespace skg

@@ -1,20 +1,859 @@
-// Ozaki split-precision path.
+// Ozaki scheme II on sm_100a: FP64-accurate GEMM / SYRK / rotation from exact
+// INT8 tensor-core products (Ozaki, Uchino, Imamura, "Ozaki Scheme II: A
+// GEMM-oriented emulation of floating-point matrix multiplication using an
+// integer modular technique", 2025).
+//
+// For C = A B (A: rows i, B: columns j, inner dimension k):
+//  1. Scaling. Row i of A is scaled by 2^mu_i, column j of B by 2^nu_j, with
+//     mu_i = gamma - ceil(log2 ||A_i||_2), so ||A_i 2^mu_i||_2 <= 2^gamma, and
+//     rounded to integers A', B'. By Cauchy-Schwarz |(A'B')_ij| <= 2^(2 gamma)
+//     (up to rounding slack), chosen below M/4 where M = m_0 ... m_{L-1}.
+//  2. Residues. A' and B' are reduced modulo L pairwise-coprime moduli
+//     m_l <= 256 into symmetric residues that fit int8.
+//  3. Products. For every l, C_l = A'_l B'_l is computed exactly on tcgen05
+//     kind::i8 (INT32 accumulation, k-segments short enough to be exact).
+//  4. Reconstruction. C' = CRT(C_l mod m_l) in [-M/2, M/2] is evaluated in
+//     FP64 with split constants: W_l = (M/m_l) * ((M/m_l)^-1 mod m_l) is
+//     stored as Wh_l + Wl_l where Wh_l has at most 40 significant bits on a
+//     common grid 2^e (so sum_l r_l Wh_l is exact in FP64) and Wl_l < 2^e;
+//     q = rint(s / M), C' = (S_hi - q Mh) + (S_lo - q Ml). Finally
+//     C = 2^(-mu_i - nu_j) C'.
+// The error is that of rounding A and B to gamma bits (about
+// sqrt(k/12) * 2^-gamma relative to ||A_i|| ||B_j|| per element); the
+// reconstruction itself adds ~2^-70 relative.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "skg_i8gemm_kernel.cuh"
 #include "skg_ozaki.h"
 
 namespace skg {
 
-int ozaki_gemm_packed(int64_t, int64_t, int64_t, const double*, const double*, double*, int64_t,
-                      double, double, skgemm_options_t*, cudaStream_t) {
-  return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki path not built yet");
+namespace {
+
+// Pairwise-coprime moduli <= 256, largest first: 2^8, 3*5*17, 11*23, 251,
+// 13*19, 241, 239, 233, 229, 227, 223, 7*31, 211, 199, 197, 193.
+constexpr uint32_t kModuli[kI8MaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                            229, 227, 223, 217, 211, 199, 197, 193};
+constexpr int kMinModuli = 6;
+constexpr int kSegKbCap = 1023;  // 1023*128 products of |x| <= 2^14 stay below 2^31
+
+struct ResidueConsts {
+  uint32_t m[kI8MaxModuli];
+  uint32_t magic[kI8MaxModuli];
+  uint32_t c1[kI8MaxModuli];  // 2^18 mod m
+  uint32_t c2[kI8MaxModuli];  // 2^36 mod m
+  uint32_t c3[kI8MaxModuli];  // 2^54 mod m
+};
+
+struct CrtConsts {  // for one moduli count L
+  double wh[kI8MaxModuli];
+  double wl[kI8MaxModuli];
+  double mh, ml, inv_m;
+};
+
+__constant__ ResidueConsts c_res;
+__constant__ CrtConsts c_crt[kI8MaxModuli + 1];
+
+typedef unsigned __int128 u128;
+
+int bitlen(u128 x) {
+  int b = 0;
+  while (x) {
+    x >>= 1;
+    ++b;
+  }
+  return b;
 }
-int ozaki_syrk_packed(int64_t, int64_t, const double*, double*, int64_t, double, double,
-                      skgemm_options_t*, cudaStream_t) {
-  return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki path not built yet");
+
+double u128_to_double(u128 x) { return (double)x; }
+
+// Host constants for L moduli (the first L of kModuli).
+CrtConsts make_crt(int L, double* log2M_out) {
+  CrtConsts c;
+  memset(&c, 0, sizeof(c));
+  u128 M = 1;
+  for (int l = 0; l < L; ++l) M *= kModuli[l];
+  const int e = bitlen(M) - 40;
+  for (int l = 0; l < L; ++l) {
+    const uint32_t m = kModuli[l];
+    const u128 Ml = M / m;
+    const uint32_t r = (uint32_t)(Ml % m);
+    uint32_t y = 0;
+    for (uint32_t t = 1; t < m; ++t)
+      if ((uint64_t)r * t % m == 1) {
+        y = t;
+        break;
+      }
+    const u128 W = (Ml * y) % M;
+    const u128 Wh = (W >> e) << e;
+    c.wh[l] = ldexp((double)(uint64_t)(W >> e), e);
+    c.wl[l] = u128_to_double(W - Wh);
+  }
+  const u128 Mh = (M >> e) << e;
+  c.mh = ldexp((double)(uint64_t)(M >> e), e);
+  c.ml = u128_to_double(M - Mh);
+  c.inv_m = 1.0 / u128_to_double(M);
+  if (log2M_out) *log2M_out = log2(u128_to_double(M));
+  return c;
 }
-int ozaki_rot(int64_t, int64_t, const double*, const double*, double*, skgemm_options_t*,
-              cudaStream_t) {
-  return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki path not built yet");
+
+// Largest gamma with (2^gamma)^2 < M / 4.2 (Cauchy-Schwarz bound of A'B').
+int gamma_for(int L) {
+  double lg = 0;
+  make_crt(L, &lg);
+  return (int)floor((lg - 2.1) / 2.0);
 }
+
+// ------------------------------------------------------------ device math
+__device__ __forceinline__ int ceil_log2_pos(double x) {
+  int e;
+  const double f = frexp(x, &e);  // x = f 2^e, f in [0.5, 1)
+  return f == 0.5 ? e - 1 : e;
+}
+
+__device__ __forceinline__ int row_exponent(double sumsq, int gamma_bits) {
+  if (!(sumsq > 0.0)) return 0;  // zero (or empty) row: any scale
+  return gamma_bits - ceil_log2_pos(sqrt(sumsq));
+}
+
+// Symmetric residues of the integer X modulo the first L moduli, as int8
+// bit patterns, for 8 consecutive elements packed into one uint64 per modulus.
+__device__ __forceinline__ uint32_t residue_u(uint64_t u, int l) {
+  const uint32_t d0 = (uint32_t)(u & 0x3FFFFu);
+  const uint32_t d1 = (uint32_t)((u >> 18) & 0x3FFFFu);
+  const uint32_t d2 = (uint32_t)((u >> 36) & 0x3FFFFu);
+  const uint32_t d3 = (uint32_t)(u >> 54);
+  const uint32_t S = d3 * c_res.c3[l] + d2 * c_res.c2[l] + d1 * c_res.c1[l] + d0;  // < 2^27
+  return i8_mod_u(S, c_res.m[l], c_res.magic[l]);
+}
+
+__device__ __forceinline__ uint32_t sym_byte(int64_t X, int l) {
+  const uint64_t u = (uint64_t)(X < 0 ? -X : X);
+  const uint32_t m = c_res.m[l];
+  uint32_t r = residue_u(u, l);
+  if (X < 0 && r) r = m - r;
+  const int rs = (int)r > (int)((m - 1) / 2) ? (int)r - (int)m : (int)r;
+  return (uint32_t)(uint8_t)(int8_t)rs;
+}
+
+__device__ __forceinline__ int64_t scaled_int(double v, int mu) {
+  return llrint(ldexp(v, mu));
+}
+
+// ------------------------------------------------- packed-T operand prep
+// Partial sums of squares of each row of a packed-T operand
+// ([ceil(R/T)][K][T]): part[(p*C + c)*T + r] over k-chunk c.
+template <int T>
+__global__ void __launch_bounds__(256) norm_partials_kernel(int64_t R, int64_t K,
+                                                           const double* __restrict__ X,
+                                                           int C, double* __restrict__ part) {
+  __shared__ double red[256];
+  const int p = blockIdx.x, c = blockIdx.y;
+  const int r = threadIdx.x % T, kl = threadIdx.x / T;
+  constexpr int KL = 256 / T;
+  const int64_t k0 = (int64_t)c * K / C, k1 = (int64_t)(c + 1) * K / C;
+  const double* src = X + (int64_t)p * K * T;
+  double acc = 0.0;
+  for (int64_t k = k0 + kl; k < k1; k += KL) {
+    const double v = src[k * T + r];
+    acc = fma(v, v, acc);
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < T) {
+    double s = 0.0;
+    for (int j = 0; j < KL; ++j) s += red[j * T + threadIdx.x];
+    const int64_t row = (int64_t)p * T + threadIdx.x;
+    part[((int64_t)p * C + c) * T + threadIdx.x] = row < R ? s : 0.0;
+  }
+}
+
+// Residues of a packed-T operand -> res[l][Rpad][KP] (K-major bytes).
+// CTA (p, kb): rows p*T .. +T, k-block kb (128 k). mu of each row from the
+// norm partials; CTAs with kb == 0 also publish mu.
+template <int T>
+__global__ void __launch_bounds__(256) convert_packed_kernel(
+    int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ X, int C,
+    const double* __restrict__ part, int gamma_bits, int L, int8_t* __restrict__ res,
+    int* __restrict__ mu_out) {
+  __shared__ double tile[128 * T];
+  __shared__ int mu[T];
+  const int p = blockIdx.x, kb = blockIdx.y;
+  const int64_t P_in = (R + T - 1) / T;
+  const int64_t k0 = (int64_t)kb * 128;
+  if (threadIdx.x < T) {
+    const int64_t row = (int64_t)p * T + threadIdx.x;
+    int m = 0;
+    if (p < P_in && row < R) {
+      double s = 0.0;
+      for (int c = 0; c < C; ++c) s += part[((int64_t)p * C + c) * T + threadIdx.x];
+      m = row_exponent(s, gamma_bits);
+    }
+    mu[threadIdx.x] = m;
+    if (kb == 0 && row < Rpad) mu_out[row] = m;
+  }
+  const double* src = X + (int64_t)p * K * T;
+  for (int i = threadIdx.x; i < 128 * T; i += 256) {
+    const int kk = i / T, r = i % T;
+    const int64_t k = k0 + kk, row = (int64_t)p * T + r;
+    tile[i] = (p < P_in && k < K && row < R) ? src[k * T + r] : 0.0;
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < 16 * T; item += 256) {
+    const int r = item % T, kk = item / T;  // 8 consecutive k: 8*kk .. 8*kk+7
+    int64_t xi[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) xi[j] = scaled_int(tile[(8 * kk + j) * T + r], mu[r]);
+    const int64_t row = (int64_t)p * T + r;
+    int8_t* dst = res + row * KP + k0 + 8 * kk;
+    for (int l = 0; l < L; ++l) {
+      uint32_t lo = 0, hi = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) lo |= sym_byte(xi[j], l) << (8 * j);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) hi |= sym_byte(xi[4 + j], l) << (8 * j);
+      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) = make_uint2(lo, hi);
+    }
+  }
+}
+
+// Rotation A: grid-packed Psi [Nd/16][nb][16]; rows are grid points g (scaled
+// over the nb bands), k = band. One CTA per 16-row panel.
+__global__ void __launch_bounds__(256) convert_grid_rows_kernel(
+    int64_t Nd, int64_t nb, int64_t KP, int64_t Rpad, const double* __restrict__ A,
+    int gamma_bits, int L, int8_t* __restrict__ res, int* __restrict__ mu_out) {
+  __shared__ double red[256];
+  __shared__ int mu[16];
+  const int64_t p = blockIdx.x;
+  const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
+  const bool live = p * 16 < Nd;
+  const double* src = A + p * nb * 16;
+  double acc = 0.0;
+  if (live)
+    for (int64_t b = kl; b < nb; b += 16) {
+      const double v = src[b * 16 + r];
+      acc = fma(v, v, acc);
+    }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    double s = 0.0;
+    for (int j = 0; j < 16; ++j) s += red[j * 16 + threadIdx.x];
+    const int m = live ? row_exponent(s, gamma_bits) : 0;
+    mu[threadIdx.x] = m;
+    if (p * 16 + threadIdx.x < Rpad) mu_out[p * 16 + threadIdx.x] = m;
+  }
+  __syncthreads();
+  const int64_t row = p * 16 + r;
+  for (int64_t kb0 = 0; kb0 < KP; kb0 += 128) {
+    const int64_t k = kb0 + 8 * kl;
+    int64_t xi[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      xi[j] = (live && k + j < nb) ? scaled_int(src[(k + j) * 16 + r], mu[r]) : 0;
+    int8_t* dst = res + row * KP + k;
+    for (int l = 0; l < L; ++l) {
+      uint32_t lo = 0, hi = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) lo |= sym_byte(xi[j], l) << (8 * j);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) hi |= sym_byte(xi[4 + j], l) << (8 * j);
+      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) = make_uint2(lo, hi);
+    }
+  }
+}
+
+// Rotation B: Q row-major nb x nb; B(k = b, n = j) = Q[b*nb + j]; rows of the
+// residue matrix are the columns j of Q (scaled over b), k = b.
+__global__ void __launch_bounds__(256) convert_q_cols_kernel(
+    int64_t nb, int64_t KP, int64_t Rpad, const double* __restrict__ Q, int gamma_bits, int L,
+    int8_t* __restrict__ res, int* __restrict__ nu_out) {
+  __shared__ double red[256];
+  __shared__ int nu[16];
+  const int64_t p = blockIdx.x;  // 16 columns
+  const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
+  const int64_t j = p * 16 + r;
+  const bool live = j < nb;
+  double acc = 0.0;
+  if (live)
+    for (int64_t b = kl; b < nb; b += 16) {
+      const double v = Q[b * nb + j];
+      acc = fma(v, v, acc);
+    }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    double s = 0.0;
+    for (int i = 0; i < 16; ++i) s += red[i * 16 + threadIdx.x];
+    const int m = (p * 16 + threadIdx.x < nb) ? row_exponent(s, gamma_bits) : 0;
+    nu[threadIdx.x] = m;
+    if (p * 16 + threadIdx.x < Rpad) nu_out[p * 16 + threadIdx.x] = m;
+  }
+  __syncthreads();
+  for (int64_t kb0 = 0; kb0 < KP; kb0 += 128) {
+    const int64_t k = kb0 + 8 * kl;
+    int64_t xi[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      xi[t] = (live && k + t < nb) ? scaled_int(Q[(k + t) * nb + j], nu[r]) : 0;
+    int8_t* dst = res + j * KP + k;
+    for (int l = 0; l < L; ++l) {
+      uint32_t lo = 0, hi = 0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) lo |= sym_byte(xi[t], l) << (8 * t);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) hi |= sym_byte(xi[4 + t], l) << (8 * t);
+      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) = make_uint2(lo, hi);
+    }
+  }
+}
+
+// ------------------------------------------------------- reconstruction
+// r[] holds the L non-negative residues (entries >= L are ignored).
+__device__ __forceinline__ double crt_value(const uint32_t (&r)[kI8MaxModuli], int L) {
+  const CrtConsts& c = c_crt[L];
+  double sh = 0.0, sl = 0.0;
+#pragma unroll
+  for (int l = 0; l < kI8MaxModuli; ++l) {
+    if (l < L) {
+      const double rd = (double)r[l];
+      sh = fma(rd, c.wh[l], sh);  // exact: 8-bit x 40-bit on a common grid
+      sl = fma(rd, c.wl[l], sl);
+    }
+  }
+  const double q = rint((sh + sl) * c.inv_m);
+  return fma(-q, c.mh, sh) + fma(-q, c.ml, sl);
+}
+
+// GEMM / SYRK: out(i, j) from the int32 partial slabs of the lane schedule.
+// mode 0: D[i*ldd + j] = alpha*v + gamma; mode 1 (SYRK, i <= j only):
+// C[i + j*ldd] = alpha*v + beta*C (beta_zero: no read).
+__global__ void __launch_bounds__(256) crt_partials_kernel(
+    int M, int N, int L, const int32_t* __restrict__ partials, int T,
+    const int* __restrict__ tile_index, int tiles_n, const int* __restrict__ mod_slot_off,
+    const int* __restrict__ mod_slots, const int* __restrict__ mu, const int* __restrict__ nu,
+    int mode, double* __restrict__ D, int64_t ldd, double alpha, double gamma, int beta_zero) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)M * N) return;
+  const int i = (int)(idx / N), j = (int)(idx % N);
+  if (mode == 1 && i > j) return;
+  const int t = tile_index[(i / kI8BM) * tiles_n + j / kI8BN];
+  const int64_t off = (int64_t)(i % kI8BM) * kI8BN + (j % kI8BN);
+  uint32_t r[kI8MaxModuli];
+#pragma unroll
+  for (int l = 0; l < kI8MaxModuli; ++l) {
+    r[l] = 0;
+    if (l < L) {
+      int64_t s = 0;
+      for (int q = mod_slot_off[l]; q < mod_slot_off[l + 1]; ++q)
+        s += partials[((int64_t)mod_slots[q] * T + t) * (kI8BM * kI8BN) + off];
+      const int64_t m = c_res.m[l];
+      int64_t rr = s % m;
+      if (rr < 0) rr += m;
+      r[l] = (uint32_t)rr;
+    }
+  }
+  const double v = ldexp(crt_value(r, L), -(mu[i] + nu[j]));
+  if (mode == 0) {
+    D[(int64_t)i * ldd + j] = alpha * v + gamma;
+  } else {
+    double* c = D + i + (int64_t)j * ldd;
+    *c = beta_zero ? alpha * v : alpha * v + gamma * (*c);
+  }
+}
+
+// Rotation: Psi'(g, b) band-packed from the residue bytes res[l][g][ldr].
+__global__ void __launch_bounds__(256) crt_residues_band_kernel(
+    int64_t Nd, int64_t nb, int L, const uint8_t* __restrict__ res, int64_t ldr,
+    const int* __restrict__ mu, const int* __restrict__ nu, double* __restrict__ Dband) {
+  const int64_t chunks = nb / 16;
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= Nd * chunks) return;
+  const int64_t g = idx / chunks, c = idx % chunks;
+  uint32_t w[kI8MaxModuli][4];  // 16 residue bytes per modulus
+#pragma unroll
+  for (int l = 0; l < kI8MaxModuli; ++l) {
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (l < L) v = *reinterpret_cast<const uint4*>(res + ((int64_t)l * Nd + g) * ldr + c * 16);
+    w[l][0] = v.x;
+    w[l][1] = v.y;
+    w[l][2] = v.z;
+    w[l][3] = v.w;
+  }
+  double out[16];
+  const int mg = mu[g];
+#pragma unroll
+  for (int t = 0; t < 16; ++t) {
+    uint32_t rr[kI8MaxModuli];
+#pragma unroll
+    for (int l = 0; l < kI8MaxModuli; ++l) rr[l] = (w[l][t >> 2] >> (8 * (t & 3))) & 0xFFu;
+    out[t] = ldexp(crt_value(rr, L), -(mg + nu[c * 16 + t]));
+  }
+  double2* dst = reinterpret_cast<double2*>(Dband + (c * Nd + g) * 16);
+#pragma unroll
+  for (int t = 0; t < 8; ++t) dst[t] = make_double2(out[2 * t], out[2 * t + 1]);
+}
+
+// Exact INT8 GEMM output: C[i*ldc + j] = sum over slots of the partial slabs.
+__global__ void __launch_bounds__(256) sum_partials_kernel(
+    int M, int N, const int32_t* __restrict__ partials, int T, const int* __restrict__ tile_index,
+    int tiles_n, const int* __restrict__ mod_slot_off, const int* __restrict__ mod_slots,
+    int32_t* __restrict__ C, int64_t ldc) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)M * N) return;
+  const int i = (int)(idx / N), j = (int)(idx % N);
+  const int t = tile_index[(i / kI8BM) * tiles_n + j / kI8BN];
+  const int64_t off = (int64_t)(i % kI8BM) * kI8BN + (j % kI8BN);
+  int64_t s = 0;
+  for (int q = mod_slot_off[0]; q < mod_slot_off[1]; ++q)
+    s += partials[((int64_t)mod_slots[q] * T + t) * (kI8BM * kI8BN) + off];
+  C[(int64_t)i * ldc + j] = (int32_t)s;
+}
+
+// ------------------------------------------------------------- host side
+struct LanePlan {
+  int T = 0, Q = 0, slots = 0, L = 0, KB = 0, tiles_m = 0, tiles_n = 0;
+  DeviceBuffer buf;  // tiles | lane_seg_off | segs | tile_index | mod_slot_off | mod_slots
+  int2* tiles = nullptr;
+  int* lane_seg_off = nullptr;
+  I8Segment* segs = nullptr;
+  int* tile_index = nullptr;
+  int* mod_slot_off = nullptr;
+  int* mod_slots = nullptr;
+};
+
+struct OzakiStream {
+  DeviceBuffer res_a, res_b, part_a, part_b, mu_a, mu_b, partials, rbytes;
+};
+
+struct OzakiDevice {
+  bool consts_ready = false;
+  std::map<std::tuple<int, int, int, int, int>, LanePlan*> plans;  // (M, N, KB, L, syrk)
+  std::map<cudaStream_t, OzakiStream*> streams;
+};
+
+std::mutex g_oz_mu;
+OzakiDevice g_oz[64];
+I8ModConsts g_modc;
+bool g_modc_ready = false;
+
+int ensure_consts(DeviceState* dev) {
+  OzakiDevice& od = g_oz[dev->device];
+  if (od.consts_ready) return SKGEMM_OK;
+  ResidueConsts rc;
+  for (int l = 0; l < kI8MaxModuli; ++l) {
+    const uint32_t m = kModuli[l];
+    rc.m[l] = m;
+    rc.magic[l] = (uint32_t)(((1ull << 32) + m - 1) / m);
+    rc.c1[l] = (uint32_t)((1ull << 18) % m);
+    rc.c2[l] = (uint32_t)((1ull << 36) % m);
+    rc.c3[l] = (uint32_t)((1ull << 54) % m);
+    g_modc.m[l] = m;
+    g_modc.magic[l] = rc.magic[l];
+    g_modc.offset[l] = (uint32_t)((((1u << 25) + m - 1) / m) * m);
+  }
+  g_modc_ready = true;
+  CrtConsts cc[kI8MaxModuli + 1];
+  memset(cc, 0, sizeof(cc));
+  for (int L = kMinModuli; L <= kI8MaxModuli; ++L) cc[L] = make_crt(L, nullptr);
+  SKG_CUDA(cudaMemcpyToSymbol(c_res, &rc, sizeof(rc)));
+  SKG_CUDA(cudaMemcpyToSymbol(c_crt, cc, sizeof(cc)));
+  od.consts_ready = true;
+  return SKGEMM_OK;
+}
+
+OzakiStream* ozaki_stream(DeviceState* dev, cudaStream_t s) {
+  OzakiStream*& o = g_oz[dev->device].streams[s];
+  if (!o) o = new OzakiStream();
+  return o;
+}
+
+// Lane schedule: T tiles x Q lanes, each lane a contiguous range of the
+// (modulus, k-block) space, cut into segments at modulus boundaries and at
+// kSegKbCap k-blocks.
+int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, LanePlan** out) {
+  OzakiDevice& od = g_oz[dev->device];
+  auto key = std::make_tuple(M, N, KB, L, syrk ? 1 : 0);
+  auto itp = od.plans.find(key);
+  if (itp != od.plans.end()) {
+    *out = itp->second;
+    return SKGEMM_OK;
+  }
+  LanePlan* pl = new LanePlan();
+  pl->L = L;
+  pl->KB = KB;
+  pl->tiles_m = (M + kI8BM - 1) / kI8BM;
+  pl->tiles_n = (N + kI8BN - 1) / kI8BN;
+  std::vector<int2> tiles;
+  std::vector<int> tile_index(pl->tiles_m * pl->tiles_n, -1);
+  for (int tm = 0; tm < pl->tiles_m; ++tm)
+    for (int tn = 0; tn < pl->tiles_n; ++tn) {
+      if (syrk && tm * kI8BM > tn * kI8BN + kI8BN - 1) continue;  // strictly lower
+      tile_index[tm * pl->tiles_n + tn] = (int)tiles.size();
+      tiles.push_back(make_int2(tm, tn));
+    }
+  pl->T = (int)tiles.size();
+  pl->Q = std::max(1, dev->num_sms / pl->T);
+  const int64_t W = (int64_t)L * KB;
+  if (pl->Q > W) pl->Q = (int)W;
+  std::vector<int> lane_off(pl->Q + 1, 0);
+  std::vector<I8Segment> segs;
+  std::vector<std::vector<int>> by_mod(L);
+  for (int q = 0; q < pl->Q; ++q) {
+    lane_off[q] = (int)segs.size();
+    int64_t it = (int64_t)q * W / pl->Q, end = (int64_t)(q + 1) * W / pl->Q;
+    while (it < end) {
+      const int l = (int)(it / KB);
+      const int kb = (int)(it % KB);
+      int64_t stop = std::min<int64_t>(end, (int64_t)(l + 1) * KB);
+      stop = std::min<int64_t>(stop, it + kSegKbCap);
+      I8Segment s;
+      s.l = l;
+      s.kb0 = kb;
+      s.kb1 = kb + (int)(stop - it);
+      s.slot = (int)segs.size();
+      by_mod[l].push_back(s.slot);
+      segs.push_back(s);
+      it = stop;
+    }
+  }
+  lane_off[pl->Q] = (int)segs.size();
+  pl->slots = (int)segs.size();
+  std::vector<int> mod_off(L + 1, 0), mod_slots;
+  for (int l = 0; l < L; ++l) {
+    mod_off[l] = (int)mod_slots.size();
+    mod_slots.insert(mod_slots.end(), by_mod[l].begin(), by_mod[l].end());
+  }
+  mod_off[L] = (int)mod_slots.size();
+  // one device buffer, 16-byte aligned sections
+  auto al = [](size_t x) { return (x + 15) / 16 * 16; };
+  const size_t s0 = al(tiles.size() * sizeof(int2)), s1 = al(lane_off.size() * sizeof(int)),
+               s2 = al(segs.size() * sizeof(I8Segment)), s3 = al(tile_index.size() * sizeof(int)),
+               s4 = al(mod_off.size() * sizeof(int)), s5 = al(mod_slots.size() * sizeof(int) + 4);
+  int st;
+  if ((st = pl->buf.ensure(s0 + s1 + s2 + s3 + s4 + s5)) != SKGEMM_OK) {
+    delete pl;
+    return st;
+  }
+  uint8_t* b = static_cast<uint8_t*>(pl->buf.ptr);
+  std::vector<uint8_t> host(s0 + s1 + s2 + s3 + s4 + s5, 0);
+  memcpy(host.data(), tiles.data(), tiles.size() * sizeof(int2));
+  memcpy(host.data() + s0, lane_off.data(), lane_off.size() * sizeof(int));
+  memcpy(host.data() + s0 + s1, segs.data(), segs.size() * sizeof(I8Segment));
+  memcpy(host.data() + s0 + s1 + s2, tile_index.data(), tile_index.size() * sizeof(int));
+  memcpy(host.data() + s0 + s1 + s2 + s3, mod_off.data(), mod_off.size() * sizeof(int));
+  memcpy(host.data() + s0 + s1 + s2 + s3 + s4, mod_slots.data(), mod_slots.size() * sizeof(int));
+  SKG_CUDA(cudaMemcpy(b, host.data(), host.size(), cudaMemcpyHostToDevice));
+  pl->tiles = reinterpret_cast<int2*>(b);
+  pl->lane_seg_off = reinterpret_cast<int*>(b + s0);
+  pl->segs = reinterpret_cast<I8Segment*>(b + s0 + s1);
+  pl->tile_index = reinterpret_cast<int*>(b + s0 + s1 + s2);
+  pl->mod_slot_off = reinterpret_cast<int*>(b + s0 + s1 + s2 + s3);
+  pl->mod_slots = reinterpret_cast<int*>(b + s0 + s1 + s2 + s3 + s4);
+  od.plans[key] = pl;
+  *out = pl;
+  return SKGEMM_OK;
+}
+
+int make_res_map(CUtensorMap* map, const void* base, int64_t KP, int64_t Rpad, int L,
+                 int box_rows) {
+  uint64_t dims[3] = {(uint64_t)KP, (uint64_t)Rpad, (uint64_t)L};
+  uint64_t strides[2] = {(uint64_t)KP, (uint64_t)(KP * Rpad)};
+  uint32_t box[3] = {128, (uint32_t)box_rows, 1};
+  return encode_tiled(map, 3, base, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                      CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+int launch_i8(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB, const I8Params& p,
+              int grid, cudaStream_t s) {
+  static bool attr_done[64] = {false};
+  if (!attr_done[dev->device]) {
+    SKG_CUDA(cudaFuncSetAttribute(i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kI8SmemBytes));
+    attr_done[dev->device] = true;
+  }
+  i8_gemm_kernel<<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, p, g_modc);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+int choose_L(const skgemm_options_t* opts, int64_t K, int* L_out, int* gamma_out) {
+  int L = opts ? opts->slices : 0;
+  if (L == 0) {
+    // Smallest L whose error estimate for random-sign data,
+    // sqrt(K/12) * 2^(1-gamma) relative, stays below 3e-14 (a factor of three
+    // under the 1e-13 gate).
+    L = kMinModuli;
+    while (L < kI8MaxModuli &&
+           std::sqrt((double)K / 12.0) * std::ldexp(2.0, -gamma_for(L)) > 3e-14)
+      ++L;
+  }
+  if (L < kMinModuli || L > kI8MaxModuli)
+    return fail(SKGEMM_ERR_INVALID_ARG, "Ozaki moduli count must be in [6, 16]");
+  *L_out = L;
+  *gamma_out = gamma_for(L);
+  return SKGEMM_OK;
+}
+
+void report(skgemm_options_t* opts, int L, int gamma_bits, int64_t K) {
+  if (!opts) return;
+  opts->slices_used_out = L;
+  opts->err_bound_out = 2.0 * std::sqrt((double)K / 12.0) * std::ldexp(1.0, -gamma_bits);
+}
+
+// Residues of a packed-T operand into res[L][Rpad][KP] + row exponents.
+template <int T>
+int prep_packed(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, int L,
+                int gamma_bits, OzakiStream* os, DeviceBuffer& res, DeviceBuffer& part,
+                DeviceBuffer& mu, cudaStream_t s) {
+  const int64_t P_in = (R + T - 1) / T;
+  const int C = (int)std::max<int64_t>(1, std::min<int64_t>(64, (600 + P_in - 1) / P_in));
+  int st;
+  if ((st = res.ensure((size_t)L * Rpad * KP)) != SKGEMM_OK) return st;
+  if ((st = part.ensure((size_t)P_in * C * T * sizeof(double))) != SKGEMM_OK) return st;
+  if ((st = mu.ensure((size_t)Rpad * sizeof(int))) != SKGEMM_OK) return st;
+  norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
+                                                                  (double*)part.ptr);
+  SKG_CUDA(cudaGetLastError());
+  convert_packed_kernel<T><<<dim3((unsigned)(Rpad / T), (unsigned)(KP / 128)), 256, 0, s>>>(
+      R, K, KP, Rpad, X, C, (const double*)part.ptr, gamma_bits, L, (int8_t*)res.ptr,
+      (int*)mu.ptr);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+// Shared body of the Ozaki GEMM and SYRK: residues of A (packed16) and B
+// (packed16 for SYRK, packed32 for GEMM), lane-scheduled INT8 products,
+// reconstruction.
+int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp, bool syrk,
+                double* D, int64_t ldd, double alpha, double gamma, skgemm_options_t* opts,
+                cudaStream_t s) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  if (!Ap || !Bp || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  if (K == 0) return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki path needs K > 0");
+  if (M > (1 << 20) || N > (1 << 20)) return fail(SKGEMM_ERR_INVALID_ARG, "dimension too large");
+  int L, gb;
+  if ((st = choose_L(opts, K, &L, &gb)) != SKGEMM_OK) return st;
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  if ((st = ensure_consts(dev)) != SKGEMM_OK) return st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  OzakiStream* os = ozaki_stream(dev, s);
+  const int64_t KP = (K + 127) / 128 * 128;
+  const int KB = (int)(KP / 128);
+  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;  // 256-multiples serve both box heights
+  const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
+  if ((st = prep_packed<16>(M, K, KP, RA, Ap, L, gb, os, os->res_a, os->part_a, os->mu_a, s)))
+    return st;
+  const DeviceBuffer* resB = &os->res_a;
+  const DeviceBuffer* muB = &os->mu_a;
+  if (!syrk) {
+    if ((st = prep_packed<32>(N, K, KP, RB, Bp, L, gb, os, os->res_b, os->part_b, os->mu_b, s)))
+      return st;
+    resB = &os->res_b;
+    muB = &os->mu_b;
+  }
+  LanePlan* pl = nullptr;
+  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, &pl)) != SKGEMM_OK) return st;
+  if ((st = os->partials.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t))))
+    return st;
+  CUtensorMap mA, mB;
+  if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, L, kI8BM))) return st;
+  if ((st = make_res_map(&mB, resB->ptr, KP, syrk ? RA : RB, L, kI8BN))) return st;
+  I8Params p;
+  memset(&p, 0, sizeof(p));
+  p.sched = kSchedLanes;
+  p.L = L;
+  p.KB = KB;
+  p.M = (int)M;
+  p.N = (int)N;
+  p.T = pl->T;
+  p.Q = pl->Q;
+  p.tiles = pl->tiles;
+  p.lane_seg_off = pl->lane_seg_off;
+  p.segs = pl->segs;
+  p.partials = (int32_t*)os->partials.ptr;
+  p.err = ws->err;
+  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s))) return st;
+  const int64_t n = M * N;
+  crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      (int)M, (int)N, L, (const int32_t*)os->partials.ptr, pl->T, pl->tile_index, pl->tiles_n,
+      pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)muB->ptr,
+      syrk ? 1 : 0, D, ldd, alpha, gamma, (syrk && gamma == 0.0) ? 1 : 0);
+  SKG_CUDA(cudaGetLastError());
+  report(opts, L, gb, K);
+  return SKGEMM_OK;
+}
+
+}  // namespace
+
+int ozaki_gemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp,
+                      double* D, int64_t ldd, double alpha, double gamma,
+                      skgemm_options_t* opts, cudaStream_t s) {
+  return ozaki_lanes(M, N, K, Ap, Bp, false, D, ldd, alpha, gamma, opts, s);
+}
+
+int ozaki_syrk_packed(int64_t K, int64_t M, const double* Ap, double* C, int64_t ldc,
+                      double alpha, double beta, skgemm_options_t* opts, cudaStream_t s) {
+  return ozaki_lanes(M, M, K, Ap, Ap, true, C, ldc, alpha, beta, opts, s);
+}
+
+int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
+              skgemm_options_t* opts, cudaStream_t s) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  if (Nd == 0 || nb == 0) return SKGEMM_OK;
+  if (!A || !Q || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  if (nb > 2048) return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki rotation supports nb <= 2048");
+  if (Nd > ((int64_t)1 << 30)) return fail(SKGEMM_ERR_INVALID_ARG, "Nd too large");
+  int L, gb;
+  if ((st = choose_L(opts, nb, &L, &gb)) != SKGEMM_OK) return st;
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  if ((st = ensure_consts(dev)) != SKGEMM_OK) return st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  OzakiStream* os = ozaki_stream(dev, s);
+  const int64_t KP = (nb + 127) / 128 * 128;
+  const int64_t RA = (Nd + kI8BM - 1) / kI8BM * kI8BM;
+  const int64_t RB = (nb + kI8BN - 1) / kI8BN * kI8BN;
+  if ((st = os->res_a.ensure((size_t)L * RA * KP))) return st;
+  if ((st = os->res_b.ensure((size_t)L * RB * KP))) return st;
+  if ((st = os->mu_a.ensure((size_t)RA * sizeof(int)))) return st;
+  if ((st = os->mu_b.ensure((size_t)RB * sizeof(int)))) return st;
+  if ((st = os->rbytes.ensure((size_t)L * Nd * nb))) return st;
+  convert_grid_rows_kernel<<<(unsigned)(RA / 16), 256, 0, s>>>(
+      Nd, nb, KP, RA, A, gb, L, (int8_t*)os->res_a.ptr, (int*)os->mu_a.ptr);
+  SKG_CUDA(cudaGetLastError());
+  convert_q_cols_kernel<<<(unsigned)(RB / 16), 256, 0, s>>>(nb, KP, RB, Q, gb, L,
+                                                             (int8_t*)os->res_b.ptr,
+                                                             (int*)os->mu_b.ptr);
+  SKG_CUDA(cudaGetLastError());
+  CUtensorMap mA, mB;
+  if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, L, kI8BM))) return st;
+  if ((st = make_res_map(&mB, os->res_b.ptr, KP, RB, L, kI8BN))) return st;
+  I8Params p;
+  memset(&p, 0, sizeof(p));
+  p.sched = kSchedUnits;
+  p.L = L;
+  p.KB = (int)(KP / 128);
+  p.M = (int)Nd;
+  p.N = (int)nb;
+  p.tiles_m = (int)(RA / kI8BM);
+  p.tiles_n = (int)(RB / kI8BN);
+  p.residues = (uint8_t*)os->rbytes.ptr;
+  p.ldr = nb;
+  p.err = ws->err;
+  const int64_t units = (int64_t)p.tiles_m * L * p.tiles_n;
+  const int grid = (int)std::min<int64_t>(dev->num_sms, units);
+  if ((st = launch_i8(dev, mA, mB, p, grid, s))) return st;
+  const int64_t n = Nd * (nb / 16);
+  crt_residues_band_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      Nd, nb, L, (const uint8_t*)os->rbytes.ptr, nb, (const int*)os->mu_a.ptr,
+      (const int*)os->mu_b.ptr, D);
+  SKG_CUDA(cudaGetLastError());
+  report(opts, L, gb, nb);
+  return SKGEMM_OK;
+}
+
 int ozaki_consume_error(DeviceState*, cudaStream_t) { return SKGEMM_OK; }
+
+// Exact INT8 GEMM (public): C[M][N] int32 = A[M][K] . B[N][K]^T with K-major
+// int8 operands (row strides lda, ldb bytes). The operands are staged into
+// the padded residue layout (one "modulus") and run on the lane schedule.
+int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, const int8_t* B,
+             int64_t ldb, int32_t* C, int64_t ldc, cudaStream_t s) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  if (M < 0 || N < 0 || K < 0) return fail(SKGEMM_ERR_INVALID_ARG, "negative dimension");
+  if (lda < K || ldb < K || ldc < N) return fail(SKGEMM_ERR_INVALID_ARG, "leading dimension");
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  if (M > (1 << 20) || N > (1 << 20)) return fail(SKGEMM_ERR_INVALID_ARG, "dimension too large");
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  if ((st = ensure_consts(dev)) != SKGEMM_OK) return st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  OzakiStream* os = ozaki_stream(dev, s);
+  const int64_t KP = std::max<int64_t>(128, (K + 127) / 128 * 128);
+  const int KB = (int)(KP / 128);
+  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
+  const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
+  if ((st = os->res_a.ensure((size_t)RA * KP))) return st;
+  if ((st = os->res_b.ensure((size_t)RB * KP))) return st;
+  SKG_CUDA(cudaMemsetAsync(os->res_a.ptr, 0, (size_t)RA * KP, s));
+  SKG_CUDA(cudaMemsetAsync(os->res_b.ptr, 0, (size_t)RB * KP, s));
+  if (K > 0) {
+    SKG_CUDA(cudaMemcpy2DAsync(os->res_a.ptr, KP, A, lda, K, M, cudaMemcpyDeviceToDevice, s));
+    SKG_CUDA(cudaMemcpy2DAsync(os->res_b.ptr, KP, B, ldb, K, N, cudaMemcpyDeviceToDevice, s));
+  }
+  LanePlan* pl = nullptr;
+  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, 1, false, &pl)) != SKGEMM_OK) return st;
+  if ((st = os->partials.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t))))
+    return st;
+  CUtensorMap mA, mB;
+  if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, 1, kI8BM))) return st;
+  if ((st = make_res_map(&mB, os->res_b.ptr, KP, RB, 1, kI8BN))) return st;
+  I8Params p;
+  memset(&p, 0, sizeof(p));
+  p.sched = kSchedLanes;
+  p.L = 1;
+  p.KB = KB;
+  p.M = (int)M;
+  p.N = (int)N;
+  p.T = pl->T;
+  p.Q = pl->Q;
+  p.tiles = pl->tiles;
+  p.lane_seg_off = pl->lane_seg_off;
+  p.segs = pl->segs;
+  p.partials = (int32_t*)os->partials.ptr;
+  p.err = ws->err;
+  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s))) return st;
+  const int64_t n = M * N;
+  sum_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      (int)M, (int)N, (const int32_t*)os->partials.ptr, pl->T, pl->tile_index, pl->tiles_n,
+      pl->mod_slot_off, pl->mod_slots, C, ldc);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+int probe_i8_peak(DeviceState* dev, double* tops) {
+  uint32_t* sink = nullptr;
+  SKG_CUDA(cudaMalloc(&sink, 2 * sizeof(uint32_t)));
+  SKG_CUDA(cudaMemset(sink, 0, 2 * sizeof(uint32_t)));
+  // More shared memory than two CTAs can share: one CTA (one 512-column TMEM
+  // allocation) per SM.
+  const int smem = 160 * 1024;
+  SKG_CUDA(cudaFuncSetAttribute(i8_peak_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  cudaEvent_t e0, e1;
+  SKG_CUDA(cudaEventCreate(&e0));
+  SKG_CUDA(cudaEventCreate(&e1));
+  const int iters = 20000;
+  i8_peak_kernel<<<dev->num_sms, 128, smem>>>(iters / 10, sink);
+  SKG_CUDA(cudaEventRecord(e0));
+  i8_peak_kernel<<<dev->num_sms, 128, smem>>>(iters, sink);
+  SKG_CUDA(cudaEventRecord(e1));
+  SKG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  SKG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  uint32_t h[2] = {0, 0};
+  SKG_CUDA(cudaMemcpy(h, sink, sizeof(h), cudaMemcpyDeviceToHost));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (h[1] != 0) return fail(SKGEMM_ERR_DEVICE_TIMEOUT, "INT8 peak probe wait ran out");
+  const double ops = 2.0 * kI8BM * kI8BN * kI8BK * (double)iters * dev->num_sms;
+  *tops = ops / (ms * 1e-3) / 1e12;
+  return SKGEMM_OK;
+}
 
 }  // namespace skg

@@ -16,5 +16,8 @@ int ozaki_syrk_packed(int64_t K, int64_t M, const double* Ap, double* C, int64_t
 int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
               skgemm_options_t* opts, cudaStream_t s);
 int ozaki_consume_error(DeviceState* dev, cudaStream_t s);
+int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, const int8_t* B,
+             int64_t ldb, int32_t* C, int64_t ldc, cudaStream_t s);
+int probe_i8_peak(DeviceState* dev, double* tops);
 
 }  // namespace skg

@@ -61,6 +61,8 @@ _lib: Optional[ctypes.CDLL] = None
 _SIGS = {
     "skgemm_stream_status": [_vp],
     "skgemm_probe_fp64_peak": [ctypes.POINTER(ctypes.c_double)],
+    "skgemm_probe_i8_peak": [ctypes.POINTER(ctypes.c_double)],
+    "skgemm_igemm_s8_dev": [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp],
     "skgemm_dgemm": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d],
     "skgemm_dgemm_packed": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d],
     "skgemm_dgemm_dev": [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _d, _d, _vp],
@@ -255,6 +257,18 @@ def grid_to_band_dev(Nd, nb, src, dst, stream=None):
 def stream_status(stream=None) -> None:
     """Synchronise ``stream``; raise if a device-side wait ran out of budget."""
     _check(lib().skgemm_stream_status(_stream(stream)))
+
+
+def igemm_s8_dev(M, N, K, A, lda, B, ldb, C, ldc, stream=None):
+    """Exact int8 x int8 -> int32 GEMM, both operands K-major (device)."""
+    _check(lib().skgemm_igemm_s8_dev(M, N, K, _dptr(A), lda, _dptr(B), ldb, _dptr(C), ldc,
+                                     _stream(stream)))
+
+
+def probe_i8_peak() -> float:
+    v = ctypes.c_double(0.0)
+    _check(lib().skgemm_probe_i8_peak(ctypes.byref(v)))
+    return v.value
 
 
 def probe_fp64_peak() -> float:
