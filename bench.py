@@ -52,7 +52,23 @@ def parse():
     ap.add_argument("--precision", default="native", choices=["native", "ozaki"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--nd", type=int, default=ND,
+                    help="grid points (default 110592 = 48^3; smaller values for profiling)")
+    ap.add_argument("--nb", type=int, default=NB, help="states (default 512)")
+    a = ap.parse_args()
+    set_shape(a.nd, a.nb)
+    return a
+
+
+def set_shape(nd, nb):
+    """Workload shape (the default is the 110592 x 512 configuration)."""
+    global ND, NB, FLOP_SYRK, FLOP_GEMM, FLOP_ROT, FLOP_STEP, WORKLOAD
+    ND, NB = nd, nb
+    FLOP_SYRK = NB * (NB + 1) * ND
+    FLOP_GEMM = 2 * NB * NB * ND
+    FLOP_ROT = 2 * ND * NB * NB
+    FLOP_STEP = FLOP_SYRK + FLOP_GEMM + FLOP_ROT
+    WORKLOAD = f"dft_subspace_step_psi{ND}x{NB}"
 
 
 # ------------------------------------------------------------------ clocks

@@ -1,8 +1,8 @@
-// INT8 x INT8 -> INT32 GEMM on tcgen05 tensor cores (sm_100a), the engine of
-// the Ozaki split-precision path. Exact: every partial product of two int8
-// residues is at most 2^14 in magnitude, so a 32-bit accumulator is exact for
-// up to 2^31 / 2^14 = 131072 products, and work is split into k-segments of
-// at most `seg_kb_cap` 128-wide k-blocks.
+// 8-bit x 8-bit -> INT32 GEMM on tcgen05 tensor cores (sm_100a), the engine of
+// the Ozaki split-precision path. Exact: operands are either unsigned residues
+// (u8 x u8, products < 2^16: the Ozaki path) or signed bytes (s8 x s8,
+// products <= 2^14: the public integer GEMM); the host cuts the k range into
+// segments short enough that a 32-bit accumulator cannot overflow.
 //
 // Operands are per-modulus residue matrices, K-major bytes:
 //   A_res[l][RA][KP], B_res[l][RB][KP]   (row r, k contiguous; zero padding)
@@ -56,6 +56,7 @@ struct I8Segment {
 
 struct I8Params {
   int sched;
+  int is_signed;     // 1: s8 x s8, 0: u8 x u8
   int L;             // moduli
   int KB;            // k-blocks of the padded K (KP / 128)
   int M, N;          // output extent (bounds of stores)
@@ -73,18 +74,22 @@ struct I8Params {
   uint32_t* err;
 };
 
-// Moduli and the constants of an unsigned remainder by multiply-high:
-// for 0 <= u < 2^26, q = umulhi(u, magic) is floor(u/m) or one more.
+// Moduli and the constants of an exact remainder by multiply-high: with
+// magic = floor(2^37 / m) + 1, q = umulhi(u, magic) >> 5 equals floor(u / m)
+// for every 0 <= u < 2^29 and m <= 256 (the rounding excess u * (magic -
+// 2^37/m) / 2^37 stays below 2^-8 <= 1/m).
 struct I8ModConsts {
   uint32_t m[kI8MaxModuli];
-  uint32_t magic[kI8MaxModuli];   // ceil(2^32 / m)
-  uint32_t offset[kI8MaxModuli];  // multiple of m >= 2^25 (makes |acc| < 2^25 positive)
+  uint32_t magic[kI8MaxModuli];
 };
 
-__device__ __forceinline__ uint32_t i8_mod_u(uint32_t u, uint32_t m, uint32_t magic) {
-  uint32_t q = __umulhi(u, magic);
-  int32_t r = (int32_t)(u - q * m);
-  return (uint32_t)(r < 0 ? r + (int32_t)m : r);
+// Moduli of the residue epilogue (constant memory: indexed by the work item's
+// modulus, uniform across the warp).
+__constant__ I8ModConsts c_i8mod;
+
+__device__ __forceinline__ uint32_t mod_exact29(uint32_t u, uint32_t m, uint32_t magic) {
+  const uint32_t q = __umulhi(u, magic) >> 5;
+  return u - q * m;
 }
 
 // Work item seen by all roles.
@@ -128,8 +133,7 @@ __device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cu
 
 __global__ void __launch_bounds__(kI8Threads, 1)
     i8_gemm_kernel(const __grid_constant__ CUtensorMap mapA,
-                   const __grid_constant__ CUtensorMap mapB, const I8Params p,
-                   const I8ModConsts mc) {
+                   const __grid_constant__ CUtensorMap mapB, const I8Params p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
@@ -216,7 +220,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
   } else if (warp == 1) {
     // --------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN);
+      const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN, p.is_signed);
       const uint32_t smem_base = smem_u32(smem);
       int stage = 0;
       uint32_t phase = 0;
@@ -288,7 +292,8 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             d4[j] = make_int4((int)v[4 * j], (int)v[4 * j + 1], (int)v[4 * j + 2], (int)v[4 * j + 3]);
         }
       } else {
-        const uint32_t m = mc.m[it.l], magic = mc.magic[it.l], off = mc.offset[it.l];
+        // u8 x u8 accumulators are non-negative and below 2^29 (K <= 2048).
+        const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic[it.l];
         const bool row_ok = row < p.M;
         uint8_t* dst = p.residues + ((int64_t)it.l * p.M + row) * p.ldr;
 #pragma unroll 1
@@ -301,11 +306,11 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             uint32_t w[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-              uint32_t b0 = i8_mod_u(v[4 * j] + off, m, magic);
-              uint32_t b1 = i8_mod_u(v[4 * j + 1] + off, m, magic);
-              uint32_t b2 = i8_mod_u(v[4 * j + 2] + off, m, magic);
-              uint32_t b3 = i8_mod_u(v[4 * j + 3] + off, m, magic);
-              w[j] = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
+              const uint32_t b0 = mod_exact29(v[4 * j], m, magic);
+              const uint32_t b1 = mod_exact29(v[4 * j + 1], m, magic);
+              const uint32_t b2 = mod_exact29(v[4 * j + 2], m, magic);
+              const uint32_t b3 = mod_exact29(v[4 * j + 3], m, magic);
+              w[j] = __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
             }
             if (col0 + 32 <= p.N) {
               uint4* d4 = reinterpret_cast<uint4*>(dst + col0);
@@ -359,7 +364,7 @@ __global__ void __launch_bounds__(128, 1) i8_peak_kernel(int iters, uint32_t* si
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
   if (threadIdx.x == 0) {
-    const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN);
+    const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN, 1);
     const uint32_t sa = smem_u32(smem);
     const uint64_t adesc = umma_desc_kmajor_sw128(sa);
     const uint64_t bdesc = umma_desc_kmajor_sw128(sa + kI8TileABytes);

@@ -41,14 +41,27 @@ namespace {
 constexpr uint32_t kModuli[kI8MaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
                                             229, 227, 223, 217, 211, 199, 197, 193};
 constexpr int kMinModuli = 6;
-constexpr int kSegKbCap = 1023;  // 1023*128 products of |x| <= 2^14 stay below 2^31
+// k-blocks (128 k) per INT32-exact segment: s8 x s8 products are <= 2^14,
+// u8 x u8 residue products < 2^16.
+constexpr int kSegKbCapSigned = 1023;   // 1023 * 128 * 2^14 < 2^31
+constexpr int kSegKbCapUnsigned = 256;  // 256 * 128 * 255^2 < 2^31
 
+// Residue constants for one moduli count L (gamma, and with it the digit
+// split of the scaled integers, depends on L). The scaled integer X
+// (|X| <= 2^gamma + 1/2) is handled as u = X + bias >= 0, bias = 2^(gamma+1),
+// split into digits d_j of W bits: X = sum_j d_j 2^(W j) - bias, so
+// X mod m = (d_0 + e + sum_{j>0} d_j c_j) mod m with c_j = 2^(W j) mod m and
+// e = (-bias) mod m.
 struct ResidueConsts {
+  int ndig;         // 3 digits of 19 bits (gamma <= 55) or 4 of 16 bits
+  int gamma_bits;
+  long long bias;
   uint32_t m[kI8MaxModuli];
-  uint32_t magic[kI8MaxModuli];
-  uint32_t c1[kI8MaxModuli];  // 2^18 mod m
-  uint32_t c2[kI8MaxModuli];  // 2^36 mod m
-  uint32_t c3[kI8MaxModuli];  // 2^54 mod m
+  uint32_t magic[kI8MaxModuli];  // floor(2^37 / m) + 1: exact remainder below 2^29
+  uint32_t c1[kI8MaxModuli];
+  uint32_t c2[kI8MaxModuli];
+  uint32_t c3[kI8MaxModuli];
+  uint32_t e[kI8MaxModuli];
 };
 
 struct CrtConsts {  // for one moduli count L
@@ -57,7 +70,7 @@ struct CrtConsts {  // for one moduli count L
   double mh, ml, inv_m;
 };
 
-__constant__ ResidueConsts c_res;
+__constant__ ResidueConsts c_res[kI8MaxModuli + 1];
 __constant__ CrtConsts c_crt[kI8MaxModuli + 1];
 
 typedef unsigned __int128 u128;
@@ -122,28 +135,85 @@ __device__ __forceinline__ int row_exponent(double sumsq, int gamma_bits) {
   return gamma_bits - ceil_log2_pos(sqrt(sumsq));
 }
 
-// Symmetric residues of the integer X modulo the first L moduli, as int8
-// bit patterns, for 8 consecutive elements packed into one uint64 per modulus.
-__device__ __forceinline__ uint32_t residue_u(uint64_t u, int l) {
-  const uint32_t d0 = (uint32_t)(u & 0x3FFFFu);
-  const uint32_t d1 = (uint32_t)((u >> 18) & 0x3FFFFu);
-  const uint32_t d2 = (uint32_t)((u >> 36) & 0x3FFFFu);
-  const uint32_t d3 = (uint32_t)(u >> 54);
-  const uint32_t S = d3 * c_res.c3[l] + d2 * c_res.c2[l] + d1 * c_res.c1[l] + d0;  // < 2^27
-  return i8_mod_u(S, c_res.m[l], c_res.magic[l]);
+// s1 * s2 = 2^mu exactly, each factor a normal double for |mu| < 2044.
+__device__ __forceinline__ void pow2_pair(int mu, double& s1, double& s2) {
+  const int h = mu / 2;
+  s1 = ldexp(1.0, h);
+  s2 = ldexp(1.0, mu - h);
 }
 
-__device__ __forceinline__ uint32_t sym_byte(int64_t X, int l) {
-  const uint64_t u = (uint64_t)(X < 0 ? -X : X);
-  const uint32_t m = c_res.m[l];
-  uint32_t r = residue_u(u, l);
-  if (X < 0 && r) r = m - r;
-  const int rs = (int)r > (int)((m - 1) / 2) ? (int)r - (int)m : (int)r;
-  return (uint32_t)(uint8_t)(int8_t)rs;
+// Shared-memory staging of a [128 k][16 rows] block as tileT[r][k'] with row
+// pitch 129 doubles and k' = k ^ ((k >> 3) & 7): the transposing stores
+// (consecutive r) and the reads of 8 consecutive k per thread (consecutive
+// threads 8 k apart) are at most 2-way bank-conflicted.
+constexpr int kTilePitch = 129;
+__device__ __forceinline__ int swz_k(int k) { return k ^ ((k >> 3) & 7); }
+
+// Digits of the biased scaled integer u = X + bias (X = rint(v 2^mu)):
+// NDIG = 3 digits of 19 bits (u < 2^57, gamma <= 55) or 4 of 16 bits.
+template <int NDIG>
+__device__ __forceinline__ void to_digits(double v, double s1, double s2, long long bias,
+                                          uint32_t (&d)[4]) {
+  const long long X = __double2ll_rn((v * s1) * s2);
+  const unsigned long long u = (unsigned long long)(X + bias);
+  const uint32_t lo = (uint32_t)u, hi = (uint32_t)(u >> 32);
+  if (NDIG == 3) {
+    d[0] = lo & 0x7FFFFu;
+    d[1] = __funnelshift_r(lo, hi, 19) & 0x7FFFFu;
+    d[2] = hi >> 6;
+    d[3] = 0;
+  } else {
+    d[0] = lo & 0xFFFFu;
+    d[1] = lo >> 16;
+    d[2] = hi & 0xFFFFu;
+    d[3] = hi >> 16;
+  }
 }
 
-__device__ __forceinline__ int64_t scaled_int(double v, int mu) {
-  return llrint(ldexp(v, mu));
+__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
+}
+
+// Residues of the staged block: thread (r, kk) handles k = 8kk .. 8kk+7 of
+// row r; per modulus, X mod m = (d_0 + e + d_1 c_1 + d_2 c_2 [+ d_3 c_3]) mod m
+// (digit sum < 2^29, exact remainder by multiply-high), packed into one
+// 8-byte word; 16 consecutive threads write one 128-byte row segment.
+template <int NDIG>
+__device__ __forceinline__ void emit_residues(const double* tileT, const double* s1,
+                                              const double* s2, int L, const ResidueConsts& rc,
+                                              uint8_t* res, int64_t row0, int64_t KP,
+                                              int64_t Rpad, int64_t k0) {
+  const int kk = threadIdx.x & 15, r = threadIdx.x >> 4;  // 256 threads: 16 rows x 16
+  uint32_t d[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    to_digits<NDIG>(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r], rc.bias, d[j]);
+  uint8_t* dst = res + (row0 + r) * KP + k0 + 8 * kk;
+  for (int l = 0; l < L; ++l) {
+    const uint32_t m = rc.m[l], magic = rc.magic[l], e = rc.e[l];
+    const uint32_t c1 = rc.c1[l], c2 = rc.c2[l], c3 = rc.c3[l];
+    uint32_t b[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      uint32_t S = d[j][0] + e + d[j][1] * c1 + d[j][2] * c2;
+      if (NDIG == 4) S += d[j][3] * c3;
+      b[j] = mod_exact29(S, m, magic);
+    }
+    *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) =
+        make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
+  }
+}
+
+// Loads element (k, r) = src[k * ks + r] of the block (zero outside
+// k < K, r < rows_valid) into the staging tile.
+template <int T>
+__device__ __forceinline__ void stage_tile(double* tileT, const double* src, int64_t ks,
+                                           int64_t k0, int64_t K, int rows_valid) {
+  for (int i = threadIdx.x; i < 128 * T; i += blockDim.x) {
+    const int kk = i / T, r = i % T;
+    const int64_t k = k0 + kk;
+    tileT[r * kTilePitch + swz_k(kk)] = (k < K && r < rows_valid) ? src[k * ks + r] : 0.0;
+  }
 }
 
 // ------------------------------------------------- packed-T operand prep
@@ -175,15 +245,17 @@ __global__ void __launch_bounds__(256) norm_partials_kernel(int64_t R, int64_t K
 }
 
 // Residues of a packed-T operand -> res[l][Rpad][KP] (K-major bytes).
-// CTA (p, kb): rows p*T .. +T, k-block kb (128 k). mu of each row from the
-// norm partials; CTAs with kb == 0 also publish mu.
-template <int T>
+// CTA (p, kb): rows p*T .. +T, k-block kb (128 k), converted in 16-row
+// sub-panels. mu of each row from the norm partials; CTAs with kb == 0 also
+// publish mu.
+template <int T, int NDIG>
 __global__ void __launch_bounds__(256) convert_packed_kernel(
     int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ X, int C,
-    const double* __restrict__ part, int gamma_bits, int L, int8_t* __restrict__ res,
+    const double* __restrict__ part, int L, uint8_t* __restrict__ res,
     int* __restrict__ mu_out) {
-  __shared__ double tile[128 * T];
-  __shared__ int mu[T];
+  __shared__ double tileT[16 * kTilePitch];
+  __shared__ double s1[T], s2[T];
+  const ResidueConsts& rc = c_res[L];
   const int p = blockIdx.x, kb = blockIdx.y;
   const int64_t P_in = (R + T - 1) / T;
   const int64_t k0 = (int64_t)kb * 128;
@@ -191,126 +263,64 @@ __global__ void __launch_bounds__(256) convert_packed_kernel(
     const int64_t row = (int64_t)p * T + threadIdx.x;
     int m = 0;
     if (p < P_in && row < R) {
-      double s = 0.0;
-      for (int c = 0; c < C; ++c) s += part[((int64_t)p * C + c) * T + threadIdx.x];
-      m = row_exponent(s, gamma_bits);
+      double sq = 0.0;
+      for (int c = 0; c < C; ++c) sq += part[((int64_t)p * C + c) * T + threadIdx.x];
+      m = row_exponent(sq, rc.gamma_bits);
     }
-    mu[threadIdx.x] = m;
+    pow2_pair(m, s1[threadIdx.x], s2[threadIdx.x]);
     if (kb == 0 && row < Rpad) mu_out[row] = m;
   }
+  const int64_t rem = R - (int64_t)p * T;
+  const int rows_valid = p < P_in ? (int)(rem < T ? rem : T) : 0;
   const double* src = X + (int64_t)p * K * T;
-  for (int i = threadIdx.x; i < 128 * T; i += 256) {
-    const int kk = i / T, r = i % T;
-    const int64_t k = k0 + kk, row = (int64_t)p * T + r;
-    tile[i] = (p < P_in && k < K && row < R) ? src[k * T + r] : 0.0;
-  }
-  __syncthreads();
-  for (int item = threadIdx.x; item < 16 * T; item += 256) {
-    const int r = item % T, kk = item / T;  // 8 consecutive k: 8*kk .. 8*kk+7
-    int64_t xi[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) xi[j] = scaled_int(tile[(8 * kk + j) * T + r], mu[r]);
-    const int64_t row = (int64_t)p * T + r;
-    int8_t* dst = res + row * KP + k0 + 8 * kk;
-    for (int l = 0; l < L; ++l) {
-      uint32_t lo = 0, hi = 0;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) lo |= sym_byte(xi[j], l) << (8 * j);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) hi |= sym_byte(xi[4 + j], l) << (8 * j);
-      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) = make_uint2(lo, hi);
-    }
+#pragma unroll 1
+  for (int sp = 0; sp < T / 16; ++sp) {
+    __syncthreads();
+    stage_tile<16>(tileT, src + sp * 16, T, k0, K, rows_valid - sp * 16);
+    __syncthreads();
+    emit_residues<NDIG>(tileT, s1 + sp * 16, s2 + sp * 16, L, rc, res, (int64_t)p * T + sp * 16,
+                        KP, Rpad, k0);
   }
 }
 
-// Rotation A: grid-packed Psi [Nd/16][nb][16]; rows are grid points g (scaled
-// over the nb bands), k = band. One CTA per 16-row panel.
-__global__ void __launch_bounds__(256) convert_grid_rows_kernel(
-    int64_t Nd, int64_t nb, int64_t KP, int64_t Rpad, const double* __restrict__ A,
-    int gamma_bits, int L, int8_t* __restrict__ res, int* __restrict__ mu_out) {
+// Residues of 16-row panels whose rows are scaled over their full (short)
+// k range, one CTA per panel: element (k, r) of panel p at
+// src[p * panel_stride + k * ks + r]. Used for the rotation's A (grid-packed
+// Psi, rows = grid points, k = bands: panel_stride nb*16, ks 16) and B
+// (Q row-major, rows = columns of Q, k = rows of Q: panel_stride 16, ks nb).
+template <int NDIG>
+__global__ void __launch_bounds__(256) convert_local_kernel(
+    int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ src,
+    int64_t panel_stride, int64_t ks, int L, uint8_t* __restrict__ res, int* __restrict__ mu_out) {
+  __shared__ double tileT[16 * kTilePitch];
   __shared__ double red[256];
-  __shared__ int mu[16];
+  __shared__ double s1[16], s2[16];
+  const ResidueConsts& rc = c_res[L];
   const int64_t p = blockIdx.x;
+  const int64_t rem = R - p * 16;
+  const int rows_valid = rem <= 0 ? 0 : (int)(rem < 16 ? rem : 16);
+  const double* base = src + p * panel_stride;
   const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
-  const bool live = p * 16 < Nd;
-  const double* src = A + p * nb * 16;
   double acc = 0.0;
-  if (live)
-    for (int64_t b = kl; b < nb; b += 16) {
-      const double v = src[b * 16 + r];
+  if (r < rows_valid)
+    for (int64_t k = kl; k < K; k += 16) {
+      const double v = base[k * ks + r];
       acc = fma(v, v, acc);
     }
   red[threadIdx.x] = acc;
   __syncthreads();
   if (threadIdx.x < 16) {
-    double s = 0.0;
-    for (int j = 0; j < 16; ++j) s += red[j * 16 + threadIdx.x];
-    const int m = live ? row_exponent(s, gamma_bits) : 0;
-    mu[threadIdx.x] = m;
+    double sq = 0.0;
+    for (int j = 0; j < 16; ++j) sq += red[j * 16 + threadIdx.x];
+    const int m = threadIdx.x < rows_valid ? row_exponent(sq, rc.gamma_bits) : 0;
+    pow2_pair(m, s1[threadIdx.x], s2[threadIdx.x]);
     if (p * 16 + threadIdx.x < Rpad) mu_out[p * 16 + threadIdx.x] = m;
   }
-  __syncthreads();
-  const int64_t row = p * 16 + r;
-  for (int64_t kb0 = 0; kb0 < KP; kb0 += 128) {
-    const int64_t k = kb0 + 8 * kl;
-    int64_t xi[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-      xi[j] = (live && k + j < nb) ? scaled_int(src[(k + j) * 16 + r], mu[r]) : 0;
-    int8_t* dst = res + row * KP + k;
-    for (int l = 0; l < L; ++l) {
-      uint32_t lo = 0, hi = 0;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) lo |= sym_byte(xi[j], l) << (8 * j);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) hi |= sym_byte(xi[4 + j], l) << (8 * j);
-      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) = make_uint2(lo, hi);
-    }
-  }
-}
-
-// Rotation B: Q row-major nb x nb; B(k = b, n = j) = Q[b*nb + j]; rows of the
-// residue matrix are the columns j of Q (scaled over b), k = b.
-__global__ void __launch_bounds__(256) convert_q_cols_kernel(
-    int64_t nb, int64_t KP, int64_t Rpad, const double* __restrict__ Q, int gamma_bits, int L,
-    int8_t* __restrict__ res, int* __restrict__ nu_out) {
-  __shared__ double red[256];
-  __shared__ int nu[16];
-  const int64_t p = blockIdx.x;  // 16 columns
-  const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
-  const int64_t j = p * 16 + r;
-  const bool live = j < nb;
-  double acc = 0.0;
-  if (live)
-    for (int64_t b = kl; b < nb; b += 16) {
-      const double v = Q[b * nb + j];
-      acc = fma(v, v, acc);
-    }
-  red[threadIdx.x] = acc;
-  __syncthreads();
-  if (threadIdx.x < 16) {
-    double s = 0.0;
-    for (int i = 0; i < 16; ++i) s += red[i * 16 + threadIdx.x];
-    const int m = (p * 16 + threadIdx.x < nb) ? row_exponent(s, gamma_bits) : 0;
-    nu[threadIdx.x] = m;
-    if (p * 16 + threadIdx.x < Rpad) nu_out[p * 16 + threadIdx.x] = m;
-  }
-  __syncthreads();
-  for (int64_t kb0 = 0; kb0 < KP; kb0 += 128) {
-    const int64_t k = kb0 + 8 * kl;
-    int64_t xi[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      xi[t] = (live && k + t < nb) ? scaled_int(Q[(k + t) * nb + j], nu[r]) : 0;
-    int8_t* dst = res + j * KP + k;
-    for (int l = 0; l < L; ++l) {
-      uint32_t lo = 0, hi = 0;
-#pragma unroll
-      for (int t = 0; t < 4; ++t) lo |= sym_byte(xi[t], l) << (8 * t);
-#pragma unroll
-      for (int t = 0; t < 4; ++t) hi |= sym_byte(xi[4 + t], l) << (8 * t);
-      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) = make_uint2(lo, hi);
-    }
+  for (int64_t k0 = 0; k0 < KP; k0 += 128) {
+    __syncthreads();
+    stage_tile<16>(tileT, base, ks, k0, K, rows_valid);
+    __syncthreads();
+    emit_residues<NDIG>(tileT, s1, s2, L, rc, res, p * 16, KP, Rpad, k0);
   }
 }
 
@@ -353,7 +363,7 @@ __global__ void __launch_bounds__(256) crt_partials_kernel(
       int64_t s = 0;
       for (int q = mod_slot_off[l]; q < mod_slot_off[l + 1]; ++q)
         s += partials[((int64_t)mod_slots[q] * T + t) * (kI8BM * kI8BN) + off];
-      const int64_t m = c_res.m[l];
+      const int64_t m = c_res[L].m[l];
       int64_t rr = s % m;
       if (rr < 0) rr += m;
       r[l] = (uint32_t)rr;
@@ -369,31 +379,39 @@ __global__ void __launch_bounds__(256) crt_partials_kernel(
 }
 
 // Rotation: Psi'(g, b) band-packed from the residue bytes res[l][g][ldr].
-__global__ void __launch_bounds__(256) crt_residues_band_kernel(
+// Thread (g, c): the 16 states of chunk c at grid point g; per modulus one
+// 16-byte load, bytes widened to doubles exactly (2^52 + r - 2^52).
+__global__ void __launch_bounds__(128) crt_residues_band_kernel(
     int64_t Nd, int64_t nb, int L, const uint8_t* __restrict__ res, int64_t ldr,
     const int* __restrict__ mu, const int* __restrict__ nu, double* __restrict__ Dband) {
   const int64_t chunks = nb / 16;
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= Nd * chunks) return;
   const int64_t g = idx / chunks, c = idx % chunks;
-  uint32_t w[kI8MaxModuli][4];  // 16 residue bytes per modulus
+  const CrtConsts& cc = c_crt[L];
+  double sh[16], sl[16];
 #pragma unroll
-  for (int l = 0; l < kI8MaxModuli; ++l) {
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (l < L) v = *reinterpret_cast<const uint4*>(res + ((int64_t)l * Nd + g) * ldr + c * 16);
-    w[l][0] = v.x;
-    w[l][1] = v.y;
-    w[l][2] = v.z;
-    w[l][3] = v.w;
+  for (int t = 0; t < 16; ++t) sh[t] = sl[t] = 0.0;
+  for (int l = 0; l < L; ++l) {
+    const uint4 v = *reinterpret_cast<const uint4*>(res + ((int64_t)l * Nd + g) * ldr + c * 16);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    const double wh = cc.wh[l], wl = cc.wl[l];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const double d =
+          __hiloint2double(0x43300000, (int)((w[t >> 2] >> (8 * (t & 3))) & 0xFFu)) -
+          4503599627370496.0;
+      sh[t] = fma(d, wh, sh[t]);
+      sl[t] = fma(d, wl, sl[t]);
+    }
   }
+  const double sg = ldexp(1.0, -mu[g]);
   double out[16];
-  const int mg = mu[g];
 #pragma unroll
   for (int t = 0; t < 16; ++t) {
-    uint32_t rr[kI8MaxModuli];
-#pragma unroll
-    for (int l = 0; l < kI8MaxModuli; ++l) rr[l] = (w[l][t >> 2] >> (8 * (t & 3))) & 0xFFu;
-    out[t] = ldexp(crt_value(rr, L), -(mg + nu[c * 16 + t]));
+    const double q = rint((sh[t] + sl[t]) * cc.inv_m);
+    const double v = fma(-q, cc.mh, sh[t]) + fma(-q, cc.ml, sl[t]);
+    out[t] = (v * sg) * ldexp(1.0, -nu[c * 16 + t]);
   }
   double2* dst = reinterpret_cast<double2*>(Dband + (c * Nd + g) * 16);
 #pragma unroll
@@ -443,26 +461,44 @@ OzakiDevice g_oz[64];
 I8ModConsts g_modc;
 bool g_modc_ready = false;
 
+int g_ndig[kI8MaxModuli + 1];
+
 int ensure_consts(DeviceState* dev) {
   OzakiDevice& od = g_oz[dev->device];
   if (od.consts_ready) return SKGEMM_OK;
-  ResidueConsts rc;
+  ResidueConsts rc[kI8MaxModuli + 1];
+  memset(rc, 0, sizeof(rc));
+  for (int L = kMinModuli; L <= kI8MaxModuli; ++L) {
+    const int gam = gamma_for(L);
+    const int ndig = (gam + 2 <= 57) ? 3 : 4;
+    const int W = ndig == 3 ? 19 : 16;
+    const long long bias = 1LL << (gam + 1);
+    rc[L].ndig = ndig;
+    rc[L].gamma_bits = gam;
+    rc[L].bias = bias;
+    g_ndig[L] = ndig;
+    for (int l = 0; l < kI8MaxModuli; ++l) {
+      const uint64_t m = kModuli[l];
+      rc[L].m[l] = (uint32_t)m;
+      rc[L].magic[l] = (uint32_t)((1ull << 37) / m + 1);
+      uint64_t p1 = 1;
+      for (int i = 0; i < W; ++i) p1 = (p1 * 2) % m;
+      rc[L].c1[l] = (uint32_t)p1;
+      rc[L].c2[l] = (uint32_t)(p1 * p1 % m);
+      rc[L].c3[l] = (uint32_t)(p1 * p1 % m * p1 % m);
+      rc[L].e[l] = (uint32_t)((m - (uint64_t)bias % m) % m);
+    }
+  }
   for (int l = 0; l < kI8MaxModuli; ++l) {
-    const uint32_t m = kModuli[l];
-    rc.m[l] = m;
-    rc.magic[l] = (uint32_t)(((1ull << 32) + m - 1) / m);
-    rc.c1[l] = (uint32_t)((1ull << 18) % m);
-    rc.c2[l] = (uint32_t)((1ull << 36) % m);
-    rc.c3[l] = (uint32_t)((1ull << 54) % m);
-    g_modc.m[l] = m;
-    g_modc.magic[l] = rc.magic[l];
-    g_modc.offset[l] = (uint32_t)((((1u << 25) + m - 1) / m) * m);
+    g_modc.m[l] = kModuli[l];
+    g_modc.magic[l] = (uint32_t)((1ull << 37) / kModuli[l] + 1);
   }
   g_modc_ready = true;
+  SKG_CUDA(cudaMemcpyToSymbol(c_i8mod, &g_modc, sizeof(g_modc)));
   CrtConsts cc[kI8MaxModuli + 1];
   memset(cc, 0, sizeof(cc));
   for (int L = kMinModuli; L <= kI8MaxModuli; ++L) cc[L] = make_crt(L, nullptr);
-  SKG_CUDA(cudaMemcpyToSymbol(c_res, &rc, sizeof(rc)));
+  SKG_CUDA(cudaMemcpyToSymbol(c_res, rc, sizeof(rc)));
   SKG_CUDA(cudaMemcpyToSymbol(c_crt, cc, sizeof(cc)));
   od.consts_ready = true;
   return SKGEMM_OK;
@@ -476,10 +512,11 @@ OzakiStream* ozaki_stream(DeviceState* dev, cudaStream_t s) {
 
 // Lane schedule: T tiles x Q lanes, each lane a contiguous range of the
 // (modulus, k-block) space, cut into segments at modulus boundaries and at
-// kSegKbCap k-blocks.
-int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, LanePlan** out) {
+// seg_cap k-blocks (INT32 exactness).
+int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int seg_cap,
+                  LanePlan** out) {
   OzakiDevice& od = g_oz[dev->device];
-  auto key = std::make_tuple(M, N, KB, L, syrk ? 1 : 0);
+  auto key = std::make_tuple(M, N, KB, L * 4096 + seg_cap, syrk ? 1 : 0);
   auto itp = od.plans.find(key);
   if (itp != od.plans.end()) {
     *out = itp->second;
@@ -512,7 +549,7 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, Lane
       const int l = (int)(it / KB);
       const int kb = (int)(it % KB);
       int64_t stop = std::min<int64_t>(end, (int64_t)(l + 1) * KB);
-      stop = std::min<int64_t>(stop, it + kSegKbCap);
+      stop = std::min<int64_t>(stop, it + seg_cap);
       I8Segment s;
       s.l = l;
       s.kb0 = kb;
@@ -578,7 +615,7 @@ int launch_i8(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB, co
                                   kI8SmemBytes));
     attr_done[dev->device] = true;
   }
-  i8_gemm_kernel<<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, p, g_modc);
+  i8_gemm_kernel<<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, p);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
@@ -610,8 +647,7 @@ void report(skgemm_options_t* opts, int L, int gamma_bits, int64_t K) {
 // Residues of a packed-T operand into res[L][Rpad][KP] + row exponents.
 template <int T>
 int prep_packed(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, int L,
-                int gamma_bits, OzakiStream* os, DeviceBuffer& res, DeviceBuffer& part,
-                DeviceBuffer& mu, cudaStream_t s) {
+                DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu, cudaStream_t s) {
   const int64_t P_in = (R + T - 1) / T;
   const int C = (int)std::max<int64_t>(1, std::min<int64_t>(64, (600 + P_in - 1) / P_in));
   int st;
@@ -621,9 +657,24 @@ int prep_packed(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X,
   norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
                                                                   (double*)part.ptr);
   SKG_CUDA(cudaGetLastError());
-  convert_packed_kernel<T><<<dim3((unsigned)(Rpad / T), (unsigned)(KP / 128)), 256, 0, s>>>(
-      R, K, KP, Rpad, X, C, (const double*)part.ptr, gamma_bits, L, (int8_t*)res.ptr,
-      (int*)mu.ptr);
+  const dim3 grid((unsigned)(Rpad / T), (unsigned)(KP / 128));
+  if (g_ndig[L] == 3)
+    convert_packed_kernel<T, 3><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, (const double*)part.ptr,
+                                                     L, (uint8_t*)res.ptr, (int*)mu.ptr);
+  else
+    convert_packed_kernel<T, 4><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, (const double*)part.ptr,
+                                                     L, (uint8_t*)res.ptr, (int*)mu.ptr);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* src,
+                 int64_t panel_stride, int64_t ks, int L, uint8_t* res, int* mu, cudaStream_t s) {
+  const unsigned grid = (unsigned)(Rpad / 16);
+  if (g_ndig[L] == 3)
+    convert_local_kernel<3><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
+  else
+    convert_local_kernel<4><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
@@ -652,18 +703,20 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
   const int KB = (int)(KP / 128);
   const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;  // 256-multiples serve both box heights
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
-  if ((st = prep_packed<16>(M, K, KP, RA, Ap, L, gb, os, os->res_a, os->part_a, os->mu_a, s)))
+  if ((st = prep_packed<16>(M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, s)))
     return st;
   const DeviceBuffer* resB = &os->res_a;
   const DeviceBuffer* muB = &os->mu_a;
   if (!syrk) {
-    if ((st = prep_packed<32>(N, K, KP, RB, Bp, L, gb, os, os->res_b, os->part_b, os->mu_b, s)))
+    if ((st = prep_packed<32>(N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b, s)))
       return st;
     resB = &os->res_b;
     muB = &os->mu_b;
   }
   LanePlan* pl = nullptr;
-  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, &pl)) != SKGEMM_OK) return st;
+  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, kSegKbCapUnsigned, &pl)) !=
+      SKGEMM_OK)
+    return st;
   if ((st = os->partials.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t))))
     return st;
   CUtensorMap mA, mB;
@@ -672,6 +725,7 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedLanes;
+  p.is_signed = 0;
   p.L = L;
   p.KB = KB;
   p.M = (int)M;
@@ -731,19 +785,19 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   if ((st = os->mu_a.ensure((size_t)RA * sizeof(int)))) return st;
   if ((st = os->mu_b.ensure((size_t)RB * sizeof(int)))) return st;
   if ((st = os->rbytes.ensure((size_t)L * Nd * nb))) return st;
-  convert_grid_rows_kernel<<<(unsigned)(RA / 16), 256, 0, s>>>(
-      Nd, nb, KP, RA, A, gb, L, (int8_t*)os->res_a.ptr, (int*)os->mu_a.ptr);
-  SKG_CUDA(cudaGetLastError());
-  convert_q_cols_kernel<<<(unsigned)(RB / 16), 256, 0, s>>>(nb, KP, RB, Q, gb, L,
-                                                             (int8_t*)os->res_b.ptr,
-                                                             (int*)os->mu_b.ptr);
-  SKG_CUDA(cudaGetLastError());
+  if ((st = launch_local(Nd, nb, KP, RA, A, nb * 16, 16, L, (uint8_t*)os->res_a.ptr,
+                         (int*)os->mu_a.ptr, s)))
+    return st;
+  if ((st = launch_local(nb, nb, KP, RB, Q, 16, nb, L, (uint8_t*)os->res_b.ptr,
+                         (int*)os->mu_b.ptr, s)))
+    return st;
   CUtensorMap mA, mB;
   if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, L, kI8BM))) return st;
   if ((st = make_res_map(&mB, os->res_b.ptr, KP, RB, L, kI8BN))) return st;
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedUnits;
+  p.is_signed = 0;
   p.L = L;
   p.KB = (int)(KP / 128);
   p.M = (int)Nd;
@@ -757,7 +811,7 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   const int grid = (int)std::min<int64_t>(dev->num_sms, units);
   if ((st = launch_i8(dev, mA, mB, p, grid, s))) return st;
   const int64_t n = Nd * (nb / 16);
-  crt_residues_band_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+  crt_residues_band_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(
       Nd, nb, L, (const uint8_t*)os->rbytes.ptr, nb, (const int*)os->mu_a.ptr,
       (const int*)os->mu_b.ptr, D);
   SKG_CUDA(cudaGetLastError());
@@ -797,7 +851,9 @@ int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, cons
     SKG_CUDA(cudaMemcpy2DAsync(os->res_b.ptr, KP, B, ldb, K, N, cudaMemcpyDeviceToDevice, s));
   }
   LanePlan* pl = nullptr;
-  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, 1, false, &pl)) != SKGEMM_OK) return st;
+  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, 1, false, kSegKbCapSigned, &pl)) !=
+      SKGEMM_OK)
+    return st;
   if ((st = os->partials.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t))))
     return st;
   CUtensorMap mA, mB;
@@ -806,6 +862,7 @@ int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, cons
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedLanes;
+  p.is_signed = 1;
   p.L = 1;
   p.KB = KB;
   p.M = (int)M;

@@ -8,7 +8,7 @@
 //   (1 on sm_100) in [46,48), base offset in [49,52), LBO mode in [52],
 //   layout type in [61,64) (2 = 128-byte swizzle);
 //   instruction descriptor (32 bit) for kind::i8: D format in [4,6) (2 = s32),
-//   A / B format in [7,10) / [10,13) (1 = signed 8-bit), A / B major in
+//   A / B format in [7,10) / [10,13) (0 = unsigned, 1 = signed 8-bit), A / B major in
 //   [15] / [16] (0 = K-major), N >> 3 in [17,23), M >> 4 in [24,29).
 #pragma once
 
@@ -32,12 +32,13 @@ __device__ __forceinline__ uint64_t umma_desc_kmajor_sw128(uint32_t smem_addr) {
   return d;
 }
 
-__host__ __device__ constexpr uint32_t umma_idesc_i8(int M, int N) {
-  return (2u << 4)                     // D: s32
-         | (1u << 7)                   // A: signed 8-bit
-         | (1u << 10)                  // B: signed 8-bit
-         | ((uint32_t)(N >> 3) << 17)  // N
-         | ((uint32_t)(M >> 4) << 24); // M
+// kind::i8 instruction descriptor; is_signed selects s8 x s8 (1) or u8 x u8 (0).
+__host__ __device__ constexpr uint32_t umma_idesc_i8(int M, int N, int is_signed) {
+  return (2u << 4)                        // D: s32
+         | ((uint32_t)(is_signed & 1) << 7)   // A: 1 = signed, 0 = unsigned 8-bit
+         | ((uint32_t)(is_signed & 1) << 10)  // B: same
+         | ((uint32_t)(N >> 3) << 17)     // N
+         | ((uint32_t)(M >> 4) << 24);    // M
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, uint32_t ncols) {
