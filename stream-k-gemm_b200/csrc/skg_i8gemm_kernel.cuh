@@ -1,8 +1,9 @@
 // 8-bit x 8-bit -> INT32 GEMM on tcgen05 tensor cores (sm_100a), the engine of
-// the Ozaki split-precision path. Exact: operands are either unsigned residues
-// (u8 x u8, products < 2^16: the Ozaki path) or signed bytes (s8 x s8,
-// products <= 2^14: the public integer GEMM); the host cuts the k range into
-// segments short enough that a 32-bit accumulator cannot overflow.
+// the Ozaki split-precision path. Exact: operands are signed bytes (s8 x s8,
+// products <= 2^14: symmetric residues and the public integer GEMM; an
+// unsigned u8 x u8 mode exists for callers with byte data); the host cuts the
+// k range into segments short enough that a 32-bit accumulator cannot
+// overflow.
 //
 // Operands are per-modulus residue matrices, K-major bytes:
 //   A_res[l][RA][KP], B_res[l][RB][KP]   (row r, k contiguous; zero padding)
@@ -77,10 +78,13 @@ struct I8Params {
 // Moduli and the constants of an exact remainder by multiply-high: with
 // magic = floor(2^37 / m) + 1, q = umulhi(u, magic) >> 5 equals floor(u / m)
 // for every 0 <= u < 2^29 and m <= 256 (the rounding excess u * (magic -
-// 2^37/m) / 2^37 stays below 2^-8 <= 1/m).
+// 2^37/m) / 2^37 stays below 2^-8 <= 1/m). `offset` is a multiple of m
+// >= 2^25 that makes a signed accumulator (|acc| < 2^25, K <= 2048)
+// non-negative.
 struct I8ModConsts {
   uint32_t m[kI8MaxModuli];
   uint32_t magic[kI8MaxModuli];
+  uint32_t offset[kI8MaxModuli];
 };
 
 // Moduli of the residue epilogue (constant memory: indexed by the work item's
@@ -292,8 +296,10 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             d4[j] = make_int4((int)v[4 * j], (int)v[4 * j + 1], (int)v[4 * j + 2], (int)v[4 * j + 3]);
         }
       } else {
-        // u8 x u8 accumulators are non-negative and below 2^29 (K <= 2048).
+        // s8 x s8 accumulators: |acc| <= K 2^14 < 2^25 (K <= 2048); acc + off
+        // is non-negative and below 2^29.
         const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic[it.l];
+        const uint32_t off = c_i8mod.offset[it.l];
         const bool row_ok = row < p.M;
         uint8_t* dst = p.residues + ((int64_t)it.l * p.M + row) * p.ldr;
 #pragma unroll 1
@@ -306,10 +312,10 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             uint32_t w[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-              const uint32_t b0 = mod_exact29(v[4 * j], m, magic);
-              const uint32_t b1 = mod_exact29(v[4 * j + 1], m, magic);
-              const uint32_t b2 = mod_exact29(v[4 * j + 2], m, magic);
-              const uint32_t b3 = mod_exact29(v[4 * j + 3], m, magic);
+              const uint32_t b0 = mod_exact29(v[4 * j] + off, m, magic);
+              const uint32_t b1 = mod_exact29(v[4 * j + 1] + off, m, magic);
+              const uint32_t b2 = mod_exact29(v[4 * j + 2] + off, m, magic);
+              const uint32_t b3 = mod_exact29(v[4 * j + 3] + off, m, magic);
               w[j] = __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
             }
             if (col0 + 32 <= p.N) {

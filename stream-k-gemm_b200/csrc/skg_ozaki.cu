@@ -41,19 +41,23 @@ namespace {
 constexpr uint32_t kModuli[kI8MaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
                                             229, 227, 223, 217, 211, 199, 197, 193};
 constexpr int kMinModuli = 6;
-// k-blocks (128 k) per INT32-exact segment: s8 x s8 products are <= 2^14,
-// u8 x u8 residue products < 2^16.
+// k-blocks (128 k) per INT32-exact segment: s8 x s8 products are <= 2^14.
 constexpr int kSegKbCapSigned = 1023;   // 1023 * 128 * 2^14 < 2^31
-constexpr int kSegKbCapUnsigned = 256;  // 256 * 128 * 255^2 < 2^31
 
-// Residue constants for one moduli count L (gamma, and with it the digit
-// split of the scaled integers, depends on L). The scaled integer X
-// (|X| <= 2^gamma + 1/2) is handled as u = X + bias >= 0, bias = 2^(gamma+1),
-// split into digits d_j of W bits: X = sum_j d_j 2^(W j) - bias, so
-// X mod m = (d_0 + e + sum_{j>0} d_j c_j) mod m with c_j = 2^(W j) mod m and
-// e = (-bias) mod m.
+// Residue constants for one moduli count L (gamma depends on L). The scaled
+// integer X (|X| <= 2^gamma + 1/2) is handled as u = X + bias >= 0,
+// bias = 2^(gamma+1), so X mod m = (digit sum of u + e) mod m with
+// e = (-bias) mod m. Residues are symmetric (signed int8).
+// The first kIntModuli moduli (256, 255, 253) use the integer pipe: 19-bit
+// digits (u < 2^57) or 16-bit digits, S = d0 + e + d1 c1 + d2 c2 [+ d3 c3]
+// < 2^29, exact remainder by multiply-high. The others (odd) use exact FP32:
+// 12-bit digits f_j, S = f0 + e + sum_j f_j c_j < 2^23 (every product < 2^20),
+// q = rint(S * inv) with inv = 1/m rounded up, r = S - q m, which lies in
+// [-(m+1)/2, (m-1)/2] (the upward bias only ever rounds q up), a signed byte.
+constexpr int kIntModuli = 3;
 struct ResidueConsts {
-  int ndig;         // 3 digits of 19 bits (gamma <= 55) or 4 of 16 bits
+  int ndig;         // integer digits: 3 of 19 bits (gamma <= 55) or 4 of 16 bits
+  int fdig;         // FP32 digits of 12 bits: 5 (gamma <= 57) or 6
   int gamma_bits;
   long long bias;
   uint32_t m[kI8MaxModuli];
@@ -62,6 +66,10 @@ struct ResidueConsts {
   uint32_t c2[kI8MaxModuli];
   uint32_t c3[kI8MaxModuli];
   uint32_t e[kI8MaxModuli];
+  float fc[6][kI8MaxModuli];     // 2^(12 j) mod m
+  float fe[kI8MaxModuli];
+  float finv[kI8MaxModuli];      // 1/m rounded up
+  float fm[kI8MaxModuli];
 };
 
 struct CrtConsts {  // for one moduli count L
@@ -149,55 +157,96 @@ __device__ __forceinline__ void pow2_pair(int mu, double& s1, double& s2) {
 constexpr int kTilePitch = 129;
 __device__ __forceinline__ int swz_k(int k) { return k ^ ((k >> 3) & 7); }
 
-// Digits of the biased scaled integer u = X + bias (X = rint(v 2^mu)):
-// NDIG = 3 digits of 19 bits (u < 2^57, gamma <= 55) or 4 of 16 bits.
-template <int NDIG>
-__device__ __forceinline__ void to_digits(double v, double s1, double s2, long long bias,
-                                          uint32_t (&d)[4]) {
-  const long long X = __double2ll_rn((v * s1) * s2);
-  const unsigned long long u = (unsigned long long)(X + bias);
-  const uint32_t lo = (uint32_t)u, hi = (uint32_t)(u >> 32);
-  if (NDIG == 3) {
-    d[0] = lo & 0x7FFFFu;
-    d[1] = __funnelshift_r(lo, hi, 19) & 0x7FFFFu;
-    d[2] = hi >> 6;
-    d[3] = 0;
-  } else {
-    d[0] = lo & 0xFFFFu;
-    d[1] = lo >> 16;
-    d[2] = hi & 0xFFFFu;
-    d[3] = hi >> 16;
-  }
+// Biased scaled integer u = rint(v 2^mu) + bias (2^mu as two exact factors).
+__device__ __forceinline__ unsigned long long biased_int(double v, double s1, double s2,
+                                                         long long bias) {
+  return (unsigned long long)(__double2ll_rn((v * s1) * s2) + bias);
 }
 
 __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
   return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
 }
 
+__device__ __forceinline__ float u2f_exact(uint32_t x) {  // x < 2^23
+  return __uint_as_float(0x4B000000u | x) - 8388608.0f;
+}
+
 // Residues of the staged block: thread (r, kk) handles k = 8kk .. 8kk+7 of
-// row r; per modulus, X mod m = (d_0 + e + d_1 c_1 + d_2 c_2 [+ d_3 c_3]) mod m
-// (digit sum < 2^29, exact remainder by multiply-high), packed into one
-// 8-byte word; 16 consecutive threads write one 128-byte row segment.
-template <int NDIG>
+// row r and writes one 8-byte word per modulus; 16 consecutive threads write
+// one 128-byte row segment.
+template <int NDIG, int FDIG>
 __device__ __forceinline__ void emit_residues(const double* tileT, const double* s1,
                                               const double* s2, int L, const ResidueConsts& rc,
                                               uint8_t* res, int64_t row0, int64_t KP,
                                               int64_t Rpad, int64_t k0) {
   const int kk = threadIdx.x & 15, r = threadIdx.x >> 4;  // 256 threads: 16 rows x 16
-  uint32_t d[8][4];
+  uint32_t lo[8], hi[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j)
-    to_digits<NDIG>(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r], rc.bias, d[j]);
+  for (int j = 0; j < 8; ++j) {
+    const unsigned long long u =
+        biased_int(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r], rc.bias);
+    lo[j] = (uint32_t)u;
+    hi[j] = (uint32_t)(u >> 32);
+  }
   uint8_t* dst = res + (row0 + r) * KP + k0 + 8 * kk;
-  for (int l = 0; l < L; ++l) {
-    const uint32_t m = rc.m[l], magic = rc.magic[l], e = rc.e[l];
-    const uint32_t c1 = rc.c1[l], c2 = rc.c2[l], c3 = rc.c3[l];
-    uint32_t b[8];
+  uint32_t b[8];
+  // m = 256: the low byte of X = u - bias.
+#pragma unroll
+  for (int j = 0; j < 8; ++j) b[j] = lo[j] - (uint32_t)rc.bias;
+  *reinterpret_cast<uint2*>(dst) =
+      make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
+  // 255 and 253 on the integer pipe.
+  {
+    uint32_t d[8][4];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      uint32_t S = d[j][0] + e + d[j][1] * c1 + d[j][2] * c2;
-      if (NDIG == 4) S += d[j][3] * c3;
-      b[j] = mod_exact29(S, m, magic);
+      if (NDIG == 3) {
+        d[j][0] = lo[j] & 0x7FFFFu;
+        d[j][1] = __funnelshift_r(lo[j], hi[j], 19) & 0x7FFFFu;
+        d[j][2] = hi[j] >> 6;
+        d[j][3] = 0;
+      } else {
+        d[j][0] = lo[j] & 0xFFFFu;
+        d[j][1] = lo[j] >> 16;
+        d[j][2] = hi[j] & 0xFFFFu;
+        d[j][3] = hi[j] >> 16;
+      }
+    }
+#pragma unroll
+    for (int l = 1; l < kIntModuli; ++l) {
+      const uint32_t m = rc.m[l], magic = rc.magic[l], e = rc.e[l], h = (m - 1) / 2;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        uint32_t S = d[j][0] + e + d[j][1] * rc.c1[l] + d[j][2] * rc.c2[l];
+        if (NDIG == 4) S += d[j][3] * rc.c3[l];
+        const uint32_t ru = mod_exact29(S, m, magic);
+        b[j] = ru > h ? ru + (256u - m) : ru;  // symmetric residue as a byte
+      }
+      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) =
+          make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
+    }
+  }
+  // Odd moduli on the FP32 pipe.
+  float f[8][FDIG];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    f[j][0] = u2f_exact(lo[j] & 0xFFFu);
+    f[j][1] = u2f_exact((lo[j] >> 12) & 0xFFFu);
+    f[j][2] = u2f_exact(__funnelshift_r(lo[j], hi[j], 24) & 0xFFFu);
+    f[j][3] = u2f_exact((hi[j] >> 4) & 0xFFFu);
+    f[j][4] = u2f_exact(FDIG == 5 ? (hi[j] >> 16) : ((hi[j] >> 16) & 0xFFFu));
+    if (FDIG == 6) f[j][FDIG - 1] = u2f_exact(hi[j] >> 28);
+  }
+  for (int l = kIntModuli; l < L; ++l) {
+    const float fe = rc.fe[l], inv = rc.finv[l], fm = rc.fm[l];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float S = f[j][0] + fe;
+#pragma unroll
+      for (int t = 1; t < FDIG; ++t) S = fmaf(f[j][t], rc.fc[t][l], S);
+      const float q = fmaf(S, inv, 12582912.0f) - 12582912.0f;  // rint(S * inv)
+      const float rr = fmaf(-q, fm, S);
+      b[j] = __float_as_uint(rr + 12582912.0f);  // low byte = rr mod 256
     }
     *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) =
         make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
@@ -248,7 +297,7 @@ __global__ void __launch_bounds__(256) norm_partials_kernel(int64_t R, int64_t K
 // CTA (p, kb): rows p*T .. +T, k-block kb (128 k), converted in 16-row
 // sub-panels. mu of each row from the norm partials; CTAs with kb == 0 also
 // publish mu.
-template <int T, int NDIG>
+template <int T, int NDIG, int FDIG>
 __global__ void __launch_bounds__(256) convert_packed_kernel(
     int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ X, int C,
     const double* __restrict__ part, int L, uint8_t* __restrict__ res,
@@ -278,8 +327,8 @@ __global__ void __launch_bounds__(256) convert_packed_kernel(
     __syncthreads();
     stage_tile<16>(tileT, src + sp * 16, T, k0, K, rows_valid - sp * 16);
     __syncthreads();
-    emit_residues<NDIG>(tileT, s1 + sp * 16, s2 + sp * 16, L, rc, res, (int64_t)p * T + sp * 16,
-                        KP, Rpad, k0);
+    emit_residues<NDIG, FDIG>(tileT, s1 + sp * 16, s2 + sp * 16, L, rc, res,
+                              (int64_t)p * T + sp * 16, KP, Rpad, k0);
   }
 }
 
@@ -288,7 +337,7 @@ __global__ void __launch_bounds__(256) convert_packed_kernel(
 // src[p * panel_stride + k * ks + r]. Used for the rotation's A (grid-packed
 // Psi, rows = grid points, k = bands: panel_stride nb*16, ks 16) and B
 // (Q row-major, rows = columns of Q, k = rows of Q: panel_stride 16, ks nb).
-template <int NDIG>
+template <int NDIG, int FDIG>
 __global__ void __launch_bounds__(256) convert_local_kernel(
     int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ src,
     int64_t panel_stride, int64_t ks, int L, uint8_t* __restrict__ res, int* __restrict__ mu_out) {
@@ -320,7 +369,7 @@ __global__ void __launch_bounds__(256) convert_local_kernel(
     __syncthreads();
     stage_tile<16>(tileT, base, ks, k0, K, rows_valid);
     __syncthreads();
-    emit_residues<NDIG>(tileT, s1, s2, L, rc, res, p * 16, KP, Rpad, k0);
+    emit_residues<NDIG, FDIG>(tileT, s1, s2, L, rc, res, p * 16, KP, Rpad, k0);
   }
 }
 
@@ -462,6 +511,7 @@ I8ModConsts g_modc;
 bool g_modc_ready = false;
 
 int g_ndig[kI8MaxModuli + 1];
+int g_fdig[kI8MaxModuli + 1];
 
 int ensure_consts(DeviceState* dev) {
   OzakiDevice& od = g_oz[dev->device];
@@ -473,10 +523,13 @@ int ensure_consts(DeviceState* dev) {
     const int ndig = (gam + 2 <= 57) ? 3 : 4;
     const int W = ndig == 3 ? 19 : 16;
     const long long bias = 1LL << (gam + 1);
+    const int fdig = (gam + 2 <= 60) ? 5 : 6;
     rc[L].ndig = ndig;
+    rc[L].fdig = fdig;
     rc[L].gamma_bits = gam;
     rc[L].bias = bias;
     g_ndig[L] = ndig;
+    g_fdig[L] = fdig;
     for (int l = 0; l < kI8MaxModuli; ++l) {
       const uint64_t m = kModuli[l];
       rc[L].m[l] = (uint32_t)m;
@@ -487,11 +540,22 @@ int ensure_consts(DeviceState* dev) {
       rc[L].c2[l] = (uint32_t)(p1 * p1 % m);
       rc[L].c3[l] = (uint32_t)(p1 * p1 % m * p1 % m);
       rc[L].e[l] = (uint32_t)((m - (uint64_t)bias % m) % m);
+      uint64_t pj = 1;
+      for (int j = 0; j < 6; ++j) {
+        rc[L].fc[j][l] = (float)pj;  // 2^(12 j) mod m
+        pj = (pj * 4096) % m;
+      }
+      rc[L].fe[l] = (float)rc[L].e[l];
+      float inv = 1.0f / (float)m;
+      if ((double)inv < 1.0 / (double)m) inv = nextafterf(inv, 1.0f);
+      rc[L].finv[l] = inv;
+      rc[L].fm[l] = (float)m;
     }
   }
   for (int l = 0; l < kI8MaxModuli; ++l) {
     g_modc.m[l] = kModuli[l];
     g_modc.magic[l] = (uint32_t)((1ull << 37) / kModuli[l] + 1);
+    g_modc.offset[l] = (uint32_t)((((1u << 25) + kModuli[l] - 1) / kModuli[l]) * kModuli[l]);
   }
   g_modc_ready = true;
   SKG_CUDA(cudaMemcpyToSymbol(c_i8mod, &g_modc, sizeof(g_modc)));
@@ -658,12 +722,15 @@ int prep_packed(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X,
                                                                   (double*)part.ptr);
   SKG_CUDA(cudaGetLastError());
   const dim3 grid((unsigned)(Rpad / T), (unsigned)(KP / 128));
+  const double* pp = (const double*)part.ptr;
+  uint8_t* rp = (uint8_t*)res.ptr;
+  int* mp = (int*)mu.ptr;
   if (g_ndig[L] == 3)
-    convert_packed_kernel<T, 3><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, (const double*)part.ptr,
-                                                     L, (uint8_t*)res.ptr, (int*)mu.ptr);
+    convert_packed_kernel<T, 3, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, pp, L, rp, mp);
+  else if (g_fdig[L] == 5)
+    convert_packed_kernel<T, 4, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, pp, L, rp, mp);
   else
-    convert_packed_kernel<T, 4><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, (const double*)part.ptr,
-                                                     L, (uint8_t*)res.ptr, (int*)mu.ptr);
+    convert_packed_kernel<T, 4, 6><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, pp, L, rp, mp);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
@@ -672,9 +739,11 @@ int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* s
                  int64_t panel_stride, int64_t ks, int L, uint8_t* res, int* mu, cudaStream_t s) {
   const unsigned grid = (unsigned)(Rpad / 16);
   if (g_ndig[L] == 3)
-    convert_local_kernel<3><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
+    convert_local_kernel<3, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
+  else if (g_fdig[L] == 5)
+    convert_local_kernel<4, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
   else
-    convert_local_kernel<4><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
+    convert_local_kernel<4, 6><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
@@ -714,7 +783,7 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
     muB = &os->mu_b;
   }
   LanePlan* pl = nullptr;
-  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, kSegKbCapUnsigned, &pl)) !=
+  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, kSegKbCapSigned, &pl)) !=
       SKGEMM_OK)
     return st;
   if ((st = os->partials.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t))))
@@ -725,7 +794,7 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedLanes;
-  p.is_signed = 0;
+  p.is_signed = 1;
   p.L = L;
   p.KB = KB;
   p.M = (int)M;
@@ -797,7 +866,7 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedUnits;
-  p.is_signed = 0;
+  p.is_signed = 1;
   p.L = L;
   p.KB = (int)(KP / 128);
   p.M = (int)Nd;
