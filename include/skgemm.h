@@ -188,6 +188,79 @@ int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src_band,
 int skgemm_grid_to_band_dev(int64_t Nd, int64_t nb, const double* src_grid,
                             double* dst_band, void* stream);
 
+/* ------------------------------------------------------ batched (grouped) */
+/* Many independent GEMM / SYRK / rotation problems of uneven sizes (k-points,
+ * spin blocks) in ONE persistent Stream-K launch: the MAC-loop iterations of
+ * all problems are concatenated and split evenly over the CTAs, so small and
+ * large problems share the GPU without tail waves. No counterpart in the
+ * reference, whose drivers call one problem at a time (the CheFSI loop calls
+ * sme_syrk<double>::compute and gemm<double>::compute_packed per k-point).
+ * Each item uses the contract of the single-problem _dev call it names. */
+#define SKGEMM_OP_GEMM_PACKED 0 /* skgemm_dgemm_packed_dev: M, N, K, A packed16,
+                                   B packed32, D row-major (ldd), alpha, beta=gamma */
+#define SKGEMM_OP_SYRK_PACKED 1 /* skgemm_dsyrk_packed_dev: M (= N), K, A packed16,
+                                   C column-major upper (ldd), alpha, beta */
+#define SKGEMM_OP_ROT 2         /* skgemm_drot_dev: M = Nd, N = nb (K ignored),
+                                   A grid-packed, B = Q row-major, D band-packed */
+
+typedef struct skgemm_batch_item {
+  int op; /* SKGEMM_OP_* */
+  int64_t M, N, K;
+  const double* A;
+  const double* B; /* unused for SYRK */
+  double* D;
+  int64_t ldd; /* unused for ROT */
+  double alpha;
+  double beta; /* GEMM: gamma (scalar added); SYRK: beta; ROT: unused */
+} skgemm_batch_item_t;
+
+/* Plan options. Zero-initialised options = autotune everything, capture a
+ * graph. Out fields report the chosen configuration. */
+typedef struct skgemm_plan_options {
+  int tile;     /* output tile: 128 (128x128), 64 (64x64) or 0 = autotune */
+  int grid;     /* persistent CTAs (Stream-K split factor); 0 = all SMs x occupancy */
+  int order;    /* problem order: 1 = as given, 2 = most work first, 0 = autotune */
+  int no_tune;  /* 1: do not time candidates, pick by the cost model alone */
+  int no_graph; /* 1: plain stream launches instead of a CUDA graph */
+  int tile_out, grid_out, order_out;
+  int candidates_timed_out;
+  double tuned_ms_out; /* device time of the chosen configuration (ms), 0 if untimed */
+  double model_efficiency_out; /* useful MACs / issued MACs of the chosen tiles */
+} skgemm_plan_options_t;
+
+typedef struct skgemm_plan* skgemm_plan_t;
+
+/* Builds a plan for `n` items on the current device: validates every item,
+ * builds the problem table and TMA descriptors in device memory, chooses the
+ * tile shape, problem order and grid (autotuning times the candidate
+ * configurations on the items' own buffers, so outputs hold unspecified
+ * values afterwards, except SYRK outputs with beta != 0, which are restored),
+ * and captures [flag reset, grouped launch] in a CUDA graph. Pointers in
+ * `items` are bound into the plan. `stream` orders the tuning runs. Results of
+ * tuning are cached per batch signature for the process. */
+int skgemm_plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* opts,
+                       void* stream, skgemm_plan_t* plan_out);
+/* Enqueues the batch on `stream` (a graph launch, or plain launches). */
+int skgemm_plan_run(skgemm_plan_t plan, void* stream);
+/* Synchronises `stream` and reports (then clears) device-side failures of the
+ * plan's launches. */
+int skgemm_plan_status(skgemm_plan_t plan, void* stream);
+/* Releases the plan (synchronises the device first: its launches may still be
+ * in flight). */
+void skgemm_plan_destroy(skgemm_plan_t plan);
+
+/* One-shot grouped launch of `n` items without tuning or graph (cost-model
+ * configuration); asynchronous on `stream`, check with skgemm_stream_status. */
+int skgemm_batch_dev(const skgemm_batch_item_t* items, int n, void* stream);
+
+/* Host-only view of a grouped schedule (no device needed): for tile 128 or
+ * 64, problem order `order` (1 or 2) and `grid` CTAs, writes the problem
+ * order (perm_out[n]), the first MAC-loop iteration of each problem in the
+ * concatenated space (iter_begin_out[n+1], in perm order), and the useful /
+ * issued MAC ratio. Items with a zero dimension get zero iterations. */
+int skgemm_batch_schedule(const skgemm_batch_item_t* items, int n, int tile, int order,
+                          int* perm_out, int64_t* iter_begin_out, double* efficiency_out);
+
 #ifdef __cplusplus
 }
 #endif

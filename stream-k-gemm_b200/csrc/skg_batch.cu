@@ -1,0 +1,585 @@
+// Batched path: many independent GEMM / SYRK / rotation problems of uneven
+// sizes in one grouped persistent Stream-K launch, a plan that autotunes the
+// tile shape, problem order and grid, and records the launch into a CUDA
+// graph.
+//
+// The reference has no batched entry point: its CheFSI driver calls
+// sme_syrk<double>::compute (include/sme_syrk.hpp:137) and
+// gemm<double>::compute_packed (gemm_opt.cpp:314) once per k-point / spin
+// block. Each item here keeps the contract of the matching single-problem
+// call (skgemm_dsyrk_packed_dev, skgemm_dgemm_packed_dev, skgemm_drot_dev).
+//
+// Schedule: problem p contributes num_tiles(p) * ceil(K(p)/16) MAC-loop
+// iterations; the iterations of all problems are concatenated in the plan's
+// problem order and split evenly over the persistent CTAs (Fp64Group). Tuning
+// candidates: tile 128x128 (1 CTA/SM) or 64x64 (2 CTAs/SM: less padding waste
+// on small state counts, same DMMA fragment code), problem order as given or
+// most-work-first, and the grid. The cost model is the useful/issued MAC
+// ratio of the tiles; tuning times each candidate with CUDA events on the
+// items' own buffers and keeps the fastest (cached per batch signature).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "skg_fp64_types.h"
+#include "skg_runtime.h"
+
+namespace skg {
+
+namespace {
+
+struct Geom {
+  int tiles_m = 0, tiles_n = 0, num_tiles = 0, ipt = 0;
+  int64_t iters = 0;
+  double useful = 0.0, issued = 0.0;  // MACs
+};
+
+// Validates one item and builds its problem descriptor (zero-size items are
+// valid and produce no iterations).
+int item_problem(const skgemm_batch_item_t& it, Fp64Problem* p) {
+  if (it.M < 0 || it.N < 0 || it.K < 0) return fail(SKGEMM_ERR_INVALID_ARG, "negative dimension");
+  switch (it.op) {
+    case SKGEMM_OP_GEMM_PACKED:
+      if (it.ldd < it.N) return fail(SKGEMM_ERR_INVALID_ARG, "batch item: ldd < N");
+      *p = gemm_packed_problem(it.M, it.N, it.K, it.A, it.B, it.D, it.ldd, it.alpha, it.beta);
+      break;
+    case SKGEMM_OP_SYRK_PACKED:
+      if (it.ldd < it.M) return fail(SKGEMM_ERR_INVALID_ARG, "batch item: ldc < M");
+      *p = syrk_problem(it.K, it.M, it.A, it.D, it.ldd, it.alpha, it.beta);
+      break;
+    case SKGEMM_OP_ROT:
+      if (it.M % 16 || it.N % 16)
+        return fail(SKGEMM_ERR_INVALID_ARG,
+                    "batch item: rotation layouts need Nd and nb multiples of 16");
+      *p = rot_problem(it.M, it.N, it.A, it.B, it.D);
+      break;
+    default:
+      return fail(SKGEMM_ERR_INVALID_ARG, "batch item: unknown op");
+  }
+  if (p->K > (int64_t)INT32_MAX - kBK || p->M > ((int64_t)1 << 31) || p->N > ((int64_t)1 << 31))
+    return fail(SKGEMM_ERR_INVALID_ARG, "batch item: dimension too large");
+  if (p->M > 0 && p->N > 0) {
+    if (!p->D) return fail(SKGEMM_ERR_INVALID_ARG, "batch item: null output pointer");
+    if (p->K > 0 && (!p->a.ptr || !p->b.ptr))
+      return fail(SKGEMM_ERR_INVALID_ARG, "batch item: null operand pointer");
+  }
+  return SKGEMM_OK;
+}
+
+Geom geom_of(const Fp64Problem& p, int BM, int BN) {
+  Geom g;
+  if (p.M == 0 || p.N == 0 || p.K == 0) return g;
+  g.tiles_m = (int)((p.M + BM - 1) / BM);
+  g.tiles_n = (int)((p.N + BN - 1) / BN);
+  if (p.tile_order == kTilesUpper) {
+    // Upper-triangle tiles: tile (tm, tn) with tm*BM <= tn*BN + BN - 1. For
+    // square tiles that is tm <= tn.
+    g.num_tiles = g.tiles_n * (g.tiles_n + 1) / 2;
+    g.useful = (double)p.M * (double)(p.M + 1) / 2.0 * (double)p.K;
+  } else {
+    g.num_tiles = g.tiles_m * g.tiles_n;
+    g.useful = (double)p.M * (double)p.N * (double)p.K;
+  }
+  g.ipt = (int)((p.K + kBK - 1) / kBK);
+  g.iters = (int64_t)g.num_tiles * g.ipt;
+  g.issued = (double)g.iters * BM * BN * kBK;
+  return g;
+}
+
+// Problem order: 1 = as given, 2 = most iterations first (stable).
+std::vector<int> make_order(const std::vector<Geom>& geo, int order) {
+  std::vector<int> perm(geo.size());
+  std::iota(perm.begin(), perm.end(), 0);
+  if (order == 2)
+    std::stable_sort(perm.begin(), perm.end(),
+                     [&](int a, int b) { return geo[a].iters > geo[b].iters; });
+  return perm;
+}
+
+struct Config {
+  int tile = 128, order = 1, grid = 0;
+};
+
+// Tuning results per batch signature (shapes, ops, device).
+std::mutex g_tune_mu;
+std::map<std::string, Config> g_tune_cache;
+
+std::string signature(int device, const std::vector<skgemm_batch_item_t>& items,
+                      const skgemm_plan_options_t& o) {
+  std::string s = std::to_string(device) + "|" + std::to_string(o.tile) + "," +
+                  std::to_string(o.order) + "," + std::to_string(o.grid) + "|";
+  char buf[96];
+  for (const auto& it : items) {
+    snprintf(buf, sizeof(buf), "%d:%lld:%lld:%lld;", it.op, (long long)it.M, (long long)it.N,
+             (long long)it.K);
+    s += buf;
+  }
+  return s;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ plan
+struct BatchPlan {
+  int device = -1;
+  DeviceState* dev = nullptr;
+  std::vector<skgemm_batch_item_t> items;
+  std::vector<Fp64Problem> probs;
+  std::vector<int> k0_items;  // items with an empty reduction and a non-empty output
+  Config cfg;
+  double efficiency = 0.0;
+  Fp64Group group{};
+  DeviceBuffer d_probs, d_maps, d_iters, d_part, d_flags, d_err;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool use_graph = true;
+
+  ~BatchPlan() {
+    // Launches of the plan may still be in flight on any stream.
+    cudaDeviceSynchronize();
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    d_probs.release();
+    d_maps.release();
+    d_iters.release();
+    d_part.release();
+    d_flags.release();
+    d_err.release();
+  }
+};
+
+namespace {
+
+int grid_cap(DeviceState* dev, int tile, int* cap) {
+  int per_sm = 0;
+  int st = fp64_group_occupancy(dev, tile, &per_sm);
+  if (st) return st;
+  *cap = dev->num_sms * per_sm;
+  return SKGEMM_OK;
+}
+
+// Builds the device-side problem table, descriptors and workspace of
+// configuration `c` (synchronous uploads; not during stream capture).
+int configure(BatchPlan* P, Config c) {
+  const int BM = c.tile, BN = c.tile;
+  const int n = (int)P->probs.size();
+  std::vector<Geom> geo(n);
+  for (int i = 0; i < n; ++i) geo[i] = geom_of(P->probs[i], BM, BN);
+  const std::vector<int> perm = make_order(geo, c.order);
+
+  std::vector<Fp64Params> hp;
+  std::vector<CUtensorMap> hm;
+  std::vector<int64_t> hb;
+  hp.reserve(n);
+  hm.reserve(2 * n);
+  hb.push_back(0);
+  double useful = 0.0, issued = 0.0;
+  for (int idx : perm) {
+    const Geom& g = geo[idx];
+    if (g.iters == 0) continue;
+    const Fp64Problem& pr = P->probs[idx];
+    Fp64Params q;
+    memset(&q, 0, sizeof(q));
+    q.M = pr.M;
+    q.N = pr.N;
+    q.K = pr.K;
+    q.tiles_m = g.tiles_m;
+    q.tiles_n = g.tiles_n;
+    q.num_tiles = g.num_tiles;
+    q.iters_per_tile = g.ipt;
+    q.total_iters = g.iters;
+    q.a_kind = pr.a.kind;
+    q.b_kind = pr.b.kind;
+    q.tile_order = pr.tile_order;
+    q.out_kind = pr.out_kind;
+    q.D = pr.D;
+    q.ldd = pr.ldd;
+    q.alpha = pr.alpha;
+    q.gamma = pr.gamma;
+    q.beta_zero = pr.beta_zero ? 1 : 0;
+    hp.push_back(q);
+    CUtensorMap ma, mb;
+    int st;
+    if ((st = make_operand_map(&ma, pr.a, pr.K, BM)) != SKGEMM_OK) return st;
+    if ((st = make_operand_map(&mb, pr.b, pr.K, BN)) != SKGEMM_OK) return st;
+    hm.push_back(ma);
+    hm.push_back(mb);
+    hb.push_back(hb.back() + g.iters);
+    useful += g.useful;
+    issued += g.issued;
+  }
+  const int np = (int)hp.size();
+  const int64_t total = hb.back();
+  if (total > ((int64_t)1 << 40)) return fail(SKGEMM_ERR_INVALID_ARG, "batch too large");
+  int cap = 0, st;
+  if ((st = grid_cap(P->dev, c.tile, &cap)) != SKGEMM_OK) return st;
+  int grid = c.grid > 0 ? std::min(c.grid, cap) : cap;
+  grid = (int)std::min<int64_t>(grid, total);
+
+  Fp64Group& G = P->group;
+  memset(&G, 0, sizeof(G));
+  G.num_problems = np;
+  G.total_iters = total;
+  G.grid = grid;
+  if (np > 0) {
+    if ((st = P->d_probs.ensure(hp.size() * sizeof(Fp64Params)))) return st;
+    if ((st = P->d_maps.ensure(hm.size() * sizeof(CUtensorMap)))) return st;
+    if ((st = P->d_iters.ensure(hb.size() * sizeof(int64_t)))) return st;
+    if ((st = P->d_part.ensure((size_t)grid * BM * BN * sizeof(double)))) return st;
+    if ((st = P->d_flags.ensure((size_t)grid * sizeof(uint32_t)))) return st;
+    SKG_CUDA(cudaMemcpy(P->d_probs.ptr, hp.data(), hp.size() * sizeof(Fp64Params),
+                        cudaMemcpyHostToDevice));
+    SKG_CUDA(cudaMemcpy(P->d_maps.ptr, hm.data(), hm.size() * sizeof(CUtensorMap),
+                        cudaMemcpyHostToDevice));
+    SKG_CUDA(cudaMemcpy(P->d_iters.ptr, hb.data(), hb.size() * sizeof(int64_t),
+                        cudaMemcpyHostToDevice));
+  }
+  if (!P->d_err.ptr) {
+    if ((st = P->d_err.ensure(sizeof(uint32_t)))) return st;
+    SKG_CUDA(cudaMemset(P->d_err.ptr, 0, sizeof(uint32_t)));
+  }
+  G.probs = (const Fp64Params*)P->d_probs.ptr;
+  G.maps = (const CUtensorMap*)P->d_maps.ptr;
+  G.iter_begin = (const int64_t*)P->d_iters.ptr;
+  G.workspace = (double*)P->d_part.ptr;
+  G.flags = (uint32_t*)P->d_flags.ptr;
+  G.err = (uint32_t*)P->d_err.ptr;
+  P->cfg = c;
+  P->cfg.grid = grid;
+  P->efficiency = issued > 0 ? useful / issued : 1.0;
+  return SKGEMM_OK;
+}
+
+// Enqueues the plan's work on `s`: the grouped launch and the K == 0 items.
+int enqueue(BatchPlan* P, cudaStream_t s) {
+  int st;
+  if (P->group.num_problems > 0 &&
+      (st = launch_fp64_group(P->cfg.tile, P->group, s)) != SKGEMM_OK)
+    return st;
+  for (int i : P->k0_items) {
+    const Fp64Problem& pr = P->probs[i];
+    if ((st = run_k0(pr.out_kind, pr.M, pr.N, pr.D, pr.ldd, pr.gamma, pr.beta_zero, s)))
+      return st;
+  }
+  return SKGEMM_OK;
+}
+
+int time_config(BatchPlan* P, cudaStream_t s, float* ms_out) {
+  int st;
+  if ((st = enqueue(P, s))) return st;  // warm-up
+  cudaEvent_t e0, e1;
+  SKG_CUDA(cudaEventCreate(&e0));
+  SKG_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int r = 0; r < 2 && st == SKGEMM_OK; ++r) {
+    cudaEventRecord(e0, s);
+    st = enqueue(P, s);
+    cudaEventRecord(e1, s);
+    if (cudaEventSynchronize(e1) != cudaSuccess) st = cuda_fail(cudaGetLastError(), "tuning run");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms_out = best;
+  return st;
+}
+
+int read_err(BatchPlan* P) {
+  uint32_t word = 0;
+  SKG_CUDA(cudaMemcpy(&word, P->d_err.ptr, sizeof(word), cudaMemcpyDeviceToHost));
+  if (word == 0) return SKGEMM_OK;
+  SKG_CUDA(cudaMemset(P->d_err.ptr, 0, sizeof(uint32_t)));
+  char buf[160];
+  snprintf(buf, sizeof(buf), "batched launch: device-side wait ran past its budget (0x%x)", word);
+  return fail(SKGEMM_ERR_DEVICE_TIMEOUT, buf);
+}
+
+int build_plan(const skgemm_batch_item_t* items, int n, BatchPlan* P) {
+  int st;
+  P->dev = current_device(&st);
+  if (!P->dev) return st;
+  P->device = P->dev->device;
+  if (n < 0 || (n > 0 && !items)) return fail(SKGEMM_ERR_INVALID_ARG, "bad item array");
+  P->items.assign(items, items + n);
+  P->probs.resize(n);
+  for (int i = 0; i < n; ++i) {
+    if ((st = item_problem(items[i], &P->probs[i])) != SKGEMM_OK) {
+      char buf[64];
+      snprintf(buf, sizeof(buf), " (item %d)", i);
+      return fail(st, skgemm_last_error() + std::string(buf));
+    }
+    const Fp64Problem& pr = P->probs[i];
+    if (pr.M > 0 && pr.N > 0 && pr.K == 0 && pr.out_kind != kOutBand16) P->k0_items.push_back(i);
+  }
+  return SKGEMM_OK;
+}
+
+}  // namespace
+
+// Host-only schedule (exported for tests and tooling).
+int batch_schedule(const skgemm_batch_item_t* items, int n, int tile, int order, int* perm_out,
+                   int64_t* iter_begin_out, double* eff_out) {
+  if (tile != 128 && tile != 64) return fail(SKGEMM_ERR_INVALID_ARG, "tile must be 128 or 64");
+  if (order != 1 && order != 2) return fail(SKGEMM_ERR_INVALID_ARG, "order must be 1 or 2");
+  if (n < 0 || (n > 0 && !items)) return fail(SKGEMM_ERR_INVALID_ARG, "bad item array");
+  std::vector<Geom> geo(n);
+  for (int i = 0; i < n; ++i) {
+    Fp64Problem p;
+    int st = item_problem(items[i], &p);
+    if (st) return st;
+    geo[i] = geom_of(p, tile, tile);
+  }
+  const std::vector<int> perm = make_order(geo, order);
+  double useful = 0.0, issued = 0.0;
+  int64_t acc = 0;
+  for (int j = 0; j < n; ++j) {
+    if (perm_out) perm_out[j] = perm[j];
+    if (iter_begin_out) iter_begin_out[j] = acc;
+    acc += geo[perm[j]].iters;
+    useful += geo[perm[j]].useful;
+    issued += geo[perm[j]].issued;
+  }
+  if (iter_begin_out) iter_begin_out[n] = acc;
+  if (eff_out) *eff_out = issued > 0 ? useful / issued : 1.0;
+  return SKGEMM_OK;
+}
+
+int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* opts,
+                cudaStream_t s, BatchPlan** out) {
+  *out = nullptr;
+  skgemm_plan_options_t o;
+  memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  if (o.tile != 0 && o.tile != 128 && o.tile != 64)
+    return fail(SKGEMM_ERR_INVALID_ARG, "plan option tile must be 0, 128 or 64");
+  if (o.order < 0 || o.order > 2) return fail(SKGEMM_ERR_INVALID_ARG, "plan option order");
+  if (o.grid < 0) return fail(SKGEMM_ERR_INVALID_ARG, "plan option grid");
+  std::unique_ptr<BatchPlan> P(new BatchPlan());
+  int st = build_plan(items, n, P.get());
+  if (st) return st;
+  P->use_graph = !o.no_graph;
+
+  // Candidates.
+  std::vector<Config> cands;
+  for (int tile : {128, 64}) {
+    if (o.tile && o.tile != tile) continue;
+    for (int order : {2, 1}) {
+      if (o.order && o.order != order) continue;
+      Config c;
+      c.tile = tile;
+      c.order = order;
+      c.grid = o.grid;
+      cands.push_back(c);
+    }
+  }
+  // Cost model: issued MACs (padding included) at a per-tile-shape rate;
+  // 64 x 64 tiles carry more staging per MAC, rated 0.9 of 128 x 128.
+  auto model_cost = [&](const Config& c) {
+    double issued = 0.0;
+    for (const auto& pr : P->probs) issued += geom_of(pr, c.tile, c.tile).issued;
+    return issued / (c.tile == 128 ? 1.0 : 0.9);
+  };
+  Config best = cands[0];
+  double best_cost = 1e300;
+  for (const auto& c : cands) {
+    const double cost = model_cost(c);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = c;
+    }
+  }
+  float best_ms = 0.f;
+  int timed = 0;
+  const std::string sig = signature(P->device, P->items, o);
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto f = g_tune_cache.find(sig);
+    if (f != g_tune_cache.end() && !o.no_tune) {
+      best = f->second;
+      cached = true;
+    }
+  }
+  bool has_work = false;
+  for (const auto& pr : P->probs) has_work |= (pr.M > 0 && pr.N > 0);
+  if (!o.no_tune && !cached && cands.size() > 1 && has_work) {
+    // SYRK outputs with beta != 0 are read by the product: keep a copy.
+    std::vector<std::pair<int, double*>> saved;
+    for (int i = 0; i < n; ++i) {
+      const auto& it = P->items[i];
+      if (it.op == SKGEMM_OP_SYRK_PACKED && it.beta != 0.0 && it.M > 0) {
+        double* b = nullptr;
+        const size_t bytes = (size_t)it.ldd * it.M * sizeof(double);
+        SKG_CUDA(cudaMalloc(&b, bytes));
+        SKG_CUDA(cudaMemcpyAsync(b, it.D, bytes, cudaMemcpyDeviceToDevice, s));
+        saved.push_back({i, b});
+      }
+    }
+    float ms_best = 1e30f;
+    for (const auto& c : cands) {
+      if ((st = configure(P.get(), c)) != SKGEMM_OK) break;
+      float ms = 0.f;
+      if ((st = time_config(P.get(), s, &ms)) != SKGEMM_OK) break;
+      ++timed;
+      if (ms < ms_best) {
+        ms_best = ms;
+        best = c;
+      }
+    }
+    for (auto& sv : saved) {
+      const auto& it = P->items[sv.first];
+      cudaMemcpyAsync(it.D, sv.second, (size_t)it.ldd * it.M * sizeof(double),
+                      cudaMemcpyDeviceToDevice, s);
+    }
+    cudaStreamSynchronize(s);
+    for (auto& sv : saved) cudaFree(sv.second);
+    if (st) return st;
+    if ((st = read_err(P.get())) != SKGEMM_OK) return st;
+    best_ms = ms_best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[sig] = best;
+  }
+  if ((st = configure(P.get(), best)) != SKGEMM_OK) return st;
+
+  if (P->use_graph && (P->group.num_problems > 0 || !P->k0_items.empty())) {
+    cudaStream_t cap;
+    SKG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      st = enqueue(P.get(), cap);
+      cudaGraph_t g = nullptr;
+      e = cudaStreamEndCapture(cap, &g);
+      if (st == SKGEMM_OK && e == cudaSuccess) {
+        P->graph = g;
+        e = cudaGraphInstantiate(&P->exec, g, 0);
+      }
+    }
+    cudaStreamDestroy(cap);
+    if (st) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "batch graph capture");
+  }
+  if (opts) {
+    opts->tile_out = P->cfg.tile;
+    opts->grid_out = P->cfg.grid;
+    opts->order_out = P->cfg.order;
+    opts->candidates_timed_out = timed;
+    opts->tuned_ms_out = best_ms;
+    opts->model_efficiency_out = P->efficiency;
+  }
+  *out = P.release();
+  return SKGEMM_OK;
+}
+
+int plan_run(BatchPlan* P, cudaStream_t s) {
+  int cur = -1;
+  SKG_CUDA(cudaGetDevice(&cur));
+  if (cur != P->device) return fail(SKGEMM_ERR_INVALID_ARG, "plan belongs to another device");
+  if (P->exec) {
+    SKG_CUDA(cudaGraphLaunch(P->exec, s));
+    return SKGEMM_OK;
+  }
+  return enqueue(P, s);
+}
+
+int plan_status(BatchPlan* P, cudaStream_t s) {
+  SKG_CUDA(cudaStreamSynchronize(s));
+  return read_err(P);
+}
+
+// One-shot grouped launch on a per-stream plan cache entry: the plan (and so
+// its workspace) stays alive until the next one-shot batch on that stream has
+// been ordered behind it.
+namespace {
+std::mutex g_oneshot_mu;
+std::map<std::pair<int, cudaStream_t>, BatchPlan*> g_oneshot;
+}  // namespace
+
+int batch_dev(const skgemm_batch_item_t* items, int n, cudaStream_t s) {
+  skgemm_plan_options_t o;
+  memset(&o, 0, sizeof(o));
+  o.no_tune = 1;
+  o.no_graph = 1;
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  std::lock_guard<std::mutex> lk(g_oneshot_mu);
+  BatchPlan*& slot = g_oneshot[{dev->device, s}];
+  if (slot) {
+    // The previous one-shot plan's launch may still be in flight on `s`:
+    // its buffers are released only after the stream has passed it.
+    SKG_CUDA(cudaStreamSynchronize(s));
+    st = read_err(slot);
+    delete slot;
+    slot = nullptr;
+    if (st) return st;
+  }
+  BatchPlan* P = nullptr;
+  if ((st = plan_create(items, n, &o, s, &P)) != SKGEMM_OK) return st;
+  slot = P;
+  return enqueue(P, s);
+}
+
+// Device-side failures of one-shot batches on `s` (called by
+// skgemm_stream_status after it has synchronised `s`).
+int batch_consume_error(DeviceState* dev, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_oneshot_mu);
+  auto f = g_oneshot.find({dev->device, s});
+  if (f == g_oneshot.end() || !f->second) return SKGEMM_OK;
+  return read_err(f->second);
+}
+
+}  // namespace skg
+
+using namespace skg;
+
+#define SKG_EXPORT extern "C" __attribute__((visibility("default")))
+
+struct skgemm_plan {
+  BatchPlan* impl;
+};
+
+SKG_EXPORT int skgemm_plan_create(const skgemm_batch_item_t* items, int n,
+                                  skgemm_plan_options_t* opts, void* stream,
+                                  skgemm_plan_t* plan_out) {
+  if (!plan_out) return fail(SKGEMM_ERR_INVALID_ARG, "null plan_out");
+  *plan_out = nullptr;
+  BatchPlan* P = nullptr;
+  int st = plan_create(items, n, opts, reinterpret_cast<cudaStream_t>(stream), &P);
+  if (st) return st;
+  *plan_out = new skgemm_plan{P};
+  return SKGEMM_OK;
+}
+
+SKG_EXPORT int skgemm_plan_run(skgemm_plan_t plan, void* stream) {
+  if (!plan || !plan->impl) return fail(SKGEMM_ERR_INVALID_ARG, "null plan");
+  return plan_run(plan->impl, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_plan_status(skgemm_plan_t plan, void* stream) {
+  if (!plan || !plan->impl) return fail(SKGEMM_ERR_INVALID_ARG, "null plan");
+  return plan_status(plan->impl, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT void skgemm_plan_destroy(skgemm_plan_t plan) {
+  if (!plan) return;
+  delete plan->impl;
+  delete plan;
+}
+
+SKG_EXPORT int skgemm_batch_dev(const skgemm_batch_item_t* items, int n, void* stream) {
+  return batch_dev(items, n, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_batch_schedule(const skgemm_batch_item_t* items, int n, int tile,
+                                     int order, int* perm_out, int64_t* iter_begin_out,
+                                     double* efficiency_out) {
+  return batch_schedule(items, n, tile, order, perm_out, iter_begin_out, efficiency_out);
+}

@@ -163,6 +163,8 @@ __global__ void k0_kernel(int mode, int64_t M, int64_t N, double* D, int64_t ld,
   }
 }
 
+}  // namespace
+
 int run_k0(int mode, int64_t M, int64_t N, double* D, int64_t ld, double gamma, bool beta_zero,
            cudaStream_t s) {
   if (M == 0 || N == 0) return SKGEMM_OK;
@@ -246,6 +248,8 @@ int check_dims(int64_t a, int64_t b, int64_t c) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+namespace {
+
 // Blocking host-pointer execution: copies `nin` inputs to device staging
 // buffers, runs `body` with the device pointers, copies `out` back.
 struct HostIO {
@@ -310,6 +314,7 @@ SKG_EXPORT int skgemm_stream_status(void* stream) {
   }
   int e = consume_device_error(ws, s);
   if (e != SKGEMM_OK) return e;
+  if ((e = batch_consume_error(dev, s)) != SKGEMM_OK) return e;
   return ozaki_consume_error(dev, s);
 }
 

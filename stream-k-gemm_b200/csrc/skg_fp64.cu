@@ -7,8 +7,6 @@
 
 namespace skg {
 
-namespace {
-
 int make_operand_map(CUtensorMap* map, const Fp64Operand& op, int64_t K, int rows_per_tile) {
   if (op.ptr == nullptr) return fail(SKGEMM_ERR_INVALID_ARG, "null operand pointer");
   if ((reinterpret_cast<uintptr_t>(op.ptr) & 15) != 0)
@@ -37,6 +35,8 @@ int make_operand_map(CUtensorMap* map, const Fp64Operand& op, int64_t K, int row
   }
   return fail(SKGEMM_ERR_INVALID_ARG, "unknown operand kind");
 }
+
+namespace {
 
 struct Schedule {
   int tiles_m, tiles_n, num_tiles, ipt;
@@ -135,6 +135,55 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
   cfg.numAttrs = 1;
   SKG_CUDA(cudaLaunchKernelEx(&cfg, fp64_streamk_kernel, mapA, mapB, p));
   return SKGEMM_OK;
+}
+
+}  // namespace skg
+
+// ------------------------------------------------------------ grouped launch
+namespace skg {
+
+namespace {
+
+template <class TS>
+int grouped_setup(int device, int* blocks_per_sm) {
+  static int occ[64] = {0};
+  if (device < 0 || device >= 64) return fail(SKGEMM_ERR_INVALID_ARG, "device index");
+  if (!occ[device]) {
+    SKG_CUDA(cudaFuncSetAttribute(fp64_grouped_kernel<TS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, TS::kSmem));
+    int n = 0;
+    SKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fp64_grouped_kernel<TS>,
+                                                           kThreads, TS::kSmem));
+    if (n < 1) return fail(SKGEMM_ERR_UNSUPPORTED, "grouped kernel does not fit on an SM");
+    occ[device] = n;
+  }
+  *blocks_per_sm = occ[device];
+  return SKGEMM_OK;
+}
+
+template <class TS>
+int grouped_launch(const Fp64Group& g, cudaStream_t s) {
+  // Flags start at zero for every launch (a stream-ordered memset, captured
+  // together with the kernel when the pair is recorded into a graph).
+  SKG_CUDA(cudaMemsetAsync(g.flags, 0, (size_t)g.grid * sizeof(uint32_t), s));
+  fp64_grouped_kernel<TS><<<g.grid, kThreads, TS::kSmem, s>>>(g);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+}  // namespace
+
+int fp64_group_occupancy(DeviceState* dev, int tile, int* blocks_per_sm) {
+  if (tile == 128) return grouped_setup<Tile128>(dev->device, blocks_per_sm);
+  if (tile == 64) return grouped_setup<Tile64>(dev->device, blocks_per_sm);
+  return fail(SKGEMM_ERR_INVALID_ARG, "tile must be 128 or 64");
+}
+
+int launch_fp64_group(int tile, const Fp64Group& g, cudaStream_t s) {
+  if (g.grid <= 0 || g.total_iters <= 0) return SKGEMM_OK;
+  if (tile == 128) return grouped_launch<Tile128>(g, s);
+  if (tile == 64) return grouped_launch<Tile64>(g, s);
+  return fail(SKGEMM_ERR_INVALID_ARG, "tile must be 128 or 64");
 }
 
 }  // namespace skg

@@ -20,6 +20,10 @@
 // runs the epilogue. The reduction order is a pure function of the schedule,
 // so results are bitwise reproducible run to run.
 //
+// The same body serves one problem (fp64_streamk_kernel, BM = BN = 128) and a
+// group of problems in one launch (fp64_grouped_kernel<TileShape>, the
+// batched path: iterations of all problems concatenated, see Fp64Group).
+//
 // Data movement: one producer warp issues TMA tile loads (128B-swizzled boxes
 // of 16 doubles x BK rows) into an NSTAGE ring; 8 consumer warps run FP64 DMMA
 // (m16n8k8) from shared memory. Every operand tile in shared memory is a set of
@@ -118,13 +122,79 @@ __device__ __forceinline__ void store_row4(const Fp64Params& p, int64_t m, int64
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
-    fp64_streamk_kernel(const __grid_constant__ CUtensorMap mapA,
-                        const __grid_constant__ CUtensorMap mapB, const Fp64Params p) {
+// One problem: its parameters and tensor maps are kernel parameters; flags
+// carry the host-side epoch of the launch.
+struct SingleSched {
+  const Fp64Params& p;
+  const CUtensorMap* mA;
+  const CUtensorMap* mB;
+  __device__ __forceinline__ int64_t total() const { return p.total_iters; }
+  __device__ __forceinline__ int grid() const { return p.grid; }
+  __device__ __forceinline__ const Fp64Params& prob(int) const { return p; }
+  __device__ __forceinline__ const CUtensorMap* map_a(int) const { return mA; }
+  __device__ __forceinline__ const CUtensorMap* map_b(int) const { return mB; }
+  __device__ __forceinline__ int64_t begin(int) const { return 0; }
+  __device__ __forceinline__ int locate(int64_t, int) const { return 0; }
+  __device__ __forceinline__ double* workspace() const { return p.workspace; }
+  __device__ __forceinline__ uint32_t* flags() const { return p.flags; }
+  __device__ __forceinline__ uint32_t* err() const { return p.err; }
+  __device__ __forceinline__ uint32_t pub() const { return p.epoch; }
+};
+
+// A group of problems: descriptors and tensor maps in global memory.
+struct GroupSched {
+  const Fp64Group& g;
+  __device__ __forceinline__ int64_t total() const { return g.total_iters; }
+  __device__ __forceinline__ int grid() const { return g.grid; }
+  __device__ __forceinline__ const Fp64Params& prob(int i) const { return g.probs[i]; }
+  __device__ __forceinline__ const CUtensorMap* map_a(int i) const { return g.maps + 2 * i; }
+  __device__ __forceinline__ const CUtensorMap* map_b(int i) const { return g.maps + 2 * i + 1; }
+  __device__ __forceinline__ int64_t begin(int i) const { return g.iter_begin[i]; }
+  // Problem containing iteration `it`; `hint` is a problem at or before it.
+  __device__ __forceinline__ int locate(int64_t it, int hint) const {
+    int i = hint;
+    if (g.iter_begin[i + 1] <= it) {
+      int lo = i + 1, hi = g.num_problems - 1;  // invariant: answer in [lo, hi]
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.iter_begin[mid] <= it) lo = mid; else hi = mid - 1;
+      }
+      i = lo;
+    }
+    return i;
+  }
+  __device__ __forceinline__ double* workspace() const { return g.workspace; }
+  __device__ __forceinline__ uint32_t* flags() const { return g.flags; }
+  __device__ __forceinline__ uint32_t* err() const { return g.err; }
+  __device__ __forceinline__ uint32_t pub() const { return 1u; }
+};
+
+// Where iteration `it` (< it_end) falls: problem, tile, k-block range of this
+// CTA inside the tile and the tile coordinates.
+struct Seg {
+  int pid, tile, kb, ke, tm, tn;
+};
+
+template <class Sched>
+__device__ __forceinline__ Seg locate_seg(const Sched& S, int64_t it, int64_t it_end, int hint) {
+  Seg sg;
+  sg.pid = S.locate(it, hint);
+  const Fp64Params& q = S.prob(sg.pid);
+  const int ipt = q.iters_per_tile;
+  const int64_t local = it - S.begin(sg.pid);
+  sg.tile = (int)(local / ipt);
+  sg.kb = (int)(local - (int64_t)sg.tile * ipt);
+  sg.ke = (int)((int64_t)ipt < sg.kb + (it_end - it) ? (int64_t)ipt : sg.kb + (it_end - it));
+  tile_coords(q, sg.tile, sg.tm, sg.tn);
+  return sg;
+}
+
+template <class TS, class Sched>
+__device__ __forceinline__ void streamk_body(const Sched& S) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
-  uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + kStages * TS::kStage);
   uint64_t* empty_bar = full_bar + kStages;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(empty_bar + kStages);
 
@@ -142,46 +212,51 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   __syncthreads();
 
-  const int64_t it_begin = (int64_t)cta * p.total_iters / p.grid;
-  const int64_t it_end = (int64_t)(cta + 1) * p.total_iters / p.grid;
-  const int ipt = p.iters_per_tile;
+  const int64_t it_begin = (int64_t)cta * S.total() / S.grid();
+  const int64_t it_end = (int64_t)(cta + 1) * S.total() / S.grid();
 
   if (warp == kConsumerWarps) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
-      tma_prefetch_desc(&mapA);
-      tma_prefetch_desc(&mapB);
       int stage = 0;
       uint32_t phase = 0;
+      int hint = S.locate(it_begin < it_end ? it_begin : 0, 0);
+      int prefetched = -1;
       for (int64_t it = it_begin; it < it_end;) {
-        int tile = (int)(it / ipt);
-        int kb = (int)(it - (int64_t)tile * ipt);
-        int ke = (int)((int64_t)ipt < kb + (it_end - it) ? (int64_t)ipt : kb + (it_end - it));
-        int tm, tn;
-        tile_coords(p, tile, tm, tn);
-        for (int k = kb; k < ke; ++k) {
-          if (!mbar_wait(&empty_bar[stage], phase ^ 1, p.err)) *abort_flag = 1;
+        const Seg sg = locate_seg(S, it, it_end, hint);
+        hint = sg.pid;
+        const Fp64Params& q = S.prob(sg.pid);
+        const CUtensorMap* mA = S.map_a(sg.pid);
+        const CUtensorMap* mB = S.map_b(sg.pid);
+        if (prefetched != sg.pid) {
+          tma_prefetch_desc(mA);
+          tma_prefetch_desc(mB);
+          prefetched = sg.pid;
+        }
+        for (int k = sg.kb; k < sg.ke; ++k) {
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1, S.err())) *abort_flag = 1;
           if (*abort_flag) break;
-          uint8_t* sa = smem + stage * kStageBytes;
-          uint8_t* sb = sa + kTileABytes;
-          mbar_arrive_expect_tx(&full_bar[stage], kStageBytes);
-          load_operand(p.a_kind, &mapA, sa, &full_bar[stage], tm, kBM, k * kBK);
-          load_operand(p.b_kind, &mapB, sb, &full_bar[stage], tn, kBN, k * kBK);
+          uint8_t* sa = smem + stage * TS::kStage;
+          uint8_t* sb = sa + TS::kABytes;
+          mbar_arrive_expect_tx(&full_bar[stage], TS::kStage);
+          load_operand(q.a_kind, mA, sa, &full_bar[stage], sg.tm, TS::BM, k * kBK);
+          load_operand(q.b_kind, mB, sb, &full_bar[stage], sg.tn, TS::BN, k * kBK);
           if (++stage == kStages) {
             stage = 0;
             phase ^= 1;
           }
         }
         if (*abort_flag) break;
-        it += ke - kb;
+        it += sg.ke - sg.kb;
       }
     }
     return;
   }
 
   // -------------------------------------------------------------- consumers
-  const int wm = warp >> 2;  // 0..1 : rows wm*64 .. +64
-  const int wn = warp & 3;   // 0..3 : cols wn*32 .. +32
+  constexpr int MI = TS::MI, NJ = TS::NJ, NQ = TS::NQ;
+  const int wm = warp >> 2;  // 0..1 : rows wm*BM/2 ..
+  const int wn = warp & 3;   // 0..3 : cols wn*BN/4 ..
   const int g = lane >> 2;
   const int t = lane & 3;
   // Byte offsets inside a chunk of the two k-rows this lane reads per k8 step.
@@ -190,64 +265,67 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t off_r0 = (2 * t) * 128 + ((g ^ (2 * t)) << 4);
   const uint32_t off_r1 = (2 * t + 1) * 128 + ((g ^ (2 * t + 1)) << 4);
   const uint32_t smem_base = smem_u32(smem);
-  // Shared-memory chunk of this warp's two B column chunks (logical 2*wn+q).
-  // A packed32 operand lands as [half][tile][BK][16]: logical chunk c sits at
-  // (c % 2) * (BN/32) + c / 2.
-  uint32_t b_chunk[2];
-#pragma unroll
-  for (int q = 0; q < 2; ++q)
-    b_chunk[q] = (p.b_kind == kOpPacked32) ? (q * (kBN / 32) + wn) : (2 * wn + q);
   __shared__ int fixup_ok;
 
-  double acc[4][4][4];
+  double acc[MI][NJ][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < MI; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
   int stage = 0;
   uint32_t phase = 0;
   bool aborted = false;
+  int hint = S.locate(it_begin < it_end ? it_begin : 0, 0);
+  const uint32_t pubval = S.pub();
 
   for (int64_t it = it_begin; it < it_end;) {
-    const int tile = (int)(it / ipt);
-    const int kb = (int)(it - (int64_t)tile * ipt);
-    const int ke = (int)((int64_t)ipt < kb + (it_end - it) ? (int64_t)ipt : kb + (it_end - it));
-    int tm, tn;
-    tile_coords(p, tile, tm, tn);
+    const Seg sg = locate_seg(S, it, it_end, hint);
+    hint = sg.pid;
+    const Fp64Params& q = S.prob(sg.pid);
+    // Shared-memory chunk of this warp's B column chunks (logical wn*NQ+qq).
+    // A packed32 operand lands as [half][tile32][BK][16]: logical chunk c
+    // sits at (c % 2) * (BN/32) + c / 2.
+    uint32_t b_chunk[NQ];
+    const bool b32 = (q.b_kind == kOpPacked32);
+#pragma unroll
+    for (int qq = 0; qq < NQ; ++qq) {
+      const int c = wn * NQ + qq;
+      b_chunk[qq] = b32 ? (uint32_t)((c & 1) * (TS::BN / 32) + (c >> 1)) : (uint32_t)c;
+    }
 
-    for (int k = kb; k < ke && !aborted; ++k) {
-      if (!mbar_wait(&full_bar[stage], phase, p.err)) {
+    for (int k = sg.kb; k < sg.ke && !aborted; ++k) {
+      if (!mbar_wait(&full_bar[stage], phase, S.err())) {
         aborted = true;
         *abort_flag = 1;
         break;
       }
-      const uint32_t sa = smem_base + stage * kStageBytes + (wm * 4) * kChunkBytes;
-      const uint32_t sb = smem_base + stage * kStageBytes + kTileABytes;
+      const uint32_t sa = smem_base + stage * TS::kStage + (wm * MI) * kChunkBytes;
+      const uint32_t sb = smem_base + stage * TS::kStage + TS::kABytes;
 #pragma unroll
       for (int s = 0; s < kBK / 8; ++s) {
         const uint32_t ks = s * 8 * 128;  // k8 step = 8 rows of 128 B
-        double2 a_lo[4], a_hi[4], b_lo[2], b_hi[2];
+        double2 a_lo[MI], a_hi[MI], b_lo[NQ], b_hi[NQ];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < MI; ++i) {
           a_lo[i] = lds128(sa + i * kChunkBytes + ks + off_r0);
           a_hi[i] = lds128(sa + i * kChunkBytes + ks + off_r1);
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          b_lo[q] = lds128(sb + b_chunk[q] * kChunkBytes + ks + off_r0);
-          b_hi[q] = lds128(sb + b_chunk[q] * kChunkBytes + ks + off_r1);
+        for (int qq = 0; qq < NQ; ++qq) {
+          b_lo[qq] = lds128(sb + b_chunk[qq] * kChunkBytes + ks + off_r0);
+          b_hi[qq] = lds128(sb + b_chunk[qq] * kChunkBytes + ks + off_r1);
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < MI; ++i) {
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            dmma_16x8x8(acc[i][2 * q], a_lo[i].x, a_lo[i].y, a_hi[i].x, a_hi[i].y, b_lo[q].x,
-                        b_hi[q].x);
-            dmma_16x8x8(acc[i][2 * q + 1], a_lo[i].x, a_lo[i].y, a_hi[i].x, a_hi[i].y,
-                        b_lo[q].y, b_hi[q].y);
+          for (int qq = 0; qq < NQ; ++qq) {
+            dmma_16x8x8(acc[i][2 * qq], a_lo[i].x, a_lo[i].y, a_hi[i].x, a_hi[i].y, b_lo[qq].x,
+                        b_hi[qq].x);
+            dmma_16x8x8(acc[i][2 * qq + 1], a_lo[i].x, a_lo[i].y, a_hi[i].x, a_hi[i].y,
+                        b_lo[qq].y, b_hi[qq].y);
           }
         }
       }
@@ -261,40 +339,41 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (aborted) break;
 
     // ---------------------------------------------------------- epilogue
-    const bool owner = (kb == 0);
-    const bool complete = owner && (ke == ipt);
+    const bool owner = (sg.kb == 0);
+    const bool complete = owner && (sg.ke == q.iters_per_tile);
     const int ctid = threadIdx.x;  // 0..255
+    constexpr int kSlot = TS::BM * TS::BN;
     if (!owner) {
       // Publish this CTA's partial tile (layout [reg][thread], coalesced).
-      double* slot = p.workspace + (int64_t)cta * (kBM * kBN);
+      double* slot = S.workspace() + (int64_t)cta * kSlot;
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < NJ; ++j)
 #pragma unroll
           for (int r = 0; r < 4; ++r)
-            __stcg(slot + ((i * 4 + j) * 4 + r) * kConsumerThreads + ctid, acc[i][j][r]);
+            __stcg(slot + ((i * NJ + j) * 4 + r) * kConsumerThreads + ctid, acc[i][j][r]);
       __threadfence();
       asm volatile("bar.sync 1, %0;" ::"n"(kConsumerThreads));
-      if (ctid == 0) st_release_gpu(p.flags + cta, p.epoch);
+      if (ctid == 0) st_release_gpu(S.flags() + cta, pubval);
     } else {
       if (!complete) {
         // Add the partials of the later CTAs that cover the rest of this tile,
         // in ascending k order. A flag that does not arrive within the budget
         // is recorded in the error word and its partial is skipped; the CTA
         // keeps consuming its pipeline so no copy is left in flight.
-        const int64_t tile_end = (int64_t)(tile + 1) * ipt;
-        for (int c2 = cta + 1; c2 < p.grid; ++c2) {
-          const int64_t s2 = (int64_t)c2 * p.total_iters / p.grid;
+        const int64_t tile_end = S.begin(sg.pid) + (int64_t)(sg.tile + 1) * q.iters_per_tile;
+        for (int c2 = cta + 1; c2 < S.grid(); ++c2) {
+          const int64_t s2 = (int64_t)c2 * S.total() / S.grid();
           if (s2 >= tile_end) break;
           if (ctid == 0) {
             const uint64_t t0 = globaltimer_ns();
             uint32_t spins = 0;
             int ok = 1;
-            while (ld_acquire_gpu(p.flags + c2) != p.epoch) {
+            while (ld_acquire_gpu(S.flags() + c2) != pubval) {
               __nanosleep(128);
               if (++spins > kFixupSpinCap || globaltimer_ns() - t0 > kFixupBudgetNs) {
-                atomicOr(p.err, kDevErrFixupTimeout);
+                atomicOr(S.err(), kDevErrFixupTimeout);
                 ok = 0;
                 break;
               }
@@ -305,43 +384,58 @@ __global__ void __launch_bounds__(kThreads, 1)
           const bool have = fixup_ok != 0;
           asm volatile("bar.sync 1, %0;" ::"n"(kConsumerThreads));
           if (!have) continue;
-          const double* slot = p.workspace + (int64_t)c2 * (kBM * kBN);
+          const double* slot = S.workspace() + (int64_t)c2 * kSlot;
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
+          for (int i = 0; i < MI; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < NJ; ++j)
 #pragma unroll
               for (int r = 0; r < 4; ++r)
-                acc[i][j][r] += __ldcg(slot + ((i * 4 + j) * 4 + r) * kConsumerThreads + ctid);
+                acc[i][j][r] += __ldcg(slot + ((i * NJ + j) * 4 + r) * kConsumerThreads + ctid);
         }
       }
       // Final epilogue for tile (tm, tn).
-      const int64_t mbase = (int64_t)tm * kBM + wm * 64;
-      const int64_t nbase = (int64_t)tn * kBN + wn * 32;
-      const bool syrk_skip = (p.out_kind == kOutSyrkUpper) && (mbase > nbase + 31);
+      const int64_t mbase = (int64_t)sg.tm * TS::BM + wm * (TS::BM / 2);
+      const int64_t nbase = (int64_t)sg.tn * TS::BN + wn * (TS::BN / 4);
+      const bool syrk_skip = (q.out_kind == kOutSyrkUpper) && (mbase > nbase + TS::BN / 4 - 1);
       if (!syrk_skip) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < MI; ++i) {
           const int64_t m0 = mbase + i * 16 + 2 * g;
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const int64_t n0 = nbase + q * 16 + 4 * t;
-            store_row4(p, m0, n0, acc[i][2 * q][0], acc[i][2 * q + 1][0], acc[i][2 * q][1],
-                       acc[i][2 * q + 1][1]);
-            store_row4(p, m0 + 1, n0, acc[i][2 * q][2], acc[i][2 * q + 1][2], acc[i][2 * q][3],
-                       acc[i][2 * q + 1][3]);
+          for (int qq = 0; qq < NQ; ++qq) {
+            const int64_t n0 = nbase + qq * 16 + 4 * t;
+            store_row4(q, m0, n0, acc[i][2 * qq][0], acc[i][2 * qq + 1][0], acc[i][2 * qq][1],
+                       acc[i][2 * qq + 1][1]);
+            store_row4(q, m0 + 1, n0, acc[i][2 * qq][2], acc[i][2 * qq + 1][2],
+                       acc[i][2 * qq][3], acc[i][2 * qq + 1][3]);
           }
         }
       }
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < NJ; ++j)
 #pragma unroll
         for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
-    it += ke - kb;
+    it += sg.ke - sg.kb;
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    fp64_streamk_kernel(const __grid_constant__ CUtensorMap mapA,
+                        const __grid_constant__ CUtensorMap mapB,
+                        const __grid_constant__ Fp64Params p) {
+  const SingleSched S{p, &mapA, &mapB};
+  streamk_body<Tile128>(S);
+}
+
+template <class TS>
+__global__ void __launch_bounds__(kThreads, TS::kMinBlocks)
+    fp64_grouped_kernel(const __grid_constant__ Fp64Group g) {
+  const GroupSched S{g};
+  streamk_body<TS>(S);
 }
 
 }  // namespace skg

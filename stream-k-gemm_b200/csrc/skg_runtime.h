@@ -93,6 +93,27 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
                 StreamWorkspace* ws_override = nullptr);
 // Number of Stream-K partial slots the launch of `prob` uses (= its grid).
 int fp64_grid_for(DeviceState* dev, const Fp64Problem& prob);
+// Grouped launch (batched path): CTAs per SM the grouped kernel of `tile`
+// (128 or 64) fits, and the launch itself (flag reset + kernel, no cooperative
+// attribute so that the pair can be captured into a CUDA graph; the grid must
+// not exceed SMs x blocks_per_sm so that every CTA can be resident).
+struct Fp64Group;
+int fp64_group_occupancy(DeviceState* dev, int tile, int* blocks_per_sm);
+int launch_fp64_group(int tile, const Fp64Group& g, cudaStream_t s);
+// TMA descriptor of one operand for tiles of `rows_per_tile` rows.
+int make_operand_map(CUtensorMap* map, const Fp64Operand& op, int64_t K, int rows_per_tile);
+
+// Problem descriptors of the three entry points (contracts of
+// skgemm_dgemm_packed_dev, skgemm_dsyrk_packed_dev, skgemm_drot_dev).
+Fp64Problem gemm_packed_problem(int64_t M, int64_t N, int64_t K, const double* Ap,
+                                const double* Bp, double* D, int64_t ldd, double alpha,
+                                double gamma);
+Fp64Problem syrk_problem(int64_t K, int64_t M, const double* Ap, double* C, int64_t ldc,
+                         double alpha, double beta);
+Fp64Problem rot_problem(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D);
+// Result of an empty reduction (K == 0): D = gamma (GEMM), C = beta*C (SYRK).
+int run_k0(int mode, int64_t M, int64_t N, double* D, int64_t ld, double gamma, bool beta_zero,
+           cudaStream_t s);
 
 // Layout kernels.
 int launch_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, int T,
@@ -104,6 +125,10 @@ int launch_grid_to_band(int64_t Nd, int64_t nb, const double* src, double* dst,
 
 // Peak probe.
 int probe_fp64_peak(DeviceState* dev, double* tflops);
+
+// Device-side failures of one-shot batched launches on `s` (read and cleared;
+// `s` already synchronised).
+int batch_consume_error(DeviceState* dev, cudaStream_t s);
 
 // Reads and clears the error word of `ws` (synchronises `s`).
 int consume_device_error(StreamWorkspace* ws, cudaStream_t s);

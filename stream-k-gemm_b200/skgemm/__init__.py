@@ -52,6 +52,28 @@ class Options(ctypes.Structure):
                 ("err_bound_out", ctypes.c_double), ("slices_used_out", ctypes.c_int)]
 
 
+OP_GEMM_PACKED = 0
+OP_SYRK_PACKED = 1
+OP_ROT = 2
+
+
+class BatchItem(ctypes.Structure):
+    """skgemm_batch_item_t: one problem of a grouped launch."""
+    _fields_ = [("op", ctypes.c_int), ("M", ctypes.c_int64), ("N", ctypes.c_int64),
+                ("K", ctypes.c_int64), ("A", ctypes.c_void_p), ("B", ctypes.c_void_p),
+                ("D", ctypes.c_void_p), ("ldd", ctypes.c_int64), ("alpha", ctypes.c_double),
+                ("beta", ctypes.c_double)]
+
+
+class PlanOptions(ctypes.Structure):
+    """skgemm_plan_options_t."""
+    _fields_ = [("tile", ctypes.c_int), ("grid", ctypes.c_int), ("order", ctypes.c_int),
+                ("no_tune", ctypes.c_int), ("no_graph", ctypes.c_int),
+                ("tile_out", ctypes.c_int), ("grid_out", ctypes.c_int),
+                ("order_out", ctypes.c_int), ("candidates_timed_out", ctypes.c_int),
+                ("tuned_ms_out", ctypes.c_double), ("model_efficiency_out", ctypes.c_double)]
+
+
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 _d = ctypes.c_double
@@ -80,6 +102,14 @@ _SIGS = {
     "skgemm_pack_dev": [_i64, _i64, _vp, _i64, _i64, ctypes.c_int, _vp, _vp],
     "skgemm_band_to_grid_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_grid_to_band_dev": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_plan_create": [ctypes.POINTER(BatchItem), ctypes.c_int,
+                           ctypes.POINTER(PlanOptions), _vp, ctypes.POINTER(_vp)],
+    "skgemm_plan_run": [_vp, _vp],
+    "skgemm_plan_status": [_vp, _vp],
+    "skgemm_batch_dev": [ctypes.POINTER(BatchItem), ctypes.c_int, _vp],
+    "skgemm_batch_schedule": [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_int,
+                              ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                              ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)],
 }
 
 
@@ -99,12 +129,14 @@ def lib() -> ctypes.CDLL:
         L.skgemm_version.argtypes = []
         L.skgemm_last_error.restype = ctypes.c_char_p
         L.skgemm_last_error.argtypes = []
+        L.skgemm_plan_destroy.restype = None
+        L.skgemm_plan_destroy.argtypes = [_vp]
         _lib = L
     return _lib
 
 
 def exported_symbols() -> list:
-    return ["skgemm_version", "skgemm_last_error"] + list(_SIGS)
+    return ["skgemm_version", "skgemm_last_error", "skgemm_plan_destroy"] + list(_SIGS)
 
 
 def version() -> str:
@@ -275,3 +307,69 @@ def probe_fp64_peak() -> float:
     v = ctypes.c_double(0.0)
     _check(lib().skgemm_probe_fp64_peak(ctypes.byref(v)))
     return v.value
+
+
+# ------------------------------------------------------------------ batched
+def batch_item(op, M, N, K, A, B, D, ldd=0, alpha=1.0, beta=0.0) -> BatchItem:
+    """One problem of a grouped launch (device buffers: torch tensors or addresses)."""
+    return BatchItem(op, M, N, K, _dptr(A), _dptr(B), _dptr(D), ldd, alpha, beta)
+
+
+def _item_array(items):
+    arr = (BatchItem * max(1, len(items)))()
+    for i, it in enumerate(items):
+        arr[i] = it
+    return arr
+
+
+class Plan:
+    """A tuned, graph-captured grouped launch of a fixed set of problems
+    (skgemm_plan_create / _run / _status / _destroy)."""
+
+    def __init__(self, items, tile=0, grid=0, order=0, tune=True, graph=True, stream=None):
+        self.options = PlanOptions(tile, grid, order, 0 if tune else 1, 0 if graph else 1)
+        self._items = _item_array(items)
+        h = ctypes.c_void_p(0)
+        _check(lib().skgemm_plan_create(self._items, len(items), ctypes.byref(self.options),
+                                        _stream(stream), ctypes.byref(h)))
+        self._h = h
+
+    def run(self, stream=None) -> None:
+        _check(lib().skgemm_plan_run(self._h, _stream(stream)))
+
+    def status(self, stream=None) -> None:
+        _check(lib().skgemm_plan_status(self._h, _stream(stream)))
+
+    @property
+    def config(self) -> dict:
+        o = self.options
+        return {"tile": o.tile_out, "grid": o.grid_out, "order": o.order_out,
+                "candidates_timed": o.candidates_timed_out, "tuned_ms": o.tuned_ms_out,
+                "model_efficiency": o.model_efficiency_out}
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            lib().skgemm_plan_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_dev(items, stream=None) -> None:
+    """One-shot grouped launch (cost-model configuration, no graph)."""
+    _check(lib().skgemm_batch_dev(_item_array(items), len(items), _stream(stream)))
+
+
+def batch_schedule(items, tile=128, order=1):
+    """Host-only grouped schedule: (perm, iter_begin, useful/issued MAC ratio)."""
+    n = len(items)
+    perm = (ctypes.c_int * max(1, n))()
+    ib = (ctypes.c_int64 * (n + 1))()
+    eff = ctypes.c_double(0.0)
+    _check(lib().skgemm_batch_schedule(_item_array(items), n, tile, order, perm, ib,
+                                       ctypes.byref(eff)))
+    return list(perm)[:n], list(ib), eff.value

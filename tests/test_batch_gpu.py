@@ -1,0 +1,255 @@
+"""GPU parity of the batched path: grouped persistent Stream-K launches of
+mixed GEMM / SYRK / rotation problems (skgemm_plan_* and skgemm_batch_dev),
+called through the C ABI.
+
+Gates: every item of a batch within relative Frobenius error 1e-13 of the
+Dot2 (double-double) oracle, whatever the tile shape, problem order, grid or
+graph capture; bytes outside each output's contract untouched; a replayed
+graph reads the current contents of the inputs; repeated runs bitwise equal;
+autotuning leaves SYRK outputs with beta != 0 as they were."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import skgemm
+from tests._cases import gaussian, uniform
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64).ravel()).cuda()
+
+
+class Item:
+    """Host inputs, device buffers, the batch item and its oracle."""
+
+    def __init__(self, op, seed, M, N, K, alpha=1.0, beta=0.0, ldd_pad=0):
+        self.op, self.M, self.N, self.K = op, M, N, K
+        self.alpha, self.beta = alpha, beta
+        rng_seed = 1000 + seed
+        if op == skgemm.OP_GEMM_PACKED:
+            self.A = uniform((M, K), rng_seed)
+            self.B = uniform((K, N), rng_seed + 1)
+            self.ldd = N + ldd_pad
+            self.dA = dev(oracle.pack(self.A, 16))
+            self.dB = dev(oracle.pack(self.B.T, 32))
+            self.D0 = np.full((M, self.ldd), 7.0)
+        elif op == skgemm.OP_SYRK_PACKED:
+            self.X = gaussian((K, M), rng_seed, 1.0 / np.sqrt(max(K, 1)))
+            self.ldd = M + ldd_pad
+            self.dA = dev(oracle.pack(self.X.T, 16))
+            self.dB = None
+            self.D0 = uniform((M, self.ldd), rng_seed + 2)  # column-major C: [col][row]
+        else:
+            self.Psi = gaussian((M, N), rng_seed, 1.0 / np.sqrt(M))
+            self.Q = uniform((N, N), rng_seed + 1)
+            self.ldd = 0
+            self.dA = dev(oracle.grid_pack(self.Psi))
+            self.dB = dev(self.Q)
+            self.D0 = np.full(M * N, 7.0)
+        self.dD = dev(self.D0)
+
+    def item(self):
+        return skgemm.batch_item(self.op, self.M, self.N, self.K, self.dA, self.dB, self.dD,
+                                 self.ldd, self.alpha, self.beta)
+
+    def reset(self):
+        self.dD.copy_(dev(self.D0))
+
+    def check(self):
+        torch.cuda.synchronize()
+        out = self.dD.cpu().numpy()
+        if self.M == 0 or self.N == 0:
+            assert out.size == 0
+            return 0.0
+        if self.op == skgemm.OP_GEMM_PACKED:
+            out = out.reshape(self.M, self.ldd)
+            ref = oracle.dot2_matmul(self.A, self.B, self.alpha, self.beta)
+            err = oracle.rel_frobenius(out[:, :self.N], ref)
+            assert np.array_equal(out[:, self.N:], self.D0[:, self.N:])
+        elif self.op == skgemm.OP_SYRK_PACKED:
+            C = out.reshape(self.M, self.ldd)  # row c = column c of C
+            S = oracle.dot2_matmul(self.X.T, self.X)  # S[i, j]
+            iu = np.triu_indices(self.M)       # i <= j: C[i + j*ldd] = row j, entry i
+            got = C[iu[1], iu[0]]
+            want = self.alpha * S[iu] + self.beta * self.D0[iu[1], iu[0]]
+            err = oracle.rel_frobenius(got, want)
+            il = np.tril_indices(self.M, -1)
+            assert np.array_equal(C[il[1], il[0]], self.D0[il[1], il[0]])
+            assert np.array_equal(C[:, self.M:], self.D0[:, self.M:])
+        else:
+            got = oracle.band_unpack(out.reshape(self.N // 16, self.M, 16), self.M)
+            ref = oracle.dot2_matmul(self.Psi, self.Q)
+            err = oracle.rel_frobenius(got, ref)
+        assert err <= TOL, (self.op, self.M, self.N, self.K, err)
+        return err
+
+
+def mixed_batch(seed):
+    G, S, R = skgemm.OP_GEMM_PACKED, skgemm.OP_SYRK_PACKED, skgemm.OP_ROT
+    return [
+        Item(S, seed + 0, 512, 512, 4096),
+        Item(G, seed + 1, 300, 200, 1000, 1.5, 0.25, ldd_pad=3),
+        Item(S, seed + 2, 100, 100, 777, 2.0, 0.5, ldd_pad=5),
+        Item(R, seed + 3, 2048, 64, 0),
+        Item(G, seed + 4, 17, 33, 5),
+        Item(S, seed + 5, 64, 64, 13824),
+        Item(G, seed + 6, 40, 50, 0, 1.0, -3.0),          # K = 0: D = gamma
+        Item(S, seed + 7, 33, 33, 0, 1.0, 0.75),          # K = 0: C = beta C
+        Item(R, seed + 8, 4096, 160, 0),
+        Item(G, seed + 9, 257, 129, 300, -1.0, 0.0),
+        Item(S, seed + 10, 1, 1, 3),
+        Item(G, seed + 11, 0, 10, 10),                    # empty output
+    ]
+
+
+@pytest.mark.parametrize("tile", [128, 64])
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("graph", [True, False])
+def test_plan_mixed_batch_matches_oracle(cuda, tile, order, graph):
+    items = mixed_batch(10 * tile + order)
+    plan = skgemm.Plan([it.item() for it in items], tile=tile, order=order, tune=False,
+                       graph=graph)
+    assert plan.config["tile"] == tile and plan.config["order"] == order
+    plan.run()
+    plan.status()
+    for it in items:
+        it.check()
+    plan.close()
+
+
+@pytest.mark.parametrize("grid", [1, 5, 148])
+def test_plan_any_grid(cuda, grid):
+    items = mixed_batch(77)
+    plan = skgemm.Plan([it.item() for it in items], tile=128, order=2, grid=grid, tune=False)
+    assert plan.config["grid"] == grid
+    plan.run()
+    plan.status()
+    for it in items:
+        it.check()
+
+
+def test_plan_autotune_keeps_syrk_beta_outputs(cuda):
+    items = mixed_batch(5)
+    before = [it.dD.clone() for it in items]
+    plan = skgemm.Plan([it.item() for it in items])  # tune tile and order
+    cfg = plan.config
+    assert cfg["candidates_timed"] == 4 and cfg["tile"] in (64, 128) and cfg["tuned_ms"] > 0
+    torch.cuda.synchronize()
+    for it, b in zip(items, before):
+        if it.op == skgemm.OP_SYRK_PACKED and it.beta != 0.0:
+            assert torch.equal(it.dD, b)
+    plan.run()
+    plan.status()
+    for it in items:
+        it.check()
+    # A second plan over the same shapes reuses the tuning result.
+    plan2 = skgemm.Plan([it.item() for it in items])
+    assert plan2.config["candidates_timed"] == 0
+    assert plan2.config["tile"] == cfg["tile"] and plan2.config["order"] == cfg["order"]
+
+
+def test_plan_graph_replay_reads_current_inputs_and_is_deterministic(cuda):
+    items = mixed_batch(9)
+    plan = skgemm.Plan([it.item() for it in items], tile=128, order=2, tune=False)
+    plan.run()
+    plan.run()
+    plan.status()
+    first = [it.dD.clone() for it in items if it.op != skgemm.OP_SYRK_PACKED or it.beta == 0]
+    plan.run()
+    plan.status()
+    again = [it.dD.clone() for it in items if it.op != skgemm.OP_SYRK_PACKED or it.beta == 0]
+    assert all(torch.equal(a, b) for a, b in zip(first, again))
+    # New operand values, same buffers: the replayed graph sees them.
+    for it in items:
+        it.reset()
+        if it.op == skgemm.OP_GEMM_PACKED and it.K > 0:
+            it.A = it.A * -0.5
+            it.dA.copy_(dev(oracle.pack(it.A, 16)))
+    torch.cuda.synchronize()
+    plan.run()
+    plan.status()
+    for it in items:
+        it.check()
+
+
+def test_batch_dev_oneshot(cuda):
+    items = mixed_batch(3)
+    skgemm.batch_dev([it.item() for it in items])
+    skgemm.stream_status()
+    for it in items:
+        it.check()
+    # A second one-shot batch on the same stream after the first.
+    for it in items:
+        it.reset()
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        skgemm.batch_dev([it.item() for it in items], stream=s)
+        skgemm.batch_dev([it.item() for it in items if it.op != skgemm.OP_SYRK_PACKED
+                          or it.beta == 0.0], stream=s)
+    skgemm.stream_status(s)
+    for it in items:
+        if it.op == skgemm.OP_SYRK_PACKED and it.beta != 0.0:
+            continue
+        it.check()
+
+
+def test_batch_rejects_bad_items(cuda):
+    it = Item(skgemm.OP_GEMM_PACKED, 1, 10, 20, 30)
+    bad = it.item()
+    bad.ldd = 5
+    with pytest.raises(skgemm.SkgemmError) as e:
+        skgemm.Plan([bad])
+    assert e.value.code == skgemm.ERR_INVALID_ARG
+    bad = it.item()
+    bad.A = 0
+    with pytest.raises(skgemm.SkgemmError):
+        skgemm.batch_dev([bad])
+    with pytest.raises(skgemm.SkgemmError):
+        skgemm.Plan([it.item()], tile=96)
+
+
+def test_batch_kpoint_set_matches_single_calls(cuda):
+    """A reduced k-point set (16 instances, grids 24^3 / 32^3, states
+    log-uniform in [64, 512]): each S and Hs of the grouped launch against the
+    single-problem native call and, on a sample of entries, against Dot2."""
+    rng = np.random.default_rng(4)
+    items, singles, keep = [], [], []
+    for i in range(16):
+        Ng = int(rng.choice([24 ** 3, 32 ** 3]))
+        nb = int(np.exp(rng.uniform(np.log(64), np.log(512))))
+        g = torch.Generator(device="cuda").manual_seed(100 + i)
+        Psi = torch.randn(Ng, nb, generator=g, dtype=torch.float64, device="cuda") / Ng ** 0.5
+        H = torch.randn(Ng, nb, generator=g, dtype=torch.float64, device="cuda") / Ng ** 0.5
+        p16 = torch.empty(((nb + 15) // 16) * 16 * Ng, dtype=torch.float64, device="cuda")
+        h32 = torch.empty(((nb + 31) // 32) * 32 * Ng, dtype=torch.float64, device="cuda")
+        skgemm.pack_dev(nb, Ng, Psi, 1, nb, 16, p16)
+        skgemm.pack_dev(nb, Ng, H, 1, nb, 32, h32)
+        S = torch.zeros(nb, nb, dtype=torch.float64, device="cuda")
+        Hs = torch.zeros_like(S)
+        S1, Hs1 = torch.zeros_like(S), torch.zeros_like(S)
+        items += [skgemm.batch_item(skgemm.OP_SYRK_PACKED, nb, nb, Ng, p16, 0, S, nb),
+                  skgemm.batch_item(skgemm.OP_GEMM_PACKED, nb, nb, Ng, p16, h32, Hs, nb)]
+        skgemm.dsyrk_packed_dev(Ng, nb, p16, S1, nb)
+        skgemm.dgemm_packed_dev(nb, nb, Ng, p16, h32, Hs1, nb)
+        singles.append((Psi, H, S, Hs, S1, Hs1, nb))
+        keep.append((p16, h32))  # the plan holds raw pointers into these
+    skgemm.stream_status()
+    plan = skgemm.Plan(items)
+    plan.run()
+    plan.status()
+    for (Psi, H, S, Hs, S1, Hs1, nb) in singles:
+        iu = np.triu_indices(nb)
+        s, s1 = S.cpu().numpy().T, S1.cpu().numpy().T   # column-major -> [i, j]
+        assert oracle.rel_frobenius(s[iu], s1[iu]) <= TOL
+        assert oracle.rel_frobenius(Hs.cpu().numpy(), Hs1.cpu().numpy()) <= TOL
+        P, Hh = Psi.cpu().numpy(), H.cpu().numpy()
+        ii = np.random.default_rng(nb).integers(0, nb, 64)
+        jj = np.random.default_rng(nb + 1).integers(0, nb, 64)
+        ref = oracle.dot2_sampled(P.T, Hh, ii, jj)
+        got = Hs.cpu().numpy()[ii, jj]
+        assert np.max(np.abs(got - ref)) <= TOL * np.sqrt(nb) * np.abs(ref).max() + 1e-300
