@@ -261,6 +261,65 @@ int skgemm_batch_dev(const skgemm_batch_item_t* items, int n, void* stream);
 int skgemm_batch_schedule(const skgemm_batch_item_t* items, int n, int tile, int order,
                           int* perm_out, int64_t* iter_begin_out, double* efficiency_out);
 
+/* ------------------------------------------------------------- serving */
+/* A serving engine for subspace requests: each request is the sequence
+ * S = Psi^T Psi (SYRK), Hs = Psi^T (H Psi) (GEMM), Psi' = Psi Q (rotation) on
+ * its own Psi, H Psi and Q, which stay resident on the device across the
+ * three steps. Requests are admitted in arrival order when a contiguous block
+ * of the HBM budget is free for all their buffers; admitted requests overlap
+ * on the device (native FP64: continuous batching of the ready steps of all
+ * admitted requests into grouped persistent launches; Ozaki: concurrent
+ * request streams). Inputs are synthetic and seeded: Psi and H Psi entries
+ * N(0,1)/sqrt(Ng), Q entries uniform[-1,1], each a pure function of
+ * (seed, index), so a request's result does not depend on what else runs.
+ * No counterpart in the reference. */
+typedef struct skgemm_serve_request {
+  int64_t Ng;       /* grid points, multiple of 16 */
+  int64_t nb;       /* states, multiple of 16 (<= 2048 for Ozaki) */
+  double arrival_s; /* arrival time, seconds after the start of the run */
+  uint64_t seed;
+  /* Optional host copies (NULL = not kept): results S (nb*nb column-major,
+   * upper triangle valid), Hs (nb*nb row-major), Psi' (band-packed Ng x nb),
+   * and the inputs Psi (band-packed), H Psi (packed32), Q (row-major). */
+  double* S_out;
+  double* Hs_out;
+  double* Psi_out;
+  double* Psi_in_out;
+  double* HPsi_in_out;
+  double* Q_in_out;
+  double admit_s; /* out: admission time */
+  double done_s;  /* out: completion time (device clock, CUDA events) */
+} skgemm_serve_request_t;
+
+typedef struct skgemm_serve_options {
+  int precision;           /* SKGEMM_PREC_NATIVE or SKGEMM_PREC_OZAKI_I8 */
+  int slices;              /* Ozaki moduli, 0 = automatic */
+  double hbm_budget_bytes; /* request data + engine scratch; 0 = 150e9 */
+  int max_inflight;        /* native: admitted requests at once (0 = 64) */
+  int ozaki_streams;       /* Ozaki: concurrent request streams (0 = 2) */
+  double max_batch_tflop;  /* native: work cap of one grouped launch (0 = 2 TFLOP) */
+  int realtime;            /* 1: release requests at arrival_s (wall clock); 0: all at 0 */
+  /* skgemm_serve_simulate only: throughput model (0 = defaults) */
+  double sim_native_tflops, sim_ozaki_tflops, sim_gen_gbs;
+  /* out */
+  double makespan_s;          /* last completion */
+  double flop;                /* S: nb^2 Ng, Hs: 2 nb^2 Ng, rotation: 2 Ng nb^2 */
+  int batches;                /* grouped launches (native) */
+  double mean_batch_problems; /* problems per grouped launch */
+  double peak_admitted_bytes; /* peak request data held */
+  double scratch_bytes;       /* engine scratch counted against the budget */
+} skgemm_serve_options_t;
+
+/* Runs `n` requests to completion on the current device (blocking). */
+int skgemm_serve_run(skgemm_serve_request_t* reqs, int n, skgemm_serve_options_t* opts);
+/* Same scheduler on a virtual clock with a throughput model instead of the
+ * GPU (no device needed): admission, batching and latency accounting. */
+int skgemm_serve_simulate(skgemm_serve_request_t* reqs, int n, skgemm_serve_options_t* opts);
+
+/* Releases the per-stream scratch the library keeps for `stream` (Stream-K
+ * partial slots, Ozaki residue buffers); synchronises the stream first. */
+int skgemm_stream_release(void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@
 #include <string>
 #include <vector>
 
+#include "skg_batch.h"
 #include "skg_fp64_types.h"
 #include "skg_runtime.h"
 
@@ -164,26 +165,27 @@ int grid_cap(DeviceState* dev, int tile, int* cap) {
   return SKGEMM_OK;
 }
 
-// Builds the device-side problem table, descriptors and workspace of
-// configuration `c` (synchronous uploads; not during stream capture).
-int configure(BatchPlan* P, Config c) {
-  const int BM = c.tile, BN = c.tile;
-  const int n = (int)P->probs.size();
-  std::vector<Geom> geo(n);
-  for (int i = 0; i < n; ++i) geo[i] = geom_of(P->probs[i], BM, BN);
-  const std::vector<int> perm = make_order(geo, c.order);
+}  // namespace
 
-  std::vector<Fp64Params> hp;
-  std::vector<CUtensorMap> hm;
-  std::vector<int64_t> hb;
-  hp.reserve(n);
-  hm.reserve(2 * n);
-  hb.push_back(0);
-  double useful = 0.0, issued = 0.0;
+// Host tables of one grouped launch: problems with work in the given order,
+// their TMA descriptors for `tile` x `tile` output tiles and the iteration
+// prefix.
+int build_group_tables(const std::vector<Fp64Problem>& probs, int tile, int order,
+                       GroupTables* T) {
+  const int n = (int)probs.size();
+  std::vector<Geom> geo(n);
+  for (int i = 0; i < n; ++i) geo[i] = geom_of(probs[i], tile, tile);
+  const std::vector<int> perm = make_order(geo, order);
+  T->params.clear();
+  T->maps.clear();
+  T->iter_begin.assign(1, 0);
+  T->params.reserve(n);
+  T->maps.reserve(2 * n);
+  T->useful = T->issued = 0.0;
   for (int idx : perm) {
     const Geom& g = geo[idx];
     if (g.iters == 0) continue;
-    const Fp64Problem& pr = P->probs[idx];
+    const Fp64Problem& pr = probs[idx];
     Fp64Params q;
     memset(&q, 0, sizeof(q));
     q.M = pr.M;
@@ -203,20 +205,48 @@ int configure(BatchPlan* P, Config c) {
     q.alpha = pr.alpha;
     q.gamma = pr.gamma;
     q.beta_zero = pr.beta_zero ? 1 : 0;
-    hp.push_back(q);
+    T->params.push_back(q);
     CUtensorMap ma, mb;
     int st;
-    if ((st = make_operand_map(&ma, pr.a, pr.K, BM)) != SKGEMM_OK) return st;
-    if ((st = make_operand_map(&mb, pr.b, pr.K, BN)) != SKGEMM_OK) return st;
-    hm.push_back(ma);
-    hm.push_back(mb);
-    hb.push_back(hb.back() + g.iters);
-    useful += g.useful;
-    issued += g.issued;
+    if ((st = make_operand_map(&ma, pr.a, pr.K, tile)) != SKGEMM_OK) return st;
+    if ((st = make_operand_map(&mb, pr.b, pr.K, tile)) != SKGEMM_OK) return st;
+    T->maps.push_back(ma);
+    T->maps.push_back(mb);
+    T->iter_begin.push_back(T->iter_begin.back() + g.iters);
+    T->useful += g.useful;
+    T->issued += g.issued;
   }
+  if (T->iter_begin.back() > ((int64_t)1 << 40))
+    return fail(SKGEMM_ERR_INVALID_ARG, "batch too large");
+  return SKGEMM_OK;
+}
+
+// Cost-model tile choice: issued MACs (padding included) at a per-shape
+// rate; 64 x 64 tiles carry more staging per MAC, rated 0.9 of 128 x 128.
+int model_tile(const std::vector<Fp64Problem>& probs) {
+  double i128 = 0.0, i64 = 0.0;
+  for (const auto& pr : probs) {
+    i128 += geom_of(pr, 128, 128).issued;
+    i64 += geom_of(pr, 64, 64).issued;
+  }
+  return (i64 / 0.9 < i128) ? 64 : 128;
+}
+
+namespace {
+
+// Builds the device-side problem table, descriptors and workspace of
+// configuration `c` (synchronous uploads; not during stream capture).
+int configure(BatchPlan* P, Config c) {
+  const int BM = c.tile, BN = c.tile;
+  GroupTables T;
+  int st0 = build_group_tables(P->probs, c.tile, c.order, &T);
+  if (st0) return st0;
+  std::vector<Fp64Params>& hp = T.params;
+  std::vector<CUtensorMap>& hm = T.maps;
+  std::vector<int64_t>& hb = T.iter_begin;
+  const double useful = T.useful, issued = T.issued;
   const int np = (int)hp.size();
   const int64_t total = hb.back();
-  if (total > ((int64_t)1 << 40)) return fail(SKGEMM_ERR_INVALID_ARG, "batch too large");
   int cap = 0, st;
   if ((st = grid_cap(P->dev, c.tile, &cap)) != SKGEMM_OK) return st;
   int grid = c.grid > 0 ? std::min(c.grid, cap) : cap;
@@ -380,21 +410,16 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
       cands.push_back(c);
     }
   }
-  // Cost model: issued MACs (padding included) at a per-tile-shape rate;
-  // 64 x 64 tiles carry more staging per MAC, rated 0.9 of 128 x 128.
-  auto model_cost = [&](const Config& c) {
-    double issued = 0.0;
-    for (const auto& pr : P->probs) issued += geom_of(pr, c.tile, c.tile).issued;
-    return issued / (c.tile == 128 ? 1.0 : 0.9);
-  };
+  // Cost model (model_tile): the tile with fewer issued MACs per unit rate;
+  // most-work-first order.
   Config best = cands[0];
-  double best_cost = 1e300;
-  for (const auto& c : cands) {
-    const double cost = model_cost(c);
-    if (cost < best_cost) {
-      best_cost = cost;
-      best = c;
-    }
+  {
+    const int mt = model_tile(P->probs);
+    for (const auto& c : cands)
+      if (c.tile == mt) {
+        best = c;
+        break;
+      }
   }
   float best_ms = 0.f;
   int timed = 0;
@@ -534,6 +559,146 @@ int batch_consume_error(DeviceState* dev, cudaStream_t s) {
   auto f = g_oneshot.find({dev->device, s});
   if (f == g_oneshot.end() || !f->second) return SKGEMM_OK;
   return read_err(f->second);
+}
+
+// ---------------------------------------------------------------- ring
+// A ring of grouped-launch workspaces: submission i uses slot i % depth, so a
+// launch's tables and partial slots stay untouched until `depth` later
+// submissions. Tables travel through pinned host memory with
+// cudaMemcpyAsync on the launch stream (no host-side synchronisation unless
+// the slot's previous launch is still running).
+struct GroupRing {
+  struct Slot {
+    DeviceBuffer probs, maps, iters, part, flags, err;
+    void* host = nullptr;  // pinned staging of the three tables
+    size_t host_bytes = 0;
+    cudaEvent_t ev = nullptr;
+    bool pending = false;
+  };
+  DeviceState* dev = nullptr;
+  std::vector<Slot> slots;
+  int next = 0;
+};
+
+GroupRing* group_ring_create(DeviceState* dev, int depth) {
+  GroupRing* R = new GroupRing();
+  R->dev = dev;
+  R->slots.resize(depth < 1 ? 1 : depth);
+  return R;
+}
+
+void group_ring_destroy(GroupRing* R) {
+  if (!R) return;
+  for (auto& sl : R->slots) {
+    if (sl.ev) {
+      cudaEventSynchronize(sl.ev);
+      cudaEventDestroy(sl.ev);
+    }
+    if (sl.host) cudaFreeHost(sl.host);
+    sl.probs.release();
+    sl.maps.release();
+    sl.iters.release();
+    sl.part.release();
+    sl.flags.release();
+    sl.err.release();
+  }
+  delete R;
+}
+
+int group_ring_reserve(GroupRing* R, int max_problems) {
+  if (!R) return fail(SKGEMM_ERR_INVALID_ARG, "null group ring");
+  int cap128 = 0, cap64 = 0, st;
+  if ((st = grid_cap(R->dev, 128, &cap128)) || (st = grid_cap(R->dev, 64, &cap64))) return st;
+  const size_t part = std::max((size_t)cap128 * 128 * 128, (size_t)cap64 * 64 * 64) * 8;
+  const int grid = std::max(cap128, cap64);
+  for (auto& sl : R->slots) {
+    if ((st = sl.probs.ensure((size_t)max_problems * sizeof(Fp64Params)))) return st;
+    if ((st = sl.maps.ensure((size_t)2 * max_problems * sizeof(CUtensorMap)))) return st;
+    if ((st = sl.iters.ensure((size_t)(max_problems + 1) * sizeof(int64_t)))) return st;
+    if ((st = sl.part.ensure(part))) return st;
+    if ((st = sl.flags.ensure((size_t)grid * sizeof(uint32_t)))) return st;
+    if (!sl.err.ptr) {
+      if ((st = sl.err.ensure(sizeof(uint32_t)))) return st;
+      SKG_CUDA(cudaMemset(sl.err.ptr, 0, sizeof(uint32_t)));
+    }
+    if (!sl.ev) SKG_CUDA(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
+  }
+  return SKGEMM_OK;
+}
+
+int group_ring_submit(GroupRing* R, const std::vector<Fp64Problem>& probs, cudaStream_t s,
+                      int* tile_out) {
+  if (!R || R->slots.empty()) return fail(SKGEMM_ERR_INVALID_ARG, "null group ring");
+  GroupRing::Slot& sl = R->slots[R->next];
+  R->next = (R->next + 1) % (int)R->slots.size();
+  if (sl.pending) {
+    SKG_CUDA(cudaEventSynchronize(sl.ev));
+    sl.pending = false;
+  }
+  const int tile = model_tile(probs);
+  GroupTables T;
+  int st = build_group_tables(probs, tile, 2, &T);
+  if (st) return st;
+  const int np = (int)T.params.size();
+  if ((st = group_ring_reserve(R, np > 0 ? np : 1))) return st;
+  Fp64Group g;
+  memset(&g, 0, sizeof(g));
+  if (np > 0) {
+    const size_t bp = (size_t)np * sizeof(Fp64Params), bm = 2 * (size_t)np * sizeof(CUtensorMap),
+                 bi = (size_t)(np + 1) * sizeof(int64_t);
+    const size_t om = (bp + 63) / 64 * 64, oi = om + bm, need = oi + bi;
+    if (sl.host_bytes < need) {
+      if (sl.host) cudaFreeHost(sl.host);
+      sl.host = nullptr;
+      sl.host_bytes = 0;
+      SKG_CUDA(cudaMallocHost(&sl.host, need));
+      sl.host_bytes = need;
+    }
+    char* h = (char*)sl.host;
+    memcpy(h, T.params.data(), bp);
+    memcpy(h + om, T.maps.data(), bm);
+    memcpy(h + oi, T.iter_begin.data(), bi);
+    SKG_CUDA(cudaMemcpyAsync(sl.probs.ptr, h, bp, cudaMemcpyHostToDevice, s));
+    SKG_CUDA(cudaMemcpyAsync(sl.maps.ptr, h + om, bm, cudaMemcpyHostToDevice, s));
+    SKG_CUDA(cudaMemcpyAsync(sl.iters.ptr, h + oi, bi, cudaMemcpyHostToDevice, s));
+    int cap = 0;
+    if ((st = grid_cap(R->dev, tile, &cap))) return st;
+    g.probs = (const Fp64Params*)sl.probs.ptr;
+    g.maps = (const CUtensorMap*)sl.maps.ptr;
+    g.iter_begin = (const int64_t*)sl.iters.ptr;
+    g.num_problems = np;
+    g.total_iters = T.iter_begin.back();
+    g.grid = (int)std::min<int64_t>(cap, g.total_iters);
+    g.workspace = (double*)sl.part.ptr;
+    g.flags = (uint32_t*)sl.flags.ptr;
+    g.err = (uint32_t*)sl.err.ptr;
+    if ((st = launch_fp64_group(tile, g, s))) return st;
+  }
+  for (const auto& pr : probs)
+    if (pr.M > 0 && pr.N > 0 && pr.K == 0 && pr.out_kind != kOutBand16)
+      if ((st = run_k0(pr.out_kind, pr.M, pr.N, pr.D, pr.ldd, pr.gamma, pr.beta_zero, s)))
+        return st;
+  SKG_CUDA(cudaEventRecord(sl.ev, s));
+  sl.pending = true;
+  if (tile_out) *tile_out = tile;
+  return SKGEMM_OK;
+}
+
+int group_ring_error(GroupRing* R) {
+  if (!R) return SKGEMM_OK;
+  for (auto& sl : R->slots) {
+    if (!sl.err.ptr) continue;
+    uint32_t word = 0;
+    SKG_CUDA(cudaMemcpy(&word, sl.err.ptr, sizeof(word), cudaMemcpyDeviceToHost));
+    if (word) {
+      SKG_CUDA(cudaMemset(sl.err.ptr, 0, sizeof(uint32_t)));
+      char buf[120];
+      snprintf(buf, sizeof(buf), "grouped launch: device-side wait ran past its budget (0x%x)",
+               word);
+      return fail(SKGEMM_ERR_DEVICE_TIMEOUT, buf);
+    }
+  }
+  return SKGEMM_OK;
 }
 
 }  // namespace skg

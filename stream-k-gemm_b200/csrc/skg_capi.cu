@@ -318,6 +318,27 @@ SKG_EXPORT int skgemm_stream_status(void* stream) {
   return ozaki_consume_error(dev, s);
 }
 
+SKG_EXPORT int skgemm_stream_release(void* stream) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  SKG_CUDA(cudaStreamSynchronize(s));
+  {
+    std::lock_guard<std::mutex> lk(dev->mu);
+    auto it = dev->ws.find(s);
+    if (it != dev->ws.end()) {
+      StreamWorkspace* ws = it->second;
+      if (ws->partials) cudaFree(ws->partials);
+      if (ws->flags) cudaFree(ws->flags);
+      if (ws->err) cudaFree(ws->err);
+      delete ws;
+      dev->ws.erase(it);
+    }
+  }
+  return ozaki_release_stream(dev, s);
+}
+
 SKG_EXPORT int skgemm_probe_fp64_peak(double* tflops_out) {
   int st;
   DeviceState* dev = current_device(&st);

@@ -819,6 +819,167 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
 
 }  // namespace
 
+namespace {
+
+// Scratch of one stream's Ozaki calls, per buffer of OzakiStream.
+struct OzakiNeed {
+  size_t res_a = 0, res_b = 0, part_a = 0, part_b = 0, mu_a = 0, mu_b = 0, partials = 0,
+         rbytes = 0;
+  void max_with(const OzakiNeed& o) {
+    res_a = std::max(res_a, o.res_a);
+    res_b = std::max(res_b, o.res_b);
+    part_a = std::max(part_a, o.part_a);
+    part_b = std::max(part_b, o.part_b);
+    mu_a = std::max(mu_a, o.mu_a);
+    mu_b = std::max(mu_b, o.mu_b);
+    partials = std::max(partials, o.partials);
+    rbytes = std::max(rbytes, o.rbytes);
+  }
+  size_t total() const { return res_a + res_b + part_a + part_b + mu_a + mu_b + partials + rbytes; }
+};
+
+size_t norm_part_bytes(int64_t R, int T) {
+  const int64_t P_in = (R + T - 1) / T;
+  const int64_t C = std::max<int64_t>(1, std::min<int64_t>(64, (600 + P_in - 1) / P_in));
+  return (size_t)P_in * C * T * sizeof(double);
+}
+
+// Tiles and segment slots of the lane plan of (M, N, KB, L) (the counting
+// part of get_lane_plan).
+void lane_counts(int num_sms, int M, int N, int KB, int L, bool syrk, int seg_cap, int* T_out,
+                 int* slots_out) {
+  const int tiles_m = (M + kI8BM - 1) / kI8BM, tiles_n = (N + kI8BN - 1) / kI8BN;
+  int T = 0;
+  for (int tm = 0; tm < tiles_m; ++tm)
+    for (int tn = 0; tn < tiles_n; ++tn)
+      if (!(syrk && tm * kI8BM > tn * kI8BN + kI8BN - 1)) ++T;
+  int Q = std::max(1, num_sms / T);
+  const int64_t W = (int64_t)L * KB;
+  if (Q > W) Q = (int)W;
+  int slots = 0;
+  for (int q = 0; q < Q; ++q) {
+    int64_t it = (int64_t)q * W / Q, end = (int64_t)(q + 1) * W / Q;
+    while (it < end) {
+      const int l = (int)(it / KB);
+      int64_t stop = std::min<int64_t>(end, (int64_t)(l + 1) * KB);
+      stop = std::min<int64_t>(stop, it + seg_cap);
+      ++slots;
+      it = stop;
+    }
+  }
+  *T_out = T;
+  *slots_out = slots;
+}
+
+OzakiNeed need_lanes(DeviceState* dev, int64_t M, int64_t N, int64_t K, int L, bool syrk) {
+  OzakiNeed n;
+  const int64_t KP = (K + 127) / 128 * 128;
+  const int KB = (int)(KP / 128);
+  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
+  const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
+  n.res_a = (size_t)L * RA * KP;
+  n.part_a = norm_part_bytes(M, 16);
+  n.mu_a = (size_t)RA * sizeof(int);
+  if (!syrk) {
+    n.res_b = (size_t)L * RB * KP;
+    n.part_b = norm_part_bytes(N, 32);
+    n.mu_b = (size_t)RB * sizeof(int);
+  }
+  int T = 0, slots = 0;
+  lane_counts(dev->num_sms, (int)M, (int)N, KB, L, syrk, kSegKbCapSigned, &T, &slots);
+  n.partials = (size_t)slots * T * kI8BM * kI8BN * sizeof(int32_t);
+  return n;
+}
+
+OzakiNeed need_rot(int64_t Nd, int64_t nb, int L) {
+  OzakiNeed n;
+  const int64_t KP = (nb + 127) / 128 * 128;
+  const int64_t RA = (Nd + kI8BM - 1) / kI8BM * kI8BM;
+  const int64_t RB = (nb + kI8BN - 1) / kI8BN * kI8BN;
+  n.res_a = (size_t)L * RA * KP;
+  n.res_b = (size_t)L * RB * KP;
+  n.mu_a = (size_t)RA * sizeof(int);
+  n.mu_b = (size_t)RB * sizeof(int);
+  n.rbytes = (size_t)L * Nd * nb;
+  return n;
+}
+
+}  // namespace
+
+// Scratch a stream needs for Ozaki calls of `op` (SKGEMM_OP_*) on the given
+// shape (GEMM: M, N, K; SYRK: M, K; rotation: Nd = M, nb = N) with `slices`
+// moduli (0 = the automatic choice).
+int ozaki_scratch_bytes(DeviceState* dev, int op, int64_t M, int64_t N, int64_t K, int slices,
+                        size_t* bytes) {
+  skgemm_options_t o;
+  memset(&o, 0, sizeof(o));
+  o.precision = SKGEMM_PREC_OZAKI_I8;
+  o.slices = slices;
+  int L, gb, st;
+  OzakiNeed n;
+  if (op == SKGEMM_OP_ROT) {
+    if ((st = choose_L(&o, N, &L, &gb))) return st;
+    n = need_rot(M, N, L);
+  } else {
+    if ((st = choose_L(&o, K, &L, &gb))) return st;
+    n = need_lanes(dev, M, op == SKGEMM_OP_SYRK_PACKED ? M : N, K, L,
+                   op == SKGEMM_OP_SYRK_PACKED);
+  }
+  *bytes = n.total();
+  return SKGEMM_OK;
+}
+
+// Grows stream `s`'s Ozaki scratch to serve every call of the three ops on
+// shapes up to (Nd, nb) with `slices` moduli without allocating later.
+int ozaki_reserve(DeviceState* dev, cudaStream_t s, int64_t Nd, int64_t nb, int slices) {
+  skgemm_options_t o;
+  memset(&o, 0, sizeof(o));
+  o.precision = SKGEMM_PREC_OZAKI_I8;
+  o.slices = slices;
+  int Lk, Lr, gb, st;
+  if ((st = choose_L(&o, Nd, &Lk, &gb))) return st;
+  if ((st = choose_L(&o, nb, &Lr, &gb))) return st;
+  OzakiNeed n = need_lanes(dev, nb, nb, Nd, Lk, false);
+  n.max_with(need_lanes(dev, nb, nb, Nd, Lk, true));
+  n.max_with(need_rot(Nd, nb, Lr));
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  if ((st = ensure_consts(dev))) return st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  OzakiStream* os = ozaki_stream(dev, s);
+  if ((st = os->res_a.ensure(n.res_a)) || (st = os->res_b.ensure(n.res_b)) ||
+      (st = os->part_a.ensure(n.part_a)) || (st = os->part_b.ensure(n.part_b)) ||
+      (st = os->mu_a.ensure(n.mu_a)) || (st = os->mu_b.ensure(n.mu_b)) ||
+      (st = os->partials.ensure(n.partials)) || (st = os->rbytes.ensure(n.rbytes)))
+    return st;
+  return SKGEMM_OK;
+}
+
+// Frees stream `s`'s Ozaki buffers (the stream has been synchronised).
+int ozaki_release_stream(DeviceState* dev, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  auto& m = g_oz[dev->device].streams;
+  auto it = m.find(s);
+  if (it == m.end()) return SKGEMM_OK;
+  OzakiStream* os = it->second;
+  for (DeviceBuffer* b : {&os->res_a, &os->res_b, &os->part_a, &os->part_b, &os->mu_a, &os->mu_b,
+                          &os->partials, &os->rbytes})
+    b->release();
+  delete os;
+  m.erase(it);
+  return SKGEMM_OK;
+}
+
+// Bytes of device scratch stream `s` holds for the Ozaki path.
+size_t ozaki_stream_bytes(DeviceState* dev, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  auto it = g_oz[dev->device].streams.find(s);
+  if (it == g_oz[dev->device].streams.end()) return 0;
+  const OzakiStream* os = it->second;
+  return os->res_a.bytes + os->res_b.bytes + os->part_a.bytes + os->part_b.bytes +
+         os->mu_a.bytes + os->mu_b.bytes + os->partials.bytes + os->rbytes.bytes;
+}
+
 int ozaki_gemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp,
                       double* D, int64_t ldd, double alpha, double gamma,
                       skgemm_options_t* opts, cudaStream_t s) {

@@ -19,5 +19,10 @@ int ozaki_consume_error(DeviceState* dev, cudaStream_t s);
 int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, const int8_t* B,
              int64_t ldb, int32_t* C, int64_t ldc, cudaStream_t s);
 int probe_i8_peak(DeviceState* dev, double* tops);
+int ozaki_scratch_bytes(DeviceState* dev, int op, int64_t M, int64_t N, int64_t K, int slices,
+                        size_t* bytes);
+int ozaki_reserve(DeviceState* dev, cudaStream_t s, int64_t Nd, int64_t nb, int slices);
+size_t ozaki_stream_bytes(DeviceState* dev, cudaStream_t s);
+int ozaki_release_stream(DeviceState* dev, cudaStream_t s);
 
 }  // namespace skg

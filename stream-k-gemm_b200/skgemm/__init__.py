@@ -74,6 +74,27 @@ class PlanOptions(ctypes.Structure):
                 ("tuned_ms_out", ctypes.c_double), ("model_efficiency_out", ctypes.c_double)]
 
 
+class ServeRequest(ctypes.Structure):
+    """skgemm_serve_request_t."""
+    _fields_ = [("Ng", ctypes.c_int64), ("nb", ctypes.c_int64), ("arrival_s", ctypes.c_double),
+                ("seed", ctypes.c_uint64), ("S_out", ctypes.c_void_p), ("Hs_out", ctypes.c_void_p),
+                ("Psi_out", ctypes.c_void_p), ("Psi_in_out", ctypes.c_void_p),
+                ("HPsi_in_out", ctypes.c_void_p), ("Q_in_out", ctypes.c_void_p),
+                ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+class ServeOptions(ctypes.Structure):
+    """skgemm_serve_options_t."""
+    _fields_ = [("precision", ctypes.c_int), ("slices", ctypes.c_int),
+                ("hbm_budget_bytes", ctypes.c_double), ("max_inflight", ctypes.c_int),
+                ("ozaki_streams", ctypes.c_int), ("max_batch_tflop", ctypes.c_double),
+                ("realtime", ctypes.c_int), ("sim_native_tflops", ctypes.c_double),
+                ("sim_ozaki_tflops", ctypes.c_double), ("sim_gen_gbs", ctypes.c_double),
+                ("makespan_s", ctypes.c_double), ("flop", ctypes.c_double),
+                ("batches", ctypes.c_int), ("mean_batch_problems", ctypes.c_double),
+                ("peak_admitted_bytes", ctypes.c_double), ("scratch_bytes", ctypes.c_double)]
+
+
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 _d = ctypes.c_double
@@ -107,6 +128,11 @@ _SIGS = {
     "skgemm_plan_run": [_vp, _vp],
     "skgemm_plan_status": [_vp, _vp],
     "skgemm_batch_dev": [ctypes.POINTER(BatchItem), ctypes.c_int, _vp],
+    "skgemm_serve_run": [ctypes.POINTER(ServeRequest), ctypes.c_int,
+                         ctypes.POINTER(ServeOptions)],
+    "skgemm_serve_simulate": [ctypes.POINTER(ServeRequest), ctypes.c_int,
+                              ctypes.POINTER(ServeOptions)],
+    "skgemm_stream_release": [_vp],
     "skgemm_batch_schedule": [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_int,
                               ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                               ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)],
@@ -373,3 +399,53 @@ def batch_schedule(items, tile=128, order=1):
     _check(lib().skgemm_batch_schedule(_item_array(items), n, tile, order, perm, ib,
                                        ctypes.byref(eff)))
     return list(perm)[:n], list(ib), eff.value
+
+
+# ------------------------------------------------------------------ serving
+def serve_trace(n, rate=200.0, ng_range=(1e4, 4e5), nb_range=(32, 2048), seed=0):
+    """Poisson arrivals (rate per second) of subspace requests with Ng and nb
+    log-uniform in the given ranges, rounded to multiples of 16 (the packed
+    layouts' granule); returns a list of (arrival_s, Ng, nb, seed)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    ng = np.exp(rng.uniform(np.log(ng_range[0]), np.log(ng_range[1]), size=n))
+    nb = np.exp(rng.uniform(np.log(nb_range[0]), np.log(nb_range[1]), size=n))
+    ng = np.maximum(16, np.round(ng / 16) * 16).astype(np.int64)
+    nb = np.maximum(16, np.round(nb / 16) * 16).astype(np.int64)
+    return [(float(t[i]), int(ng[i]), int(nb[i]), int(seed * 1000003 + i)) for i in range(n)]
+
+
+def serve(trace, precision=PREC_NATIVE, slices=0, hbm_budget=150e9, max_inflight=0,
+          ozaki_streams=0, max_batch_tflop=0.0, realtime=True, simulate=False, keep=None,
+          sim=(0.0, 0.0, 0.0)):
+    """Runs (or simulates) a request trace; returns (per-request rows, options).
+
+    ``keep``: optional dict index -> dict of host numpy buffers to fill
+    (keys S, Hs, Psi, Psi_in, HPsi_in, Q)."""
+    n = len(trace)
+    reqs = (ServeRequest * max(1, n))()
+    hold = []
+    for i, (t, ng, nb, sd) in enumerate(trace):
+        r = reqs[i]
+        r.Ng, r.nb, r.arrival_s, r.seed = ng, nb, t, sd
+        if keep and i in keep:
+            k = keep[i]
+            for key, field in (("S", "S_out"), ("Hs", "Hs_out"), ("Psi", "Psi_out"),
+                               ("Psi_in", "Psi_in_out"), ("HPsi_in", "HPsi_in_out"),
+                               ("Q", "Q_in_out")):
+                if key in k:
+                    setattr(r, field, _hptr(k[key], True))
+                    hold.append(k[key])
+    o = ServeOptions()
+    o.precision, o.slices, o.hbm_budget_bytes = precision, slices, hbm_budget
+    o.max_inflight, o.ozaki_streams, o.max_batch_tflop = max_inflight, ozaki_streams, max_batch_tflop
+    o.realtime = 1 if realtime else 0
+    o.sim_native_tflops, o.sim_ozaki_tflops, o.sim_gen_gbs = sim
+    f = lib().skgemm_serve_simulate if simulate else lib().skgemm_serve_run
+    _check(f(reqs, n, ctypes.byref(o)))
+    rows = [(trace[i][0] if realtime else 0.0, reqs[i].admit_s, reqs[i].done_s) for i in range(n)]
+    return rows, o
+
+
+def stream_release(stream=None) -> None:
+    _check(lib().skgemm_stream_release(_stream(stream)))

@@ -1,0 +1,122 @@
+"""GPU tests of the serving engine (skgemm_serve_run through the C ABI).
+
+Each request's results are the same alone and in the mix: native FP64 within
+relative Frobenius error 1e-13 (a request's grouped launch shares its
+Stream-K split with whatever else is batched, so the summation order of a
+tile's partials can differ), the Ozaki path bitwise (its schedule depends
+only on the request's own shape). Results also match the Dot2 oracle on the
+request's own inputs within 1e-13, and admission holds the HBM budget."""
+import numpy as np
+import pytest
+
+import oracle
+import skgemm
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13
+NATIVE, OZAKI = skgemm.PREC_NATIVE, skgemm.PREC_OZAKI_I8
+BUDGET = 4e9
+
+
+def small_trace(n, seed, gap=0.001):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        ng = 16 * int(np.exp(rng.uniform(np.log(64), np.log(1024))))
+        nb = 16 * int(rng.integers(2, 17))
+        out.append((i * gap, ng, nb, 7919 * seed + i))
+    return out
+
+
+def buffers(ng, nb):
+    nb32 = (nb + 31) // 32 * 32
+    return {"S": np.zeros(nb * nb), "Hs": np.zeros(nb * nb), "Psi": np.zeros(ng * nb),
+            "Psi_in": np.zeros(ng * nb), "HPsi_in": np.zeros(ng * nb32), "Q": np.zeros(nb * nb)}
+
+
+def run(trace, precision, **kw):
+    keep = {i: buffers(t[1], t[2]) for i, t in enumerate(trace)}
+    rows, o = skgemm.serve(trace, precision=precision, hbm_budget=kw.pop("budget", BUDGET),
+                           keep=keep, **kw)
+    return keep, rows, o
+
+
+def upper(S, nb):
+    C = S.reshape(nb, nb)  # row j = column j of column-major C
+    iu = np.triu_indices(nb)
+    return C[iu[1], iu[0]]
+
+
+def check_oracle(k, ng, nb):
+    X = oracle.band_unpack(k["Psi_in"].reshape(nb // 16, ng, 16), ng)        # (Ng, nb)
+    Y = _unpack32(k["HPsi_in"], ng, nb)                                     # (Ng, nb)
+    Q = k["Q"].reshape(nb, nb)
+    S_ref = oracle.dot2_matmul(X.T, X)
+    assert oracle.rel_frobenius(upper(k["S"], nb), S_ref[np.triu_indices(nb)]) <= TOL
+    assert oracle.rel_frobenius(k["Hs"].reshape(nb, nb), oracle.dot2_matmul(X.T, Y)) <= TOL
+    P = oracle.band_unpack(k["Psi"].reshape(nb // 16, ng, 16), ng)
+    assert oracle.rel_frobenius(P, oracle.dot2_matmul(X, Q)) <= TOL
+
+
+def _unpack32(buf, ng, nb):
+    """packed32 [ceil(nb/32)][Ng][32] -> (Ng, nb)."""
+    nb32 = (nb + 31) // 32 * 32
+    P = buf.reshape(nb32 // 32, ng, 32)
+    return np.concatenate(list(P), axis=1)[:, :nb]
+
+
+@pytest.mark.parametrize("precision", [NATIVE, OZAKI])
+def test_serve_results_same_alone_and_in_mix(cuda, precision):
+    trace = small_trace(10, seed=1)
+    mix, rows, o = run(trace, precision, realtime=False)
+    assert o.makespan_s > 0 and o.flop > 0
+    if precision == NATIVE:
+        assert o.batches >= 2 and o.mean_batch_problems > 2  # requests shared launches
+    for i, (t, ng, nb, sd) in enumerate(trace):
+        alone, _, _ = run([(0.0, ng, nb, sd)], precision, realtime=False)
+        a, m = alone[0], mix[i]
+        for key in ("Psi_in", "HPsi_in", "Q"):
+            assert np.array_equal(a[key], m[key])  # seeded inputs
+        if precision == OZAKI:
+            # S: upper triangle only (the strict lower one is not written).
+            assert np.array_equal(upper(a["S"], nb), upper(m["S"], nb))
+            for key in ("Hs", "Psi"):
+                assert np.array_equal(a[key], m[key]), key
+        else:
+            assert oracle.rel_frobenius(upper(m["S"], nb), upper(a["S"], nb)) <= TOL
+            assert oracle.rel_frobenius(m["Hs"], a["Hs"]) <= TOL
+            assert oracle.rel_frobenius(m["Psi"], a["Psi"]) <= TOL
+        if i < 4:
+            check_oracle(m, ng, nb)
+
+
+def test_serve_budget_holds_and_results_unchanged(cuda):
+    trace = small_trace(8, seed=2)
+    sizes = []
+    for _, ng, nb, _ in trace:
+        al = lambda x: (x + 511) // 512 * 512
+        sizes.append(3 * al(ng * nb * 8) + al(ng * ((nb + 31) // 32 * 32) * 8) + 3 * al(nb * nb * 8))
+    budget = 100e6 + 1.2 * max(sizes)   # the engine's fixed scratch + about one request
+    tight, rows, o = run(trace, NATIVE, realtime=False, budget=budget)
+    assert o.peak_admitted_bytes <= budget - o.scratch_bytes
+    loose, _, _ = run(trace, NATIVE, realtime=False)
+    for i, (_, ng, nb, _) in enumerate(trace):
+        assert oracle.rel_frobenius(tight[i]["Psi"], loose[i]["Psi"]) <= TOL
+        assert oracle.rel_frobenius(tight[i]["Hs"], loose[i]["Hs"]) <= TOL
+
+
+@pytest.mark.parametrize("precision", [NATIVE, OZAKI])
+def test_serve_realtime_latencies(cuda, precision):
+    trace = small_trace(12, seed=3, gap=0.002)
+    rows, o = skgemm.serve(trace, precision=precision, hbm_budget=BUDGET, realtime=True)
+    arr = np.array([r[0] for r in rows])
+    adm = np.array([r[1] for r in rows])
+    done = np.array([r[2] for r in rows])
+    assert np.all(adm >= arr - 1e-9) and np.all(done > adm)
+    assert o.makespan_s == pytest.approx(done.max())
+
+
+def test_serve_rejects_oversized_request(cuda):
+    with pytest.raises(skgemm.SkgemmError) as e:
+        skgemm.serve([(0.0, 16000, 512, 1)], hbm_budget=200e6)
+    assert e.value.code == skgemm.ERR_OOM
