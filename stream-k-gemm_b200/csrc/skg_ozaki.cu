@@ -45,31 +45,21 @@ constexpr int kMinModuli = 6;
 constexpr int kSegKbCapSigned = 1023;   // 1023 * 128 * 2^14 < 2^31
 
 // Residue constants for one moduli count L (gamma depends on L). The scaled
-// integer X (|X| <= 2^gamma + 1/2) is handled as u = X + bias >= 0,
-// bias = 2^(gamma+1), so X mod m = (digit sum of u + e) mod m with
-// e = (-bias) mod m. Residues are symmetric (signed int8).
-// The first kIntModuli moduli (256, 255, 253) use the integer pipe: 19-bit
-// digits (u < 2^57) or 16-bit digits, S = d0 + e + d1 c1 + d2 c2 [+ d3 c3]
-// < 2^29, exact remainder by multiply-high. The others (odd) use exact FP32:
-// 12-bit digits f_j, S = f0 + e + sum_j f_j c_j < 2^23 (every product < 2^20),
-// q = rint(S * inv) with inv = 1/m rounded up, r = S - q m, which lies in
-// [-(m+1)/2, (m-1)/2] (the upward bias only ever rounds q up), a signed byte.
-constexpr int kIntModuli = 3;
+// integer X = rint(v 2^mu) (int64, |X| <= 2^gamma + 1/2) is cut into digits
+// X = d0 + d1 2^12 + d2 2^24 + d3 2^36 + d4 2^48, d0..d3 in [0, 4096) (the low
+// 48 bits of X) and d4 = floor(X / 2^48) signed (|d4| <= 2^12 for gamma <=
+// 60), so X = S (mod m) with S = d0 + sum_j d_j c_j, c_j = 2^(12 j) mod m. In
+// FP32 every product is below 2^20 and |S| < 2^22: all exact. For odd m,
+// q = rint(S fl(1/m)) equals rint(S / m): |S| |fl(1/m) - 1/m| < 2^22 2^-31 =
+// 2^-9 < 1/(2m), the least distance of S/m from a half-integer. Then
+// r = S - q m in [-(m-1)/2, (m-1)/2] is the symmetric residue, a signed byte,
+// read from the low mantissa byte of r + 1.5 2^23. m = 256: the low byte of X.
 struct ResidueConsts {
-  int ndig;         // integer digits: 3 of 19 bits (gamma <= 55) or 4 of 16 bits
-  int fdig;         // FP32 digits of 12 bits: 5 (gamma <= 57) or 6
   int gamma_bits;
-  long long bias;
-  uint32_t m[kI8MaxModuli];
-  uint32_t magic[kI8MaxModuli];  // floor(2^37 / m) + 1: exact remainder below 2^29
-  uint32_t c1[kI8MaxModuli];
-  uint32_t c2[kI8MaxModuli];
-  uint32_t c3[kI8MaxModuli];
-  uint32_t e[kI8MaxModuli];
-  float fc[6][kI8MaxModuli];     // 2^(12 j) mod m
-  float fe[kI8MaxModuli];
-  float finv[kI8MaxModuli];      // 1/m rounded up
-  float fm[kI8MaxModuli];
+  float c[4][kI8MaxModuli];  // 2^(12 (j+1)) mod m
+  float inv[kI8MaxModuli];   // fl(1/m)
+  float m[kI8MaxModuli];
+  uint32_t mi[kI8MaxModuli];
 };
 
 struct CrtConsts {  // for one moduli count L
@@ -157,104 +147,6 @@ __device__ __forceinline__ void pow2_pair(int mu, double& s1, double& s2) {
 constexpr int kTilePitch = 129;
 __device__ __forceinline__ int swz_k(int k) { return k ^ ((k >> 3) & 7); }
 
-// Biased scaled integer u = rint(v 2^mu) + bias (2^mu as two exact factors).
-__device__ __forceinline__ unsigned long long biased_int(double v, double s1, double s2,
-                                                         long long bias) {
-  return (unsigned long long)(__double2ll_rn((v * s1) * s2) + bias);
-}
-
-__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
-}
-
-__device__ __forceinline__ float u2f_exact(uint32_t x) {  // x < 2^23
-  return __uint_as_float(0x4B000000u | x) - 8388608.0f;
-}
-
-// Residues of the staged block: thread (r, kk) handles k = 8kk .. 8kk+7 of
-// row r and writes one 8-byte word per modulus; 16 consecutive threads write
-// one 128-byte row segment.
-template <int NDIG, int FDIG>
-__device__ __forceinline__ void emit_residues(const double* tileT, const double* s1,
-                                              const double* s2, int L, const ResidueConsts& rc,
-                                              uint8_t* res, int64_t row0, int64_t KP,
-                                              int64_t Rpad, int64_t k0) {
-  const int kk = threadIdx.x & 15, r = threadIdx.x >> 4;  // 256 threads: 16 rows x 16
-  uint32_t lo[8], hi[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const unsigned long long u =
-        biased_int(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r], rc.bias);
-    lo[j] = (uint32_t)u;
-    hi[j] = (uint32_t)(u >> 32);
-  }
-  uint8_t* dst = res + (row0 + r) * KP + k0 + 8 * kk;
-  uint32_t b[8];
-  // m = 256: the low byte of X = u - bias.
-#pragma unroll
-  for (int j = 0; j < 8; ++j) b[j] = lo[j] - (uint32_t)rc.bias;
-  *reinterpret_cast<uint2*>(dst) =
-      make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
-  // 255 and 253 on the integer pipe.
-  {
-    uint32_t d[8][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (NDIG == 3) {
-        d[j][0] = lo[j] & 0x7FFFFu;
-        d[j][1] = __funnelshift_r(lo[j], hi[j], 19) & 0x7FFFFu;
-        d[j][2] = hi[j] >> 6;
-        d[j][3] = 0;
-      } else {
-        d[j][0] = lo[j] & 0xFFFFu;
-        d[j][1] = lo[j] >> 16;
-        d[j][2] = hi[j] & 0xFFFFu;
-        d[j][3] = hi[j] >> 16;
-      }
-    }
-#pragma unroll
-    for (int l = 1; l < kIntModuli; ++l) {
-      const uint32_t m = rc.m[l], magic = rc.magic[l], e = rc.e[l], h = (m - 1) / 2;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        uint32_t S = d[j][0] + e + d[j][1] * rc.c1[l] + d[j][2] * rc.c2[l];
-        if (NDIG == 4) S += d[j][3] * rc.c3[l];
-        const uint32_t ru = mod_exact29(S, m, magic);
-        b[j] = ru > h ? ru + (256u - m) : ru;  // symmetric residue as a byte
-      }
-      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) =
-          make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
-    }
-  }
-  // Odd moduli on the FP32 pipe.
-  float f[8][FDIG];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    f[j][0] = u2f_exact(lo[j] & 0xFFFu);
-    f[j][1] = u2f_exact((lo[j] >> 12) & 0xFFFu);
-    f[j][2] = u2f_exact(__funnelshift_r(lo[j], hi[j], 24) & 0xFFFu);
-    f[j][3] = u2f_exact((hi[j] >> 4) & 0xFFFu);
-    f[j][4] = u2f_exact(FDIG == 5 ? (hi[j] >> 16) : ((hi[j] >> 16) & 0xFFFu));
-    if (FDIG == 6) f[j][FDIG - 1] = u2f_exact(hi[j] >> 28);
-  }
-  for (int l = kIntModuli; l < L; ++l) {
-    const float fe = rc.fe[l], inv = rc.finv[l], fm = rc.fm[l];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float S = f[j][0] + fe;
-#pragma unroll
-      for (int t = 1; t < FDIG; ++t) S = fmaf(f[j][t], rc.fc[t][l], S);
-      const float q = fmaf(S, inv, 12582912.0f) - 12582912.0f;  // rint(S * inv)
-      const float rr = fmaf(-q, fm, S);
-      b[j] = __float_as_uint(rr + 12582912.0f);  // low byte = rr mod 256
-    }
-    *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) =
-        make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
-  }
-}
-
-// Loads element (k, r) = src[k * ks + r] of the block (zero outside
-// k < K, r < rows_valid) into the staging tile.
 template <int T>
 __device__ __forceinline__ void stage_tile(double* tileT, const double* src, int64_t ks,
                                            int64_t k0, int64_t K, int rows_valid) {
@@ -263,6 +155,47 @@ __device__ __forceinline__ void stage_tile(double* tileT, const double* src, int
     const int64_t k = k0 + kk;
     tileT[r * kTilePitch + swz_k(kk)] = (k < K && r < rows_valid) ? src[k * ks + r] : 0.0;
   }
+}
+
+__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  return __byte_perm(__byte_perm(a, b, 0x0040), __byte_perm(c, d, 0x0040), 0x5410);
+}
+
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: integers below 2^22 sit in the low mantissa
+
+// Exact FP32 value of a 12-bit field (the bits 0x4B000000 | x are 2^23 + x).
+__device__ __forceinline__ float field12(uint32_t x) {
+  return __uint_as_float(0x4B000000u | (x & 0xFFFu)) - 8388608.0f;
+}
+
+// The five digits of X = rint((v s1) s2) as exact floats, and X's low word.
+struct Digits {
+  float f0, f1, f2, f3, f4;
+  uint32_t lo;
+};
+__device__ __forceinline__ Digits digits_of(double v, double s1, double s2) {
+  const long long X = __double2ll_rn((v * s1) * s2);
+  const uint32_t lo = (uint32_t)X, hi = (uint32_t)((unsigned long long)X >> 32);
+  Digits d;
+  d.lo = lo;  // m = 256: its low byte
+  d.f0 = field12(lo);
+  d.f1 = field12(lo >> 12);
+  d.f2 = field12(__funnelshift_r(lo, hi, 24));
+  d.f3 = field12(hi >> 4);
+  d.f4 = __int_as_float(0x4B400000 + ((int)hi >> 16)) - kMagic;  // signed d4
+  return d;
+}
+
+// Symmetric residue of the digits modulo odd kModuli[l], as the low byte of
+// the returned word.
+template <int L>
+__device__ __forceinline__ uint32_t residue_byte(const Digits& d, int l) {
+  const ResidueConsts& rc = c_res[L];
+  const float S = fmaf(d.f4, rc.c[3][l],
+                       fmaf(d.f3, rc.c[2][l], fmaf(d.f2, rc.c[1][l], fmaf(d.f1, rc.c[0][l], d.f0))));
+  const float q = fmaf(S, rc.inv[l], kMagic) - kMagic;
+  const float r = fmaf(-q, rc.m[l], S);
+  return __float_as_uint(r + kMagic);
 }
 
 // ------------------------------------------------- packed-T operand prep
@@ -294,41 +227,122 @@ __global__ void __launch_bounds__(256) norm_partials_kernel(int64_t R, int64_t K
 }
 
 // Residues of a packed-T operand -> res[l][Rpad][KP] (K-major bytes).
-// CTA (p, kb): rows p*T .. +T, k-block kb (128 k), converted in 16-row
-// sub-panels. mu of each row from the norm partials; CTAs with kb == 0 also
-// publish mu.
-template <int T, int NDIG, int FDIG>
-__global__ void __launch_bounds__(256) convert_packed_kernel(
-    int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ X, int C,
-    const double* __restrict__ part, int L, uint8_t* __restrict__ res,
-    int* __restrict__ mu_out) {
-  __shared__ double tileT[16 * kTilePitch];
-  __shared__ double s1[T], s2[T];
-  const ResidueConsts& rc = c_res[L];
-  const int p = blockIdx.x, kb = blockIdx.y;
-  const int64_t P_in = (R + T - 1) / T;
-  const int64_t k0 = (int64_t)kb * 128;
-  if (threadIdx.x < T) {
-    const int64_t row = (int64_t)p * T + threadIdx.x;
-    int m = 0;
-    if (p < P_in && row < R) {
-      double sq = 0.0;
-      for (int c = 0; c < C; ++c) sq += part[((int64_t)p * C + c) * T + threadIdx.x];
-      m = row_exponent(sq, rc.gamma_bits);
-    }
-    pow2_pair(m, s1[threadIdx.x], s2[threadIdx.x]);
-    if (kb == 0 && row < Rpad) mu_out[row] = m;
+// Every warp runs its own pipeline over a contiguous range of tiles of 16
+// rows x 32 k (group g = 16-row group, kb = 32-k block, g-major): a TMA box
+// {16 rows, 32 k} of the operand lands as [32 k][16 rows] doubles in one of
+// the warp's three 4 KB stages (zero-filled past K and past the operand's
+// panels), the tile two ahead already in flight. Lane (r = lane % 16,
+// h = lane / 16) converts k = 16 h .. 16 h + 15 of row r: its shared-memory
+// reads are conflict-free (16 consecutive rows per k) and each residue
+// leaves as one 16-byte store, the warp covering 16 rows x 32 bytes (whole
+// sectors). No CTA-wide barrier. Row exponents come from the norm partials;
+// the lanes converting k-block 0 of a group publish them.
+constexpr int kConvStages = 3;
+constexpr int kConvWarps = 8;
+constexpr int kConvTile = 16 * 32;  // doubles per warp tile
+constexpr int kConvSmem = kConvWarps * (kConvStages * kConvTile * 8 + kConvStages * 8);
+
+template <int T, int L>
+__global__ void __launch_bounds__(256, 2) convert_tma_kernel(
+    const __grid_constant__ CUtensorMap map, int64_t R, int64_t KP, int64_t Rpad, int C,
+    const double* __restrict__ part, uint8_t* __restrict__ res, int* __restrict__ mu_out,
+    uint32_t* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* buf = reinterpret_cast<double*>(sm) + warp * kConvStages * kConvTile;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kConvWarps * kConvStages * kConvTile * 8) +
+                  warp * kConvStages;
+  const int64_t KB = KP / 32;
+  const int64_t ntiles = (Rpad / 16) * KB;
+  // Warp gw takes tiles gw, gw + nw, gw + 2 nw, ...: at any moment the
+  // machine converts one contiguous window of tiles, so the stores of all
+  // warps land in a narrow band of each residue plane (page-local writes)
+  // and the loads stream one contiguous span.
+  const int64_t gw = (int64_t)blockIdx.x * kConvWarps + warp, nw = (int64_t)gridDim.x * kConvWarps;
+  if (gw >= ntiles) return;
+  const int64_t nmine = (ntiles - gw + nw - 1) / nw;  // tiles of this warp
+  const int64_t dq = nw / KB, dr = nw % KB;           // stride nw as (groups, k-blocks)
+  if (lane == 0) {
+    for (int st = 0; st < kConvStages; ++st) mbar_init(&bar[st], 1);
+    fence_mbar_init();
   }
-  const int64_t rem = R - (int64_t)p * T;
-  const int rows_valid = p < P_in ? (int)(rem < T ? rem : T) : 0;
-  const double* src = X + (int64_t)p * K * T;
-#pragma unroll 1
-  for (int sp = 0; sp < T / 16; ++sp) {
-    __syncthreads();
-    stage_tile<16>(tileT, src + sp * 16, T, k0, K, rows_valid - sp * 16);
-    __syncthreads();
-    emit_residues<NDIG, FDIG>(tileT, s1 + sp * 16, s2 + sp * 16, L, rc, res,
-                              (int64_t)p * T + sp * 16, KP, Rpad, k0);
+  __syncwarp();
+  // Tile (g, kb): rows 16 g .. +16 = panel g / (T/16), rows 16 (g % (T/16)) ..
+  // of that panel.
+  auto issue = [&](int64_t g, int64_t kb, int st) {
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&bar[st], kConvTile * 8);
+    tma_load_3d(buf + st * kConvTile, &map, &bar[st], (int)(16 * (g % (T / 16))), (int)(kb * 32),
+                (int)(g / (T / 16)));
+  };
+  auto advance = [&](int64_t& g, int64_t& kb) {
+    g += dq;
+    kb += dr;
+    if (kb >= KB) {
+      kb -= KB;
+      ++g;
+    }
+  };
+  int64_t g = gw / KB, kb = gw % KB;
+  // Counters of the next tile to issue.
+  int64_t gi = g, ki = kb;
+  if (lane == 0) tma_prefetch_desc(&map);
+  for (int st = 0; st < kConvStages - 1; ++st) {
+    if (lane == 0 && st < nmine) issue(gi, ki, st);
+    advance(gi, ki);
+  }
+  const int r = lane & 15, h = lane >> 4;
+  const int gam = c_res[L].gamma_bits;
+  double s1 = 1.0, s2 = 1.0;
+  int64_t cur_g = -1;
+  uint32_t phase = 0;  // bit s: parity of stage s's next completion
+  int s = 0;
+  for (int64_t n = 0; n < nmine; ++n) {
+    if (lane == 0 && n + kConvStages - 1 < nmine) issue(gi, ki, (s + kConvStages - 1) % kConvStages);
+    advance(gi, ki);
+    if (g != cur_g) {
+      const int64_t row = g * 16 + r;
+      const int64_t p = g / (T / 16);
+      const int rin = (int)(row - p * T);
+      int m = 0;
+      if (row < R) {
+        double sq = 0.0;
+        for (int c = 0; c < C; ++c) sq += part[(p * C + c) * T + rin];
+        m = row_exponent(sq, gam);
+      }
+      pow2_pair(m, s1, s2);
+      if (kb == 0 && h == 0) mu_out[row] = m;
+      cur_g = g;
+    }
+    const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, err);
+    phase ^= 1u << s;
+    uint8_t* dst = res + (g * 16 + r) * KP + kb * 32 + 16 * h;
+    const int64_t lstride = Rpad * KP;
+    if (ok) {
+      const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
+      Digits d[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) d[j] = digits_of(blk[j * 16], s1, s2);
+      *reinterpret_cast<uint4*>(dst) =
+          make_uint4(pack4(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pack4(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
+                     pack4(d[8].lo, d[9].lo, d[10].lo, d[11].lo),
+                     pack4(d[12].lo, d[13].lo, d[14].lo, d[15].lo));
+#pragma unroll
+      for (int l = 1; l < L; ++l) {
+        uint32_t b[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) b[j] = residue_byte<L>(d[j], l);
+        *reinterpret_cast<uint4*>(dst + l * lstride) =
+            make_uint4(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]),
+                       pack4(b[8], b[9], b[10], b[11]), pack4(b[12], b[13], b[14], b[15]));
+      }
+    } else {
+#pragma unroll
+      for (int l = 0; l < L; ++l) *reinterpret_cast<uint4*>(dst + l * lstride) = make_uint4(0, 0, 0, 0);
+    }
+    __syncwarp();  // stage s consumed by every lane before it is refilled
+    s = (s + 1) % kConvStages;
+    advance(g, kb);
   }
 }
 
@@ -337,39 +351,54 @@ __global__ void __launch_bounds__(256) convert_packed_kernel(
 // src[p * panel_stride + k * ks + r]. Used for the rotation's A (grid-packed
 // Psi, rows = grid points, k = bands: panel_stride nb*16, ks 16) and B
 // (Q row-major, rows = columns of Q, k = rows of Q: panel_stride 16, ks nb).
-template <int NDIG, int FDIG>
+template <int L>
 __global__ void __launch_bounds__(256) convert_local_kernel(
     int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ src,
-    int64_t panel_stride, int64_t ks, int L, uint8_t* __restrict__ res, int* __restrict__ mu_out) {
+    int64_t panel_stride, int64_t ks, uint8_t* __restrict__ res, int* __restrict__ mu_out) {
   __shared__ double tileT[16 * kTilePitch];
   __shared__ double red[256];
   __shared__ double s1[16], s2[16];
-  const ResidueConsts& rc = c_res[L];
   const int64_t p = blockIdx.x;
   const int64_t rem = R - p * 16;
   const int rows_valid = rem <= 0 ? 0 : (int)(rem < 16 ? rem : 16);
   const double* base = src + p * panel_stride;
-  const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
-  double acc = 0.0;
-  if (r < rows_valid)
-    for (int64_t k = kl; k < K; k += 16) {
-      const double v = base[k * ks + r];
-      acc = fma(v, v, acc);
-    }
-  red[threadIdx.x] = acc;
+  {
+    const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
+    double acc = 0.0;
+    if (r < rows_valid)
+      for (int64_t k = kl; k < K; k += 16) {
+        const double v = base[k * ks + r];
+        acc = fma(v, v, acc);
+      }
+    red[threadIdx.x] = acc;
+  }
   __syncthreads();
   if (threadIdx.x < 16) {
     double sq = 0.0;
     for (int j = 0; j < 16; ++j) sq += red[j * 16 + threadIdx.x];
-    const int m = threadIdx.x < rows_valid ? row_exponent(sq, rc.gamma_bits) : 0;
+    const int m = threadIdx.x < rows_valid ? row_exponent(sq, c_res[L].gamma_bits) : 0;
     pow2_pair(m, s1[threadIdx.x], s2[threadIdx.x]);
     if (p * 16 + threadIdx.x < Rpad) mu_out[p * 16 + threadIdx.x] = m;
   }
+  const int kk = threadIdx.x & 15, r = threadIdx.x >> 4;
   for (int64_t k0 = 0; k0 < KP; k0 += 128) {
     __syncthreads();
     stage_tile<16>(tileT, base, ks, k0, K, rows_valid);
     __syncthreads();
-    emit_residues<NDIG, FDIG>(tileT, s1, s2, L, rc, res, p * 16, KP, Rpad, k0);
+    Digits d[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) d[j] = digits_of(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r]);
+    uint8_t* dst = res + (p * 16 + r) * KP + k0 + 8 * kk;
+    *reinterpret_cast<uint2*>(dst) = make_uint2(pack4(d[0].lo, d[1].lo, d[2].lo, d[3].lo),
+                                                pack4(d[4].lo, d[5].lo, d[6].lo, d[7].lo));
+#pragma unroll
+    for (int l = 1; l < L; ++l) {
+      uint32_t b[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = residue_byte<L>(d[j], l);
+      *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) =
+          make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
+    }
   }
 }
 
@@ -412,7 +441,7 @@ __global__ void __launch_bounds__(256) crt_partials_kernel(
       int64_t s = 0;
       for (int q = mod_slot_off[l]; q < mod_slot_off[l + 1]; ++q)
         s += partials[((int64_t)mod_slots[q] * T + t) * (kI8BM * kI8BN) + off];
-      const int64_t m = c_res[L].m[l];
+      const int64_t m = c_res[L].mi[l];
       int64_t rr = s % m;
       if (rr < 0) rr += m;
       r[l] = (uint32_t)rr;
@@ -510,8 +539,6 @@ OzakiDevice g_oz[64];
 I8ModConsts g_modc;
 bool g_modc_ready = false;
 
-int g_ndig[kI8MaxModuli + 1];
-int g_fdig[kI8MaxModuli + 1];
 
 int ensure_consts(DeviceState* dev) {
   OzakiDevice& od = g_oz[dev->device];
@@ -519,37 +546,17 @@ int ensure_consts(DeviceState* dev) {
   ResidueConsts rc[kI8MaxModuli + 1];
   memset(rc, 0, sizeof(rc));
   for (int L = kMinModuli; L <= kI8MaxModuli; ++L) {
-    const int gam = gamma_for(L);
-    const int ndig = (gam + 2 <= 57) ? 3 : 4;
-    const int W = ndig == 3 ? 19 : 16;
-    const long long bias = 1LL << (gam + 1);
-    const int fdig = (gam + 2 <= 60) ? 5 : 6;
-    rc[L].ndig = ndig;
-    rc[L].fdig = fdig;
-    rc[L].gamma_bits = gam;
-    rc[L].bias = bias;
-    g_ndig[L] = ndig;
-    g_fdig[L] = fdig;
+    rc[L].gamma_bits = gamma_for(L);
     for (int l = 0; l < kI8MaxModuli; ++l) {
       const uint64_t m = kModuli[l];
-      rc[L].m[l] = (uint32_t)m;
-      rc[L].magic[l] = (uint32_t)((1ull << 37) / m + 1);
-      uint64_t p1 = 1;
-      for (int i = 0; i < W; ++i) p1 = (p1 * 2) % m;
-      rc[L].c1[l] = (uint32_t)p1;
-      rc[L].c2[l] = (uint32_t)(p1 * p1 % m);
-      rc[L].c3[l] = (uint32_t)(p1 * p1 % m * p1 % m);
-      rc[L].e[l] = (uint32_t)((m - (uint64_t)bias % m) % m);
       uint64_t pj = 1;
-      for (int j = 0; j < 6; ++j) {
-        rc[L].fc[j][l] = (float)pj;  // 2^(12 j) mod m
+      for (int j = 0; j < 4; ++j) {
         pj = (pj * 4096) % m;
+        rc[L].c[j][l] = (float)pj;  // 2^(12 (j+1)) mod m
       }
-      rc[L].fe[l] = (float)rc[L].e[l];
-      float inv = 1.0f / (float)m;
-      if ((double)inv < 1.0 / (double)m) inv = nextafterf(inv, 1.0f);
-      rc[L].finv[l] = inv;
-      rc[L].fm[l] = (float)m;
+      rc[L].inv[l] = 1.0f / (float)m;
+      rc[L].m[l] = (float)m;
+      rc[L].mi[l] = (uint32_t)m;
     }
   }
   for (int l = 0; l < kI8MaxModuli; ++l) {
@@ -708,10 +715,56 @@ void report(skgemm_options_t* opts, int L, int gamma_bits, int64_t K) {
   opts->err_bound_out = 2.0 * std::sqrt((double)K / 12.0) * std::ldexp(1.0, -gamma_bits);
 }
 
-// Residues of a packed-T operand into res[L][Rpad][KP] + row exponents.
+// L-dispatch of a launcher template (L in [kMinModuli, 16]).
+#define SKG_DISPATCH_L(L, CALL)                                                  \
+  switch (L) {                                                                   \
+    case 6: { constexpr int LL = 6; return CALL; }                               \
+    case 7: { constexpr int LL = 7; return CALL; }                               \
+    case 8: { constexpr int LL = 8; return CALL; }                               \
+    case 9: { constexpr int LL = 9; return CALL; }                               \
+    case 10: { constexpr int LL = 10; return CALL; }                             \
+    case 11: { constexpr int LL = 11; return CALL; }                             \
+    case 12: { constexpr int LL = 12; return CALL; }                             \
+    case 13: { constexpr int LL = 13; return CALL; }                             \
+    case 14: { constexpr int LL = 14; return CALL; }                             \
+    case 15: { constexpr int LL = 15; return CALL; }                             \
+    case 16: { constexpr int LL = 16; return CALL; }                             \
+    default: return fail(SKGEMM_ERR_INVALID_ARG, "moduli count out of range");   \
+  }
+
+template <int T, int L>
+int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t R, int64_t KP, int64_t Rpad,
+                   int C, const double* part, uint8_t* res, int* mu, uint32_t* err,
+                   cudaStream_t s) {
+  static int occ[64] = {0};
+  if (!occ[dev->device]) {
+    SKG_CUDA(cudaFuncSetAttribute(convert_tma_kernel<T, L>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+    int n = 0;
+    SKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, convert_tma_kernel<T, L>, 256,
+                                                           kConvSmem));
+    occ[dev->device] = n > 0 ? n : 1;
+  }
+  const int64_t ntiles = (Rpad / 16) * (KP / 32);
+  const int64_t blocks = std::min<int64_t>((ntiles + kConvWarps - 1) / kConvWarps,
+                                           (int64_t)dev->num_sms * occ[dev->device]);
+  // (every warp of the grid gets at least one tile only if ntiles >= warps;
+  // warps without a tile return at once)
+  convert_tma_kernel<T, L><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, R, KP, Rpad, C, part,
+                                                                    res, mu, err);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+// Residues of a packed-T operand (rows R, reduction K) into res[L][Rpad][KP]
+// plus row exponents: norm partials, then the TMA-fed conversion.
 template <int T>
-int prep_packed(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, int L,
-                DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu, cudaStream_t s) {
+int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
+                const double* X, int L, DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu,
+                uint32_t* err, cudaStream_t s) {
+  if ((reinterpret_cast<uintptr_t>(X) & 15) != 0)
+    return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
+  if (K > ((int64_t)1 << 31) - 128) return fail(SKGEMM_ERR_INVALID_ARG, "K too large");
   const int64_t P_in = (R + T - 1) / T;
   const int C = (int)std::max<int64_t>(1, std::min<int64_t>(64, (600 + P_in - 1) / P_in));
   int st;
@@ -721,31 +774,32 @@ int prep_packed(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X,
   norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
                                                                   (double*)part.ptr);
   SKG_CUDA(cudaGetLastError());
-  const dim3 grid((unsigned)(Rpad / T), (unsigned)(KP / 128));
+  // [P_in][K][T] doubles; boxes of 16 rows x 32 k (zero fill past K / P_in).
+  CUtensorMap map;
+  const uint64_t dims[3] = {(uint64_t)T, (uint64_t)K, (uint64_t)P_in};
+  const uint64_t strides[2] = {(uint64_t)T * 8, (uint64_t)K * T * 8};
+  const uint32_t box[3] = {16, 32, 1};
+  if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         CU_TENSOR_MAP_SWIZZLE_NONE)))
+    return st;
   const double* pp = (const double*)part.ptr;
   uint8_t* rp = (uint8_t*)res.ptr;
   int* mp = (int*)mu.ptr;
-  if (g_ndig[L] == 3)
-    convert_packed_kernel<T, 3, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, pp, L, rp, mp);
-  else if (g_fdig[L] == 5)
-    convert_packed_kernel<T, 4, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, pp, L, rp, mp);
-  else
-    convert_packed_kernel<T, 4, 6><<<grid, 256, 0, s>>>(R, K, KP, Rpad, X, C, pp, L, rp, mp);
+  SKG_DISPATCH_L(L, (launch_convert<T, LL>(dev, map, R, KP, Rpad, C, pp, rp, mp, err, s)))
+}
+
+template <int L>
+int launch_local_L(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* src,
+                   int64_t panel_stride, int64_t ks, uint8_t* res, int* mu, cudaStream_t s) {
+  convert_local_kernel<L><<<(unsigned)(Rpad / 16), 256, 0, s>>>(R, K, KP, Rpad, src,
+                                                                panel_stride, ks, res, mu);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
 
 int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* src,
                  int64_t panel_stride, int64_t ks, int L, uint8_t* res, int* mu, cudaStream_t s) {
-  const unsigned grid = (unsigned)(Rpad / 16);
-  if (g_ndig[L] == 3)
-    convert_local_kernel<3, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
-  else if (g_fdig[L] == 5)
-    convert_local_kernel<4, 5><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
-  else
-    convert_local_kernel<4, 6><<<grid, 256, 0, s>>>(R, K, KP, Rpad, src, panel_stride, ks, L, res, mu);
-  SKG_CUDA(cudaGetLastError());
-  return SKGEMM_OK;
+  SKG_DISPATCH_L(L, (launch_local_L<LL>(R, K, KP, Rpad, src, panel_stride, ks, res, mu, s)))
 }
 
 // Shared body of the Ozaki GEMM and SYRK: residues of A (packed16) and B
@@ -772,12 +826,14 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
   const int KB = (int)(KP / 128);
   const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;  // 256-multiples serve both box heights
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
-  if ((st = prep_packed<16>(M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, s)))
+  if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, ws->err,
+                            s)))
     return st;
   const DeviceBuffer* resB = &os->res_a;
   const DeviceBuffer* muB = &os->mu_a;
   if (!syrk) {
-    if ((st = prep_packed<32>(N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b, s)))
+    if ((st = prep_packed<32>(dev, N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b,
+                              ws->err, s)))
       return st;
     resB = &os->res_b;
     muB = &os->mu_b;
@@ -898,6 +954,7 @@ OzakiNeed need_rot(int64_t Nd, int64_t nb, int L) {
   const int64_t RB = (nb + kI8BN - 1) / kI8BN * kI8BN;
   n.res_a = (size_t)L * RA * KP;
   n.res_b = (size_t)L * RB * KP;
+  n.part_a = norm_part_bytes(Nd, 16);
   n.mu_a = (size_t)RA * sizeof(int);
   n.mu_b = (size_t)RB * sizeof(int);
   n.rbytes = (size_t)L * Nd * nb;
@@ -1010,13 +1067,12 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   const int64_t KP = (nb + 127) / 128 * 128;
   const int64_t RA = (Nd + kI8BM - 1) / kI8BM * kI8BM;
   const int64_t RB = (nb + kI8BN - 1) / kI8BN * kI8BN;
-  if ((st = os->res_a.ensure((size_t)L * RA * KP))) return st;
   if ((st = os->res_b.ensure((size_t)L * RB * KP))) return st;
-  if ((st = os->mu_a.ensure((size_t)RA * sizeof(int)))) return st;
   if ((st = os->mu_b.ensure((size_t)RB * sizeof(int)))) return st;
   if ((st = os->rbytes.ensure((size_t)L * Nd * nb))) return st;
-  if ((st = launch_local(Nd, nb, KP, RA, A, nb * 16, 16, L, (uint8_t*)os->res_a.ptr,
-                         (int*)os->mu_a.ptr, s)))
+  // Grid-packed Psi is a packed16 operand with rows = grid points, K = bands.
+  if ((st = prep_packed<16>(dev, Nd, nb, KP, RA, A, L, os->res_a, os->part_a, os->mu_a, ws->err,
+                            s)))
     return st;
   if ((st = launch_local(nb, nb, KP, RB, Q, 16, nb, L, (uint8_t*)os->res_b.ptr,
                          (int*)os->mu_b.ptr, s)))
