@@ -226,6 +226,24 @@ __global__ void __launch_bounds__(256) norm_partials_kernel(int64_t R, int64_t K
   }
 }
 
+// Row exponents mu[row] (row < Rpad) of a packed-T operand from its norm
+// partials; rows past R (padding) get 0.
+template <int T>
+__global__ void row_exponents_kernel(int64_t R, int64_t Rpad, int C, const double* __restrict__ part,
+                                     int gamma_bits, int* __restrict__ mu) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= Rpad) return;
+  int m = 0;
+  if (row < R) {
+    const int64_t p = row / T;
+    const int rin = (int)(row - p * T);
+    double sq = 0.0;
+    for (int c = 0; c < C; ++c) sq += part[(p * C + c) * T + rin];
+    m = row_exponent(sq, gamma_bits);
+  }
+  mu[row] = m;
+}
+
 // Residues of a packed-T operand -> res[l][Rpad][KP] (K-major bytes).
 // Every warp runs its own pipeline over a contiguous range of tiles of 16
 // rows x 32 k (group g = 16-row group, kb = 32-k block, g-major): a TMA box
@@ -235,8 +253,8 @@ __global__ void __launch_bounds__(256) norm_partials_kernel(int64_t R, int64_t K
 // h = lane / 16) converts k = 16 h .. 16 h + 15 of row r: its shared-memory
 // reads are conflict-free (16 consecutive rows per k) and each residue
 // leaves as one 16-byte store, the warp covering 16 rows x 32 bytes (whole
-// sectors). No CTA-wide barrier. Row exponents come from the norm partials;
-// the lanes converting k-block 0 of a group publish them.
+// sectors). No CTA-wide barrier. Row exponents mu[row] are read from the
+// exponent pass.
 constexpr int kConvStages = 3;
 constexpr int kConvWarps = 8;
 constexpr int kConvTile = 16 * 32;  // doubles per warp tile
@@ -244,9 +262,8 @@ constexpr int kConvSmem = kConvWarps * (kConvStages * kConvTile * 8 + kConvStage
 
 template <int T, int L>
 __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
-    const __grid_constant__ CUtensorMap map, int64_t R, int64_t KP, int64_t Rpad, int C,
-    const double* __restrict__ part, uint8_t* __restrict__ res, int* __restrict__ mu_out,
-    uint32_t* __restrict__ err) {
+    const __grid_constant__ CUtensorMap map, int64_t KP, int64_t Rpad,
+    const int* __restrict__ mu, uint8_t* __restrict__ res, uint32_t* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* buf = reinterpret_cast<double*>(sm) + warp * kConvStages * kConvTile;
@@ -292,7 +309,6 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     advance(gi, ki);
   }
   const int r = lane & 15, h = lane >> 4;
-  const int gam = c_res[L].gamma_bits;
   double s1 = 1.0, s2 = 1.0;
   int64_t cur_g = -1;
   uint32_t phase = 0;  // bit s: parity of stage s's next completion
@@ -301,17 +317,7 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     if (lane == 0 && n + kConvStages - 1 < nmine) issue(gi, ki, (s + kConvStages - 1) % kConvStages);
     advance(gi, ki);
     if (g != cur_g) {
-      const int64_t row = g * 16 + r;
-      const int64_t p = g / (T / 16);
-      const int rin = (int)(row - p * T);
-      int m = 0;
-      if (row < R) {
-        double sq = 0.0;
-        for (int c = 0; c < C; ++c) sq += part[(p * C + c) * T + rin];
-        m = row_exponent(sq, gam);
-      }
-      pow2_pair(m, s1, s2);
-      if (kb == 0 && h == 0) mu_out[row] = m;
+      pow2_pair(mu[g * 16 + r], s1, s2);
       cur_g = g;
     }
     const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, err);
@@ -733,9 +739,8 @@ void report(skgemm_options_t* opts, int L, int gamma_bits, int64_t K) {
   }
 
 template <int T, int L>
-int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t R, int64_t KP, int64_t Rpad,
-                   int C, const double* part, uint8_t* res, int* mu, uint32_t* err,
-                   cudaStream_t s) {
+int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t Rpad,
+                   const int* mu, uint8_t* res, uint32_t* err, cudaStream_t s) {
   static int occ[64] = {0};
   if (!occ[dev->device]) {
     SKG_CUDA(cudaFuncSetAttribute(convert_tma_kernel<T, L>,
@@ -750,8 +755,7 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t R, int64_t 
                                            (int64_t)dev->num_sms * occ[dev->device]);
   // (every warp of the grid gets at least one tile only if ntiles >= warps;
   // warps without a tile return at once)
-  convert_tma_kernel<T, L><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, R, KP, Rpad, C, part,
-                                                                    res, mu, err);
+  convert_tma_kernel<T, L><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, KP, Rpad, mu, res, err);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
@@ -782,10 +786,12 @@ int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad
   if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                          CU_TENSOR_MAP_SWIZZLE_NONE)))
     return st;
-  const double* pp = (const double*)part.ptr;
-  uint8_t* rp = (uint8_t*)res.ptr;
   int* mp = (int*)mu.ptr;
-  SKG_DISPATCH_L(L, (launch_convert<T, LL>(dev, map, R, KP, Rpad, C, pp, rp, mp, err, s)))
+  row_exponents_kernel<T><<<(unsigned)((Rpad + 255) / 256), 256, 0, s>>>(
+      R, Rpad, C, (const double*)part.ptr, gamma_for(L), mp);
+  SKG_CUDA(cudaGetLastError());
+  uint8_t* rp = (uint8_t*)res.ptr;
+  SKG_DISPATCH_L(L, (launch_convert<T, LL>(dev, map, KP, Rpad, mp, rp, err, s)))
 }
 
 template <int L>
