@@ -532,6 +532,10 @@ struct LanePlan {
 
 struct OzakiStream {
   DeviceBuffer res_a, res_b, part_a, part_b, mu_a, mu_b, partials, rbytes;
+  // Helper stream forked from the caller's stream: the norm pass of B runs
+  // there while A is converted (the conversion leaves HBM bandwidth idle).
+  cudaStream_t aux = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 struct OzakiDevice {
@@ -761,11 +765,12 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
 }
 
 // Residues of a packed-T operand (rows R, reduction K) into res[L][Rpad][KP]
-// plus row exponents: norm partials, then the TMA-fed conversion.
+// plus row exponents, in two steps: prep_norms (norm partials, then the row
+// exponents) and prep_convert (the TMA-fed conversion). The steps may run on
+// different streams with an event between them.
 template <int T>
-int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
-                const double* X, int L, DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu,
-                uint32_t* err, cudaStream_t s) {
+int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, int L,
+               DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu, cudaStream_t s) {
   if ((reinterpret_cast<uintptr_t>(X) & 15) != 0)
     return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
   if (K > ((int64_t)1 << 31) - 128) return fail(SKGEMM_ERR_INVALID_ARG, "K too large");
@@ -778,20 +783,38 @@ int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad
   norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
                                                                   (double*)part.ptr);
   SKG_CUDA(cudaGetLastError());
+  row_exponents_kernel<T><<<(unsigned)((Rpad + 255) / 256), 256, 0, s>>>(
+      R, Rpad, C, (const double*)part.ptr, gamma_for(L), (int*)mu.ptr);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+template <int T>
+int prep_convert(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
+                 const double* X, int L, DeviceBuffer& res, DeviceBuffer& mu, uint32_t* err,
+                 cudaStream_t s) {
   // [P_in][K][T] doubles; boxes of 16 rows x 32 k (zero fill past K / P_in).
+  const int64_t P_in = (R + T - 1) / T;
   CUtensorMap map;
   const uint64_t dims[3] = {(uint64_t)T, (uint64_t)K, (uint64_t)P_in};
   const uint64_t strides[2] = {(uint64_t)T * 8, (uint64_t)K * T * 8};
   const uint32_t box[3] = {16, 32, 1};
+  int st;
   if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                          CU_TENSOR_MAP_SWIZZLE_NONE)))
     return st;
-  int* mp = (int*)mu.ptr;
-  row_exponents_kernel<T><<<(unsigned)((Rpad + 255) / 256), 256, 0, s>>>(
-      R, Rpad, C, (const double*)part.ptr, gamma_for(L), mp);
-  SKG_CUDA(cudaGetLastError());
+  const int* mp = (const int*)mu.ptr;
   uint8_t* rp = (uint8_t*)res.ptr;
   SKG_DISPATCH_L(L, (launch_convert<T, LL>(dev, map, KP, Rpad, mp, rp, err, s)))
+}
+
+template <int T>
+int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
+                const double* X, int L, DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu,
+                uint32_t* err, cudaStream_t s) {
+  int st;
+  if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s))) return st;
+  return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s);
 }
 
 template <int L>
@@ -832,14 +855,29 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
   const int KB = (int)(KP / 128);
   const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;  // 256-multiples serve both box heights
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
-  if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, ws->err,
-                            s)))
-    return st;
   const DeviceBuffer* resB = &os->res_a;
   const DeviceBuffer* muB = &os->mu_a;
-  if (!syrk) {
-    if ((st = prep_packed<32>(dev, N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b,
+  if (syrk) {
+    if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a,
                               ws->err, s)))
+      return st;
+  } else {
+    // norms(A) | norms(B) on the helper stream; convert(A); join; convert(B).
+    if (!os->aux) {
+      SKG_CUDA(cudaStreamCreateWithFlags(&os->aux, cudaStreamNonBlocking));
+      SKG_CUDA(cudaEventCreateWithFlags(&os->fork, cudaEventDisableTiming));
+      SKG_CUDA(cudaEventCreateWithFlags(&os->join, cudaEventDisableTiming));
+    }
+    SKG_CUDA(cudaEventRecord(os->fork, s));
+    SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork, 0));
+    const int st_b = prep_norms<32>(N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b, os->aux);
+    SKG_CUDA(cudaEventRecord(os->join, os->aux));  // join even when the B step failed
+    if (st_b) return st_b;
+    if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a,
+                              ws->err, s)))
+      return st;
+    SKG_CUDA(cudaStreamWaitEvent(s, os->join, 0));
+    if ((st = prep_convert<32>(dev, N, K, KP, RB, Bp, L, os->res_b, os->mu_b, ws->err, s)))
       return st;
     resB = &os->res_b;
     muB = &os->mu_b;
@@ -1025,6 +1063,12 @@ int ozaki_release_stream(DeviceState* dev, cudaStream_t s) {
   auto it = m.find(s);
   if (it == m.end()) return SKGEMM_OK;
   OzakiStream* os = it->second;
+  if (os->aux) {
+    cudaStreamSynchronize(os->aux);
+    cudaStreamDestroy(os->aux);
+    cudaEventDestroy(os->fork);
+    cudaEventDestroy(os->join);
+  }
   for (DeviceBuffer* b : {&os->res_a, &os->res_b, &os->part_a, &os->part_b, &os->mu_a, &os->mu_b,
                           &os->partials, &os->rbytes})
     b->release();
