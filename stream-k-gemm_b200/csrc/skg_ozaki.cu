@@ -463,43 +463,69 @@ __global__ void __launch_bounds__(256) crt_partials_kernel(
 }
 
 // Rotation: Psi'(g, b) band-packed from the residue bytes res[l][g][ldr].
-// Thread (g, c): the 16 states of chunk c at grid point g; per modulus one
-// 16-byte load, bytes widened to doubles exactly (2^52 + r - 2^52).
+// Thread (g, c): the 16 states of chunk c at grid point g. All L 16-byte
+// residue loads are issued before any arithmetic (the kernel is bound by
+// their latency otherwise); bytes widen to doubles exactly (2^52 + r - 2^52).
+// The scale 2^-(mu[g] + nu[b]) is built from exponent bits (four 16-byte
+// loads of nu per thread).
+__device__ __forceinline__ double pow2i(int e) {  // 2^e, e in [-1022, 1023]
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+template <int L>
 __global__ void __launch_bounds__(128) crt_residues_band_kernel(
-    int64_t Nd, int64_t nb, int L, const uint8_t* __restrict__ res, int64_t ldr,
+    int64_t Nd, int64_t nb, const uint8_t* __restrict__ res, int64_t ldr,
     const int* __restrict__ mu, const int* __restrict__ nu, double* __restrict__ Dband) {
-  const int64_t chunks = nb / 16;
+  // Thread (g, c, hf): states 16 c + 8 hf .. + 8 at grid point g (hf fastest:
+  // a lane pair writes one whole 128-byte line of the band-packed output).
+  const int64_t halves = nb / 8;
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= Nd * chunks) return;
-  const int64_t g = idx / chunks, c = idx % chunks;
+  if (idx >= Nd * halves) return;
+  const int64_t g = idx / halves, hc = idx % halves;
+  const int64_t c = hc >> 1, hf = hc & 1;
   const CrtConsts& cc = c_crt[L];
-  double sh[16], sl[16];
+  uint2 v[L];
 #pragma unroll
-  for (int t = 0; t < 16; ++t) sh[t] = sl[t] = 0.0;
-  for (int l = 0; l < L; ++l) {
-    const uint4 v = *reinterpret_cast<const uint4*>(res + ((int64_t)l * Nd + g) * ldr + c * 16);
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    const double wh = cc.wh[l], wl = cc.wl[l];
+  for (int l = 0; l < L; ++l)
+    v[l] = __ldcs(reinterpret_cast<const uint2*>(res + ((int64_t)l * Nd + g) * ldr + hc * 8));
+  int e[8];
+  {
+    const int4* n4 = reinterpret_cast<const int4*>(nu + hc * 8);
+    const int4 t0 = __ldg(n4), t1 = __ldg(n4 + 1);
+    e[0] = t0.x; e[1] = t0.y; e[2] = t0.z; e[3] = t0.w;
+    e[4] = t1.x; e[5] = t1.y; e[6] = t1.z; e[7] = t1.w;
+  }
+  const int mg = mu[g];
+  double out[8];
 #pragma unroll
-    for (int t = 0; t < 16; ++t) {
+  for (int t = 0; t < 8; ++t) {
+    double sh = 0.0, sl = 0.0;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const uint32_t w = t < 4 ? v[l].x : v[l].y;
       const double d =
-          __hiloint2double(0x43300000, (int)((w[t >> 2] >> (8 * (t & 3))) & 0xFFu)) -
-          4503599627370496.0;
-      sh[t] = fma(d, wh, sh[t]);
-      sl[t] = fma(d, wl, sl[t]);
+          __hiloint2double(0x43300000, (int)((w >> (8 * (t & 3))) & 0xFFu)) - 4503599627370496.0;
+      sh = fma(d, cc.wh[l], sh);  // exact: 8-bit x 40-bit on a common grid
+      sl = fma(d, cc.wl[l], sl);
     }
+    const double q = rint((sh + sl) * cc.inv_m);
+    const double x = fma(-q, cc.mh, sh) + fma(-q, cc.ml, sl);
+    const int ex = -(mg + e[t]);
+    out[t] = (ex >= -1022 && ex <= 1023) ? x * pow2i(ex) : ldexp(ldexp(x, -mg), -e[t]);
   }
-  const double sg = ldexp(1.0, -mu[g]);
-  double out[16];
+  double2* dst = reinterpret_cast<double2*>(Dband + (c * Nd + g) * 16 + hf * 8);
 #pragma unroll
-  for (int t = 0; t < 16; ++t) {
-    const double q = rint((sh[t] + sl[t]) * cc.inv_m);
-    const double v = fma(-q, cc.mh, sh[t]) + fma(-q, cc.ml, sl[t]);
-    out[t] = (v * sg) * ldexp(1.0, -nu[c * 16 + t]);
-  }
-  double2* dst = reinterpret_cast<double2*>(Dband + (c * Nd + g) * 16);
-#pragma unroll
-  for (int t = 0; t < 8; ++t) dst[t] = make_double2(out[2 * t], out[2 * t + 1]);
+  for (int t = 0; t < 4; ++t) __stcs(dst + t, make_double2(out[2 * t], out[2 * t + 1]));
+}
+
+template <int L>
+int launch_crt_band(int64_t Nd, int64_t nb, const uint8_t* res, const int* mu, const int* nu,
+                    double* D, cudaStream_t s) {
+  const int64_t n = Nd * (nb / 8);
+  crt_residues_band_kernel<L><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(Nd, nb, res, nb, mu,
+                                                                          nu, D);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
 }
 
 // Exact INT8 GEMM output: C[i*ldc + j] = sum over slots of the partial slabs.
@@ -1146,11 +1172,15 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   const int64_t units = (int64_t)p.tiles_m * L * p.tiles_n;
   const int grid = (int)std::min<int64_t>(dev->num_sms, units);
   if ((st = launch_i8(dev, mA, mB, p, grid, s))) return st;
-  const int64_t n = Nd * (nb / 16);
-  crt_residues_band_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(
-      Nd, nb, L, (const uint8_t*)os->rbytes.ptr, nb, (const int*)os->mu_a.ptr,
-      (const int*)os->mu_b.ptr, D);
-  SKG_CUDA(cudaGetLastError());
+  {
+    const uint8_t* rb = (const uint8_t*)os->rbytes.ptr;
+    const int* mua = (const int*)os->mu_a.ptr;
+    const int* mub = (const int*)os->mu_b.ptr;
+    auto crt = [&]() -> int {
+      SKG_DISPATCH_L(L, (launch_crt_band<LL>(Nd, nb, rb, mua, mub, D, s)))
+    };
+    if ((st = crt())) return st;
+  }
   report(opts, L, gb, nb);
   return SKGEMM_OK;
 }
