@@ -10,8 +10,10 @@
 // loaded by TMA boxes {128 B of k, 128 (A) / 256 (B) rows, 1 modulus} with the
 // 128-byte swizzle, which is the canonical K-major SW128 UMMA layout.
 //
-// CTA: 192 threads = warp 0 TMA producer, warp 1 MMA issuer (one thread) and
-// TMEM owner, warps 2-5 epilogue (warp w reads TMEM lanes 32*(w%4)..+31).
+// CTA: 320 threads = warp 0 TMA producer, warp 1 MMA issuer (one thread) and
+// TMEM owner, warps 2-9 epilogue (warp w reads TMEM lanes 32*(w%4)..+31 and
+// columns 128*((w-2)/4)..+127: two epilogue warps per TMEM lane quarter keep
+// the epilogue's latency hidden).
 // Tile 128 x 256 (UMMA M=128, N=256, K=32), 4-stage smem ring (48 KB/stage),
 // two 256-column TMEM accumulators so the epilogue of one work item overlaps
 // the MMAs of the next.
@@ -40,7 +42,8 @@ constexpr int kI8BN = 256;
 constexpr int kI8BK = 128;  // bytes of k per stage
 constexpr int kI8UmmaK = 32;
 constexpr int kI8Stages = 4;
-constexpr int kI8Threads = 192;
+constexpr int kI8EpiWarps = 8;
+constexpr int kI8Threads = 64 + 32 * kI8EpiWarps;
 constexpr int kI8TileABytes = kI8BM * kI8BK;  // 16 KB
 constexpr int kI8TileBBytes = kI8BN * kI8BK;  // 32 KB
 constexpr int kI8StageBytes = kI8TileABytes + kI8TileBBytes;
@@ -166,7 +169,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&tfull_bar[a], 1);
-      mbar_init(&tempty_bar[a], 4);  // one arrival per epilogue warp
+      mbar_init(&tempty_bar[a], kI8EpiWarps);  // one arrival per epilogue warp
     }
     *abort_flag = 0;
     fence_mbar_init();
@@ -271,6 +274,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     // ---------------------------------------------------------- epilogue
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
     const int row_in_tile = quarter * 32 + lane;
+    const int c_begin = ((warp - 2) >> 2) * (kI8BN / 64), c_end = c_begin + kI8BN / 64;
     int acc = 0;
     uint32_t acc_phase = 0;
     int cur = 0;
@@ -286,7 +290,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
       if (p.sched == kSchedLanes) {
         int32_t* dst = p.partials + ((int64_t)it.slot * kI8BM + row_in_tile) * kI8BN;
 #pragma unroll 1
-        for (int c = 0; c < kI8BN / 32; ++c) {
+        for (int c = c_begin; c < c_end; ++c) {
           uint32_t v[32];
           tmem_ld_32x32b_x32(taddr + c * 32, v);
           tmem_ld_wait();
@@ -303,7 +307,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
         const bool row_ok = row < p.M;
         uint8_t* dst = p.residues + ((int64_t)it.l * p.M + row) * p.ldr;
 #pragma unroll 1
-        for (int c = 0; c < kI8BN / 32; ++c) {
+        for (int c = c_begin; c < c_end; ++c) {
           uint32_t v[32];
           tmem_ld_32x32b_x32(taddr + c * 32, v);
           tmem_ld_wait();
