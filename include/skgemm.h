@@ -158,6 +158,21 @@ int skgemm_dsyrk_packed_dev_opt(int64_t K, int64_t M, const double* A_packed16,
                                 double* C, int64_t ldc, double alpha, double beta,
                                 skgemm_options_t* opts, void* stream);
 
+/* ------------------------------------------------------- subspace pair */
+/* S = Psi^T Psi (upper triangle of the column-major nb x nb S, column stride
+ * lds) and Hs = Psi^T (H Psi) (row-major nb x nb, row stride ldh) from one
+ * band-packed Psi (packed16, K = Ng grid points x M = nb states) and a
+ * 32-band-packed H Psi: the two products of one CheFSI subspace step, which
+ * the reference computes with two calls on the same Psi
+ * (sme_syrk<double>::compute, include/sme_syrk.hpp:137, then
+ * gemm<double>::compute_packed, gemm_opt.cpp:314). Results equal those two
+ * calls (alpha = 1, beta = gamma = 0). With the Ozaki precision Psi is
+ * split once and its residues serve both products. */
+int skgemm_dsubspace_packed_dev(int64_t K, int64_t M, const double* Psi_packed16,
+                                const double* HPsi_packed32, double* S, int64_t lds,
+                                double* Hs, int64_t ldh, skgemm_options_t* opts,
+                                void* stream);
+
 /* ----------------------------------------------------- subspace rotation */
 /* D = A * Q: Psi' = Psi Q. A grid-packed Nd x nb, Q row-major nb x nb,
  * D band-packed Nd x nb. No scaling (the CheFSI rotation never needs it).

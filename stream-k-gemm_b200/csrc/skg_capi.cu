@@ -475,6 +475,25 @@ SKG_EXPORT int skgemm_dsyrk_packed_dev_opt(int64_t K, int64_t M, const double* A
                            reinterpret_cast<cudaStream_t>(stream));
 }
 
+SKG_EXPORT int skgemm_dsubspace_packed_dev(int64_t K, int64_t M, const double* Psi,
+                                           const double* HPsi, double* S, int64_t lds, double* Hs,
+                                           int64_t ldh, skgemm_options_t* opts, void* stream) {
+  int st = check_dims(K, M, 0);
+  if (st) return st;
+  if (lds < M || ldh < M) return fail(SKGEMM_ERR_INVALID_ARG, "lds or ldh < M");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (!opts || opts->precision == SKGEMM_PREC_NATIVE || K == 0) {
+    // Native FP64 (an empty reduction needs no split either).
+    if (opts) {
+      opts->err_bound_out = 0.0;
+      opts->slices_used_out = 0;
+    }
+    if ((st = run_native(syrk_problem(K, M, Psi, S, lds, 1.0, 0.0), s))) return st;
+    return run_native(gemm_packed_problem(M, M, K, Psi, HPsi, Hs, ldh, 1.0, 0.0), s);
+  }
+  return ozaki_subspace(K, M, Psi, HPsi, S, lds, 1.0, 0.0, Hs, ldh, 1.0, 0.0, opts, s);
+}
+
 SKG_EXPORT int skgemm_dsyrk_packed(int64_t K, int64_t M, const double* Ap, double* C,
                                    double alpha, double beta) {
   int st = check_dims(K, M, 0);

@@ -860,54 +860,17 @@ int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* s
 // Shared body of the Ozaki GEMM and SYRK: residues of A (packed16) and B
 // (packed16 for SYRK, packed32 for GEMM), lane-scheduled INT8 products,
 // reconstruction.
-int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp, bool syrk,
-                double* D, int64_t ldd, double alpha, double gamma, skgemm_options_t* opts,
-                cudaStream_t s) {
+// Lane-scheduled INT8 products of prepared residues (A: os->res_a / mu_a,
+// B: resB / muB) and their reconstruction into D: SYRK (upper triangle of
+// the column-major M x M C = alpha A^T A + beta C) or GEMM (row-major
+// D = alpha A B + gamma).
+int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M, int64_t N,
+                  int64_t KP, int L, bool syrk, const DeviceBuffer* resB, const DeviceBuffer* muB,
+                  double* D, int64_t ldd, double alpha, double gamma, cudaStream_t s) {
   int st;
-  DeviceState* dev = current_device(&st);
-  if (!dev) return st;
-  if (M == 0 || N == 0) return SKGEMM_OK;
-  if (!Ap || !Bp || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
-  if (K == 0) return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki path needs K > 0");
-  if (M > (1 << 20) || N > (1 << 20)) return fail(SKGEMM_ERR_INVALID_ARG, "dimension too large");
-  int L, gb;
-  if ((st = choose_L(opts, K, &L, &gb)) != SKGEMM_OK) return st;
-  std::lock_guard<std::mutex> lk(g_oz_mu);
-  if ((st = ensure_consts(dev)) != SKGEMM_OK) return st;
-  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
-  if (!ws) return st;
-  OzakiStream* os = ozaki_stream(dev, s);
-  const int64_t KP = (K + 127) / 128 * 128;
   const int KB = (int)(KP / 128);
-  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;  // 256-multiples serve both box heights
+  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
-  const DeviceBuffer* resB = &os->res_a;
-  const DeviceBuffer* muB = &os->mu_a;
-  if (syrk) {
-    if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a,
-                              ws->err, s)))
-      return st;
-  } else {
-    // norms(A) | norms(B) on the helper stream; convert(A); join; convert(B).
-    if (!os->aux) {
-      SKG_CUDA(cudaStreamCreateWithFlags(&os->aux, cudaStreamNonBlocking));
-      SKG_CUDA(cudaEventCreateWithFlags(&os->fork, cudaEventDisableTiming));
-      SKG_CUDA(cudaEventCreateWithFlags(&os->join, cudaEventDisableTiming));
-    }
-    SKG_CUDA(cudaEventRecord(os->fork, s));
-    SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork, 0));
-    const int st_b = prep_norms<32>(N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b, os->aux);
-    SKG_CUDA(cudaEventRecord(os->join, os->aux));  // join even when the B step failed
-    if (st_b) return st_b;
-    if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a,
-                              ws->err, s)))
-      return st;
-    SKG_CUDA(cudaStreamWaitEvent(s, os->join, 0));
-    if ((st = prep_convert<32>(dev, N, K, KP, RB, Bp, L, os->res_b, os->mu_b, ws->err, s)))
-      return st;
-    resB = &os->res_b;
-    muB = &os->mu_b;
-  }
   LanePlan* pl = nullptr;
   if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, kSegKbCapSigned, &pl)) !=
       SKGEMM_OK)
@@ -939,6 +902,94 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
       pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)muB->ptr,
       syrk ? 1 : 0, D, ldd, alpha, gamma, (syrk && gamma == 0.0) ? 1 : 0);
   SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+// Residues of A (packed16, M rows) into os->res_a and, unless Bp is null, of
+// B (packed32, N rows) into os->res_b: norms(A) | norms(B) on the helper
+// stream, convert(A), join, convert(B).
+int prep_pair(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M, int64_t N,
+              int64_t K, int L, const double* Ap, const double* Bp, cudaStream_t s) {
+  int st;
+  const int64_t KP = (K + 127) / 128 * 128;
+  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;  // 256-multiples serve both box heights
+  const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
+  if (!Bp)
+    return prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, ws->err, s);
+  if (!os->aux) {
+    SKG_CUDA(cudaStreamCreateWithFlags(&os->aux, cudaStreamNonBlocking));
+    SKG_CUDA(cudaEventCreateWithFlags(&os->fork, cudaEventDisableTiming));
+    SKG_CUDA(cudaEventCreateWithFlags(&os->join, cudaEventDisableTiming));
+  }
+  SKG_CUDA(cudaEventRecord(os->fork, s));
+  SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork, 0));
+  const int st_b = prep_norms<32>(N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b, os->aux);
+  SKG_CUDA(cudaEventRecord(os->join, os->aux));  // join even when the B step failed
+  if (st_b) return st_b;
+  if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, ws->err,
+                            s)))
+    return st;
+  SKG_CUDA(cudaStreamWaitEvent(s, os->join, 0));
+  return prep_convert<32>(dev, N, K, KP, RB, Bp, L, os->res_b, os->mu_b, ws->err, s);
+}
+
+// Shared body of the Ozaki GEMM and SYRK: residues of A (packed16) and B
+// (packed32 for GEMM; the SYRK reuses A's), lane-scheduled INT8 products,
+// reconstruction.
+int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp, bool syrk,
+                double* D, int64_t ldd, double alpha, double gamma, skgemm_options_t* opts,
+                cudaStream_t s) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  if (!Ap || !Bp || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  if (K == 0) return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki path needs K > 0");
+  if (M > (1 << 20) || N > (1 << 20)) return fail(SKGEMM_ERR_INVALID_ARG, "dimension too large");
+  int L, gb;
+  if ((st = choose_L(opts, K, &L, &gb)) != SKGEMM_OK) return st;
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  if ((st = ensure_consts(dev)) != SKGEMM_OK) return st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  OzakiStream* os = ozaki_stream(dev, s);
+  const int64_t KP = (K + 127) / 128 * 128;
+  if ((st = prep_pair(dev, os, ws, M, N, K, L, Ap, syrk ? nullptr : Bp, s))) return st;
+  const DeviceBuffer* resB = syrk ? &os->res_a : &os->res_b;
+  const DeviceBuffer* muB = syrk ? &os->mu_a : &os->mu_b;
+  if ((st = lanes_product(dev, os, ws, M, N, KP, L, syrk, resB, muB, D, ldd, alpha, gamma, s)))
+    return st;
+  report(opts, L, gb, K);
+  return SKGEMM_OK;
+}
+
+// Subspace pair S = alpha_s Psi^T Psi + beta_s S (upper, column-major) and
+// Hs = alpha_h Psi^T HPsi + gamma_h (row-major) sharing Psi's residues.
+int subspace_impl(int64_t K, int64_t M, const double* Psi, const double* HPsi, double* S,
+                   int64_t lds, double alpha_s, double beta_s, double* Hs, int64_t ldh,
+                   double alpha_h, double gamma_h, skgemm_options_t* opts, cudaStream_t s) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  if (M == 0) return SKGEMM_OK;
+  if (!Psi || !HPsi || !S || !Hs) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  if (K == 0) return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki path needs K > 0");
+  if (M > (1 << 20)) return fail(SKGEMM_ERR_INVALID_ARG, "dimension too large");
+  int L, gb;
+  if ((st = choose_L(opts, K, &L, &gb)) != SKGEMM_OK) return st;
+  std::lock_guard<std::mutex> lk(g_oz_mu);
+  if ((st = ensure_consts(dev)) != SKGEMM_OK) return st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  OzakiStream* os = ozaki_stream(dev, s);
+  const int64_t KP = (K + 127) / 128 * 128;
+  if ((st = prep_pair(dev, os, ws, M, M, K, L, Psi, HPsi, s))) return st;
+  if ((st = lanes_product(dev, os, ws, M, M, KP, L, true, &os->res_a, &os->mu_a, S, lds, alpha_s,
+                          beta_s, s)))
+    return st;
+  if ((st = lanes_product(dev, os, ws, M, M, KP, L, false, &os->res_b, &os->mu_b, Hs, ldh,
+                          alpha_h, gamma_h, s)))
+    return st;
   report(opts, L, gb, K);
   return SKGEMM_OK;
 }
@@ -1111,6 +1162,13 @@ size_t ozaki_stream_bytes(DeviceState* dev, cudaStream_t s) {
   const OzakiStream* os = it->second;
   return os->res_a.bytes + os->res_b.bytes + os->part_a.bytes + os->part_b.bytes +
          os->mu_a.bytes + os->mu_b.bytes + os->partials.bytes + os->rbytes.bytes;
+}
+
+int ozaki_subspace(int64_t K, int64_t M, const double* Psi, const double* HPsi, double* S,
+                   int64_t lds, double alpha_s, double beta_s, double* Hs, int64_t ldh,
+                   double alpha_h, double gamma_h, skgemm_options_t* opts, cudaStream_t s) {
+  return subspace_impl(K, M, Psi, HPsi, S, lds, alpha_s, beta_s, Hs, ldh, alpha_h, gamma_h, opts,
+                       s);
 }
 
 int ozaki_gemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp,

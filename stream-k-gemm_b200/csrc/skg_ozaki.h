@@ -13,6 +13,9 @@ int ozaki_gemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap, const d
                       skgemm_options_t* opts, cudaStream_t s);
 int ozaki_syrk_packed(int64_t K, int64_t M, const double* Ap, double* C, int64_t ldc,
                       double alpha, double beta, skgemm_options_t* opts, cudaStream_t s);
+int ozaki_subspace(int64_t K, int64_t M, const double* Psi, const double* HPsi, double* S,
+                   int64_t lds, double alpha_s, double beta_s, double* Hs, int64_t ldh,
+                   double alpha_h, double gamma_h, skgemm_options_t* opts, cudaStream_t s);
 int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
               skgemm_options_t* opts, cudaStream_t s);
 int ozaki_consume_error(DeviceState* dev, cudaStream_t s);

@@ -117,6 +117,8 @@ _SIGS = {
     "skgemm_dsyrk_packed_dev": [_i64, _i64, _vp, _vp, _i64, _d, _d, _vp],
     "skgemm_dsyrk_packed_dev_opt": [_i64, _i64, _vp, _vp, _i64, _d, _d,
                                     ctypes.POINTER(Options), _vp],
+    "skgemm_dsubspace_packed_dev": [_i64, _i64, _vp, _vp, _vp, _i64, _vp, _i64,
+                                    ctypes.POINTER(Options), _vp],
     "skgemm_drot": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_drot_dev": [_i64, _i64, _vp, _vp, _vp, _vp],
     "skgemm_drot_dev_opt": [_i64, _i64, _vp, _vp, _vp, ctypes.POINTER(Options), _vp],
@@ -286,6 +288,18 @@ def dsyrk_packed_dev(K, M, A_packed, C, ldc=None, alpha=1.0, beta=0.0, stream=No
         return None
     _check(lib().skgemm_dsyrk_packed_dev_opt(K, M, _dptr(A_packed), _dptr(C), ldc or M, alpha,
                                              beta, ctypes.byref(o), _stream(stream)))
+    return o
+
+
+def dsubspace_packed_dev(K, M, Psi_packed16, HPsi_packed32, S, Hs, lds=None, ldh=None,
+                         stream=None, precision=None, slices=0):
+    """S = Psi^T Psi (upper, column-major) and Hs = Psi^T HPsi (row-major) in one
+    call; with the Ozaki precision Psi is split once for both products."""
+    o = _opts(precision, slices)
+    _check(lib().skgemm_dsubspace_packed_dev(K, M, _dptr(Psi_packed16), _dptr(HPsi_packed32),
+                                             _dptr(S), lds or M, _dptr(Hs), ldh or M,
+                                             ctypes.byref(o) if o is not None else None,
+                                             _stream(stream)))
     return o
 
 

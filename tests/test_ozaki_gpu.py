@@ -121,3 +121,31 @@ def test_ozaki_deterministic(cuda):
     D1, _ = _gemm(A, B)
     D2, _ = _gemm(A, B)
     assert np.array_equal(D1, D2)
+
+
+@pytest.mark.parametrize("K,M,kind", [(20000, 512, "gauss"), (4099, 100, "uniform"),
+                                      (8000, 200, "stress"), (77, 33, "gauss")])
+@pytest.mark.parametrize("precision", [skgemm.PREC_NATIVE, OZ])
+def test_subspace_pair_equals_separate_calls(cuda, K, M, kind, precision):
+    """skgemm_dsubspace_packed_dev (one split of Psi for S and Hs) returns what
+    the two separate calls return, bit for bit, and both are within 1e-13 of
+    the Dot2 oracle."""
+    gen = {"gauss": gaussian, "uniform": uniform, "stress": stress}[kind]
+    Psi = gen((K, M), 11 + M)
+    H = gen((K, M), 12 + M)
+    P16 = dev(oracle.pack(np.ascontiguousarray(Psi.T), 16))
+    H32 = dev(oracle.pack(np.ascontiguousarray(H.T), 32))
+    S = torch.zeros((M, M), dtype=torch.float64, device="cuda")
+    Hs = torch.full((M, M), np.nan, dtype=torch.float64, device="cuda")
+    S1, Hs1 = torch.zeros_like(S), torch.full_like(Hs, np.nan)
+    prec = None if precision == skgemm.PREC_NATIVE else OZ
+    skgemm.dsubspace_packed_dev(K, M, P16, H32, S, Hs, precision=prec)
+    skgemm.dsyrk_packed_dev(K, M, P16, S1, M, precision=prec)
+    skgemm.dgemm_packed_dev(M, M, K, P16, H32, Hs1, M, precision=prec)
+    skgemm.stream_status()
+    iu = np.triu_indices(M)
+    s, s1 = S.cpu().numpy().T, S1.cpu().numpy().T  # column-major -> [i, j]
+    assert np.array_equal(s[iu], s1[iu])
+    assert np.array_equal(Hs.cpu().numpy(), Hs1.cpu().numpy())
+    assert oracle.rel_frobenius(s[iu], oracle.dot2_matmul(Psi.T, Psi)[iu]) <= TOL
+    assert oracle.rel_frobenius(Hs.cpu().numpy(), oracle.dot2_matmul(Psi.T, H)) <= TOL
