@@ -68,6 +68,11 @@ def parse():
     ap.add_argument("--workload", default="subspace", choices=["subspace", "batched", "serving"])
     ap.add_argument("--requests", type=int, default=2000, help="serving: trace length")
     ap.add_argument("--instances", type=int, default=64, help="batched: k-point instances")
+    ap.add_argument("--max-grid", type=int, default=0,
+                    help="batched: cap on grid points per instance (smaller cases for profiling)")
+    ap.add_argument("--tile", type=int, default=0, choices=[0, 64, 128],
+                    help="batched: output tile (0 = autotune)")
+    ap.add_argument("--no-tune", action="store_true", help="batched: cost-model plan, no timing")
     a = ap.parse_args()
     set_shape(a.nd, a.nb)
     return a
@@ -211,11 +216,16 @@ def run_gpu(args):
     def step(evs=None):
         if evs:
             evs[0].record(stream)
-        skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, 1.0, 0.0, stream=stream, precision=prec)
-        if evs:
-            evs[1].record(stream)
-        skgemm.dgemm_packed_dev(NB, NB, ND, band, h32, Hs, NB, 1.0, 0.0, stream=stream,
-                                precision=prec)
+        if prec is None:
+            skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, 1.0, 0.0, stream=stream)
+            if evs:
+                evs[1].record(stream)
+            skgemm.dgemm_packed_dev(NB, NB, ND, band, h32, Hs, NB, 1.0, 0.0, stream=stream)
+        else:
+            # S and Hs share one split of Psi (skgemm_dsubspace_packed_dev).
+            skgemm.dsubspace_packed_dev(ND, NB, band, h32, S, Hs, stream=stream, precision=prec)
+            if evs:
+                evs[1].record(stream)
         if evs:
             evs[2].record(stream)
         skgemm.drot_dev(ND, NB, grid, q, Pn, stream=stream, precision=prec)
@@ -243,6 +253,19 @@ def run_gpu(args):
     step_ms = per_op.sum(axis=1)
     kernel_ms = float(per_op.sum())
     achieved = FLOP_STEP * args.steps / (kernel_ms * 1e-3) / 1e12
+    if prec is None:
+        op_ms = {"syrk": round(float(per_op[:, 0].mean()), 4),
+                 "gemm": round(float(per_op[:, 1].mean()), 4),
+                 "rotation": round(float(per_op[:, 2].mean()), 4)}
+        op_tf = {"syrk": round(FLOP_SYRK / per_op[:, 0].mean() / 1e9, 3),
+                 "gemm": round(FLOP_GEMM / per_op[:, 1].mean() / 1e9, 3),
+                 "rotation": round(FLOP_ROT / per_op[:, 2].mean() / 1e9, 3)}
+    else:
+        pair = per_op[:, 0] + per_op[:, 1]
+        op_ms = {"syrk+gemm": round(float(pair.mean()), 4),
+                 "rotation": round(float(per_op[:, 2].mean()), 4)}
+        op_tf = {"syrk+gemm": round((FLOP_SYRK + FLOP_GEMM) / pair.mean() / 1e9, 3),
+                 "rotation": round(FLOP_ROT / per_op[:, 2].mean() / 1e9, 3)}
 
     line = {
         "metric": METRIC, "value": round(FLOP_STEP * args.steps * world / (total_ms * 1e-3) / 1e12, 3),
@@ -252,21 +275,17 @@ def run_gpu(args):
         "config": {"workload": WORKLOAD, "Nd": ND, "nb": NB, "ops": ["syrk", "gemm", "rotation"],
                    "precision": args.precision, "parallelism": f"replicas{world}",
                    "flop_per_step": FLOP_STEP, "l2": "inputs larger than L2 (453 MB each)"},
-        "latency_ms": {"p50": round(float(np.percentile(step_ms, 50)), 4),
-                       "p99": round(float(np.percentile(step_ms, 99)), 4),
-                       "syrk": round(float(per_op[:, 0].mean()), 4),
-                       "gemm": round(float(per_op[:, 1].mean()), 4),
-                       "rotation": round(float(per_op[:, 2].mean()), 4)},
-        "op_tflops": {"syrk": round(FLOP_SYRK / per_op[:, 0].mean() / 1e9, 3),
-                      "gemm": round(FLOP_GEMM / per_op[:, 1].mean() / 1e9, 3),
-                      "rotation": round(FLOP_ROT / per_op[:, 2].mean() / 1e9, 3)},
+        "latency_ms": dict({"p50": round(float(np.percentile(step_ms, 50)), 4),
+                            "p99": round(float(np.percentile(step_ms, 99)), 4)}, **op_ms),
+        "op_tflops": op_tf,
         "roofline": {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
                      "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
                      "peak_source": "measured FP64 DMMA peak (skgemm_probe_fp64_peak, this run)",
-                     "kernel": "fp64_streamk_kernel",
-                     "traffic": read_profile_traffic()},
+                     "kernel": "fp64_streamk_kernel" if prec is None else
+                     "Ozaki split (i8_gemm_kernel + residue conversion), FP64-equivalent flops",
+                     "traffic": read_profile_traffic() if prec is None else None},
         "clocks": clk,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": (3 if prec is None else 16) * args.steps,
     }
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, band, h32, grid, q, dist)
@@ -451,6 +470,8 @@ def run_batched(args):
     rank, world, dist = dist_setup(args.gpus)
     dev = torch.device("cuda", torch.cuda.current_device())
     shapes = batched_instances(args.instances)
+    if args.max_grid:
+        shapes = [(min(ng, args.max_grid), nb) for ng, nb in shapes]
     g = torch.Generator(device=dev).manual_seed(7 + rank)
     items, keep, flop = [], [], 0.0
     for ng, nb in shapes:
@@ -467,7 +488,8 @@ def run_batched(args):
                   skgemm.batch_item(skgemm.OP_GEMM_PACKED, nb, nb, ng, p16, h32, Hs, nb)]
         flop += nb * nb * ng + 2.0 * nb * nb * ng
     stream = torch.cuda.current_stream()
-    plan = skgemm.Plan(items, stream=stream)
+    plan = skgemm.Plan(items, tile=args.tile, order=2 if args.no_tune else 0,
+                       tune=not args.no_tune, stream=stream)
     cfg = plan.config
     peak = skgemm.probe_fp64_peak()
     for _ in range(args.warmup):
@@ -493,7 +515,8 @@ def run_batched(args):
         "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"kpoint_batch_{args.instances}x_syrk_gemm",
+        "config": {"workload": f"kpoint_batch_{args.instances}x_syrk_gemm"
+                               + (f"_grid_le_{args.max_grid}" if args.max_grid else ""),
                    "instances": args.instances, "flop_per_step": flop,
                    "bytes_resident": mem, "tile": cfg["tile"], "grid": cfg["grid"],
                    "order": cfg["order"], "candidates_timed": cfg["candidates_timed"],
