@@ -149,3 +149,63 @@ def test_subspace_pair_equals_separate_calls(cuda, K, M, kind, precision):
     assert np.array_equal(Hs.cpu().numpy(), Hs1.cpu().numpy())
     assert oracle.rel_frobenius(s[iu], oracle.dot2_matmul(Psi.T, Psi)[iu]) <= TOL
     assert oracle.rel_frobenius(Hs.cpu().numpy(), oracle.dot2_matmul(Psi.T, H)) <= TOL
+
+
+@pytest.mark.slow
+def test_ozaki_error_table_subspace_shapes(cuda):
+    """Errors of S, Hs and Psi Q against the Dot2 oracle per moduli count, at
+    the DFT subspace shapes (Psi, HPsi 110592 x 512, Q 512 x 512) on
+    Gaussian N(0,1)/sqrt(Nd) and exponent-stress inputs. The relative
+    Frobenius error is estimated from 4096 sampled entries per result (Dot2
+    on the sample). Printed as a table (pytest -s); the automatic choice must
+    meet the 1e-13 gate on every result and input."""
+    Nd, nb, ns = 110592, 512, 4096
+    rng = np.random.default_rng(77)
+    ii, jj = rng.integers(0, nb, ns), rng.integers(0, nb, ns)
+    iu_i, iu_j = np.minimum(ii, jj), np.maximum(ii, jj)  # SYRK: upper triangle
+    gg, bb = rng.integers(0, Nd, ns), rng.integers(0, nb, ns)
+    table = []
+    for kind in ("gauss", "stress"):
+        if kind == "gauss":
+            Psi = gaussian((Nd, nb), 5, 1.0 / np.sqrt(Nd))
+            H = gaussian((Nd, nb), 6, 1.0 / np.sqrt(Nd))
+        else:
+            Psi = stress((Nd, nb), 5)
+            H = stress((Nd, nb), 6)
+        Q = uniform((nb, nb), 7)
+        P16 = dev(oracle.pack(np.ascontiguousarray(Psi.T), 16))
+        H32 = dev(oracle.pack(np.ascontiguousarray(H.T), 32))
+        PG = dev(oracle.grid_pack(Psi))
+        dQ = dev(Q)
+        PsiT = np.ascontiguousarray(Psi.T)
+        ref_s = oracle.dot2_sampled(PsiT, Psi, iu_i, iu_j)
+        ref_h = oracle.dot2_sampled(PsiT, H, ii, jj)
+        ref_r = oracle.dot2_sampled(Psi, Q, gg, bb)
+        del PsiT
+        S = torch.zeros((nb, nb), dtype=torch.float64, device="cuda")
+        Hs = torch.zeros_like(S)
+        Pn = torch.empty(Nd * nb, dtype=torch.float64, device="cuda")
+        for L in (8, 10, 12, 13, 14, 15, 16, 0, -1):  # -1: native FP64 for comparison
+            prec = None if L < 0 else OZ
+            o = skgemm.dsubspace_packed_dev(Nd, nb, P16, H32, S, Hs, precision=prec,
+                                            slices=max(L, 0))
+            Ls = o.slices_used_out if o is not None else 0
+            orot = skgemm.drot_dev(Nd, nb, PG, dQ, Pn, precision=prec, slices=max(L, 0))
+            Lr = orot.slices_used_out if orot is not None else 0
+            skgemm.stream_status()
+            s = S.cpu().numpy().T[iu_i, iu_j]            # column-major S -> [i, j]
+            h = Hs.cpu().numpy()[ii, jj]
+            pr = oracle.band_unpack(Pn.cpu().numpy().reshape(nb // 16, Nd, 16), Nd)[gg, bb]
+            e = [float(np.linalg.norm(x - r) / np.linalg.norm(r))
+                 for x, r in ((s, ref_s), (h, ref_h), (pr, ref_r))]
+            table.append((kind, L, Ls, Lr, *e))
+    print("\ninput   slices(req; -1 native) used(S,Hs) used(rot)  err(S)  err(Hs)  err(PsiQ)")
+    for kind, L, Ls, Lr, es, eh, er in table:
+        print(f"{kind:7s} {L:11d} {Ls:10d} {Lr:9d}  {es:.2e}   {eh:.2e}   {er:.2e}")
+    for kind, L, Ls, Lr, es, eh, er in table:
+        if L == 0:
+            assert max(es, eh, er) <= TOL, (kind, es, eh, er)
+    for kind in ("gauss", "stress"):
+        rows = {L: (es, eh) for k, L, _, _, es, eh, _ in table if k == kind}
+        assert rows[8][0] > rows[12][0] > rows[16][0] * 0.999
+        assert rows[8][1] > rows[12][1] > rows[16][1] * 0.999
