@@ -558,6 +558,8 @@ struct LanePlan {
 
 struct OzakiStream {
   DeviceBuffer res_a, res_b, part_a, part_b, mu_a, mu_b, partials, rbytes;
+  DeviceBuffer partials2;  // Hs's slabs in the subspace pair (S's CRT still reads `partials`)
+  cudaEvent_t fork2 = nullptr, join2 = nullptr;
   // Helper stream forked from the caller's stream: the norm pass of B runs
   // there while A is converted (the conversion leaves HBM bandwidth idle).
   cudaStream_t aux = nullptr;
@@ -866,17 +868,18 @@ int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* s
 // D = alpha A B + gamma).
 int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M, int64_t N,
                   int64_t KP, int L, bool syrk, const DeviceBuffer* resB, const DeviceBuffer* muB,
-                  double* D, int64_t ldd, double alpha, double gamma, cudaStream_t s) {
+                  double* D, int64_t ldd, double alpha, double gamma, cudaStream_t s,
+                  DeviceBuffer* slabs = nullptr, cudaStream_t crt_stream = nullptr) {
   int st;
   const int KB = (int)(KP / 128);
   const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
+  DeviceBuffer& part = slabs ? *slabs : os->partials;
   LanePlan* pl = nullptr;
   if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, kSegKbCapSigned, &pl)) !=
       SKGEMM_OK)
     return st;
-  if ((st = os->partials.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t))))
-    return st;
+  if ((st = part.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t)))) return st;
   CUtensorMap mA, mB;
   if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, L, kI8BM))) return st;
   if ((st = make_res_map(&mB, resB->ptr, KP, syrk ? RA : RB, L, kI8BN))) return st;
@@ -893,15 +896,24 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   p.tiles = pl->tiles;
   p.lane_seg_off = pl->lane_seg_off;
   p.segs = pl->segs;
-  p.partials = (int32_t*)os->partials.ptr;
+  p.partials = (int32_t*)part.ptr;
   p.err = ws->err;
   if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s))) return st;
+  // The reconstruction runs on `crt_stream` (forked after the products) when
+  // given, so that it can overlap the caller's next launch on `s`.
+  cudaStream_t cs = s;
+  if (crt_stream) {
+    SKG_CUDA(cudaEventRecord(os->fork2, s));
+    SKG_CUDA(cudaStreamWaitEvent(crt_stream, os->fork2, 0));
+    cs = crt_stream;
+  }
   const int64_t n = M * N;
-  crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
-      (int)M, (int)N, L, (const int32_t*)os->partials.ptr, pl->T, pl->tile_index, pl->tiles_n,
+  crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, cs>>>(
+      (int)M, (int)N, L, (const int32_t*)part.ptr, pl->T, pl->tile_index, pl->tiles_n,
       pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)muB->ptr,
       syrk ? 1 : 0, D, ldd, alpha, gamma, (syrk && gamma == 0.0) ? 1 : 0);
   SKG_CUDA(cudaGetLastError());
+  if (crt_stream) SKG_CUDA(cudaEventRecord(os->join2, crt_stream));
   return SKGEMM_OK;
 }
 
@@ -984,12 +996,19 @@ int subspace_impl(int64_t K, int64_t M, const double* Psi, const double* HPsi, d
   OzakiStream* os = ozaki_stream(dev, s);
   const int64_t KP = (K + 127) / 128 * 128;
   if ((st = prep_pair(dev, os, ws, M, M, K, L, Psi, HPsi, s))) return st;
+  if (!os->fork2) {
+    SKG_CUDA(cudaEventCreateWithFlags(&os->fork2, cudaEventDisableTiming));
+    SKG_CUDA(cudaEventCreateWithFlags(&os->join2, cudaEventDisableTiming));
+  }
+  // S: products on s, reconstruction on the helper stream (overlaps Hs's
+  // products, which write their own slabs); join before returning.
   if ((st = lanes_product(dev, os, ws, M, M, KP, L, true, &os->res_a, &os->mu_a, S, lds, alpha_s,
-                          beta_s, s)))
+                          beta_s, s, &os->partials, os->aux)))
     return st;
-  if ((st = lanes_product(dev, os, ws, M, M, KP, L, false, &os->res_b, &os->mu_b, Hs, ldh,
-                          alpha_h, gamma_h, s)))
-    return st;
+  st = lanes_product(dev, os, ws, M, M, KP, L, false, &os->res_b, &os->mu_b, Hs, ldh, alpha_h,
+                     gamma_h, s, &os->partials2, nullptr);
+  SKG_CUDA(cudaStreamWaitEvent(s, os->join2, 0));
+  if (st) return st;
   report(opts, L, gb, K);
   return SKGEMM_OK;
 }
@@ -1146,8 +1165,12 @@ int ozaki_release_stream(DeviceState* dev, cudaStream_t s) {
     cudaEventDestroy(os->fork);
     cudaEventDestroy(os->join);
   }
+  if (os->fork2) {
+    cudaEventDestroy(os->fork2);
+    cudaEventDestroy(os->join2);
+  }
   for (DeviceBuffer* b : {&os->res_a, &os->res_b, &os->part_a, &os->part_b, &os->mu_a, &os->mu_b,
-                          &os->partials, &os->rbytes})
+                          &os->partials, &os->partials2, &os->rbytes})
     b->release();
   delete os;
   m.erase(it);
@@ -1161,7 +1184,8 @@ size_t ozaki_stream_bytes(DeviceState* dev, cudaStream_t s) {
   if (it == g_oz[dev->device].streams.end()) return 0;
   const OzakiStream* os = it->second;
   return os->res_a.bytes + os->res_b.bytes + os->part_a.bytes + os->part_b.bytes +
-         os->mu_a.bytes + os->mu_b.bytes + os->partials.bytes + os->rbytes.bytes;
+         os->mu_a.bytes + os->mu_b.bytes + os->partials.bytes + os->partials2.bytes +
+         os->rbytes.bytes;
 }
 
 int ozaki_subspace(int64_t K, int64_t M, const double* Psi, const double* HPsi, double* S,
