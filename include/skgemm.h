@@ -59,6 +59,9 @@ extern "C" {
  * FP64 reconstruction. */
 #define SKGEMM_PREC_NATIVE 0
 #define SKGEMM_PREC_OZAKI_I8 1
+/* Batched plans only: per problem, whichever of the two is faster (cost
+ * model, confirmed by timing when the plan tunes). */
+#define SKGEMM_PREC_AUTO 2
 
 typedef struct skgemm_options {
   int precision;        /* SKGEMM_PREC_* */
@@ -232,11 +235,14 @@ typedef struct skgemm_batch_item {
 /* Plan options. Zero-initialised options = autotune everything, capture a
  * graph. Out fields report the chosen configuration. */
 typedef struct skgemm_plan_options {
-  int tile;     /* output tile: 128 (128x128), 64 (64x64) or 0 = autotune */
-  int grid;     /* persistent CTAs (Stream-K split factor); 0 = all SMs x occupancy */
-  int order;    /* problem order: 1 = as given, 2 = most work first, 0 = autotune */
-  int no_tune;  /* 1: do not time candidates, pick by the cost model alone */
-  int no_graph; /* 1: plain stream launches instead of a CUDA graph */
+  int tile;      /* output tile: 128 (128x128), 64 (64x64) or 0 = autotune */
+  int grid;      /* persistent CTAs (Stream-K split factor); 0 = all SMs x occupancy */
+  int order;     /* problem order: 1 = as given, 2 = most work first, 0 = autotune */
+  int no_tune;   /* 1: do not time candidates, pick by the cost model alone */
+  int no_graph;  /* 1: plain stream launches instead of a CUDA graph */
+  int precision; /* SKGEMM_PREC_NATIVE (default), _OZAKI_I8 or _AUTO */
+  int slices;    /* Ozaki moduli, 0 = automatic (accuracy target 1e-13) */
+  int ozaki_problems_out; /* problems the plan runs on the Ozaki path */
   int tile_out, grid_out, order_out;
   int candidates_timed_out;
   double tuned_ms_out; /* device time of the chosen configuration (ms), 0 if untimed */
@@ -246,8 +252,10 @@ typedef struct skgemm_plan_options {
 typedef struct skgemm_plan* skgemm_plan_t;
 
 /* Builds a plan for `n` items on the current device: validates every item,
- * builds the problem table and TMA descriptors in device memory, chooses the
- * tile shape, problem order and grid (autotuning times the candidate
+ * chooses each problem's precision (SKGEMM_PREC_AUTO: native FP64 in the
+ * grouped launch, or the Ozaki split with the moduli count the accuracy
+ * target needs), builds the problem table and TMA descriptors in device
+ * memory, chooses the tile shape, problem order and grid (autotuning times the candidate
  * configurations on the items' own buffers, so outputs hold unspecified
  * values afterwards, except SYRK outputs with beta != 0, which are restored),
  * and captures [flag reset, grouped launch] in a CUDA graph. Pointers in

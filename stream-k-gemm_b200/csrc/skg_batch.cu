@@ -17,6 +17,16 @@
 // most-work-first, and the grid. The cost model is the useful/issued MAC
 // ratio of the tiles; tuning times each candidate with CUDA events on the
 // items' own buffers and keeps the fastest (cached per batch signature).
+//
+// Precision per problem: a plan may run some problems through the Ozaki
+// split (skg_ozaki.cu) instead of the grouped FP64 launch. Under
+// SKGEMM_PREC_AUTO the cost model compares each problem's share of the
+// grouped launch (issued MACs at the measured DMMA rate) with the Ozaki
+// kernels' estimate (ozaki_time_estimate) and picks Ozaki where it is below
+// 0.8 of native; tuning also times the all-native assignment and keeps the
+// faster. Ozaki problems run one after another on a stream the plan owns, so
+// their scratch buffers (which the captured graph references) belong to the
+// plan and cannot be regrown by unrelated calls.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -29,6 +39,7 @@
 
 #include "skg_batch.h"
 #include "skg_fp64_types.h"
+#include "skg_ozaki.h"
 #include "skg_runtime.h"
 
 namespace skg {
@@ -107,14 +118,21 @@ struct Config {
   int tile = 128, order = 1, grid = 0;
 };
 
-// Tuning results per batch signature (shapes, ops, device).
+// A tuned configuration and the items it runs through the Ozaki split.
+struct Tuned {
+  Config cfg;
+  std::vector<char> oz;
+};
+
+// Tuning results per batch signature (shapes, ops, device, options).
 std::mutex g_tune_mu;
-std::map<std::string, Config> g_tune_cache;
+std::map<std::string, Tuned> g_tune_cache;
 
 std::string signature(int device, const std::vector<skgemm_batch_item_t>& items,
                       const skgemm_plan_options_t& o) {
   std::string s = std::to_string(device) + "|" + std::to_string(o.tile) + "," +
-                  std::to_string(o.order) + "," + std::to_string(o.grid) + "|";
+                  std::to_string(o.order) + "," + std::to_string(o.grid) + "," +
+                  std::to_string(o.precision) + "," + std::to_string(o.slices) + "|";
   char buf[96];
   for (const auto& it : items) {
     snprintf(buf, sizeof(buf), "%d:%lld:%lld:%lld;", it.op, (long long)it.M, (long long)it.N,
@@ -133,6 +151,8 @@ struct BatchPlan {
   std::vector<skgemm_batch_item_t> items;
   std::vector<Fp64Problem> probs;
   std::vector<int> k0_items;  // items with an empty reduction and a non-empty output
+  std::vector<char> oz;       // per item: runs through the Ozaki split
+  int slices = 0;             // Ozaki moduli (0 = accuracy target)
   Config cfg;
   double efficiency = 0.0;
   Fp64Group group{};
@@ -140,12 +160,24 @@ struct BatchPlan {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
+  // Ozaki problems run on `ostream` (its scratch is the plan's), forked from
+  // and joined back to the caller's stream.
+  cudaStream_t ostream = nullptr;
+  cudaEvent_t ofork = nullptr, ojoin = nullptr;
+
+  int num_ozaki() const { return (int)std::count(oz.begin(), oz.end(), (char)1); }
 
   ~BatchPlan() {
     // Launches of the plan may still be in flight on any stream.
     cudaDeviceSynchronize();
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    if (ostream) {
+      skgemm_stream_release(ostream);
+      cudaStreamDestroy(ostream);
+    }
+    if (ofork) cudaEventDestroy(ofork);
+    if (ojoin) cudaEventDestroy(ojoin);
     d_probs.release();
     d_maps.release();
     d_iters.release();
@@ -239,7 +271,11 @@ namespace {
 int configure(BatchPlan* P, Config c) {
   const int BM = c.tile, BN = c.tile;
   GroupTables T;
-  int st0 = build_group_tables(P->probs, c.tile, c.order, &T);
+  std::vector<Fp64Problem> native;
+  native.reserve(P->probs.size());
+  for (size_t i = 0; i < P->probs.size(); ++i)
+    if (!P->oz[i]) native.push_back(P->probs[i]);
+  int st0 = build_group_tables(native, c.tile, c.order, &T);
   if (st0) return st0;
   std::vector<Fp64Params>& hp = T.params;
   std::vector<CUtensorMap>& hm = T.maps;
@@ -286,7 +322,27 @@ int configure(BatchPlan* P, Config c) {
   return SKGEMM_OK;
 }
 
-// Enqueues the plan's work on `s`: the grouped launch and the K == 0 items.
+// One item through the Ozaki split on `s`.
+int run_ozaki_item(const skgemm_batch_item_t& it, int slices, cudaStream_t s) {
+  skgemm_options_t o;
+  memset(&o, 0, sizeof(o));
+  o.precision = SKGEMM_PREC_OZAKI_I8;
+  o.slices = slices;
+  switch (it.op) {
+    case SKGEMM_OP_GEMM_PACKED:
+      return ozaki_gemm_packed(it.M, it.N, it.K, it.A, it.B, it.D, it.ldd, it.alpha, it.beta, &o,
+                               s);
+    case SKGEMM_OP_SYRK_PACKED:
+      return ozaki_syrk_packed(it.K, it.M, it.A, it.D, it.ldd, it.alpha, it.beta, &o, s);
+    case SKGEMM_OP_ROT:
+      return ozaki_rot(it.M, it.N, it.A, it.B, it.D, &o, s);
+    default:
+      return fail(SKGEMM_ERR_INVALID_ARG, "batch item: unknown op");
+  }
+}
+
+// Enqueues the plan's work on `s`: the grouped launch, the K == 0 items, then
+// the Ozaki items on the plan's stream (ordered after the grouped launch).
 int enqueue(BatchPlan* P, cudaStream_t s) {
   int st;
   if (P->group.num_problems > 0 &&
@@ -296,6 +352,23 @@ int enqueue(BatchPlan* P, cudaStream_t s) {
     const Fp64Problem& pr = P->probs[i];
     if ((st = run_k0(pr.out_kind, pr.M, pr.N, pr.D, pr.ldd, pr.gamma, pr.beta_zero, s)))
       return st;
+  }
+  if (P->num_ozaki() > 0) {
+    SKG_CUDA(cudaEventRecord(P->ofork, s));
+    SKG_CUDA(cudaStreamWaitEvent(P->ostream, P->ofork, 0));
+    for (size_t i = 0; i < P->items.size(); ++i) {
+      if (!P->oz[i]) continue;
+      if ((st = run_ozaki_item(P->items[i], P->slices, P->ostream)) != SKGEMM_OK) {
+        char buf[64];
+        snprintf(buf, sizeof(buf), " (Ozaki item %d)", (int)i);
+        const std::string msg = skgemm_last_error() + std::string(buf);
+        cudaEventRecord(P->ojoin, P->ostream);
+        cudaStreamWaitEvent(s, P->ojoin, 0);
+        return fail(st, msg);
+      }
+    }
+    SKG_CUDA(cudaEventRecord(P->ojoin, P->ostream));
+    SKG_CUDA(cudaStreamWaitEvent(s, P->ojoin, 0));
   }
   return SKGEMM_OK;
 }
@@ -323,6 +396,11 @@ int time_config(BatchPlan* P, cudaStream_t s, float* ms_out) {
 }
 
 int read_err(BatchPlan* P) {
+  if (P->ostream) {
+    // Device error word of the Ozaki kernels (kept per stream).
+    int st = skgemm_stream_status(P->ostream);
+    if (st) return st;
+  }
   uint32_t word = 0;
   SKG_CUDA(cudaMemcpy(&word, P->d_err.ptr, sizeof(word), cudaMemcpyDeviceToHost));
   if (word == 0) return SKGEMM_OK;
@@ -340,6 +418,7 @@ int build_plan(const skgemm_batch_item_t* items, int n, BatchPlan* P) {
   if (n < 0 || (n > 0 && !items)) return fail(SKGEMM_ERR_INVALID_ARG, "bad item array");
   P->items.assign(items, items + n);
   P->probs.resize(n);
+  P->oz.assign(n, 0);
   for (int i = 0; i < n; ++i) {
     if ((st = item_problem(items[i], &P->probs[i])) != SKGEMM_OK) {
       char buf[64];
@@ -350,6 +429,71 @@ int build_plan(const skgemm_batch_item_t* items, int n, BatchPlan* P) {
     if (pr.M > 0 && pr.N > 0 && pr.K == 0 && pr.out_kind != kOutBand16) P->k0_items.push_back(i);
   }
   return SKGEMM_OK;
+}
+
+// Cost-model time (s) of a problem's share of the grouped FP64 launch: issued
+// MACs at the sustained DMMA rate (16e12 MAC/s for 128 x 128 tiles, 0.9 of it
+// for 64 x 64).
+double native_estimate(const Fp64Problem& p) {
+  const double i128 = geom_of(p, 128, 128).issued, i64 = geom_of(p, 64, 64).issued;
+  return std::min(i128 / 16e12, i64 / (0.9 * 16e12));
+}
+
+// Items run through the Ozaki split: none (native), every one the Ozaki path
+// takes (Ozaki), or those whose estimate is below 0.8 of native (auto).
+std::vector<char> assign_precision(const BatchPlan& P, int precision, int slices) {
+  std::vector<char> oz(P.items.size(), 0);
+  if (precision == SKGEMM_PREC_NATIVE) return oz;
+  for (size_t i = 0; i < P.items.size(); ++i) {
+    const skgemm_batch_item_t& it = P.items[i];
+    const Fp64Problem& pr = P.probs[i];
+    if (pr.M == 0 || pr.N == 0 || pr.K == 0) continue;
+    const int64_t n = (it.op == SKGEMM_OP_SYRK_PACKED) ? it.M : it.N;
+    const double t = ozaki_time_estimate(it.op, it.M, n, it.K, slices);
+    if (t < 0.0) continue;
+    if (precision == SKGEMM_PREC_OZAKI_I8 || t < 0.8 * native_estimate(pr)) oz[i] = 1;
+  }
+  return oz;
+}
+
+// Copies of the SYRK outputs with beta != 0 (the product reads them), taken
+// before the runs made while building a plan and written back after them.
+struct SavedOutputs {
+  std::vector<std::pair<int, double*>> saved;
+
+  int save(const BatchPlan& P, cudaStream_t s) {
+    for (size_t i = 0; i < P.items.size(); ++i) {
+      const auto& it = P.items[i];
+      if (it.op == SKGEMM_OP_SYRK_PACKED && it.beta != 0.0 && it.M > 0) {
+        double* b = nullptr;
+        const size_t bytes = (size_t)it.ldd * it.M * sizeof(double);
+        SKG_CUDA(cudaMalloc(&b, bytes));
+        saved.push_back({(int)i, b});
+        SKG_CUDA(cudaMemcpyAsync(b, it.D, bytes, cudaMemcpyDeviceToDevice, s));
+      }
+    }
+    return SKGEMM_OK;
+  }
+  void restore(const BatchPlan& P, cudaStream_t s) {
+    for (auto& sv : saved) {
+      const auto& it = P.items[sv.first];
+      cudaMemcpyAsync(it.D, sv.second, (size_t)it.ldd * it.M * sizeof(double),
+                      cudaMemcpyDeviceToDevice, s);
+    }
+    cudaStreamSynchronize(s);
+    for (auto& sv : saved) cudaFree(sv.second);
+    saved.clear();
+  }
+  ~SavedOutputs() {
+    for (auto& sv : saved) cudaFree(sv.second);
+  }
+};
+
+std::vector<Fp64Problem> native_subset(const BatchPlan& P) {
+  std::vector<Fp64Problem> v;
+  for (size_t i = 0; i < P.probs.size(); ++i)
+    if (!P.oz[i]) v.push_back(P.probs[i]);
+  return v;
 }
 
 }  // namespace
@@ -392,12 +536,30 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
     return fail(SKGEMM_ERR_INVALID_ARG, "plan option tile must be 0, 128 or 64");
   if (o.order < 0 || o.order > 2) return fail(SKGEMM_ERR_INVALID_ARG, "plan option order");
   if (o.grid < 0) return fail(SKGEMM_ERR_INVALID_ARG, "plan option grid");
+  if (o.precision != SKGEMM_PREC_NATIVE && o.precision != SKGEMM_PREC_OZAKI_I8 &&
+      o.precision != SKGEMM_PREC_AUTO)
+    return fail(SKGEMM_ERR_INVALID_ARG, "plan option precision");
+  if (o.slices != 0 && (o.slices < 6 || o.slices > 16))
+    return fail(SKGEMM_ERR_INVALID_ARG, "plan option slices must be 0 or in [6, 16]");
   std::unique_ptr<BatchPlan> P(new BatchPlan());
   int st = build_plan(items, n, P.get());
   if (st) return st;
   P->use_graph = !o.no_graph;
+  P->slices = o.slices;
 
-  // Candidates.
+  // Precision assignments: the cost model's, and under auto also all-native
+  // (tuning keeps the faster).
+  std::vector<std::vector<char>> assigns;
+  assigns.push_back(assign_precision(*P, o.precision, o.slices));
+  const bool any_oz = std::count(assigns[0].begin(), assigns[0].end(), (char)1) > 0;
+  if (o.precision == SKGEMM_PREC_AUTO && any_oz) assigns.push_back(std::vector<char>(n, 0));
+  if (any_oz) {
+    SKG_CUDA(cudaStreamCreateWithFlags(&P->ostream, cudaStreamNonBlocking));
+    SKG_CUDA(cudaEventCreateWithFlags(&P->ofork, cudaEventDisableTiming));
+    SKG_CUDA(cudaEventCreateWithFlags(&P->ojoin, cudaEventDisableTiming));
+  }
+
+  // Configuration candidates of the grouped launch.
   std::vector<Config> cands;
   for (int tile : {128, 64}) {
     if (o.tile && o.tile != tile) continue;
@@ -410,17 +572,20 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
       cands.push_back(c);
     }
   }
-  // Cost model (model_tile): the tile with fewer issued MACs per unit rate;
-  // most-work-first order.
-  Config best = cands[0];
-  {
-    const int mt = model_tile(P->probs);
+  // Cost model (model_tile on the native problems): the tile with fewer
+  // issued MACs per unit rate; most-work-first order.
+  auto model_config = [&]() {
+    Config best = cands[0];
+    const int mt = model_tile(native_subset(*P));
     for (const auto& c : cands)
       if (c.tile == mt) {
         best = c;
         break;
       }
-  }
+    return best;
+  };
+  P->oz = assigns[0];
+  Tuned best{model_config(), assigns[0]};
   float best_ms = 0.f;
   int timed = 0;
   const std::string sig = signature(P->device, P->items, o);
@@ -435,46 +600,51 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
   }
   bool has_work = false;
   for (const auto& pr : P->probs) has_work |= (pr.M > 0 && pr.N > 0);
-  if (!o.no_tune && !cached && cands.size() > 1 && has_work) {
-    // SYRK outputs with beta != 0 are read by the product: keep a copy.
-    std::vector<std::pair<int, double*>> saved;
-    for (int i = 0; i < n; ++i) {
-      const auto& it = P->items[i];
-      if (it.op == SKGEMM_OP_SYRK_PACKED && it.beta != 0.0 && it.M > 0) {
-        double* b = nullptr;
-        const size_t bytes = (size_t)it.ldd * it.M * sizeof(double);
-        SKG_CUDA(cudaMalloc(&b, bytes));
-        SKG_CUDA(cudaMemcpyAsync(b, it.D, bytes, cudaMemcpyDeviceToDevice, s));
-        saved.push_back({i, b});
-      }
-    }
+  SavedOutputs saved;
+  bool ran = false;  // the plan's work has run on `s` (scratch allocated)
+  if (!o.no_tune && !cached && has_work && (cands.size() > 1 || assigns.size() > 1)) {
+    if ((st = saved.save(*P, s)) != SKGEMM_OK) return st;
     float ms_best = 1e30f;
-    for (const auto& c : cands) {
-      if ((st = configure(P.get(), c)) != SKGEMM_OK) break;
-      float ms = 0.f;
-      if ((st = time_config(P.get(), s, &ms)) != SKGEMM_OK) break;
-      ++timed;
-      if (ms < ms_best) {
-        ms_best = ms;
-        best = c;
+    for (const auto& asg : assigns) {
+      P->oz = asg;
+      bool native_work = false;
+      for (const auto& pr : native_subset(*P)) native_work |= (pr.M > 0 && pr.N > 0 && pr.K > 0);
+      for (size_t ci = 0; ci < cands.size() && st == SKGEMM_OK; ++ci) {
+        // Without native problems the grouped configuration does not matter.
+        if (!native_work && ci > 0) break;
+        if ((st = configure(P.get(), cands[ci])) != SKGEMM_OK) break;
+        float ms = 0.f;
+        if ((st = time_config(P.get(), s, &ms)) != SKGEMM_OK) break;
+        ran = true;
+        ++timed;
+        if (ms < ms_best) {
+          ms_best = ms;
+          best = Tuned{cands[ci], asg};
+        }
       }
+      if (st) break;
     }
-    for (auto& sv : saved) {
-      const auto& it = P->items[sv.first];
-      cudaMemcpyAsync(it.D, sv.second, (size_t)it.ldd * it.M * sizeof(double),
-                      cudaMemcpyDeviceToDevice, s);
-    }
-    cudaStreamSynchronize(s);
-    for (auto& sv : saved) cudaFree(sv.second);
+    saved.restore(*P, s);
     if (st) return st;
     if ((st = read_err(P.get())) != SKGEMM_OK) return st;
     best_ms = ms_best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[sig] = best;
   }
-  if ((st = configure(P.get(), best)) != SKGEMM_OK) return st;
+  P->oz = best.oz;
+  if ((st = configure(P.get(), best.cfg)) != SKGEMM_OK) return st;
 
-  if (P->use_graph && (P->group.num_problems > 0 || !P->k0_items.empty())) {
+  const bool has_oz = P->num_ozaki() > 0;
+  if (P->use_graph && (P->group.num_problems > 0 || !P->k0_items.empty() || has_oz)) {
+    if (has_oz && !ran) {
+      // The Ozaki calls allocate their scratch, lane plans and constants on
+      // first use, which stream capture does not allow: run once before.
+      if ((st = saved.save(*P, s)) != SKGEMM_OK) return st;
+      st = enqueue(P.get(), s);
+      saved.restore(*P, s);
+      if (st) return st;
+      if ((st = read_err(P.get())) != SKGEMM_OK) return st;
+    }
     cudaStream_t cap;
     SKG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
@@ -485,6 +655,8 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
       if (st == SKGEMM_OK && e == cudaSuccess) {
         P->graph = g;
         e = cudaGraphInstantiate(&P->exec, g, 0);
+      } else if (g) {
+        cudaGraphDestroy(g);
       }
     }
     cudaStreamDestroy(cap);
@@ -498,6 +670,7 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
     opts->candidates_timed_out = timed;
     opts->tuned_ms_out = best_ms;
     opts->model_efficiency_out = P->efficiency;
+    opts->ozaki_problems_out = P->num_ozaki();
   }
   *out = P.release();
   return SKGEMM_OK;

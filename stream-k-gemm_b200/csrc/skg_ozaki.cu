@@ -1195,6 +1195,47 @@ int ozaki_subspace(int64_t K, int64_t M, const double* Psi, const double* HPsi, 
                        s);
 }
 
+// Estimated device time (s) of one Ozaki call on this shape, from the
+// measured rates of its kernels on B200: conversion 0.38 ps per element and
+// modulus, the norm pass at 6 TB/s, INT8 products at 2.5 POP/s on the issued
+// (128 x 256-tile, 128-k padded) MACs of the lanes schedule or 1.4 POP/s on
+// the rotation's units schedule, reconstruction 15 ps per output and modulus
+// (lanes) or 4.4 ps per output (rotation band CRT), plus ~40 us of launches.
+// Negative when the Ozaki path does not take the shape (empty product,
+// nb > 2048 for the rotation). Batched plans use it to choose precision.
+double ozaki_time_estimate(int op, int64_t M, int64_t N, int64_t K, int slices) {
+  skgemm_options_t o;
+  memset(&o, 0, sizeof(o));
+  o.precision = SKGEMM_PREC_OZAKI_I8;
+  o.slices = slices;
+  int L, gb;
+  const double tile = (double)kI8BM * kI8BN;
+  if (op == SKGEMM_OP_ROT) {
+    if (N <= 0 || N > 2048 || M <= 0 || M > ((int64_t)1 << 30)) return -1.0;
+    if (choose_L(&o, N, &L, &gb)) return -1.0;
+    const double el = (double)M * N;
+    const double tiles = (double)((M + kI8BM - 1) / kI8BM) * ((N + kI8BN - 1) / kI8BN);
+    const double kp = (double)((N + 127) / 128 * 128);
+    return el * L * 0.38e-12 + el * 8 / 6e12 + 2.0 * tiles * tile * kp * L / 1.4e15 +
+           el * 4.4e-12 + 40e-6;
+  }
+  if (K <= 0 || M <= 0 || N <= 0 || M > (1 << 20) || N > (1 << 20)) return -1.0;
+  if (choose_L(&o, K, &L, &gb)) return -1.0;
+  const bool syrk = (op == SKGEMM_OP_SYRK_PACKED);
+  const int64_t tm = (M + kI8BM - 1) / kI8BM, tn = (N + kI8BN - 1) / kI8BN;
+  double tiles = 0.0;
+  if (syrk) {
+    for (int64_t j = 0; j < tn; ++j)
+      tiles += (double)std::min<int64_t>(tm, (j * kI8BN + kI8BN - 1) / kI8BM + 1);
+  } else {
+    tiles = (double)tm * tn;
+  }
+  const double el = (double)K * (syrk ? M : M + N);
+  const double kp = (double)((K + 127) / 128 * 128);
+  return el * L * 0.38e-12 + el * 8 / 6e12 + 2.0 * tiles * tile * kp * L / 2.5e15 +
+         (double)M * N * L * 15e-12 + 40e-6;
+}
+
 int ozaki_gemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp,
                       double* D, int64_t ldd, double alpha, double gamma,
                       skgemm_options_t* opts, cudaStream_t s) {

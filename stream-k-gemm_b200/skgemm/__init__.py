@@ -39,6 +39,7 @@ ERR_UNSUPPORTED = -6
 
 PREC_NATIVE = 0
 PREC_OZAKI_I8 = 1
+PREC_AUTO = 2  # batched plans: per problem, the faster path
 
 
 class SkgemmError(RuntimeError):
@@ -69,7 +70,8 @@ class PlanOptions(ctypes.Structure):
     """skgemm_plan_options_t."""
     _fields_ = [("tile", ctypes.c_int), ("grid", ctypes.c_int), ("order", ctypes.c_int),
                 ("no_tune", ctypes.c_int), ("no_graph", ctypes.c_int),
-                ("tile_out", ctypes.c_int), ("grid_out", ctypes.c_int),
+                ("precision", ctypes.c_int), ("slices", ctypes.c_int),
+                ("ozaki_problems_out", ctypes.c_int), ("tile_out", ctypes.c_int), ("grid_out", ctypes.c_int),
                 ("order_out", ctypes.c_int), ("candidates_timed_out", ctypes.c_int),
                 ("tuned_ms_out", ctypes.c_double), ("model_efficiency_out", ctypes.c_double)]
 
@@ -366,8 +368,10 @@ class Plan:
     """A tuned, graph-captured grouped launch of a fixed set of problems
     (skgemm_plan_create / _run / _status / _destroy)."""
 
-    def __init__(self, items, tile=0, grid=0, order=0, tune=True, graph=True, stream=None):
-        self.options = PlanOptions(tile, grid, order, 0 if tune else 1, 0 if graph else 1)
+    def __init__(self, items, tile=0, grid=0, order=0, tune=True, graph=True, stream=None,
+                 precision=PREC_NATIVE, slices=0):
+        self.options = PlanOptions(tile, grid, order, 0 if tune else 1, 0 if graph else 1,
+                                   precision, slices)
         self._items = _item_array(items)
         h = ctypes.c_void_p(0)
         _check(lib().skgemm_plan_create(self._items, len(items), ctypes.byref(self.options),
@@ -384,6 +388,7 @@ class Plan:
     def config(self) -> dict:
         o = self.options
         return {"tile": o.tile_out, "grid": o.grid_out, "order": o.order_out,
+                "ozaki_problems": o.ozaki_problems_out,
                 "candidates_timed": o.candidates_timed_out, "tuned_ms": o.tuned_ms_out,
                 "model_efficiency": o.model_efficiency_out}
 

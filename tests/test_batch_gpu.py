@@ -6,7 +6,9 @@ Gates: every item of a batch within relative Frobenius error 1e-13 of the
 Dot2 (double-double) oracle, whatever the tile shape, problem order, grid or
 graph capture; bytes outside each output's contract untouched; a replayed
 graph reads the current contents of the inputs; repeated runs bitwise equal;
-autotuning leaves SYRK outputs with beta != 0 as they were."""
+autotuning leaves SYRK outputs with beta != 0 as they were. Plans that run
+problems through the Ozaki split (precision Ozaki or auto) meet the same
+gates."""
 import numpy as np
 import pytest
 import torch
@@ -59,7 +61,9 @@ class Item:
     def reset(self):
         self.dD.copy_(dev(self.D0))
 
-    def check(self):
+    def check(self, sample=0):
+        """Relative Frobenius error against Dot2: over every entry, or over
+        `sample` random entries (long SYRK reductions)."""
         torch.cuda.synchronize()
         out = self.dD.cpu().numpy()
         if self.M == 0 or self.N == 0:
@@ -70,6 +74,16 @@ class Item:
             ref = oracle.dot2_matmul(self.A, self.B, self.alpha, self.beta)
             err = oracle.rel_frobenius(out[:, :self.N], ref)
             assert np.array_equal(out[:, self.N:], self.D0[:, self.N:])
+        elif self.op == skgemm.OP_SYRK_PACKED and sample:
+            C = out.reshape(self.M, self.ldd)
+            rng = np.random.default_rng(self.M + self.K)
+            a, b = rng.integers(0, self.M, sample), rng.integers(0, self.M, sample)
+            i, j = np.minimum(a, b), np.maximum(a, b)
+            S = oracle.dot2_sampled(self.X, self.X, i, j, x_strides=(1, self.M),
+                                    y_strides=(self.M, 1), K=self.K)
+            err = oracle.rel_frobenius(C[j, i], self.alpha * S + self.beta * self.D0[j, i])
+            il = np.tril_indices(self.M, -1)
+            assert np.array_equal(C[il[1], il[0]], self.D0[il[1], il[0]])
         elif self.op == skgemm.OP_SYRK_PACKED:
             C = out.reshape(self.M, self.ldd)  # row c = column c of C
             S = oracle.dot2_matmul(self.X.T, self.X)  # S[i, j]
@@ -253,3 +267,97 @@ def test_batch_kpoint_set_matches_single_calls(cuda):
         ref = oracle.dot2_sampled(P.T, Hh, ii, jj)
         got = Hs.cpu().numpy()[ii, jj]
         assert np.max(np.abs(got - ref)) <= TOL * np.sqrt(nb) * np.abs(ref).max() + 1e-300
+
+
+def ozaki_takes(it):
+    """Items the Ozaki path runs: a non-empty product (rotations up to 2048 states)."""
+    if it.M == 0 or it.N == 0:
+        return False
+    if it.op == skgemm.OP_ROT:
+        return it.N <= 2048
+    return it.K > 0
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_plan_ozaki_precision_mixed_batch(cuda, graph):
+    """Precision Ozaki: every item the split takes runs through it (K == 0 and
+    empty items stay on the native path); all within 1e-13 of Dot2; a replay
+    is bitwise equal to the first run."""
+    items = mixed_batch(500 + int(graph))
+    plan = skgemm.Plan([it.item() for it in items], tune=False, graph=graph,
+                       precision=skgemm.PREC_OZAKI_I8)
+    assert plan.config["ozaki_problems"] == sum(ozaki_takes(it) for it in items)
+    plan.run()
+    plan.status()
+    for it in items:
+        it.check()
+    first = [it.dD.clone() for it in items]
+    for it in items:
+        it.reset()
+    torch.cuda.synchronize()
+    plan.run()
+    plan.status()
+    assert all(torch.equal(it.dD, f) for it, f in zip(items, first))
+    plan.close()
+
+
+def test_plan_ozaki_graph_reads_current_inputs(cuda):
+    """The captured Ozaki kernels read the operands' current contents."""
+    items = mixed_batch(640)
+    plan = skgemm.Plan([it.item() for it in items], tune=False, precision=skgemm.PREC_OZAKI_I8)
+    plan.run()
+    plan.status()
+    for it in items:
+        it.reset()
+        if it.op == skgemm.OP_GEMM_PACKED and it.K > 0:
+            it.A = it.A * -0.5
+            it.dA.copy_(dev(oracle.pack(it.A, 16)))
+        elif it.op == skgemm.OP_ROT:
+            it.Q = it.Q[::-1].copy()
+            it.dB.copy_(dev(it.Q))
+    torch.cuda.synchronize()
+    plan.run()
+    plan.status()
+    for it in items:
+        it.check()
+
+
+def test_plan_auto_precision(cuda):
+    """Precision auto: the cost model sends the long-reduction SYRK through the
+    Ozaki split and keeps the small problems native; tuning times both
+    assignments and restores SYRK outputs with beta != 0; results within
+    1e-13 of Dot2 either way."""
+    G, S, R = skgemm.OP_GEMM_PACKED, skgemm.OP_SYRK_PACKED, skgemm.OP_ROT
+    big = Item(S, 900, 512, 512, 65536)
+    small = [Item(G, 901, 64, 64, 300), Item(S, 902, 100, 100, 777, 2.0, 0.5),
+             Item(R, 903, 2048, 64, 0), Item(G, 904, 40, 50, 0, 1.0, -3.0)]
+    items = [big] + small
+    plan = skgemm.Plan([it.item() for it in items], tune=False, precision=skgemm.PREC_AUTO)
+    assert plan.config["ozaki_problems"] == 1
+    plan.run()
+    plan.status()
+    big.check(sample=4096)
+    for it in small:
+        it.check()
+    for it in items:
+        it.reset()
+    torch.cuda.synchronize()
+    before = small[1].dD.clone()
+    tuned = skgemm.Plan([it.item() for it in items], precision=skgemm.PREC_AUTO)
+    cfg = tuned.config
+    assert cfg["candidates_timed"] > 4 and cfg["ozaki_problems"] in (0, 1)
+    torch.cuda.synchronize()
+    assert torch.equal(small[1].dD, before)
+    tuned.run()
+    tuned.status()
+    big.check(sample=4096)
+    for it in small:
+        it.check()
+
+
+def test_plan_precision_options_rejected(cuda):
+    it = Item(skgemm.OP_GEMM_PACKED, 1, 10, 20, 30)
+    with pytest.raises(skgemm.SkgemmError):
+        skgemm.Plan([it.item()], precision=7)
+    with pytest.raises(skgemm.SkgemmError):
+        skgemm.Plan([it.item()], precision=skgemm.PREC_OZAKI_I8, slices=5)
