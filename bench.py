@@ -17,7 +17,8 @@ Other workloads (not the default line):
     --workload batched   64 independent SYRK+GEMM k-point instances (grid
                          points from {24^3, 32^3, 40^3, 48^3, 64^3}, states
                          log-uniform in [64, 1024]) in one tuned, graph-captured
-                         grouped launch per step
+                         grouped launch per step; --precision ozaki|auto lets the
+                         plan send problems through the Ozaki split
     --workload serving   a Poisson stream (200 requests/s) of S -> Hs -> rotate
                          requests, grid points log-uniform in [1e4, 4e5], states
                          in [32, 2048], admitted under a 150 GB HBM budget;
@@ -59,7 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="skgemm", choices=["skgemm", "reference"])
-    ap.add_argument("--precision", default="native", choices=["native", "ozaki"])
+    ap.add_argument("--precision", default="native", choices=["native", "ozaki", "auto"],
+                    help="auto: batched workload only (the plan picks per problem)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nd", type=int, default=ND,
@@ -201,6 +203,8 @@ def run_gpu(args):
     import torch
     import skgemm
 
+    if args.precision == "auto":
+        raise SystemExit("--precision auto applies to --workload batched")
     rank, world, dist = dist_setup(args.gpus)
     dev = torch.device("cuda", torch.cuda.current_device())
     prec = skgemm.PREC_OZAKI_I8 if args.precision == "ozaki" else None
@@ -488,8 +492,10 @@ def run_batched(args):
                   skgemm.batch_item(skgemm.OP_GEMM_PACKED, nb, nb, ng, p16, h32, Hs, nb)]
         flop += nb * nb * ng + 2.0 * nb * nb * ng
     stream = torch.cuda.current_stream()
+    prec = {"native": skgemm.PREC_NATIVE, "ozaki": skgemm.PREC_OZAKI_I8,
+            "auto": skgemm.PREC_AUTO}[args.precision]
     plan = skgemm.Plan(items, tile=args.tile, order=2 if args.no_tune else 0,
-                       tune=not args.no_tune, stream=stream)
+                       tune=not args.no_tune, stream=stream, precision=prec)
     cfg = plan.config
     peak = skgemm.probe_fp64_peak()
     for _ in range(args.warmup):
@@ -521,15 +527,19 @@ def run_batched(args):
                    "bytes_resident": mem, "tile": cfg["tile"], "grid": cfg["grid"],
                    "order": cfg["order"], "candidates_timed": cfg["candidates_timed"],
                    "model_efficiency": round(cfg["model_efficiency"], 4),
-                   "launch": "one grouped persistent Stream-K launch per step, CUDA graph",
+                   "precision": args.precision, "ozaki_problems": cfg["ozaki_problems"],
+                   "launch": "one CUDA graph per step: the grouped persistent Stream-K "
+                             "launch (+ the Ozaki kernels of the problems sent there)",
                    "l2": "inputs larger than L2", "parallelism": f"replicas{world}"},
         "latency_ms": {"p50": round(float(np.percentile(per, 50)), 3),
                        "p99": round(float(np.percentile(per, 99)), 3)},
         "roofline": {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
                      "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
                      "peak_source": "measured FP64 DMMA peak (skgemm_probe_fp64_peak, this run)",
-                     "kernel": "fp64_grouped_kernel", "traffic": None},
-        "clocks": clk, "gpu_launches": 2 * args.steps,
+                     "kernel": "fp64_grouped_kernel" if cfg["ozaki_problems"] == 0 else
+                     "fp64_grouped_kernel + Ozaki split, FP64-equivalent flops",
+                     "traffic": None},
+        "clocks": clk, "gpu_launches": cfg["graph_kernels"] * args.steps,
     }
     plan.close()
     if rank == 0:
@@ -543,6 +553,8 @@ def run_serving(args):
     import numpy as np
     import torch
     import skgemm
+    if args.precision == "auto":
+        raise SystemExit("--precision auto applies to --workload batched")
     rank, world, dist = dist_setup(args.gpus)
     prec = skgemm.PREC_OZAKI_I8 if args.precision == "ozaki" else skgemm.PREC_NATIVE
     trace = skgemm.serve_trace(args.requests, rate=200.0, seed=11 + rank)

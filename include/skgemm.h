@@ -247,6 +247,7 @@ typedef struct skgemm_plan_options {
   int candidates_timed_out;
   double tuned_ms_out; /* device time of the chosen configuration (ms), 0 if untimed */
   double model_efficiency_out; /* useful MACs / issued MACs of the chosen tiles */
+  int graph_kernels_out; /* kernel nodes in the captured graph (0 without a graph) */
 } skgemm_plan_options_t;
 
 typedef struct skgemm_plan* skgemm_plan_t;
@@ -268,6 +269,9 @@ int skgemm_plan_run(skgemm_plan_t plan, void* stream);
 /* Synchronises `stream` and reports (then clears) device-side failures of the
  * plan's launches. */
 int skgemm_plan_status(skgemm_plan_t plan, void* stream);
+/* The path each of the plan's `n` items runs on: prec_out[i] =
+ * SKGEMM_PREC_NATIVE or SKGEMM_PREC_OZAKI_I8 (n must equal the item count). */
+int skgemm_plan_precisions(skgemm_plan_t plan, int* prec_out, int n);
 /* Releases the plan (synchronises the device first: its launches may still be
  * in flight). */
 void skgemm_plan_destroy(skgemm_plan_t plan);

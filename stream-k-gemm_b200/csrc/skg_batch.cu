@@ -24,7 +24,10 @@
 // grouped launch (issued MACs at the measured DMMA rate) with the Ozaki
 // kernels' estimate (ozaki_time_estimate) and picks Ozaki where it is below
 // 0.8 of native; tuning also times the all-native assignment and keeps the
-// faster. Ozaki problems run one after another on a stream the plan owns, so
+// faster. A SYRK and a GEMM of the same band-packed operand (S = Psi^T Psi and
+// Hs = Psi^T HPsi of one k-point) both sent to the Ozaki split run as one
+// subspace pair that converts Psi once (ozaki_subspace), and the cost model
+// prices them as a pair. Ozaki problems run one after another on a stream the plan owns, so
 // their scratch buffers (which the captured graph references) belong to the
 // plan and cannot be regrown by unrelated calls.
 #include <algorithm>
@@ -35,6 +38,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "skg_batch.h"
@@ -152,6 +156,9 @@ struct BatchPlan {
   std::vector<Fp64Problem> probs;
   std::vector<int> k0_items;  // items with an empty reduction and a non-empty output
   std::vector<char> oz;       // per item: runs through the Ozaki split
+  // Ozaki subspace pairs: for a SYRK item the index of its GEMM partner, -2
+  // for a GEMM item run by its SYRK partner, -1 otherwise.
+  std::vector<int> partner;
   int slices = 0;             // Ozaki moduli (0 = accuracy target)
   Config cfg;
   double efficiency = 0.0;
@@ -160,6 +167,7 @@ struct BatchPlan {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool use_graph = true;
+  int graph_kernels = 0;  // kernel nodes of the captured graph
   // Ozaki problems run on `ostream` (its scratch is the plan's), forked from
   // and joined back to the caller's stream.
   cudaStream_t ostream = nullptr;
@@ -266,6 +274,29 @@ int model_tile(const std::vector<Fp64Problem>& probs) {
 
 namespace {
 
+// Pairs (SYRK i, GEMM j) with the same band-packed operand, K and M = N = M_i
+// among the items flagged in `oz`: partner[i] = j, partner[j] = -2.
+std::vector<int> pair_items(const std::vector<skgemm_batch_item_t>& items,
+                            const std::vector<char>& oz) {
+  std::vector<int> partner(items.size(), -1);
+  std::map<std::tuple<const void*, int64_t, int64_t>, int> open;
+  for (size_t i = 0; i < items.size(); ++i) {
+    const auto& it = items[i];
+    if (oz[i] && it.op == SKGEMM_OP_SYRK_PACKED && it.M > 0 && it.K > 0)
+      open.emplace(std::make_tuple((const void*)it.A, it.K, it.M), (int)i);
+  }
+  for (size_t j = 0; j < items.size(); ++j) {
+    const auto& it = items[j];
+    if (!oz[j] || it.op != SKGEMM_OP_GEMM_PACKED || it.M != it.N) continue;
+    auto f = open.find(std::make_tuple((const void*)it.A, it.K, it.M));
+    if (f == open.end()) continue;
+    partner[f->second] = (int)j;
+    partner[j] = -2;
+    open.erase(f);
+  }
+  return partner;
+}
+
 // Builds the device-side problem table, descriptors and workspace of
 // configuration `c` (synchronous uploads; not during stream capture).
 int configure(BatchPlan* P, Config c) {
@@ -275,6 +306,7 @@ int configure(BatchPlan* P, Config c) {
   native.reserve(P->probs.size());
   for (size_t i = 0; i < P->probs.size(); ++i)
     if (!P->oz[i]) native.push_back(P->probs[i]);
+  P->partner = pair_items(P->items, P->oz);
   int st0 = build_group_tables(native, c.tile, c.order, &T);
   if (st0) return st0;
   std::vector<Fp64Params>& hp = T.params;
@@ -357,8 +389,20 @@ int enqueue(BatchPlan* P, cudaStream_t s) {
     SKG_CUDA(cudaEventRecord(P->ofork, s));
     SKG_CUDA(cudaStreamWaitEvent(P->ostream, P->ofork, 0));
     for (size_t i = 0; i < P->items.size(); ++i) {
-      if (!P->oz[i]) continue;
-      if ((st = run_ozaki_item(P->items[i], P->slices, P->ostream)) != SKGEMM_OK) {
+      if (!P->oz[i] || P->partner[i] == -2) continue;
+      if (P->partner[i] >= 0) {
+        const skgemm_batch_item_t& a = P->items[i];
+        const skgemm_batch_item_t& b = P->items[P->partner[i]];
+        skgemm_options_t o;
+        memset(&o, 0, sizeof(o));
+        o.precision = SKGEMM_PREC_OZAKI_I8;
+        o.slices = P->slices;
+        st = ozaki_subspace(a.K, a.M, a.A, b.B, a.D, a.ldd, a.alpha, a.beta, b.D, b.ldd, b.alpha,
+                            b.beta, &o, P->ostream);
+      } else {
+        st = run_ozaki_item(P->items[i], P->slices, P->ostream);
+      }
+      if (st != SKGEMM_OK) {
         char buf[64];
         snprintf(buf, sizeof(buf), " (Ozaki item %d)", (int)i);
         const std::string msg = skgemm_last_error() + std::string(buf);
@@ -452,6 +496,20 @@ std::vector<char> assign_precision(const BatchPlan& P, int precision, int slices
     const double t = ozaki_time_estimate(it.op, it.M, n, it.K, slices);
     if (t < 0.0) continue;
     if (precision == SKGEMM_PREC_OZAKI_I8 || t < 0.8 * native_estimate(pr)) oz[i] = 1;
+  }
+  if (precision == SKGEMM_PREC_AUTO) {
+    // Subspace pairs are priced together (one conversion of the shared operand).
+    std::vector<char> all(P.items.size(), 1);
+    const std::vector<int> partner = pair_items(P.items, all);
+    for (size_t i = 0; i < P.items.size(); ++i) {
+      const int j = partner[i];
+      if (j < 0) continue;
+      const skgemm_batch_item_t& it = P.items[i];
+      const double t = ozaki_pair_time_estimate(it.K, it.M, slices);
+      if (t < 0.0) continue;
+      const char pick = t < 0.8 * (native_estimate(P.probs[i]) + native_estimate(P.probs[j]));
+      oz[i] = oz[j] = pick;
+    }
   }
   return oz;
 }
@@ -655,6 +713,16 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
       if (st == SKGEMM_OK && e == cudaSuccess) {
         P->graph = g;
         e = cudaGraphInstantiate(&P->exec, g, 0);
+        size_t nn = 0;
+        if (e == cudaSuccess) e = cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (e == cudaSuccess && nn) e = cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (size_t i = 0; e == cudaSuccess && i < nn; ++i) {
+          cudaGraphNodeType t;
+          if ((e = cudaGraphNodeGetType(nodes[i], &t)) == cudaSuccess &&
+              t == cudaGraphNodeTypeKernel)
+            ++P->graph_kernels;
+        }
       } else if (g) {
         cudaGraphDestroy(g);
       }
@@ -671,6 +739,7 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
     opts->tuned_ms_out = best_ms;
     opts->model_efficiency_out = P->efficiency;
     opts->ozaki_problems_out = P->num_ozaki();
+    opts->graph_kernels_out = P->graph_kernels;
   }
   *out = P.release();
   return SKGEMM_OK;
@@ -904,6 +973,15 @@ SKG_EXPORT int skgemm_plan_run(skgemm_plan_t plan, void* stream) {
 SKG_EXPORT int skgemm_plan_status(skgemm_plan_t plan, void* stream) {
   if (!plan || !plan->impl) return fail(SKGEMM_ERR_INVALID_ARG, "null plan");
   return plan_status(plan->impl, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_plan_precisions(skgemm_plan_t plan, int* prec_out, int n) {
+  if (!plan || !plan->impl) return fail(SKGEMM_ERR_INVALID_ARG, "null plan");
+  const BatchPlan* P = plan->impl;
+  if (n != (int)P->oz.size() || (n > 0 && !prec_out))
+    return fail(SKGEMM_ERR_INVALID_ARG, "plan precisions: n must equal the item count");
+  for (int i = 0; i < n; ++i) prec_out[i] = P->oz[i] ? SKGEMM_PREC_OZAKI_I8 : SKGEMM_PREC_NATIVE;
+  return SKGEMM_OK;
 }
 
 SKG_EXPORT void skgemm_plan_destroy(skgemm_plan_t plan) {

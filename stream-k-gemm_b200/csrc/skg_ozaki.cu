@@ -1236,6 +1236,22 @@ double ozaki_time_estimate(int op, int64_t M, int64_t N, int64_t K, int slices) 
          (double)M * N * L * 15e-12 + 40e-6;
 }
 
+// Estimated device time (s) of ozaki_subspace (S and Hs from one split of
+// Psi): the SYRK and GEMM estimates less the conversion and norm pass of Psi
+// that the pair shares. Negative when the shape is not eligible.
+double ozaki_pair_time_estimate(int64_t K, int64_t M, int slices) {
+  const double ts = ozaki_time_estimate(SKGEMM_OP_SYRK_PACKED, M, M, K, slices);
+  const double tg = ozaki_time_estimate(SKGEMM_OP_GEMM_PACKED, M, M, K, slices);
+  if (ts < 0.0 || tg < 0.0) return -1.0;
+  skgemm_options_t o;
+  memset(&o, 0, sizeof(o));
+  o.slices = slices;
+  int L, gb;
+  if (choose_L(&o, K, &L, &gb)) return -1.0;
+  const double el = (double)K * M;
+  return ts + tg - (el * L * 0.38e-12 + el * 8 / 6e12);
+}
+
 int ozaki_gemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap, const double* Bp,
                       double* D, int64_t ldd, double alpha, double gamma,
                       skgemm_options_t* opts, cudaStream_t s) {

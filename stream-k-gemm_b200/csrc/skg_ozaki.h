@@ -22,6 +22,8 @@ int ozaki_consume_error(DeviceState* dev, cudaStream_t s);
 // Estimated device time (s) of an Ozaki call (op = SKGEMM_OP_*), < 0 if the
 // shape is not eligible.
 double ozaki_time_estimate(int op, int64_t M, int64_t N, int64_t K, int slices);
+// Estimated device time (s) of ozaki_subspace on (K, M), < 0 if not eligible.
+double ozaki_pair_time_estimate(int64_t K, int64_t M, int slices);
 int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, const int8_t* B,
              int64_t ldb, int32_t* C, int64_t ldc, cudaStream_t s);
 int probe_i8_peak(DeviceState* dev, double* tops);

@@ -73,7 +73,8 @@ class PlanOptions(ctypes.Structure):
                 ("precision", ctypes.c_int), ("slices", ctypes.c_int),
                 ("ozaki_problems_out", ctypes.c_int), ("tile_out", ctypes.c_int), ("grid_out", ctypes.c_int),
                 ("order_out", ctypes.c_int), ("candidates_timed_out", ctypes.c_int),
-                ("tuned_ms_out", ctypes.c_double), ("model_efficiency_out", ctypes.c_double)]
+                ("tuned_ms_out", ctypes.c_double), ("model_efficiency_out", ctypes.c_double),
+                ("graph_kernels_out", ctypes.c_int)]
 
 
 class ServeRequest(ctypes.Structure):
@@ -131,6 +132,7 @@ _SIGS = {
                            ctypes.POINTER(PlanOptions), _vp, ctypes.POINTER(_vp)],
     "skgemm_plan_run": [_vp, _vp],
     "skgemm_plan_status": [_vp, _vp],
+    "skgemm_plan_precisions": [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int],
     "skgemm_batch_dev": [ctypes.POINTER(BatchItem), ctypes.c_int, _vp],
     "skgemm_serve_run": [ctypes.POINTER(ServeRequest), ctypes.c_int,
                          ctypes.POINTER(ServeOptions)],
@@ -373,6 +375,7 @@ class Plan:
         self.options = PlanOptions(tile, grid, order, 0 if tune else 1, 0 if graph else 1,
                                    precision, slices)
         self._items = _item_array(items)
+        self._n = len(items)
         h = ctypes.c_void_p(0)
         _check(lib().skgemm_plan_create(self._items, len(items), ctypes.byref(self.options),
                                         _stream(stream), ctypes.byref(h)))
@@ -390,7 +393,15 @@ class Plan:
         return {"tile": o.tile_out, "grid": o.grid_out, "order": o.order_out,
                 "ozaki_problems": o.ozaki_problems_out,
                 "candidates_timed": o.candidates_timed_out, "tuned_ms": o.tuned_ms_out,
-                "model_efficiency": o.model_efficiency_out}
+                "model_efficiency": o.model_efficiency_out,
+                "graph_kernels": o.graph_kernels_out}
+
+    def precisions(self) -> list:
+        """Per item: PREC_NATIVE or PREC_OZAKI_I8 (the path the plan runs it on)."""
+        n = self._n
+        out = (ctypes.c_int * max(1, n))()
+        _check(lib().skgemm_plan_precisions(self._h, out, n))
+        return list(out)[:n]
 
     def close(self) -> None:
         if self._h and self._h.value:

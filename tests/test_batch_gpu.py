@@ -361,3 +361,48 @@ def test_plan_precision_options_rejected(cuda):
         skgemm.Plan([it.item()], precision=7)
     with pytest.raises(skgemm.SkgemmError):
         skgemm.Plan([it.item()], precision=skgemm.PREC_OZAKI_I8, slices=5)
+
+
+def test_plan_ozaki_subspace_pairs(cuda):
+    """A SYRK and a GEMM of the same band-packed Psi in one Ozaki plan run as a
+    subspace pair (one split of Psi): S and Hs bitwise equal to each item
+    planned alone, and within 1e-13 of Dot2. An unpaired GEMM on the same Psi
+    (a second H) runs on its own."""
+    SY, GE = skgemm.OP_SYRK_PACKED, skgemm.OP_GEMM_PACKED
+    cases, items, keep = [], [], []
+    for i, (K, M) in enumerate([(4099, 100), (13824, 200), (777, 33)]):
+        Psi = gaussian((K, M), 60 + i, 1.0 / np.sqrt(K))
+        H = uniform((K, M), 70 + i)
+        H2 = uniform((K, M), 80 + i)
+        P16 = dev(oracle.pack(np.ascontiguousarray(Psi.T), 16))
+        H32 = dev(oracle.pack(np.ascontiguousarray(H.T), 32))
+        H32b = dev(oracle.pack(np.ascontiguousarray(H2.T), 32))
+        outs = [torch.zeros(M * M, dtype=torch.float64, device="cuda") for _ in range(3)]
+        its = [skgemm.batch_item(SY, M, M, K, P16, 0, outs[0], M),
+               skgemm.batch_item(GE, M, M, K, P16, H32, outs[1], M, 1.5, 0.25),
+               skgemm.batch_item(GE, M, M, K, P16, H32b, outs[2], M)]
+        items += its
+        keep.append((P16, H32, H32b))
+        cases.append((Psi, H, H2, outs, its, M))
+    plan = skgemm.Plan(items, tune=False, precision=skgemm.PREC_OZAKI_I8)
+    assert plan.precisions() == [skgemm.PREC_OZAKI_I8] * len(items)
+    plan.run()
+    plan.status()
+    for (Psi, H, H2, outs, its, M) in cases:
+        got = [o.clone() for o in outs]
+        for it, o in zip(its, outs):
+            o.zero_()
+            alone = skgemm.Plan([it], tune=False, graph=False, precision=skgemm.PREC_OZAKI_I8)
+            alone.run()
+            alone.status()
+            alone.close()
+        iu = np.triu_indices(M)
+        s = got[0].cpu().numpy().reshape(M, M).T
+        assert np.array_equal(s[iu], outs[0].cpu().numpy().reshape(M, M).T[iu])
+        assert torch.equal(got[1], outs[1]) and torch.equal(got[2], outs[2])
+        assert oracle.rel_frobenius(s[iu], oracle.dot2_matmul(Psi.T, Psi)[iu]) <= TOL
+        assert oracle.rel_frobenius(got[1].cpu().numpy().reshape(M, M),
+                                    oracle.dot2_matmul(Psi.T, H, 1.5, 0.25)) <= TOL
+        assert oracle.rel_frobenius(got[2].cpu().numpy().reshape(M, M),
+                                    oracle.dot2_matmul(Psi.T, H2)) <= TOL
+    plan.close()
