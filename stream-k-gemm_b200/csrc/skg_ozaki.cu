@@ -1020,7 +1020,7 @@ namespace {
 // Scratch of one stream's Ozaki calls, per buffer of OzakiStream.
 struct OzakiNeed {
   size_t res_a = 0, res_b = 0, part_a = 0, part_b = 0, mu_a = 0, mu_b = 0, partials = 0,
-         rbytes = 0;
+         partials2 = 0, rbytes = 0;
   void max_with(const OzakiNeed& o) {
     res_a = std::max(res_a, o.res_a);
     res_b = std::max(res_b, o.res_b);
@@ -1029,9 +1029,12 @@ struct OzakiNeed {
     mu_a = std::max(mu_a, o.mu_a);
     mu_b = std::max(mu_b, o.mu_b);
     partials = std::max(partials, o.partials);
+    partials2 = std::max(partials2, o.partials2);
     rbytes = std::max(rbytes, o.rbytes);
   }
-  size_t total() const { return res_a + res_b + part_a + part_b + mu_a + mu_b + partials + rbytes; }
+  size_t total() const {
+    return res_a + res_b + part_a + part_b + mu_a + mu_b + partials + partials2 + rbytes;
+  }
 };
 
 size_t norm_part_bytes(int64_t R, int T) {
@@ -1126,8 +1129,9 @@ int ozaki_scratch_bytes(DeviceState* dev, int op, int64_t M, int64_t N, int64_t 
   return SKGEMM_OK;
 }
 
-// Grows stream `s`'s Ozaki scratch to serve every call of the three ops on
-// shapes up to (Nd, nb) with `slices` moduli without allocating later.
+// Grows stream `s`'s Ozaki scratch to serve every call of the three ops and
+// of the subspace pair on shapes up to (Nd, nb) with `slices` moduli without
+// allocating later.
 int ozaki_reserve(DeviceState* dev, cudaStream_t s, int64_t Nd, int64_t nb, int slices) {
   skgemm_options_t o;
   memset(&o, 0, sizeof(o));
@@ -1139,6 +1143,8 @@ int ozaki_reserve(DeviceState* dev, cudaStream_t s, int64_t Nd, int64_t nb, int 
   OzakiNeed n = need_lanes(dev, nb, nb, Nd, Lk, false);
   n.max_with(need_lanes(dev, nb, nb, Nd, Lk, true));
   n.max_with(need_rot(Nd, nb, Lr));
+  // The subspace pair keeps S's slabs in `partials` while Hs's go to `partials2`.
+  n.partials2 = need_lanes(dev, nb, nb, Nd, Lk, false).partials;
   std::lock_guard<std::mutex> lk(g_oz_mu);
   if ((st = ensure_consts(dev))) return st;
   StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
@@ -1147,7 +1153,8 @@ int ozaki_reserve(DeviceState* dev, cudaStream_t s, int64_t Nd, int64_t nb, int 
   if ((st = os->res_a.ensure(n.res_a)) || (st = os->res_b.ensure(n.res_b)) ||
       (st = os->part_a.ensure(n.part_a)) || (st = os->part_b.ensure(n.part_b)) ||
       (st = os->mu_a.ensure(n.mu_a)) || (st = os->mu_b.ensure(n.mu_b)) ||
-      (st = os->partials.ensure(n.partials)) || (st = os->rbytes.ensure(n.rbytes)))
+      (st = os->partials.ensure(n.partials)) || (st = os->partials2.ensure(n.partials2)) ||
+      (st = os->rbytes.ensure(n.rbytes)))
     return st;
   return SKGEMM_OK;
 }

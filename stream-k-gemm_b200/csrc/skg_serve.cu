@@ -316,11 +316,9 @@ struct GpuExec : Exec {
     memset(&o, 0, sizeof(o));
     o.precision = SKGEMM_PREC_OZAKI_I8;
     o.slices = slices;
-    if ((st = skgemm_dsyrk_packed_dev_opt(r.Ng, r.nb, p(r, r.lay.psi16), p(r, r.lay.S), r.nb, 1.0,
-                                          0.0, &o, s)))
-      return st;
-    if ((st = skgemm_dgemm_packed_dev_opt(r.nb, r.nb, r.Ng, p(r, r.lay.psi16), p(r, r.lay.h32),
-                                          p(r, r.lay.Hs), r.nb, 1.0, 0.0, &o, s)))
+    // S and Hs from one split of Psi (the subspace pair).
+    if ((st = skgemm_dsubspace_packed_dev(r.Ng, r.nb, p(r, r.lay.psi16), p(r, r.lay.h32),
+                                          p(r, r.lay.S), r.nb, p(r, r.lay.Hs), r.nb, &o, s)))
       return st;
     if ((st = skgemm_drot_dev_opt(r.Ng, r.nb, p(r, r.lay.grid), p(r, r.lay.Q), p(r, r.lay.out),
                                   &o, s)))
