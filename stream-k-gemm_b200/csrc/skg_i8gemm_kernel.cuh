@@ -138,6 +138,46 @@ __device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cu
   return true;
 }
 
+// Residue epilogue of one 128 x 256 work item (modulus it.l): this thread's
+// row `row` of the tile, TMEM column chunks [c_begin, c_end) of 32, written
+// as (acc mod m_l) bytes to residues[l][row][col] (row stride ldr).
+// s8 x s8 accumulators: |acc| <= K 2^14 < 2^25 (K <= 2048); acc + offset is
+// non-negative and below 2^29.
+__device__ __forceinline__ void i8_residue_epilogue(uint32_t taddr, int c_begin, int c_end,
+                                                    const I8Item& it, int row, int M, int N,
+                                                    uint8_t* residues, int64_t ldr) {
+  const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic[it.l];
+  const uint32_t off = c_i8mod.offset[it.l];
+  const bool row_ok = row < M;
+  uint8_t* dst = residues + ((int64_t)it.l * M + row) * ldr;
+#pragma unroll 1
+  for (int c = c_begin; c < c_end; ++c) {
+    uint32_t v[32];
+    tmem_ld_32x32b_x32(taddr + c * 32, v);
+    tmem_ld_wait();
+    const int col0 = it.tn * kI8BN + c * 32;
+    if (row_ok && col0 < N) {
+      uint32_t w[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint32_t b0 = mod_exact29(v[4 * j] + off, m, magic);
+        const uint32_t b1 = mod_exact29(v[4 * j + 1] + off, m, magic);
+        const uint32_t b2 = mod_exact29(v[4 * j + 2] + off, m, magic);
+        const uint32_t b3 = mod_exact29(v[4 * j + 3] + off, m, magic);
+        w[j] = __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+      }
+      if (col0 + 32 <= N) {
+        uint4* d4 = reinterpret_cast<uint4*>(dst + col0);
+        d4[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        d4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+      } else {
+        for (int j = 0; j < 32 && col0 + j < N; ++j)
+          dst[col0 + j] = (uint8_t)(w[j >> 2] >> (8 * (j & 3)));
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kI8Threads, 1)
     i8_gemm_kernel(const __grid_constant__ CUtensorMap mapA,
                    const __grid_constant__ CUtensorMap mapB, const I8Params p) {
@@ -300,38 +340,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
             d4[j] = make_int4((int)v[4 * j], (int)v[4 * j + 1], (int)v[4 * j + 2], (int)v[4 * j + 3]);
         }
       } else {
-        // s8 x s8 accumulators: |acc| <= K 2^14 < 2^25 (K <= 2048); acc + off
-        // is non-negative and below 2^29.
-        const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic[it.l];
-        const uint32_t off = c_i8mod.offset[it.l];
-        const bool row_ok = row < p.M;
-        uint8_t* dst = p.residues + ((int64_t)it.l * p.M + row) * p.ldr;
-#pragma unroll 1
-        for (int c = c_begin; c < c_end; ++c) {
-          uint32_t v[32];
-          tmem_ld_32x32b_x32(taddr + c * 32, v);
-          tmem_ld_wait();
-          const int col0 = it.tn * kI8BN + c * 32;
-          if (row_ok && col0 < p.N) {
-            uint32_t w[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              const uint32_t b0 = mod_exact29(v[4 * j] + off, m, magic);
-              const uint32_t b1 = mod_exact29(v[4 * j + 1] + off, m, magic);
-              const uint32_t b2 = mod_exact29(v[4 * j + 2] + off, m, magic);
-              const uint32_t b3 = mod_exact29(v[4 * j + 3] + off, m, magic);
-              w[j] = __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
-            }
-            if (col0 + 32 <= p.N) {
-              uint4* d4 = reinterpret_cast<uint4*>(dst + col0);
-              d4[0] = make_uint4(w[0], w[1], w[2], w[3]);
-              d4[1] = make_uint4(w[4], w[5], w[6], w[7]);
-            } else {
-              for (int j = 0; j < 32 && col0 + j < p.N; ++j)
-                dst[col0 + j] = (uint8_t)(w[j >> 2] >> (8 * (j & 3)));
-            }
-          }
-        }
+        i8_residue_epilogue(taddr, c_begin, c_end, it, row, p.M, p.N, p.residues, p.ldr);
       }
       tc_fence_before();
       __syncwarp();
@@ -344,6 +353,300 @@ __global__ void __launch_bounds__(kI8Threads, 1)
   }
 
   // Teardown: every role's loop is bounded, so all threads arrive here.
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc(tmem_base, kI8TmemCols);
+}
+
+
+// ---------------------------------------------------------------------------
+// Rotation kernel with B resident in shared memory (Psi' = Psi Q, K = nb
+// <= 512). Work units (l, tm, tn) as in kSchedUnits, but CTA c belongs to
+// group q = c / tiles_n and fixed column tile tn = c % tiles_n; group q walks
+// the contiguous range [q V / G, (q+1) V / G) of the V = L * tiles_m units
+// (l, tm) (l major). The CTA keeps B_l[tn] (256 rows x KP bytes, all k
+// blocks) in shared memory while l stays the same and streams only A tiles,
+// so the per-unit shared-memory fill is 128 x KP bytes instead of 384 x KP;
+// the tiles_n CTAs of a group read the same A tiles at the same time, so HBM
+// serves each A tile about once and L2 the rest.
+//
+// Epilogue: each epilogue warp owns a 32-row x 128-column box of the tile;
+// it writes the box's residue bytes to shared memory in the TMA 128-byte
+// swizzle (conflict-free: 4 wavefronts per 16-byte store) and one lane issues
+// a TMA store of the box, so global writes go out as whole 128-byte lines
+// instead of 32 scattered 16-byte pieces per store instruction.
+//
+// Shared memory: B region (kI8RotKbMax x 32 KB) | A ring (kI8RotStages x
+// 16 KB) | 8 store boxes (4 KB each) | barriers. B reloads wait for the MMAs
+// that read the old B (bempty, committed by the MMA issuer when l changes).
+constexpr int kI8RotKbMax = 4;  // KP <= 512
+constexpr int kI8RotStages = 4;
+constexpr int kI8RotBBytes = kI8RotKbMax * kI8TileBBytes;
+constexpr int kI8RotBoxBytes = 32 * 128;
+constexpr int kI8RotSmemBytes = kI8RotBBytes + kI8RotStages * kI8TileABytes +
+                                kI8EpiWarps * kI8RotBoxBytes + 1024 + 256;
+static_assert(kI8RotSmemBytes <= 232448, "rotation kernel exceeds 227 KB of shared memory");
+static_assert((2 * kI8RotStages + 6) * 8 + 8 <= 256, "rotation kernel barrier area");
+
+struct I8RotParams {
+  int L, KB;            // moduli, k-blocks of KP (KB <= kI8RotKbMax)
+  int M, N;             // output extent (Nd, nb); residues [L][M][N] through mapR
+  int tiles_m, tiles_n;
+  int groups;           // grid = groups * tiles_n
+  uint32_t* err;
+};
+
+__device__ __forceinline__ bool rot_next_item(const I8RotParams& p, int cta, int& cursor,
+                                              I8Item& it) {
+  const int q = cta / p.tiles_n;
+  if (q >= p.groups) return false;
+  const int64_t V = (int64_t)p.L * p.tiles_m;
+  const int64_t b = V * q / p.groups, e = V * (q + 1) / p.groups;
+  const int64_t v = b + cursor;
+  if (v >= e) return false;
+  it.l = (int)(v / p.tiles_m);
+  it.tm = (int)(v - (int64_t)it.l * p.tiles_m);
+  it.tn = cta - q * p.tiles_n;
+  it.kb0 = 0;
+  it.kb1 = p.KB;
+  it.slot = 0;
+  ++cursor;
+  return true;
+}
+
+__global__ void __launch_bounds__(kI8Threads, 1)
+    i8_rot_kernel(const __grid_constant__ CUtensorMap mapA,
+                  const __grid_constant__ CUtensorMap mapB,
+                  const __grid_constant__ CUtensorMap mapR, const I8RotParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint8_t* sB = smem;
+  uint8_t* sA = smem + kI8RotBBytes;
+  uint8_t* sR = sA + kI8RotStages * kI8TileABytes;
+  uint64_t* full_bar = reinterpret_cast<uint64_t*>(sR + kI8EpiWarps * kI8RotBoxBytes);
+  uint64_t* empty_bar = full_bar + kI8RotStages;
+  uint64_t* bfull = empty_bar + kI8RotStages;
+  uint64_t* bempty = bfull + 1;
+  uint64_t* tfull_bar = bempty + 1;
+  uint64_t* tempty_bar = tfull_bar + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty_bar + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int cta = blockIdx.x;
+
+  // Idle CTAs and shapes outside the B region leave before touching TMEM.
+  if (p.KB < 1 || p.KB > kI8RotKbMax) return;
+  {
+    int cur = 0;
+    I8Item probe;
+    if (!rot_next_item(p, cta, cur, probe)) return;
+  }
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kI8RotStages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(bfull, 1);
+    mbar_init(bempty, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull_bar[a], 1);
+      mbar_init(&tempty_bar[a], kI8EpiWarps);
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, kI8TmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    if (lane == 0) {
+      tma_prefetch_desc(&mapA);
+      tma_prefetch_desc(&mapB);
+      tma_prefetch_desc(&mapR);
+      int stage = 0;
+      uint32_t phase = 0;
+      int cur = 0;
+      int64_t issued = 0;
+      int cur_l = -1;
+      uint32_t bempty_ph = 0;
+      int b_loads = 0;
+      I8Item it;
+      while (!*abort_flag && rot_next_item(p, cta, cur, it)) {
+        if (it.l != cur_l) {
+          // B_l[tn] for the next run of units: all k blocks, one barrier.
+          if (cur_l >= 0) {
+            if (!mbar_wait(bempty, bempty_ph, p.err)) {
+              *abort_flag = 1;
+              break;
+            }
+            bempty_ph ^= 1;
+          }
+          mbar_arrive_expect_tx(bfull, (uint32_t)(p.KB * kI8TileBBytes));
+          for (int kb = 0; kb < p.KB; ++kb)
+            tma_load_3d(sB + kb * kI8TileBBytes, &mapB, bfull, kb * kI8BK, it.tn * kI8BN, it.l);
+          ++b_loads;
+          cur_l = it.l;
+        }
+        for (int kb = 0; kb < p.KB; ++kb) {
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1, p.err)) {
+            *abort_flag = 1;
+            break;
+          }
+          ++issued;
+          mbar_arrive_expect_tx(&full_bar[stage], kI8TileABytes);
+          tma_load_3d(sA + stage * kI8TileABytes, &mapA, &full_bar[stage], kb * kI8BK,
+                      it.tm * kI8BM, it.l);
+          if (++stage == kI8RotStages) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+      }
+      // Drain: the last A loads and the last B load have landed before the
+      // CTA may exit (immediate on the normal path; bounded on an abort path).
+      for (int j = 1; j <= kI8RotStages && j <= issued; ++j) {
+        int s2 = stage - j;
+        uint32_t ph = phase;
+        if (s2 < 0) {
+          s2 += kI8RotStages;
+          ph ^= 1;
+        }
+        mbar_wait(&full_bar[s2], ph, p.err);
+      }
+      if (b_loads > 0) mbar_wait(bfull, (uint32_t)((b_loads - 1) & 1), p.err);
+    }
+  } else if (warp == 1) {
+    // --------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN, 1);
+      const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+      int stage = 0;
+      uint32_t phase = 0;
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      int cur = 0;
+      int cur_l = -1;
+      uint32_t bfull_ph = 0;
+      I8Item it;
+      while (!*abort_flag && rot_next_item(p, cta, cur, it)) {
+        if (it.l != cur_l) {
+          // Every MMA issued so far read the old B: release it once they finish.
+          if (cur_l >= 0) umma_commit(bempty);
+          if (!mbar_wait(bfull, bfull_ph, p.err)) {
+            *abort_flag = 1;
+            break;
+          }
+          bfull_ph ^= 1;
+          cur_l = it.l;
+        }
+        if (!mbar_wait(&tempty_bar[acc], acc_phase ^ 1, p.err)) {
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tmem_d = tmem_base + (uint32_t)(acc * kI8BN);
+        for (int kb = 0; kb < p.KB; ++kb) {
+          if (!mbar_wait(&full_bar[stage], phase, p.err)) {
+            *abort_flag = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t adesc = umma_desc_kmajor_sw128(a_base + stage * kI8TileABytes);
+          const uint64_t bdesc = umma_desc_kmajor_sw128(b_base + kb * kI8TileBBytes);
+#pragma unroll
+          for (int kk = 0; kk < kI8BK / kI8UmmaK; ++kk)
+            umma_i8(tmem_d, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
+                    (kb > 0 || kk > 0) ? 1u : 0u);
+          umma_commit(&empty_bar[stage]);
+          if (++stage == kI8RotStages) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+        umma_commit(&tfull_bar[acc]);
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1;
+        }
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int quarter = warp & 3;                  // TMEM lanes / tile rows 32*quarter..+31
+    const int half = (warp - 2) >> 2;              // tile columns 128*half..+127
+    uint8_t* box = sR + (warp - 2) * kI8RotBoxBytes;
+    uint8_t* my_row = box + lane * 128;
+    const int sw = lane & 7;                       // 128-byte swizzle of this box row
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    int cur = 0;
+    I8Item it;
+    while (rot_next_item(p, cta, cur, it)) {
+      if (*abort_flag || !mbar_wait(&tfull_bar[acc], acc_phase, p.err)) {
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
+                             (uint32_t)(acc * kI8BN + half * 128);
+      // The box is free once the previous unit's store has read it.
+      if (lane == 0) bulk_wait_read_all();
+      __syncwarp();
+      // s8 x s8 accumulators: |acc| <= K 2^14 < 2^25; acc + offset is
+      // non-negative and below 2^29.
+      const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic[it.l];
+      const uint32_t off = c_i8mod.offset[it.l];
+#pragma unroll 1
+      for (int c = 0; c < 4; ++c) {
+        uint32_t v[32];
+        tmem_ld_32x32b_x32(taddr + c * 32, v);
+        tmem_ld_wait();
+        uint32_t w[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const uint32_t b0 = mod_exact29(v[4 * j] + off, m, magic);
+          const uint32_t b1 = mod_exact29(v[4 * j + 1] + off, m, magic);
+          const uint32_t b2 = mod_exact29(v[4 * j + 2] + off, m, magic);
+          const uint32_t b3 = mod_exact29(v[4 * j + 3] + off, m, magic);
+          w[j] = __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+        }
+        *reinterpret_cast<uint4*>(my_row + (((2 * c) ^ sw) << 4)) =
+            make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(my_row + (((2 * c + 1) ^ sw) << 4)) =
+            make_uint4(w[4], w[5], w[6], w[7]);
+      }
+      // TMEM reads done: hand the accumulator back before the store.
+      tc_fence_before();
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&tempty_bar[acc]);
+        const int x = it.tn * kI8BN + half * 128, y = it.tm * kI8BM + quarter * 32;
+        if (x < p.N && y < p.M) {
+          tma_store_3d(&mapR, box, x, y, it.l);
+          bulk_commit_group();
+        }
+      }
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1;
+      }
+    }
+    if (lane == 0) bulk_wait_all();
+  }
+
   tc_fence_before();
   __syncthreads();
   tc_fence_after();

@@ -729,6 +729,19 @@ int launch_i8(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB, co
   return SKGEMM_OK;
 }
 
+int launch_i8_rot(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
+                  const CUtensorMap& mR, const I8RotParams& p, int grid, cudaStream_t s) {
+  static bool attr_done[64] = {false};
+  if (!attr_done[dev->device]) {
+    SKG_CUDA(cudaFuncSetAttribute(i8_rot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kI8RotSmemBytes));
+    attr_done[dev->device] = true;
+  }
+  i8_rot_kernel<<<grid, kI8Threads, kI8RotSmemBytes, s>>>(mA, mB, mR, p);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
 int choose_L(const skgemm_options_t* opts, int64_t K, int* L_out, int* gamma_out) {
   int L = opts ? opts->slices : 0;
   if (L == 0) {
@@ -1302,22 +1315,48 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   CUtensorMap mA, mB;
   if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, L, kI8BM))) return st;
   if ((st = make_res_map(&mB, os->res_b.ptr, KP, RB, L, kI8BN))) return st;
-  I8Params p;
-  memset(&p, 0, sizeof(p));
-  p.sched = kSchedUnits;
-  p.is_signed = 1;
-  p.L = L;
-  p.KB = (int)(KP / 128);
-  p.M = (int)Nd;
-  p.N = (int)nb;
-  p.tiles_m = (int)(RA / kI8BM);
-  p.tiles_n = (int)(RB / kI8BN);
-  p.residues = (uint8_t*)os->rbytes.ptr;
-  p.ldr = nb;
-  p.err = ws->err;
-  const int64_t units = (int64_t)p.tiles_m * L * p.tiles_n;
-  const int grid = (int)std::min<int64_t>(dev->num_sms, units);
-  if ((st = launch_i8(dev, mA, mB, p, grid, s))) return st;
+  if (KP / 128 <= kI8RotKbMax && nb % 16 == 0 && nb >= 128 && Nd >= 128) {
+    // B_l[tn] fits in shared memory: the B-resident schedule, residue bytes
+    // [L][Nd][nb] written by 32 x 128-byte TMA store boxes.
+    CUtensorMap mR;
+    {
+      uint64_t dims[3] = {(uint64_t)nb, (uint64_t)Nd, (uint64_t)L};
+      uint64_t strides[2] = {(uint64_t)nb, (uint64_t)(Nd * nb)};
+      uint32_t box[3] = {128, 32, 1};
+      if ((st = encode_tiled(&mR, 3, os->rbytes.ptr, dims, strides, box,
+                             CU_TENSOR_MAP_DATA_TYPE_UINT8, CU_TENSOR_MAP_SWIZZLE_128B)))
+        return st;
+    }
+    I8RotParams p;
+    memset(&p, 0, sizeof(p));
+    p.L = L;
+    p.KB = (int)(KP / 128);
+    p.M = (int)Nd;
+    p.N = (int)nb;
+    p.tiles_m = (int)(RA / kI8BM);
+    p.tiles_n = (int)(RB / kI8BN);
+    const int64_t V = (int64_t)L * p.tiles_m;
+    p.groups = (int)std::max<int64_t>(1, std::min<int64_t>(dev->num_sms / p.tiles_n, V));
+    p.err = ws->err;
+    if ((st = launch_i8_rot(dev, mA, mB, mR, p, p.groups * p.tiles_n, s))) return st;
+  } else {
+    I8Params p;
+    memset(&p, 0, sizeof(p));
+    p.sched = kSchedUnits;
+    p.is_signed = 1;
+    p.L = L;
+    p.KB = (int)(KP / 128);
+    p.M = (int)Nd;
+    p.N = (int)nb;
+    p.tiles_m = (int)(RA / kI8BM);
+    p.tiles_n = (int)(RB / kI8BN);
+    p.residues = (uint8_t*)os->rbytes.ptr;
+    p.ldr = nb;
+    p.err = ws->err;
+    const int64_t units = (int64_t)p.tiles_m * L * p.tiles_n;
+    const int grid = (int)std::min<int64_t>(dev->num_sms, units);
+    if ((st = launch_i8(dev, mA, mB, p, grid, s))) return st;
+  }
   {
     const uint8_t* rb = (const uint8_t*)os->rbytes.ptr;
     const int* mua = (const int*)os->mu_a.ptr;

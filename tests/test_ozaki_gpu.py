@@ -103,7 +103,9 @@ def test_ozaki_syrk_accuracy(cuda, K, M, alpha, beta, kind):
 
 
 @pytest.mark.parametrize("Nd,nb,kind", [(4096, 512, "gauss"), (2048, 128, "uniform"),
-                                        (1024, 256, "stress"), (48, 80, "gauss")])
+                                        (1024, 256, "stress"), (48, 80, "gauss"),
+                                        (1040, 208, "gauss"), (2000, 400, "uniform"),
+                                        (1024, 576, "gauss"), (144, 496, "stress")])
 def test_ozaki_rot_accuracy(cuda, Nd, nb, kind):
     gen = {"gauss": gaussian, "uniform": uniform, "stress": stress}[kind]
     Psi = gen((Nd, nb), 7)
