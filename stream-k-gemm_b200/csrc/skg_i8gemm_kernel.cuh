@@ -84,10 +84,18 @@ struct I8Params {
 // 2^37/m) / 2^37 stays below 2^-8 <= 1/m). `offset` is a multiple of m
 // >= 2^25 that makes a signed accumulator (|acc| < 2^25, K <= 2048)
 // non-negative.
+// For K <= 512 and symmetric residues of an odd modulus (|r| <= 127, so
+// |acc| <= 512 * 127^2 = 8258048) the rotation kernel uses a shorter form:
+// offset24 = the smallest multiple of m >= 8258048 puts u = acc + offset24
+// in [0, 2^24), where q = umulhi(u, magic24 = ceil(2^32 / m)) is already
+// floor(u / m) (excess below u / 2^32 < 2^-8 < 1/m), with no shift. For
+// m = 256 the residue is the accumulator's low byte.
 struct I8ModConsts {
   uint32_t m[kI8MaxModuli];
   uint32_t magic[kI8MaxModuli];
   uint32_t offset[kI8MaxModuli];
+  uint32_t magic24[kI8MaxModuli];
+  uint32_t offset24[kI8MaxModuli];
 };
 
 // Moduli of the residue epilogue (constant memory: indexed by the work item's
@@ -97,6 +105,10 @@ __constant__ I8ModConsts c_i8mod;
 __device__ __forceinline__ uint32_t mod_exact29(uint32_t u, uint32_t m, uint32_t magic) {
   const uint32_t q = __umulhi(u, magic) >> 5;
   return u - q * m;
+}
+
+__device__ __forceinline__ uint32_t mod_exact24(uint32_t u, uint32_t m, uint32_t magic24) {
+  return u - __umulhi(u, magic24) * m;
 }
 
 // Work item seen by all roles.
@@ -604,28 +616,36 @@ __global__ void __launch_bounds__(kI8Threads, 1)
       // The box is free once the previous unit's store has read it.
       if (lane == 0) bulk_wait_read_all();
       __syncwarp();
-      // s8 x s8 accumulators: |acc| <= K 2^14 < 2^25; acc + offset is
-      // non-negative and below 2^29.
-      const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic[it.l];
-      const uint32_t off = c_i8mod.offset[it.l];
+      // K <= 512: the 24-bit remainder (no shift); m = 256 keeps the low
+      // byte of the accumulator as it is.
+      const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic24[it.l];
+      const uint32_t off = c_i8mod.offset24[it.l];
+      const bool pow2 = (m == 256u);
 #pragma unroll 1
-      for (int c = 0; c < 4; ++c) {
-        uint32_t v[32];
-        tmem_ld_32x32b_x32(taddr + c * 32, v);
+      for (int c = 0; c < 4; c += 2) {
+        uint32_t v0[32], v1[32];
+        tmem_ld_32x32b_x32(taddr + c * 32, v0);
+        tmem_ld_32x32b_x32(taddr + c * 32 + 32, v1);
         tmem_ld_wait();
-        uint32_t w[8];
+        if (!pow2) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            v0[j] = mod_exact24(v0[j] + off, m, magic);
+            v1[j] = mod_exact24(v1[j] + off, m, magic);
+          }
+        }
+        uint32_t w[16];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          const uint32_t b0 = mod_exact29(v[4 * j] + off, m, magic);
-          const uint32_t b1 = mod_exact29(v[4 * j + 1] + off, m, magic);
-          const uint32_t b2 = mod_exact29(v[4 * j + 2] + off, m, magic);
-          const uint32_t b3 = mod_exact29(v[4 * j + 3] + off, m, magic);
-          w[j] = __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+          w[j] = __byte_perm(__byte_perm(v0[4 * j], v0[4 * j + 1], 0x0040),
+                             __byte_perm(v0[4 * j + 2], v0[4 * j + 3], 0x0040), 0x5410);
+          w[8 + j] = __byte_perm(__byte_perm(v1[4 * j], v1[4 * j + 1], 0x0040),
+                                 __byte_perm(v1[4 * j + 2], v1[4 * j + 3], 0x0040), 0x5410);
         }
-        *reinterpret_cast<uint4*>(my_row + (((2 * c) ^ sw) << 4)) =
-            make_uint4(w[0], w[1], w[2], w[3]);
-        *reinterpret_cast<uint4*>(my_row + (((2 * c + 1) ^ sw) << 4)) =
-            make_uint4(w[4], w[5], w[6], w[7]);
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+          *reinterpret_cast<uint4*>(my_row + (((2 * c + h) ^ sw) << 4)) =
+              make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
       }
       // TMEM reads done: hand the accumulator back before the store.
       tc_fence_before();

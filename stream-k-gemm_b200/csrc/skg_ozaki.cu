@@ -601,6 +601,9 @@ int ensure_consts(DeviceState* dev) {
     g_modc.m[l] = kModuli[l];
     g_modc.magic[l] = (uint32_t)((1ull << 37) / kModuli[l] + 1);
     g_modc.offset[l] = (uint32_t)((((1u << 25) + kModuli[l] - 1) / kModuli[l]) * kModuli[l]);
+    const uint32_t acc24 = 512u * 127u * 127u;  // |acc| bound for K <= 512, odd m
+    g_modc.magic24[l] = (uint32_t)(((1ull << 32) + kModuli[l] - 1) / kModuli[l]);
+    g_modc.offset24[l] = (uint32_t)((acc24 + kModuli[l] - 1) / kModuli[l] * kModuli[l]);
   }
   g_modc_ready = true;
   SKG_CUDA(cudaMemcpyToSymbol(c_i8mod, &g_modc, sizeof(g_modc)));
