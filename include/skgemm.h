@@ -62,6 +62,11 @@ extern "C" {
 /* Batched plans only: per problem, whichever of the two is faster (cost
  * model, confirmed by timing when the plan tunes). */
 #define SKGEMM_PREC_AUTO 2
+/* SKGEMM_PREC_OZAKI_BF16: the same Ozaki scheme II with the residues stored
+ * as BF16 and kind::f16 products (FP32 accumulation over at most 1024
+ * products, exact, summed in INT32): results identical to _OZAKI_I8 bit for
+ * bit, at half its tensor throughput. Rotation: nb <= 1024. */
+#define SKGEMM_PREC_OZAKI_BF16 3
 
 typedef struct skgemm_options {
   int precision;        /* SKGEMM_PREC_* */
@@ -240,7 +245,7 @@ typedef struct skgemm_plan_options {
   int order;     /* problem order: 1 = as given, 2 = most work first, 0 = autotune */
   int no_tune;   /* 1: do not time candidates, pick by the cost model alone */
   int no_graph;  /* 1: plain stream launches instead of a CUDA graph */
-  int precision; /* SKGEMM_PREC_NATIVE (default), _OZAKI_I8 or _AUTO */
+  int precision; /* SKGEMM_PREC_NATIVE (default), _OZAKI_I8, _OZAKI_BF16 or _AUTO */
   int slices;    /* Ozaki moduli, 0 = automatic (accuracy target 1e-13) */
   int ozaki_problems_out; /* problems the plan runs on the Ozaki path */
   int tile_out, grid_out, order_out;
@@ -270,7 +275,7 @@ int skgemm_plan_run(skgemm_plan_t plan, void* stream);
  * plan's launches. */
 int skgemm_plan_status(skgemm_plan_t plan, void* stream);
 /* The path each of the plan's `n` items runs on: prec_out[i] =
- * SKGEMM_PREC_NATIVE or SKGEMM_PREC_OZAKI_I8 (n must equal the item count). */
+ * SKGEMM_PREC_NATIVE, _OZAKI_I8 or _OZAKI_BF16 (n must equal the item count). */
 int skgemm_plan_precisions(skgemm_plan_t plan, int* prec_out, int n);
 /* Releases the plan (synchronises the device first: its launches may still be
  * in flight). */

@@ -160,6 +160,7 @@ struct BatchPlan {
   // for a GEMM item run by its SYRK partner, -1 otherwise.
   std::vector<int> partner;
   int slices = 0;             // Ozaki moduli (0 = accuracy target)
+  int oz_precision = SKGEMM_PREC_OZAKI_I8;  // residue type of the Ozaki items
   Config cfg;
   double efficiency = 0.0;
   Fp64Group group{};
@@ -355,10 +356,10 @@ int configure(BatchPlan* P, Config c) {
 }
 
 // One item through the Ozaki split on `s`.
-int run_ozaki_item(const skgemm_batch_item_t& it, int slices, cudaStream_t s) {
+int run_ozaki_item(const skgemm_batch_item_t& it, int precision, int slices, cudaStream_t s) {
   skgemm_options_t o;
   memset(&o, 0, sizeof(o));
-  o.precision = SKGEMM_PREC_OZAKI_I8;
+  o.precision = precision;
   o.slices = slices;
   switch (it.op) {
     case SKGEMM_OP_GEMM_PACKED:
@@ -395,12 +396,12 @@ int enqueue(BatchPlan* P, cudaStream_t s) {
         const skgemm_batch_item_t& b = P->items[P->partner[i]];
         skgemm_options_t o;
         memset(&o, 0, sizeof(o));
-        o.precision = SKGEMM_PREC_OZAKI_I8;
+        o.precision = P->oz_precision;
         o.slices = P->slices;
         st = ozaki_subspace(a.K, a.M, a.A, b.B, a.D, a.ldd, a.alpha, a.beta, b.D, b.ldd, b.alpha,
                             b.beta, &o, P->ostream);
       } else {
-        st = run_ozaki_item(P->items[i], P->slices, P->ostream);
+        st = run_ozaki_item(P->items[i], P->oz_precision, P->slices, P->ostream);
       }
       if (st != SKGEMM_OK) {
         char buf[64];
@@ -495,6 +496,10 @@ std::vector<char> assign_precision(const BatchPlan& P, int precision, int slices
     const int64_t n = (it.op == SKGEMM_OP_SYRK_PACKED) ? it.M : it.N;
     const double t = ozaki_time_estimate(it.op, it.M, n, it.K, slices);
     if (t < 0.0) continue;
+    if (precision == SKGEMM_PREC_OZAKI_BF16) {
+      if (it.op != SKGEMM_OP_ROT || it.N <= 1024) oz[i] = 1;  // BF16 rotation: nb <= 1024
+      continue;
+    }
     if (precision == SKGEMM_PREC_OZAKI_I8 || t < 0.8 * native_estimate(pr)) oz[i] = 1;
   }
   if (precision == SKGEMM_PREC_AUTO) {
@@ -595,7 +600,7 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
   if (o.order < 0 || o.order > 2) return fail(SKGEMM_ERR_INVALID_ARG, "plan option order");
   if (o.grid < 0) return fail(SKGEMM_ERR_INVALID_ARG, "plan option grid");
   if (o.precision != SKGEMM_PREC_NATIVE && o.precision != SKGEMM_PREC_OZAKI_I8 &&
-      o.precision != SKGEMM_PREC_AUTO)
+      o.precision != SKGEMM_PREC_AUTO && o.precision != SKGEMM_PREC_OZAKI_BF16)
     return fail(SKGEMM_ERR_INVALID_ARG, "plan option precision");
   if (o.slices != 0 && (o.slices < 6 || o.slices > 16))
     return fail(SKGEMM_ERR_INVALID_ARG, "plan option slices must be 0 or in [6, 16]");
@@ -604,6 +609,7 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
   if (st) return st;
   P->use_graph = !o.no_graph;
   P->slices = o.slices;
+  if (o.precision == SKGEMM_PREC_OZAKI_BF16) P->oz_precision = SKGEMM_PREC_OZAKI_BF16;
 
   // Precision assignments: the cost model's, and under auto also all-native
   // (tuning keeps the faster).
@@ -980,7 +986,7 @@ SKG_EXPORT int skgemm_plan_precisions(skgemm_plan_t plan, int* prec_out, int n) 
   const BatchPlan* P = plan->impl;
   if (n != (int)P->oz.size() || (n > 0 && !prec_out))
     return fail(SKGEMM_ERR_INVALID_ARG, "plan precisions: n must equal the item count");
-  for (int i = 0; i < n; ++i) prec_out[i] = P->oz[i] ? SKGEMM_PREC_OZAKI_I8 : SKGEMM_PREC_NATIVE;
+  for (int i = 0; i < n; ++i) prec_out[i] = P->oz[i] ? P->oz_precision : SKGEMM_PREC_NATIVE;
   return SKGEMM_OK;
 }
 

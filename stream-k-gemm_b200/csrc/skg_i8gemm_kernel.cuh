@@ -18,6 +18,15 @@
 // two 256-column TMEM accumulators so the epilogue of one work item overlaps
 // the MMAs of the next.
 //
+// BF16 variant (template BF): the same residues stored as BF16 (|r| <= 128
+// is exact in BF16), kind::f16 MMAs with FP32 accumulators, 64 k per 128-byte
+// k-block. A sum of at most 1024 products of magnitude <= 2^14 is an integer
+// of magnitude <= 2^24, which FP32 holds exactly, so the host cuts the k range
+// into sub-segments of <= 16 k-blocks; the lanes epilogue converts each
+// sub-segment's FP32 tile to int32 and adds it into registers until the
+// slot changes (<= 127 sub-segments per slot keeps |sum| < 2^31), then writes
+// the slab. Results equal the INT8 path's bit for bit.
+//
 // Schedules:
 //  kSchedLanes   (huge K, small M x N: S = Psi^T Psi, Hs = Psi^T H Psi)
 //     CTA c -> tile t = c % T, lane q = c / T. Lane q owns a contiguous range
@@ -155,6 +164,7 @@ __device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cu
 // as (acc mod m_l) bytes to residues[l][row][col] (row stride ldr).
 // s8 x s8 accumulators: |acc| <= K 2^14 < 2^25 (K <= 2048); acc + offset is
 // non-negative and below 2^29.
+template <bool BF>
 __device__ __forceinline__ void i8_residue_epilogue(uint32_t taddr, int c_begin, int c_end,
                                                     const I8Item& it, int row, int M, int N,
                                                     uint8_t* residues, int64_t ldr) {
@@ -167,6 +177,11 @@ __device__ __forceinline__ void i8_residue_epilogue(uint32_t taddr, int c_begin,
     uint32_t v[32];
     tmem_ld_32x32b_x32(taddr + c * 32, v);
     tmem_ld_wait();
+    if (BF) {
+      // FP32 accumulators hold exact integers (K <= 1024): back to int32.
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = (uint32_t)__float2int_rn(__uint_as_float(v[j]));
+    }
     const int col0 = it.tn * kI8BN + c * 32;
     if (row_ok && col0 < N) {
       uint32_t w[8];
@@ -190,6 +205,7 @@ __device__ __forceinline__ void i8_residue_epilogue(uint32_t taddr, int c_begin,
   }
 }
 
+template <bool BF>
 __global__ void __launch_bounds__(kI8Threads, 1)
     i8_gemm_kernel(const __grid_constant__ CUtensorMap mapA,
                    const __grid_constant__ CUtensorMap mapB, const I8Params p) {
@@ -279,7 +295,8 @@ __global__ void __launch_bounds__(kI8Threads, 1)
   } else if (warp == 1) {
     // --------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = umma_idesc_i8(kI8BM, kI8BN, p.is_signed);
+      const uint32_t idesc =
+          BF ? umma_idesc_bf16(kI8BM, kI8BN) : umma_idesc_i8(kI8BM, kI8BN, p.is_signed);
       const uint32_t smem_base = smem_u32(smem);
       int stage = 0;
       uint32_t phase = 0;
@@ -305,9 +322,15 @@ __global__ void __launch_bounds__(kI8Threads, 1)
           const uint64_t bdesc = umma_desc_kmajor_sw128(sa + kI8TileABytes);
 #pragma unroll
           for (int kk = 0; kk < kI8BK / kI8UmmaK; ++kk) {
-            // advance 32 bytes of k inside the 128-byte swizzle atom
-            umma_i8(tmem_d, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
-                    (kb > it.kb0 || kk > 0) ? 1u : 0u);
+            // advance 32 bytes of k inside the 128-byte swizzle atom (32 INT8
+            // or 16 BF16 values: one MMA's K either way)
+            const uint32_t accum = (kb > it.kb0 || kk > 0) ? 1u : 0u;
+            if (BF)
+              umma_bf16(tmem_d, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
+                        accum);
+            else
+              umma_i8(tmem_d, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
+                      accum);
           }
           umma_commit(&empty_bar[stage]);  // frees the smem stage when these MMAs finish
           if (++stage == kI8Stages) {
@@ -331,6 +354,9 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     uint32_t acc_phase = 0;
     int cur = 0;
     I8Item it;
+    int32_t run[BF ? 128 : 1];  // BF16 lanes: int32 sums of this slot's sub-segments
+#pragma unroll
+    for (int j = 0; j < (BF ? 128 : 1); ++j) run[j] = 0;
     while (i8_next_item(p, cta, cur, it)) {
       if (*abort_flag || !mbar_wait(&tfull_bar[acc], acc_phase, p.err)) {
         *abort_flag = 1;
@@ -339,24 +365,60 @@ __global__ void __launch_bounds__(kI8Threads, 1)
       tc_fence_after();
       const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * kI8BN);
       const int row = it.tm * kI8BM + row_in_tile;
+      bool released = false;
       if (p.sched == kSchedLanes) {
         int32_t* dst = p.partials + ((int64_t)it.slot * kI8BM + row_in_tile) * kI8BN;
-#pragma unroll 1
-        for (int c = c_begin; c < c_end; ++c) {
-          uint32_t v[32];
-          tmem_ld_32x32b_x32(taddr + c * 32, v);
-          tmem_ld_wait();
-          int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
+        if (BF) {
 #pragma unroll
-          for (int j = 0; j < 8; ++j)
-            d4[j] = make_int4((int)v[4 * j], (int)v[4 * j + 1], (int)v[4 * j + 2], (int)v[4 * j + 3]);
+          for (int cc = 0; cc < 8; ++cc) {
+            uint32_t v[16];
+            tmem_ld_32x32b_x16(taddr + c_begin * 32 + cc * 16, v);
+            tmem_ld_wait();
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              run[(BF ? cc * 16 + j : 0)] += __float2int_rn(__uint_as_float(v[j]));
+          }
+          // The accumulator is free as soon as it has been read.
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty_bar[acc]);
+          released = true;
+          I8Item nx;
+          int peek = cur;
+          if (!i8_next_item(p, cta, peek, nx) || nx.slot != it.slot) {
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+              int4* d4 = reinterpret_cast<int4*>(dst + (c_begin + cc) * 32);
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                const int b = BF ? cc * 32 + 4 * j : 0;
+                d4[j] = make_int4(run[b], run[(BF ? b + 1 : 0)], run[(BF ? b + 2 : 0)],
+                                  run[(BF ? b + 3 : 0)]);
+              }
+            }
+#pragma unroll
+            for (int j = 0; j < (BF ? 128 : 1); ++j) run[j] = 0;
+          }
+        } else {
+#pragma unroll 1
+          for (int c = c_begin; c < c_end; ++c) {
+            uint32_t v[32];
+            tmem_ld_32x32b_x32(taddr + c * 32, v);
+            tmem_ld_wait();
+            int4* d4 = reinterpret_cast<int4*>(dst + c * 32);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              d4[j] = make_int4((int)v[4 * j], (int)v[4 * j + 1], (int)v[4 * j + 2], (int)v[4 * j + 3]);
+          }
         }
       } else {
-        i8_residue_epilogue(taddr, c_begin, c_end, it, row, p.M, p.N, p.residues, p.ldr);
+        i8_residue_epilogue<BF>(taddr, c_begin, c_end, it, row, p.M, p.N, p.residues, p.ldr);
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty_bar[acc]);
+      if (!released) {
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty_bar[acc]);
+      }
       if (++acc == 2) {
         acc = 0;
         acc_phase ^= 1;

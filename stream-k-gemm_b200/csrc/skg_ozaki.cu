@@ -43,6 +43,10 @@ constexpr uint32_t kModuli[kI8MaxModuli] = {256, 255, 253, 251, 247, 241, 239, 2
 constexpr int kMinModuli = 6;
 // k-blocks (128 k) per INT32-exact segment: s8 x s8 products are <= 2^14.
 constexpr int kSegKbCapSigned = 1023;   // 1023 * 128 * 2^14 < 2^31
+// BF16 residues: FP32 tile sums exact for <= 1024 products (16 k-blocks of
+// 64), int32 slots for <= 127 such sub-segments.
+constexpr int kSubKbCapBf16 = 16;
+constexpr int kSegKbCapBf16 = 127 * kSubKbCapBf16;
 
 // Residue constants for one moduli count L (gamma depends on L). The scaled
 // integer X = rint(v 2^mu) (int64, |X| <= 2^gamma + 1/2) is cut into digits
@@ -186,6 +190,27 @@ __device__ __forceinline__ Digits digits_of(double v, double s1, double s2) {
   return d;
 }
 
+// Symmetric residue of the digits modulo odd kModuli[l] as an exact float
+// (|r| <= 127).
+template <int L>
+__device__ __forceinline__ float residue_float(const Digits& d, int l) {
+  const ResidueConsts& rc = c_res[L];
+  const float S = fmaf(d.f4, rc.c[3][l],
+                       fmaf(d.f3, rc.c[2][l], fmaf(d.f2, rc.c[1][l], fmaf(d.f1, rc.c[0][l], d.f0))));
+  const float q = fmaf(S, rc.inv[l], kMagic) - kMagic;
+  return fmaf(-q, rc.m[l], S);
+}
+
+// BF16 bits of residue l of the digits (l = 0: X mod 256 as a signed byte).
+// Integers of magnitude <= 128 are exact in BF16: the top half of the FP32.
+template <int L>
+__device__ __forceinline__ uint32_t residue_bf16(const Digits& d, int l) {
+  const float r = (l == 0) ? (float)((int)(d.lo << 24) >> 24) : residue_float<L>(d, l);
+  return __float_as_uint(r) >> 16;
+}
+
+__device__ __forceinline__ uint32_t pack2(uint32_t a, uint32_t b) { return a | (b << 16); }
+
 // Symmetric residue of the digits modulo odd kModuli[l], as the low byte of
 // the returned word.
 template <int L>
@@ -260,7 +285,7 @@ constexpr int kConvWarps = 8;
 constexpr int kConvTile = 16 * 32;  // doubles per warp tile
 constexpr int kConvSmem = kConvWarps * (kConvStages * kConvTile * 8 + kConvStages * 8);
 
-template <int T, int L>
+template <int T, int L, bool BF>
 __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     const __grid_constant__ CUtensorMap map, int64_t KP, int64_t Rpad,
     const int* __restrict__ mu, uint8_t* __restrict__ res, uint32_t* __restrict__ err) {
@@ -322,9 +347,26 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     }
     const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, err);
     phase ^= 1u << s;
-    uint8_t* dst = res + (g * 16 + r) * KP + kb * 32 + 16 * h;
-    const int64_t lstride = Rpad * KP;
-    if (ok) {
+    constexpr int ES = BF ? 2 : 1;  // bytes per residue
+    uint8_t* dst = res + ((g * 16 + r) * KP + kb * 32 + 16 * h) * ES;
+    const int64_t lstride = Rpad * KP * ES;
+    if (ok && BF) {
+      const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
+      Digits d[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) d[j] = digits_of(blk[j * 16], s1, s2);
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        uint32_t b[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) b[j] = residue_bf16<L>(d[j], l);
+        uint4* d4 = reinterpret_cast<uint4*>(dst + l * lstride);
+        d4[0] = make_uint4(pack2(b[0], b[1]), pack2(b[2], b[3]), pack2(b[4], b[5]),
+                           pack2(b[6], b[7]));
+        d4[1] = make_uint4(pack2(b[8], b[9]), pack2(b[10], b[11]), pack2(b[12], b[13]),
+                           pack2(b[14], b[15]));
+      }
+    } else if (ok) {
       const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
       Digits d[16];
 #pragma unroll
@@ -344,7 +386,10 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
       }
     } else {
 #pragma unroll
-      for (int l = 0; l < L; ++l) *reinterpret_cast<uint4*>(dst + l * lstride) = make_uint4(0, 0, 0, 0);
+      for (int l = 0; l < L; ++l)
+#pragma unroll
+        for (int e = 0; e < ES; ++e)
+          reinterpret_cast<uint4*>(dst + l * lstride)[e] = make_uint4(0, 0, 0, 0);
     }
     __syncwarp();  // stage s consumed by every lane before it is refilled
     s = (s + 1) % kConvStages;
@@ -357,7 +402,7 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
 // src[p * panel_stride + k * ks + r]. Used for the rotation's A (grid-packed
 // Psi, rows = grid points, k = bands: panel_stride nb*16, ks 16) and B
 // (Q row-major, rows = columns of Q, k = rows of Q: panel_stride 16, ks nb).
-template <int L>
+template <int L, bool BF>
 __global__ void __launch_bounds__(256) convert_local_kernel(
     int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* __restrict__ src,
     int64_t panel_stride, int64_t ks, uint8_t* __restrict__ res, int* __restrict__ mu_out) {
@@ -394,6 +439,18 @@ __global__ void __launch_bounds__(256) convert_local_kernel(
     Digits d[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) d[j] = digits_of(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r]);
+    if (BF) {
+      uint8_t* dst = res + ((p * 16 + r) * KP + k0 + 8 * kk) * 2;
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        uint32_t b[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) b[j] = residue_bf16<L>(d[j], l);
+        *reinterpret_cast<uint4*>(dst + (int64_t)l * Rpad * KP * 2) =
+            make_uint4(pack2(b[0], b[1]), pack2(b[2], b[3]), pack2(b[4], b[5]), pack2(b[6], b[7]));
+      }
+      continue;
+    }
     uint8_t* dst = res + (p * 16 + r) * KP + k0 + 8 * kk;
     *reinterpret_cast<uint2*>(dst) = make_uint2(pack4(d[0].lo, d[1].lo, d[2].lo, d[3].lo),
                                                 pack4(d[4].lo, d[5].lo, d[6].lo, d[7].lo));
@@ -626,9 +683,9 @@ OzakiStream* ozaki_stream(DeviceState* dev, cudaStream_t s) {
 // (modulus, k-block) space, cut into segments at modulus boundaries and at
 // seg_cap k-blocks (INT32 exactness).
 int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int seg_cap,
-                  LanePlan** out) {
+                  LanePlan** out, int sub_cap = 0) {
   OzakiDevice& od = g_oz[dev->device];
-  auto key = std::make_tuple(M, N, KB, L * 4096 + seg_cap, syrk ? 1 : 0);
+  auto key = std::make_tuple(M, N, KB, (L * 4096 + seg_cap) * 64 + sub_cap, syrk ? 1 : 0);
   auto itp = od.plans.find(key);
   if (itp != od.plans.end()) {
     *out = itp->second;
@@ -653,27 +710,33 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
   if (pl->Q > W) pl->Q = (int)W;
   std::vector<int> lane_off(pl->Q + 1, 0);
   std::vector<I8Segment> segs;
+  int nslots = 0;
   std::vector<std::vector<int>> by_mod(L);
   for (int q = 0; q < pl->Q; ++q) {
     lane_off[q] = (int)segs.size();
     int64_t it = (int64_t)q * W / pl->Q, end = (int64_t)(q + 1) * W / pl->Q;
     while (it < end) {
       const int l = (int)(it / KB);
-      const int kb = (int)(it % KB);
       int64_t stop = std::min<int64_t>(end, (int64_t)(l + 1) * KB);
       stop = std::min<int64_t>(stop, it + seg_cap);
-      I8Segment s;
-      s.l = l;
-      s.kb0 = kb;
-      s.kb1 = kb + (int)(stop - it);
-      s.slot = (int)segs.size();
-      by_mod[l].push_back(s.slot);
-      segs.push_back(s);
+      // One slot per segment; with sub_cap > 0 the segment is issued as
+      // sub-segments of <= sub_cap k-blocks that accumulate into that slot.
+      const int slot = nslots++;
+      const int step = sub_cap > 0 ? sub_cap : (int)(stop - it);
+      for (int64_t a = it; a < stop; a += step) {
+        I8Segment sg;
+        sg.l = l;
+        sg.kb0 = (int)(a - (int64_t)l * KB);
+        sg.kb1 = (int)(std::min<int64_t>(stop, a + step) - (int64_t)l * KB);
+        sg.slot = slot;
+        segs.push_back(sg);
+      }
+      by_mod[l].push_back(slot);
       it = stop;
     }
   }
   lane_off[pl->Q] = (int)segs.size();
-  pl->slots = (int)segs.size();
+  pl->slots = nslots;
   std::vector<int> mod_off(L + 1, 0), mod_slots;
   for (int l = 0; l < L; ++l) {
     mod_off[l] = (int)mod_slots.size();
@@ -719,17 +782,25 @@ int make_res_map(CUtensorMap* map, const void* base, int64_t KP, int64_t Rpad, i
                       CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
-int launch_i8(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB, const I8Params& p,
-              int grid, cudaStream_t s) {
+template <bool BF>
+int launch_i8_t(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
+                const I8Params& p, int grid, cudaStream_t s) {
   static bool attr_done[64] = {false};
   if (!attr_done[dev->device]) {
-    SKG_CUDA(cudaFuncSetAttribute(i8_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SKG_CUDA(cudaFuncSetAttribute(i8_gemm_kernel<BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kI8SmemBytes));
     attr_done[dev->device] = true;
   }
-  i8_gemm_kernel<<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, p);
+  i8_gemm_kernel<BF><<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, p);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
+}
+
+// INT8 (bf = false) or BF16 (bf = true) residue products.
+int launch_i8(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB, const I8Params& p,
+              int grid, cudaStream_t s, bool bf = false) {
+  return bf ? launch_i8_t<true>(dev, mA, mB, p, grid, s)
+            : launch_i8_t<false>(dev, mA, mB, p, grid, s);
 }
 
 int launch_i8_rot(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
@@ -745,7 +816,13 @@ int launch_i8_rot(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB
   return SKGEMM_OK;
 }
 
+bool is_bf16(const skgemm_options_t* opts) {
+  return opts && opts->precision == SKGEMM_PREC_OZAKI_BF16;
+}
+
 int choose_L(const skgemm_options_t* opts, int64_t K, int* L_out, int* gamma_out) {
+  if (opts && opts->precision != SKGEMM_PREC_OZAKI_I8 && opts->precision != SKGEMM_PREC_OZAKI_BF16)
+    return fail(SKGEMM_ERR_INVALID_ARG, "precision must be native, Ozaki INT8 or Ozaki BF16");
   int L = opts ? opts->slices : 0;
   if (L == 0) {
     // Smallest L whose error estimate for random-sign data,
@@ -786,15 +863,15 @@ void report(skgemm_options_t* opts, int L, int gamma_bits, int64_t K) {
     default: return fail(SKGEMM_ERR_INVALID_ARG, "moduli count out of range");   \
   }
 
-template <int T, int L>
+template <int T, int L, bool BF>
 int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t Rpad,
                    const int* mu, uint8_t* res, uint32_t* err, cudaStream_t s) {
   static int occ[64] = {0};
   if (!occ[dev->device]) {
-    SKG_CUDA(cudaFuncSetAttribute(convert_tma_kernel<T, L>,
+    SKG_CUDA(cudaFuncSetAttribute(convert_tma_kernel<T, L, BF>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
     int n = 0;
-    SKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, convert_tma_kernel<T, L>, 256,
+    SKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, convert_tma_kernel<T, L, BF>, 256,
                                                            kConvSmem));
     occ[dev->device] = n > 0 ? n : 1;
   }
@@ -803,7 +880,8 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
                                            (int64_t)dev->num_sms * occ[dev->device]);
   // (every warp of the grid gets at least one tile only if ntiles >= warps;
   // warps without a tile return at once)
-  convert_tma_kernel<T, L><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, KP, Rpad, mu, res, err);
+  convert_tma_kernel<T, L, BF><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, KP, Rpad, mu, res,
+                                                                        err);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
@@ -814,14 +892,15 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
 // different streams with an event between them.
 template <int T>
 int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, int L,
-               DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu, cudaStream_t s) {
+               DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu, cudaStream_t s,
+               bool bf = false) {
   if ((reinterpret_cast<uintptr_t>(X) & 15) != 0)
     return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
   if (K > ((int64_t)1 << 31) - 128) return fail(SKGEMM_ERR_INVALID_ARG, "K too large");
   const int64_t P_in = (R + T - 1) / T;
   const int C = (int)std::max<int64_t>(1, std::min<int64_t>(64, (600 + P_in - 1) / P_in));
   int st;
-  if ((st = res.ensure((size_t)L * Rpad * KP)) != SKGEMM_OK) return st;
+  if ((st = res.ensure((size_t)L * Rpad * KP * (bf ? 2 : 1))) != SKGEMM_OK) return st;
   if ((st = part.ensure((size_t)P_in * C * T * sizeof(double))) != SKGEMM_OK) return st;
   if ((st = mu.ensure((size_t)Rpad * sizeof(int))) != SKGEMM_OK) return st;
   norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
@@ -836,7 +915,7 @@ int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, 
 template <int T>
 int prep_convert(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
                  const double* X, int L, DeviceBuffer& res, DeviceBuffer& mu, uint32_t* err,
-                 cudaStream_t s) {
+                 cudaStream_t s, bool bf = false) {
   // [P_in][K][T] doubles; boxes of 16 rows x 32 k (zero fill past K / P_in).
   const int64_t P_in = (R + T - 1) / T;
   CUtensorMap map;
@@ -849,30 +928,38 @@ int prep_convert(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpa
     return st;
   const int* mp = (const int*)mu.ptr;
   uint8_t* rp = (uint8_t*)res.ptr;
-  SKG_DISPATCH_L(L, (launch_convert<T, LL>(dev, map, KP, Rpad, mp, rp, err, s)))
+  if (bf) {
+    SKG_DISPATCH_L(L, (launch_convert<T, LL, true>(dev, map, KP, Rpad, mp, rp, err, s)))
+  }
+  SKG_DISPATCH_L(L, (launch_convert<T, LL, false>(dev, map, KP, Rpad, mp, rp, err, s)))
 }
 
 template <int T>
 int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
                 const double* X, int L, DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu,
-                uint32_t* err, cudaStream_t s) {
+                uint32_t* err, cudaStream_t s, bool bf = false) {
   int st;
-  if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s))) return st;
-  return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s);
+  if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s, bf))) return st;
+  return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s, bf);
 }
 
-template <int L>
+template <int L, bool BF>
 int launch_local_L(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* src,
                    int64_t panel_stride, int64_t ks, uint8_t* res, int* mu, cudaStream_t s) {
-  convert_local_kernel<L><<<(unsigned)(Rpad / 16), 256, 0, s>>>(R, K, KP, Rpad, src,
-                                                                panel_stride, ks, res, mu);
+  convert_local_kernel<L, BF><<<(unsigned)(Rpad / 16), 256, 0, s>>>(R, K, KP, Rpad, src,
+                                                                    panel_stride, ks, res, mu);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
 
 int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* src,
-                 int64_t panel_stride, int64_t ks, int L, uint8_t* res, int* mu, cudaStream_t s) {
-  SKG_DISPATCH_L(L, (launch_local_L<LL>(R, K, KP, Rpad, src, panel_stride, ks, res, mu, s)))
+                 int64_t panel_stride, int64_t ks, int L, uint8_t* res, int* mu, cudaStream_t s,
+                 bool bf = false) {
+  if (bf) {
+    SKG_DISPATCH_L(L, (launch_local_L<LL, true>(R, K, KP, Rpad, src, panel_stride, ks, res, mu,
+                                                s)))
+  }
+  SKG_DISPATCH_L(L, (launch_local_L<LL, false>(R, K, KP, Rpad, src, panel_stride, ks, res, mu, s)))
 }
 
 // Shared body of the Ozaki GEMM and SYRK: residues of A (packed16) and B
@@ -885,20 +972,26 @@ int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* s
 int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M, int64_t N,
                   int64_t KP, int L, bool syrk, const DeviceBuffer* resB, const DeviceBuffer* muB,
                   double* D, int64_t ldd, double alpha, double gamma, cudaStream_t s,
-                  DeviceBuffer* slabs = nullptr, cudaStream_t crt_stream = nullptr) {
+                  DeviceBuffer* slabs = nullptr, cudaStream_t crt_stream = nullptr,
+                  bool bf = false) {
   int st;
-  const int KB = (int)(KP / 128);
+  // Residue rows are KP * es bytes; a k-block is 128 bytes (128 INT8 or 64
+  // BF16 values). BF16: sub-segments of 16 k-blocks (1024 products, exact in
+  // FP32), 127 of them per int32 slot.
+  const int64_t KPb = KP * (bf ? 2 : 1);
+  const int KB = (int)(KPb / 128);
   const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
   DeviceBuffer& part = slabs ? *slabs : os->partials;
   LanePlan* pl = nullptr;
-  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk, kSegKbCapSigned, &pl)) !=
-      SKGEMM_OK)
+  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk,
+                          bf ? kSegKbCapBf16 : kSegKbCapSigned, &pl,
+                          bf ? kSubKbCapBf16 : 0)) != SKGEMM_OK)
     return st;
   if ((st = part.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t)))) return st;
   CUtensorMap mA, mB;
-  if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, L, kI8BM))) return st;
-  if ((st = make_res_map(&mB, resB->ptr, KP, syrk ? RA : RB, L, kI8BN))) return st;
+  if ((st = make_res_map(&mA, os->res_a.ptr, KPb, RA, L, kI8BM))) return st;
+  if ((st = make_res_map(&mB, resB->ptr, KPb, syrk ? RA : RB, L, kI8BN))) return st;
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedLanes;
@@ -914,7 +1007,7 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   p.segs = pl->segs;
   p.partials = (int32_t*)part.ptr;
   p.err = ws->err;
-  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s))) return st;
+  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s, bf))) return st;
   // The reconstruction runs on `crt_stream` (forked after the products) when
   // given, so that it can overlap the caller's next launch on `s`.
   cudaStream_t cs = s;
@@ -937,13 +1030,15 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
 // B (packed32, N rows) into os->res_b: norms(A) | norms(B) on the helper
 // stream, convert(A), join, convert(B).
 int prep_pair(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M, int64_t N,
-              int64_t K, int L, const double* Ap, const double* Bp, cudaStream_t s) {
+              int64_t K, int L, const double* Ap, const double* Bp, cudaStream_t s,
+              bool bf = false) {
   int st;
   const int64_t KP = (K + 127) / 128 * 128;
   const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;  // 256-multiples serve both box heights
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
   if (!Bp)
-    return prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, ws->err, s);
+    return prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, ws->err, s,
+                           bf);
   if (!os->aux) {
     SKG_CUDA(cudaStreamCreateWithFlags(&os->aux, cudaStreamNonBlocking));
     SKG_CUDA(cudaEventCreateWithFlags(&os->fork, cudaEventDisableTiming));
@@ -951,14 +1046,15 @@ int prep_pair(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M,
   }
   SKG_CUDA(cudaEventRecord(os->fork, s));
   SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork, 0));
-  const int st_b = prep_norms<32>(N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b, os->aux);
+  const int st_b =
+      prep_norms<32>(N, K, KP, RB, Bp, L, os->res_b, os->part_b, os->mu_b, os->aux, bf);
   SKG_CUDA(cudaEventRecord(os->join, os->aux));  // join even when the B step failed
   if (st_b) return st_b;
   if ((st = prep_packed<16>(dev, M, K, KP, RA, Ap, L, os->res_a, os->part_a, os->mu_a, ws->err,
-                            s)))
+                            s, bf)))
     return st;
   SKG_CUDA(cudaStreamWaitEvent(s, os->join, 0));
-  return prep_convert<32>(dev, N, K, KP, RB, Bp, L, os->res_b, os->mu_b, ws->err, s);
+  return prep_convert<32>(dev, N, K, KP, RB, Bp, L, os->res_b, os->mu_b, ws->err, s, bf);
 }
 
 // Shared body of the Ozaki GEMM and SYRK: residues of A (packed16) and B
@@ -982,10 +1078,12 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
   if (!ws) return st;
   OzakiStream* os = ozaki_stream(dev, s);
   const int64_t KP = (K + 127) / 128 * 128;
-  if ((st = prep_pair(dev, os, ws, M, N, K, L, Ap, syrk ? nullptr : Bp, s))) return st;
+  const bool bf = is_bf16(opts);
+  if ((st = prep_pair(dev, os, ws, M, N, K, L, Ap, syrk ? nullptr : Bp, s, bf))) return st;
   const DeviceBuffer* resB = syrk ? &os->res_a : &os->res_b;
   const DeviceBuffer* muB = syrk ? &os->mu_a : &os->mu_b;
-  if ((st = lanes_product(dev, os, ws, M, N, KP, L, syrk, resB, muB, D, ldd, alpha, gamma, s)))
+  if ((st = lanes_product(dev, os, ws, M, N, KP, L, syrk, resB, muB, D, ldd, alpha, gamma, s,
+                          nullptr, nullptr, bf)))
     return st;
   report(opts, L, gb, K);
   return SKGEMM_OK;
@@ -1011,7 +1109,8 @@ int subspace_impl(int64_t K, int64_t M, const double* Psi, const double* HPsi, d
   if (!ws) return st;
   OzakiStream* os = ozaki_stream(dev, s);
   const int64_t KP = (K + 127) / 128 * 128;
-  if ((st = prep_pair(dev, os, ws, M, M, K, L, Psi, HPsi, s))) return st;
+  const bool bf = is_bf16(opts);
+  if ((st = prep_pair(dev, os, ws, M, M, K, L, Psi, HPsi, s, bf))) return st;
   if (!os->fork2) {
     SKG_CUDA(cudaEventCreateWithFlags(&os->fork2, cudaEventDisableTiming));
     SKG_CUDA(cudaEventCreateWithFlags(&os->join2, cudaEventDisableTiming));
@@ -1019,10 +1118,10 @@ int subspace_impl(int64_t K, int64_t M, const double* Psi, const double* HPsi, d
   // S: products on s, reconstruction on the helper stream (overlaps Hs's
   // products, which write their own slabs); join before returning.
   if ((st = lanes_product(dev, os, ws, M, M, KP, L, true, &os->res_a, &os->mu_a, S, lds, alpha_s,
-                          beta_s, s, &os->partials, os->aux)))
+                          beta_s, s, &os->partials, os->aux, bf)))
     return st;
   st = lanes_product(dev, os, ws, M, M, KP, L, false, &os->res_b, &os->mu_b, Hs, ldh, alpha_h,
-                     gamma_h, s, &os->partials2, nullptr);
+                     gamma_h, s, &os->partials2, nullptr, bf);
   SKG_CUDA(cudaStreamWaitEvent(s, os->join2, 0));
   if (st) return st;
   report(opts, L, gb, K);
@@ -1294,6 +1393,10 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   if (Nd == 0 || nb == 0) return SKGEMM_OK;
   if (!A || !Q || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
   if (nb > 2048) return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki rotation supports nb <= 2048");
+  const bool bf = is_bf16(opts);
+  // BF16: one FP32 accumulation over K = nb must stay exact (<= 1024 products).
+  if (bf && nb > 1024)
+    return fail(SKGEMM_ERR_UNSUPPORTED, "Ozaki BF16 rotation supports nb <= 1024");
   if (Nd > ((int64_t)1 << 30)) return fail(SKGEMM_ERR_INVALID_ARG, "Nd too large");
   int L, gb;
   if ((st = choose_L(opts, nb, &L, &gb)) != SKGEMM_OK) return st;
@@ -1305,20 +1408,21 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   const int64_t KP = (nb + 127) / 128 * 128;
   const int64_t RA = (Nd + kI8BM - 1) / kI8BM * kI8BM;
   const int64_t RB = (nb + kI8BN - 1) / kI8BN * kI8BN;
-  if ((st = os->res_b.ensure((size_t)L * RB * KP))) return st;
+  const int64_t KPb = KP * (bf ? 2 : 1);
+  if ((st = os->res_b.ensure((size_t)L * RB * KPb))) return st;
   if ((st = os->mu_b.ensure((size_t)RB * sizeof(int)))) return st;
   if ((st = os->rbytes.ensure((size_t)L * Nd * nb))) return st;
   // Grid-packed Psi is a packed16 operand with rows = grid points, K = bands.
   if ((st = prep_packed<16>(dev, Nd, nb, KP, RA, A, L, os->res_a, os->part_a, os->mu_a, ws->err,
-                            s)))
+                            s, bf)))
     return st;
   if ((st = launch_local(nb, nb, KP, RB, Q, 16, nb, L, (uint8_t*)os->res_b.ptr,
-                         (int*)os->mu_b.ptr, s)))
+                         (int*)os->mu_b.ptr, s, bf)))
     return st;
   CUtensorMap mA, mB;
-  if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, L, kI8BM))) return st;
-  if ((st = make_res_map(&mB, os->res_b.ptr, KP, RB, L, kI8BN))) return st;
-  if (KP / 128 <= kI8RotKbMax && nb % 16 == 0 && nb >= 128 && Nd >= 128) {
+  if ((st = make_res_map(&mA, os->res_a.ptr, KPb, RA, L, kI8BM))) return st;
+  if ((st = make_res_map(&mB, os->res_b.ptr, KPb, RB, L, kI8BN))) return st;
+  if (!bf && KP / 128 <= kI8RotKbMax && nb % 16 == 0 && nb >= 128 && Nd >= 128) {
     // B_l[tn] fits in shared memory: the B-resident schedule, residue bytes
     // [L][Nd][nb] written by 32 x 128-byte TMA store boxes.
     CUtensorMap mR;
@@ -1348,7 +1452,7 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
     p.sched = kSchedUnits;
     p.is_signed = 1;
     p.L = L;
-    p.KB = (int)(KP / 128);
+    p.KB = (int)(KPb / 128);
     p.M = (int)Nd;
     p.N = (int)nb;
     p.tiles_m = (int)(RA / kI8BM);
@@ -1358,7 +1462,7 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
     p.err = ws->err;
     const int64_t units = (int64_t)p.tiles_m * L * p.tiles_n;
     const int grid = (int)std::min<int64_t>(dev->num_sms, units);
-    if ((st = launch_i8(dev, mA, mB, p, grid, s))) return st;
+    if ((st = launch_i8(dev, mA, mB, p, grid, s, bf))) return st;
   }
   {
     const uint8_t* rb = (const uint8_t*)os->rbytes.ptr;

@@ -40,6 +40,7 @@ ERR_UNSUPPORTED = -6
 PREC_NATIVE = 0
 PREC_OZAKI_I8 = 1
 PREC_AUTO = 2  # batched plans: per problem, the faster path
+PREC_OZAKI_BF16 = 3  # Ozaki with BF16 residues (results equal PREC_OZAKI_I8)
 
 
 class SkgemmError(RuntimeError):
@@ -397,7 +398,8 @@ class Plan:
                 "graph_kernels": o.graph_kernels_out}
 
     def precisions(self) -> list:
-        """Per item: PREC_NATIVE or PREC_OZAKI_I8 (the path the plan runs it on)."""
+        """Per item: PREC_NATIVE, PREC_OZAKI_I8 or PREC_OZAKI_BF16 (the path the
+        plan runs it on)."""
         n = self._n
         out = (ctypes.c_int * max(1, n))()
         _check(lib().skgemm_plan_precisions(self._h, out, n))

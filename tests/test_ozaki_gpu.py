@@ -211,3 +211,78 @@ def test_ozaki_error_table_subspace_shapes(cuda):
         rows = {L: (es, eh) for k, L, _, _, es, eh, _ in table if k == kind}
         assert rows[8][0] > rows[12][0] > rows[16][0] * 0.999
         assert rows[8][1] > rows[12][1] > rows[16][1] * 0.999
+
+
+BF = skgemm.PREC_OZAKI_BF16
+
+
+@pytest.mark.parametrize("M,N,K", [(200, 136, 3000), (64, 300, 140000), (1, 1, 5), (257, 33, 1024)])
+def test_ozaki_bf16_gemm_equals_int8(cuda, M, N, K):
+    """BF16 residues on kind::f16 MMAs (FP32 sums of <= 1024 products, exact,
+    added in INT32) give the INT8 path's integers: results equal bit for bit.
+    K = 140000 crosses a 127-sub-segment slot; K = 1024 is one full
+    sub-segment."""
+    A = gaussian((M, K), 31)
+    B = gaussian((K, N), 32)
+    Ap, Bp = dev(oracle.pack(A, 16)), dev(oracle.pack(np.ascontiguousarray(B.T), 32))
+    D8 = torch.full((M * N,), np.nan, dtype=torch.float64, device="cuda")
+    Db = torch.full_like(D8, np.nan)
+    skgemm.dgemm_packed_dev(M, N, K, Ap, Bp, D8, N, 1.25, 0.5, precision=OZ)
+    skgemm.dgemm_packed_dev(M, N, K, Ap, Bp, Db, N, 1.25, 0.5, precision=BF)
+    skgemm.stream_status()
+    assert torch.equal(D8, Db)
+    if M * N * K <= 2e8:
+        ref = oracle.dot2_matmul(A, B, 1.25, 0.5)
+        assert oracle.rel_frobenius(Db.cpu().numpy().reshape(M, N), ref) <= TOL
+
+
+@pytest.mark.parametrize("K,M", [(20000, 300), (4099, 100)])
+def test_ozaki_bf16_syrk_and_pair_equal_int8(cuda, K, M):
+    Psi = gaussian((K, M), 41)
+    H = uniform((K, M), 42)
+    P16 = dev(oracle.pack(np.ascontiguousarray(Psi.T), 16))
+    H32 = dev(oracle.pack(np.ascontiguousarray(H.T), 32))
+    outs = {}
+    for prec in (OZ, BF):
+        C = torch.zeros((M, M), dtype=torch.float64, device="cuda")
+        S = torch.zeros_like(C)
+        Hs = torch.zeros_like(C)
+        skgemm.dsyrk_packed_dev(K, M, P16, C, M, precision=prec)
+        skgemm.dsubspace_packed_dev(K, M, P16, H32, S, Hs, precision=prec)
+        skgemm.stream_status()
+        outs[prec] = (C, S, Hs)
+    iu = np.triu_indices(M)
+    for idx, (a, b) in enumerate(zip(outs[OZ], outs[BF])):
+        x, y = a.cpu().numpy(), b.cpu().numpy()
+        if idx < 2:  # SYRK outputs: the upper triangle (column-major)
+            assert np.array_equal(x.T[iu], y.T[iu])
+        else:
+            assert np.array_equal(x, y)
+    s = outs[BF][0].cpu().numpy().T
+    assert oracle.rel_frobenius(s[iu], oracle.dot2_matmul(Psi.T, Psi)[iu]) <= TOL
+
+
+@pytest.mark.parametrize("Nd,nb", [(2048, 512), (1040, 208), (512, 1024)])
+def test_ozaki_bf16_rot_equals_int8(cuda, Nd, nb):
+    Psi = gaussian((Nd, nb), 51)
+    Q = uniform((nb, nb), 52)
+    A = dev(oracle.grid_pack(Psi))
+    q = dev(Q)
+    D8 = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+    Db = torch.full_like(D8, np.nan)
+    skgemm.drot_dev(Nd, nb, A, q, D8, precision=OZ)
+    skgemm.drot_dev(Nd, nb, A, q, Db, precision=BF)
+    skgemm.stream_status()
+    assert torch.equal(D8, Db)
+    ref = oracle.band_pack(oracle.dot2_matmul(Psi, Q)).ravel()
+    assert oracle.rel_frobenius(Db.cpu().numpy(), ref) <= TOL
+
+
+def test_ozaki_bf16_rot_rejects_large_nb(cuda):
+    Nd, nb = 64, 1040
+    A = torch.zeros(Nd * nb, dtype=torch.float64, device="cuda")
+    q = torch.zeros(nb * nb, dtype=torch.float64, device="cuda")
+    D = torch.zeros_like(A)
+    with pytest.raises(skgemm.SkgemmError) as e:
+        skgemm.drot_dev(Nd, nb, A, q, D, precision=BF)
+    assert e.value.code == skgemm.ERR_UNSUPPORTED
