@@ -10,7 +10,7 @@ Q = 512 x 512 U[-1,1]:
 in the reference's packed layouts (band-packed Psi for SYRK/GEMM, 32-band-
 packed H*Psi, grid-packed Psi for the rotation, band-packed Psi').
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision native|ozaki]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision native|ozaki|ozaki_bf16]
     python bench.py --impl reference ...     # the reference's CPU kernels
 
 Other workloads (not the default line):
@@ -60,8 +60,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="skgemm", choices=["skgemm", "reference"])
-    ap.add_argument("--precision", default="native", choices=["native", "ozaki", "auto"],
-                    help="auto: batched workload only (the plan picks per problem)")
+    ap.add_argument("--precision", default="native",
+                    choices=["native", "ozaki", "ozaki_bf16", "auto"],
+                    help="ozaki: INT8 residues; ozaki_bf16: BF16 residues (same results); "
+                         "auto: batched workload only (the plan picks per problem)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nd", type=int, default=ND,
@@ -207,7 +209,8 @@ def run_gpu(args):
         raise SystemExit("--precision auto applies to --workload batched")
     rank, world, dist = dist_setup(args.gpus)
     dev = torch.device("cuda", torch.cuda.current_device())
-    prec = skgemm.PREC_OZAKI_I8 if args.precision == "ozaki" else None
+    prec = {"native": None, "ozaki": skgemm.PREC_OZAKI_I8,
+            "ozaki_bf16": skgemm.PREC_OZAKI_BF16}[args.precision]
     band, h32, grid, q = make_inputs(dev)
     S = torch.zeros(NB, NB, dtype=torch.float64, device=dev)
     Hs = torch.zeros_like(S)
@@ -493,6 +496,7 @@ def run_batched(args):
         flop += nb * nb * ng + 2.0 * nb * nb * ng
     stream = torch.cuda.current_stream()
     prec = {"native": skgemm.PREC_NATIVE, "ozaki": skgemm.PREC_OZAKI_I8,
+            "ozaki_bf16": skgemm.PREC_OZAKI_BF16,
             "auto": skgemm.PREC_AUTO}[args.precision]
     plan = skgemm.Plan(items, tile=args.tile, order=2 if args.no_tune else 0,
                        tune=not args.no_tune, stream=stream, precision=prec)
@@ -553,10 +557,10 @@ def run_serving(args):
     import numpy as np
     import torch
     import skgemm
-    if args.precision == "auto":
-        raise SystemExit("--precision auto applies to --workload batched")
+    if args.precision in ("auto", "ozaki_bf16"):
+        raise SystemExit("the serving workload runs --precision native or ozaki")
     rank, world, dist = dist_setup(args.gpus)
-    prec = skgemm.PREC_OZAKI_I8 if args.precision == "ozaki" else skgemm.PREC_NATIVE
+    prec = {"native": skgemm.PREC_NATIVE, "ozaki": skgemm.PREC_OZAKI_I8}[args.precision]
     trace = skgemm.serve_trace(args.requests, rate=200.0, seed=11 + rank)
     warm = skgemm.serve_trace(8, rate=200.0, seed=99, nb_range=(32, 256), ng_range=(1e4, 5e4))
     skgemm.serve(warm, precision=prec, hbm_budget=150e9)
