@@ -288,7 +288,8 @@ def run_gpu(args):
         "roofline": {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
                      "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
                      "peak_source": "measured FP64 DMMA peak (skgemm_probe_fp64_peak, this run)",
-                     "kernel": "fp64_streamk_kernel" if prec is None else
+                     "kernel": "fp64_streamk_kernel64 (SYRK, rotation), fp64_streamk_kernel "
+                               "(GEMM)" if prec is None else
                      "Ozaki split (i8_gemm_kernel + residue conversion), FP64-equivalent flops",
                      "traffic": read_profile_traffic() if prec is None else None},
         "clocks": clk,

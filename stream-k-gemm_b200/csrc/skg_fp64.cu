@@ -44,27 +44,65 @@ struct Schedule {
   int grid;
 };
 
-Schedule make_schedule(DeviceState* dev, const Fp64Problem& prob) {
+Schedule make_schedule(DeviceState* dev, const Fp64Problem& prob, int tile, int per_sm) {
   Schedule sc;
-  sc.tiles_m = (int)((prob.M + kBM - 1) / kBM);
-  sc.tiles_n = (int)((prob.N + kBN - 1) / kBN);
+  sc.tiles_m = (int)((prob.M + tile - 1) / tile);
+  sc.tiles_n = (int)((prob.N + tile - 1) / tile);
   sc.num_tiles = prob.tile_order == kTilesUpper ? sc.tiles_n * (sc.tiles_n + 1) / 2
                                                 : sc.tiles_m * sc.tiles_n;
   sc.ipt = (int)((prob.K + kBK - 1) / kBK);
   sc.total = (int64_t)sc.num_tiles * sc.ipt;
-  sc.grid = (int)std::min<int64_t>(dev->num_sms, sc.total);
+  sc.grid = (int)std::min<int64_t>((int64_t)dev->num_sms * per_sm, sc.total);
   return sc;
+}
+
+// Issued MACs (padding included) of `prob` on tile x tile outputs.
+double issued_macs(const Fp64Problem& prob, int tile) {
+  const double tm = (double)((prob.M + tile - 1) / tile), tn = (double)((prob.N + tile - 1) / tile);
+  const double tiles = prob.tile_order == kTilesUpper ? tn * (tn + 1) / 2 : tm * tn;
+  return tiles * tile * tile * (double)((prob.K + kBK - 1) / kBK * kBK);
+}
+
+// Tile of a single-problem launch: 64 x 64 when it issues fewer MACs than
+// 128 x 128 (triangles, ragged edges) or when the output has so many
+// 128 x 128 tiles (>= 4 per SM) that two CTAs per SM pay off; 128 x 128
+// otherwise. Measured on B200 with 110592 x 512 operands: SYRK 0.95 ms on
+// 64 x 64 vs 1.08 ms on 128 x 128, rotation 1.72 vs 1.77 ms, GEMM
+// (M = N = 512, 16 tiles) 1.68 vs 1.67 ms.
+int single_tile(DeviceState* dev, const Fp64Problem& prob) {
+  const double i64 = issued_macs(prob, 64), i128 = issued_macs(prob, 128);
+  if (i64 < i128) return 64;
+  const double t128 = i128 / (128.0 * 128.0 * (double)((prob.K + kBK - 1) / kBK * kBK));
+  return (i64 == i128 && t128 >= 4.0 * dev->num_sms) ? 64 : 128;
+}
+
+// CTAs per SM of the single-problem kernel of `tile` (its shared-memory
+// attribute set once per device).
+template <class TS>
+int single_setup(int device, const void* kernel, int* per_sm) {
+  static int occ[2][64] = {};
+  int& o = occ[TS::BM == 64 ? 1 : 0][device];
+  if (!o) {
+    SKG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TS::kSmem));
+    int n = 0;
+    SKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreads, TS::kSmem));
+    if (n < 1) return fail(SKGEMM_ERR_CUDA, "FP64 kernel does not fit on an SM");
+    o = std::min(n, TS::kMinBlocks);
+  }
+  *per_sm = o;
+  return SKGEMM_OK;
 }
 
 }  // namespace
 
 int fp64_grid_for(DeviceState* dev, const Fp64Problem& prob) {
   if (prob.M <= 0 || prob.N <= 0 || prob.K <= 0) return 0;
-  return make_schedule(dev, prob).grid;
+  return make_schedule(dev, prob, 128, 1).grid;
 }
 
 int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
-                StreamWorkspace* ws_override) {
+                StreamWorkspace* ws_override, int tile) {
   if (prob.M < 0 || prob.N < 0 || prob.K < 0)
     return fail(SKGEMM_ERR_INVALID_ARG, "negative dimension");
   if (prob.tile_order == kTilesUpper && prob.M != prob.N)
@@ -78,19 +116,26 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
     // Empty reduction: D = gamma (GEMM), C = beta*C (SYRK), D = 0 (rotation).
     return fail(SKGEMM_ERR_UNSUPPORTED, "K == 0 is handled by the caller");
   }
-  Schedule sc = make_schedule(dev, prob);
+  if (tile == 0) tile = single_tile(dev, prob);
+  if (tile != 128 && tile != 64) return fail(SKGEMM_ERR_INVALID_ARG, "tile must be 128 or 64");
+  const void* kernel = tile == 64 ? (const void*)fp64_streamk_kernel64
+                                  : (const void*)fp64_streamk_kernel;
+  int per_sm = 1, st = SKGEMM_OK;
+  if ((st = tile == 64 ? single_setup<Tile64>(dev->device, kernel, &per_sm)
+                       : single_setup<Tile128>(dev->device, kernel, &per_sm)))
+    return st;
+  Schedule sc = make_schedule(dev, prob, tile, per_sm);
   if ((int64_t)sc.num_tiles * sc.ipt > ((int64_t)1 << 40))
     return fail(SKGEMM_ERR_INVALID_ARG, "problem too large");
 
-  int st = SKGEMM_OK;
   StreamWorkspace* ws = ws_override ? ws_override : stream_workspace(dev, s, sc.grid, &st);
   if (!ws) return st;
   if ((int)ws->partial_slots < sc.grid)
     return fail(SKGEMM_ERR_INVALID_ARG, "workspace has fewer partial slots than the grid");
 
   CUtensorMap mapA, mapB;
-  if ((st = make_operand_map(&mapA, prob.a, prob.K, kBM)) != SKGEMM_OK) return st;
-  if ((st = make_operand_map(&mapB, prob.b, prob.K, kBN)) != SKGEMM_OK) return st;
+  if ((st = make_operand_map(&mapA, prob.a, prob.K, tile)) != SKGEMM_OK) return st;
+  if ((st = make_operand_map(&mapB, prob.b, prob.K, tile)) != SKGEMM_OK) return st;
 
   Fp64Params p;
   p.M = prob.M;
@@ -117,23 +162,20 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
   if (p.epoch == 0) p.epoch = ++ws->epoch;  // 0 is the value of a fresh flag
   p.err = ws->err;
 
-  static bool attr_done[64] = {false};
-  if (dev->device < 64 && !attr_done[dev->device]) {
-    SKG_CUDA(cudaFuncSetAttribute(fp64_streamk_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    attr_done[dev->device] = true;
-  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(sc.grid);
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = kSmemBytes;
+  cfg.dynamicSmemBytes = tile == 64 ? Tile64::kSmem : Tile128::kSmem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  SKG_CUDA(cudaLaunchKernelEx(&cfg, fp64_streamk_kernel, mapA, mapB, p));
+  if (tile == 64)
+    SKG_CUDA(cudaLaunchKernelEx(&cfg, fp64_streamk_kernel64, mapA, mapB, p));
+  else
+    SKG_CUDA(cudaLaunchKernelEx(&cfg, fp64_streamk_kernel, mapA, mapB, p));
   return SKGEMM_OK;
 }
 

@@ -20,7 +20,8 @@
 // runs the epilogue. The reduction order is a pure function of the schedule,
 // so results are bitwise reproducible run to run.
 //
-// The same body serves one problem (fp64_streamk_kernel, BM = BN = 128) and a
+// The same body serves one problem (fp64_streamk_kernel, BM = BN = 128, or
+// fp64_streamk_kernel64, BM = BN = 64) and a
 // group of problems in one launch (fp64_grouped_kernel<TileShape>, the
 // batched path: iterations of all problems concatenated, see Fp64Group).
 //
@@ -429,6 +430,15 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const __grid_constant__ Fp64Params p) {
   const SingleSched S{p, &mapA, &mapB};
   streamk_body<Tile128>(S);
+}
+
+// One problem on 64 x 64 tiles, two CTAs per SM.
+__global__ void __launch_bounds__(kThreads, Tile64::kMinBlocks)
+    fp64_streamk_kernel64(const __grid_constant__ CUtensorMap mapA,
+                          const __grid_constant__ CUtensorMap mapB,
+                          const __grid_constant__ Fp64Params p) {
+  const SingleSched S{p, &mapA, &mapB};
+  streamk_body<Tile64>(S);
 }
 
 template <class TS>

@@ -123,7 +123,8 @@ extern "C" __attribute__((visibility("default"))) int skgemm_dgemm_packed_dev_no
     return fail(SKGEMM_ERR_INVALID_ARG, buf);
   }
   SKG_CUDA(cudaMemsetAsync(nd.ws.err, 0, sizeof(uint32_t), s));
-  if ((st = launch_fp64(dev, p, s, &nd.ws)) != SKGEMM_OK) return st;
+  // 128 x 128 tiles: the static scratch holds that launch's slots.
+  if ((st = launch_fp64(dev, p, s, &nd.ws, 128)) != SKGEMM_OK) return st;
   SKG_CUDA(cudaStreamSynchronize(s));
   uint32_t word = 0;
   SKG_CUDA(cudaMemcpy(&word, nd.ws.err, sizeof(word), cudaMemcpyDeviceToHost));

@@ -89,9 +89,11 @@ struct Fp64Problem {
 
 // Enqueues the native FP64 Stream-K kernel on `s`. `ws_override` (optional)
 // supplies caller-owned partial slots/flags/err instead of the stream cache.
+// `tile` 128 or 64 fixes the output tile; 0 lets the cost model choose.
 int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
-                StreamWorkspace* ws_override = nullptr);
-// Number of Stream-K partial slots the launch of `prob` uses (= its grid).
+                StreamWorkspace* ws_override = nullptr, int tile = 0);
+// Number of Stream-K partial slots the 128 x 128-tile launch of `prob` uses
+// (= its grid).
 int fp64_grid_for(DeviceState* dev, const Fp64Problem& prob);
 // Grouped launch (batched path): CTAs per SM the grouped kernel of `tile`
 // (128 or 64) fits, and the launch itself (flag reset + kernel, no cooperative
