@@ -75,6 +75,7 @@ struct I8Params {
   int M, N;          // output extent (bounds of stores)
   // kSchedLanes
   int T;             // tiles
+  int T1;            // tiles t >= T1 (T1 > 0) take B from mapB2 (fused subspace pair)
   int Q;             // lanes
   const int2* tiles;            // [T] (tm, tn)
   const int* lane_seg_off;      // [Q+1] offsets into segs
@@ -122,7 +123,7 @@ __device__ __forceinline__ uint32_t mod_exact24(uint32_t u, uint32_t m, uint32_t
 
 // Work item seen by all roles.
 struct I8Item {
-  int l, tm, tn, kb0, kb1, slot;
+  int l, tm, tn, kb0, kb1, slot, t;
 };
 
 __device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cursor,
@@ -138,6 +139,7 @@ __device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cu
     it.kb0 = s.kb0;
     it.kb1 = s.kb1;
     it.slot = s.slot * p.T + t;
+    it.t = t;
     it.tm = tt.x;
     it.tn = tt.y;
     ++cursor;
@@ -155,6 +157,7 @@ __device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cu
   it.kb0 = 0;
   it.kb1 = p.KB;
   it.slot = 0;
+  it.t = 0;
   ++cursor;
   return true;
 }
@@ -208,7 +211,8 @@ __device__ __forceinline__ void i8_residue_epilogue(uint32_t taddr, int c_begin,
 template <bool BF>
 __global__ void __launch_bounds__(kI8Threads, 1)
     i8_gemm_kernel(const __grid_constant__ CUtensorMap mapA,
-                   const __grid_constant__ CUtensorMap mapB, const I8Params p) {
+                   const __grid_constant__ CUtensorMap mapB,
+                   const __grid_constant__ CUtensorMap mapB2, const I8Params p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
@@ -256,12 +260,14 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     if (lane == 0) {
       tma_prefetch_desc(&mapA);
       tma_prefetch_desc(&mapB);
+      if (p.T1 > 0) tma_prefetch_desc(&mapB2);
       int stage = 0;
       uint32_t phase = 0;
       int cur = 0;
       int64_t issued = 0;
       I8Item it;
       while (!*abort_flag && i8_next_item(p, cta, cur, it)) {
+        const CUtensorMap* mb = (p.T1 > 0 && it.t >= p.T1) ? &mapB2 : &mapB;
         for (int kb = it.kb0; kb < it.kb1; ++kb) {
           if (!mbar_wait(&empty_bar[stage], phase ^ 1, p.err)) {
             *abort_flag = 1;
@@ -271,8 +277,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
           uint8_t* sa = smem + stage * kI8StageBytes;
           mbar_arrive_expect_tx(&full_bar[stage], kI8StageBytes);
           tma_load_3d(sa, &mapA, &full_bar[stage], kb * kI8BK, it.tm * kI8BM, it.l);
-          tma_load_3d(sa + kI8TileABytes, &mapB, &full_bar[stage], kb * kI8BK, it.tn * kI8BN,
-                      it.l);
+          tma_load_3d(sa + kI8TileABytes, mb, &full_bar[stage], kb * kI8BK, it.tn * kI8BN, it.l);
           if (++stage == kI8Stages) {
             stage = 0;
             phase ^= 1;

@@ -58,9 +58,16 @@ constexpr int kSegKbCapBf16 = 127 * kSubKbCapBf16;
 // 2^-9 < 1/(2m), the least distance of S/m from a half-integer. Then
 // r = S - q m in [-(m-1)/2, (m-1)/2] is the symmetric residue, a signed byte,
 // read from the low mantissa byte of r + 1.5 2^23. m = 256: the low byte of X.
+// Residue digit sets: for L <= kShortDigitsMaxL moduli (|X| <= 2^57) three
+// unsigned 14-bit digits and a signed X >> 42 with symmetric constants
+// (|c| <= 127), so |S| < 2^23 with one FMA fewer per modulus; for L = 16
+// (|X| <= 2^61) four unsigned 12-bit digits and a signed X >> 48.
+constexpr int kShortDigitsMaxL = 15;
+
 struct ResidueConsts {
   int gamma_bits;
   float c[4][kI8MaxModuli];  // 2^(12 (j+1)) mod m
+  float cs[3][kI8MaxModuli]; // 2^(14 (j+1)) mod m, symmetric representative
   float inv[kI8MaxModuli];   // fl(1/m)
   float m[kI8MaxModuli];
   uint32_t mi[kI8MaxModuli];
@@ -172,21 +179,35 @@ __device__ __forceinline__ float field12(uint32_t x) {
   return __uint_as_float(0x4B000000u | (x & 0xFFFu)) - 8388608.0f;
 }
 
-// The five digits of X = rint((v s1) s2) as exact floats, and X's low word.
+// Exact FP32 value of a 14-bit field.
+__device__ __forceinline__ float field14(uint32_t x) {
+  return __uint_as_float(0x4B000000u | (x & 0x3FFFu)) - 8388608.0f;
+}
+
+// The digits of X = rint((v s1) s2) as exact floats, and X's low word.
 struct Digits {
   float f0, f1, f2, f3, f4;
   uint32_t lo;
 };
+template <int L>
 __device__ __forceinline__ Digits digits_of(double v, double s1, double s2) {
   const long long X = __double2ll_rn((v * s1) * s2);
   const uint32_t lo = (uint32_t)X, hi = (uint32_t)((unsigned long long)X >> 32);
   Digits d;
   d.lo = lo;  // m = 256: its low byte
-  d.f0 = field12(lo);
-  d.f1 = field12(lo >> 12);
-  d.f2 = field12(__funnelshift_r(lo, hi, 24));
-  d.f3 = field12(hi >> 4);
-  d.f4 = __int_as_float(0x4B400000 + ((int)hi >> 16)) - kMagic;  // signed d4
+  if constexpr (L <= kShortDigitsMaxL) {
+    d.f0 = field14(lo);
+    d.f1 = field14(lo >> 14);
+    d.f2 = field14(__funnelshift_r(lo, hi, 28));
+    d.f3 = __int_as_float(0x4B400000 + ((int)hi >> 10)) - kMagic;  // signed X >> 42
+    d.f4 = 0.0f;
+  } else {
+    d.f0 = field12(lo);
+    d.f1 = field12(lo >> 12);
+    d.f2 = field12(__funnelshift_r(lo, hi, 24));
+    d.f3 = field12(hi >> 4);
+    d.f4 = __int_as_float(0x4B400000 + ((int)hi >> 16)) - kMagic;  // signed X >> 48
+  }
   return d;
 }
 
@@ -195,8 +216,12 @@ __device__ __forceinline__ Digits digits_of(double v, double s1, double s2) {
 template <int L>
 __device__ __forceinline__ float residue_float(const Digits& d, int l) {
   const ResidueConsts& rc = c_res[L];
-  const float S = fmaf(d.f4, rc.c[3][l],
-                       fmaf(d.f3, rc.c[2][l], fmaf(d.f2, rc.c[1][l], fmaf(d.f1, rc.c[0][l], d.f0))));
+  float S;
+  if constexpr (L <= kShortDigitsMaxL)
+    S = fmaf(d.f3, rc.cs[2][l], fmaf(d.f2, rc.cs[1][l], fmaf(d.f1, rc.cs[0][l], d.f0)));
+  else
+    S = fmaf(d.f4, rc.c[3][l],
+             fmaf(d.f3, rc.c[2][l], fmaf(d.f2, rc.c[1][l], fmaf(d.f1, rc.c[0][l], d.f0))));
   const float q = fmaf(S, rc.inv[l], kMagic) - kMagic;
   return fmaf(-q, rc.m[l], S);
 }
@@ -215,12 +240,7 @@ __device__ __forceinline__ uint32_t pack2(uint32_t a, uint32_t b) { return a | (
 // the returned word.
 template <int L>
 __device__ __forceinline__ uint32_t residue_byte(const Digits& d, int l) {
-  const ResidueConsts& rc = c_res[L];
-  const float S = fmaf(d.f4, rc.c[3][l],
-                       fmaf(d.f3, rc.c[2][l], fmaf(d.f2, rc.c[1][l], fmaf(d.f1, rc.c[0][l], d.f0))));
-  const float q = fmaf(S, rc.inv[l], kMagic) - kMagic;
-  const float r = fmaf(-q, rc.m[l], S);
-  return __float_as_uint(r + kMagic);
+  return __float_as_uint(residue_float<L>(d, l) + kMagic);
 }
 
 // ------------------------------------------------- packed-T operand prep
@@ -354,7 +374,7 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
       const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
       Digits d[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) d[j] = digits_of(blk[j * 16], s1, s2);
+      for (int j = 0; j < 16; ++j) d[j] = digits_of<L>(blk[j * 16], s1, s2);
 #pragma unroll
       for (int l = 0; l < L; ++l) {
         uint32_t b[16];
@@ -370,7 +390,7 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
       const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
       Digits d[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) d[j] = digits_of(blk[j * 16], s1, s2);
+      for (int j = 0; j < 16; ++j) d[j] = digits_of<L>(blk[j * 16], s1, s2);
       *reinterpret_cast<uint4*>(dst) =
           make_uint4(pack4(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pack4(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
                      pack4(d[8].lo, d[9].lo, d[10].lo, d[11].lo),
@@ -438,7 +458,8 @@ __global__ void __launch_bounds__(256) convert_local_kernel(
     __syncthreads();
     Digits d[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) d[j] = digits_of(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r]);
+    for (int j = 0; j < 8; ++j)
+      d[j] = digits_of<L>(tileT[r * kTilePitch + swz_k(8 * kk + j)], s1[r], s2[r]);
     if (BF) {
       uint8_t* dst = res + ((p * 16 + r) * KP + k0 + 8 * kk) * 2;
 #pragma unroll
@@ -603,19 +624,20 @@ __global__ void __launch_bounds__(256) sum_partials_kernel(
 
 // ------------------------------------------------------------- host side
 struct LanePlan {
-  int T = 0, Q = 0, slots = 0, L = 0, KB = 0, tiles_m = 0, tiles_n = 0;
-  DeviceBuffer buf;  // tiles | lane_seg_off | segs | tile_index | mod_slot_off | mod_slots
+  int T = 0, T1 = 0, Q = 0, slots = 0, L = 0, KB = 0, tiles_m = 0, tiles_n = 0;
+  // tiles | lane_seg_off | segs | tile_index | mod_slot_off | mod_slots | tile_index2
+  DeviceBuffer buf;
   int2* tiles = nullptr;
   int* lane_seg_off = nullptr;
   I8Segment* segs = nullptr;
   int* tile_index = nullptr;
+  int* tile_index2 = nullptr;  // fused pair: the GEMM's tiles (t >= T1)
   int* mod_slot_off = nullptr;
   int* mod_slots = nullptr;
 };
 
 struct OzakiStream {
   DeviceBuffer res_a, res_b, part_a, part_b, mu_a, mu_b, partials, rbytes;
-  DeviceBuffer partials2;  // Hs's slabs in the subspace pair (S's CRT still reads `partials`)
   cudaEvent_t fork2 = nullptr, join2 = nullptr;
   // Helper stream forked from the caller's stream: the norm pass of B runs
   // there while A is converted (the conversion leaves HBM bandwidth idle).
@@ -648,6 +670,12 @@ int ensure_consts(DeviceState* dev) {
       for (int j = 0; j < 4; ++j) {
         pj = (pj * 4096) % m;
         rc[L].c[j][l] = (float)pj;  // 2^(12 (j+1)) mod m
+      }
+      uint64_t p14 = 1;
+      for (int j = 0; j < 3; ++j) {
+        p14 = (p14 * 16384) % m;
+        const int64_t sym = p14 > m / 2 ? (int64_t)p14 - (int64_t)m : (int64_t)p14;
+        rc[L].cs[j][l] = (float)sym;  // 2^(14 (j+1)) mod m in (-m/2, m/2]
       }
       rc[L].inv[l] = 1.0f / (float)m;
       rc[L].m[l] = (float)m;
@@ -682,10 +710,14 @@ OzakiStream* ozaki_stream(DeviceState* dev, cudaStream_t s) {
 // Lane schedule: T tiles x Q lanes, each lane a contiguous range of the
 // (modulus, k-block) space, cut into segments at modulus boundaries and at
 // seg_cap k-blocks (INT32 exactness).
+// With `pair` (M == N) the tile list is the SYRK's upper tiles (t < T1,
+// tile_index) followed by all tiles of the GEMM (tile_index2): one launch
+// computes S = A^T A and Hs = A^T B from the same A panels.
 int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int seg_cap,
-                  LanePlan** out, int sub_cap = 0) {
+                  LanePlan** out, int sub_cap = 0, bool pair = false) {
   OzakiDevice& od = g_oz[dev->device];
-  auto key = std::make_tuple(M, N, KB, (L * 4096 + seg_cap) * 64 + sub_cap, syrk ? 1 : 0);
+  auto key = std::make_tuple(M, N, KB, (L * 4096 + seg_cap) * 64 + sub_cap,
+                             (syrk ? 1 : 0) + (pair ? 2 : 0));
   auto itp = od.plans.find(key);
   if (itp != od.plans.end()) {
     *out = itp->second;
@@ -697,13 +729,23 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
   pl->tiles_m = (M + kI8BM - 1) / kI8BM;
   pl->tiles_n = (N + kI8BN - 1) / kI8BN;
   std::vector<int2> tiles;
-  std::vector<int> tile_index(pl->tiles_m * pl->tiles_n, -1);
+  std::vector<int> tile_index(pl->tiles_m * pl->tiles_n, -1), tile_index2;
   for (int tm = 0; tm < pl->tiles_m; ++tm)
     for (int tn = 0; tn < pl->tiles_n; ++tn) {
-      if (syrk && tm * kI8BM > tn * kI8BN + kI8BN - 1) continue;  // strictly lower
+      if ((syrk || pair) && tm * kI8BM > tn * kI8BN + kI8BN - 1) continue;  // strictly lower
       tile_index[tm * pl->tiles_n + tn] = (int)tiles.size();
       tiles.push_back(make_int2(tm, tn));
     }
+  pl->T1 = 0;
+  if (pair) {
+    pl->T1 = (int)tiles.size();
+    tile_index2.assign(pl->tiles_m * pl->tiles_n, -1);
+    for (int tm = 0; tm < pl->tiles_m; ++tm)
+      for (int tn = 0; tn < pl->tiles_n; ++tn) {
+        tile_index2[tm * pl->tiles_n + tn] = (int)tiles.size();
+        tiles.push_back(make_int2(tm, tn));
+      }
+  }
   pl->T = (int)tiles.size();
   pl->Q = std::max(1, dev->num_sms / pl->T);
   const int64_t W = (int64_t)L * KB;
@@ -747,14 +789,18 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
   auto al = [](size_t x) { return (x + 15) / 16 * 16; };
   const size_t s0 = al(tiles.size() * sizeof(int2)), s1 = al(lane_off.size() * sizeof(int)),
                s2 = al(segs.size() * sizeof(I8Segment)), s3 = al(tile_index.size() * sizeof(int)),
-               s4 = al(mod_off.size() * sizeof(int)), s5 = al(mod_slots.size() * sizeof(int) + 4);
+               s4 = al(mod_off.size() * sizeof(int)), s5 = al(mod_slots.size() * sizeof(int) + 4),
+               s6 = al(tile_index2.size() * sizeof(int) + 4);
   int st;
-  if ((st = pl->buf.ensure(s0 + s1 + s2 + s3 + s4 + s5)) != SKGEMM_OK) {
+  if ((st = pl->buf.ensure(s0 + s1 + s2 + s3 + s4 + s5 + s6)) != SKGEMM_OK) {
     delete pl;
     return st;
   }
   uint8_t* b = static_cast<uint8_t*>(pl->buf.ptr);
-  std::vector<uint8_t> host(s0 + s1 + s2 + s3 + s4 + s5, 0);
+  std::vector<uint8_t> host(s0 + s1 + s2 + s3 + s4 + s5 + s6, 0);
+  if (!tile_index2.empty())
+    memcpy(host.data() + s0 + s1 + s2 + s3 + s4 + s5, tile_index2.data(),
+           tile_index2.size() * sizeof(int));
   memcpy(host.data(), tiles.data(), tiles.size() * sizeof(int2));
   memcpy(host.data() + s0, lane_off.data(), lane_off.size() * sizeof(int));
   memcpy(host.data() + s0 + s1, segs.data(), segs.size() * sizeof(I8Segment));
@@ -768,6 +814,7 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
   pl->tile_index = reinterpret_cast<int*>(b + s0 + s1 + s2);
   pl->mod_slot_off = reinterpret_cast<int*>(b + s0 + s1 + s2 + s3);
   pl->mod_slots = reinterpret_cast<int*>(b + s0 + s1 + s2 + s3 + s4);
+  pl->tile_index2 = pair ? reinterpret_cast<int*>(b + s0 + s1 + s2 + s3 + s4 + s5) : nullptr;
   od.plans[key] = pl;
   *out = pl;
   return SKGEMM_OK;
@@ -784,23 +831,24 @@ int make_res_map(CUtensorMap* map, const void* base, int64_t KP, int64_t Rpad, i
 
 template <bool BF>
 int launch_i8_t(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
-                const I8Params& p, int grid, cudaStream_t s) {
+                const CUtensorMap& mB2, const I8Params& p, int grid, cudaStream_t s) {
   static bool attr_done[64] = {false};
   if (!attr_done[dev->device]) {
     SKG_CUDA(cudaFuncSetAttribute(i8_gemm_kernel<BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kI8SmemBytes));
     attr_done[dev->device] = true;
   }
-  i8_gemm_kernel<BF><<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, p);
+  i8_gemm_kernel<BF><<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, mB2, p);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
 
 // INT8 (bf = false) or BF16 (bf = true) residue products.
 int launch_i8(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB, const I8Params& p,
-              int grid, cudaStream_t s, bool bf = false) {
-  return bf ? launch_i8_t<true>(dev, mA, mB, p, grid, s)
-            : launch_i8_t<false>(dev, mA, mB, p, grid, s);
+              int grid, cudaStream_t s, bool bf = false, const CUtensorMap* mB2 = nullptr) {
+  const CUtensorMap& b2 = mB2 ? *mB2 : mB;
+  return bf ? launch_i8_t<true>(dev, mA, mB, b2, p, grid, s)
+            : launch_i8_t<false>(dev, mA, mB, b2, p, grid, s);
 }
 
 int launch_i8_rot(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
@@ -1026,6 +1074,64 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   return SKGEMM_OK;
 }
 
+// Fused subspace pair products: one lane-scheduled launch over S's upper
+// tiles (B = A's residues) and Hs's tiles (B = os->res_b), so each A panel
+// is read once for both; then the two reconstructions from the shared slabs,
+// S's on the helper stream.
+int pair_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M, int64_t KP,
+                 int L, double* S, int64_t lds, double alpha_s, double beta_s, double* Hs,
+                 int64_t ldh, double alpha_h, double gamma_h, cudaStream_t s, bool bf) {
+  int st;
+  const int64_t KPb = KP * (bf ? 2 : 1);
+  const int KB = (int)(KPb / 128);
+  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
+  LanePlan* pl = nullptr;
+  if ((st = get_lane_plan(dev, (int)M, (int)M, KB, L, false,
+                          bf ? kSegKbCapBf16 : kSegKbCapSigned, &pl, bf ? kSubKbCapBf16 : 0,
+                          true)) != SKGEMM_OK)
+    return st;
+  DeviceBuffer& part = os->partials;
+  if ((st = part.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t)))) return st;
+  CUtensorMap mA, mB, mB2;
+  if ((st = make_res_map(&mA, os->res_a.ptr, KPb, RA, L, kI8BM))) return st;
+  if ((st = make_res_map(&mB, os->res_a.ptr, KPb, RA, L, kI8BN))) return st;
+  if ((st = make_res_map(&mB2, os->res_b.ptr, KPb, RA, L, kI8BN))) return st;
+  I8Params p;
+  memset(&p, 0, sizeof(p));
+  p.sched = kSchedLanes;
+  p.is_signed = 1;
+  p.L = L;
+  p.KB = KB;
+  p.M = (int)M;
+  p.N = (int)M;
+  p.T = pl->T;
+  p.T1 = pl->T1;
+  p.Q = pl->Q;
+  p.tiles = pl->tiles;
+  p.lane_seg_off = pl->lane_seg_off;
+  p.segs = pl->segs;
+  p.partials = (int32_t*)part.ptr;
+  p.err = ws->err;
+  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s, bf, &mB2))) return st;
+  SKG_CUDA(cudaEventRecord(os->fork2, s));
+  SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork2, 0));
+  const int64_t n = M * M;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  crt_partials_kernel<<<blocks, 256, 0, os->aux>>>(
+      (int)M, (int)M, L, (const int32_t*)part.ptr, pl->T, pl->tile_index, pl->tiles_n,
+      pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)os->mu_a.ptr, 1, S,
+      lds, alpha_s, beta_s, beta_s == 0.0 ? 1 : 0);
+  const cudaError_t e1 = cudaGetLastError();
+  SKG_CUDA(cudaEventRecord(os->join2, os->aux));
+  if (e1 != cudaSuccess) return cuda_fail(e1, "crt_partials_kernel");
+  crt_partials_kernel<<<blocks, 256, 0, s>>>(
+      (int)M, (int)M, L, (const int32_t*)part.ptr, pl->T, pl->tile_index2, pl->tiles_n,
+      pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)os->mu_b.ptr, 0, Hs,
+      ldh, alpha_h, gamma_h, 0);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
 // Residues of A (packed16, M rows) into os->res_a and, unless Bp is null, of
 // B (packed32, N rows) into os->res_b: norms(A) | norms(B) on the helper
 // stream, convert(A), join, convert(B).
@@ -1110,18 +1216,40 @@ int subspace_impl(int64_t K, int64_t M, const double* Psi, const double* HPsi, d
   OzakiStream* os = ozaki_stream(dev, s);
   const int64_t KP = (K + 127) / 128 * 128;
   const bool bf = is_bf16(opts);
-  if ((st = prep_pair(dev, os, ws, M, M, K, L, Psi, HPsi, s, bf))) return st;
+  if (!os->aux) {
+    SKG_CUDA(cudaStreamCreateWithFlags(&os->aux, cudaStreamNonBlocking));
+    SKG_CUDA(cudaEventCreateWithFlags(&os->fork, cudaEventDisableTiming));
+    SKG_CUDA(cudaEventCreateWithFlags(&os->join, cudaEventDisableTiming));
+  }
   if (!os->fork2) {
     SKG_CUDA(cudaEventCreateWithFlags(&os->fork2, cudaEventDisableTiming));
     SKG_CUDA(cudaEventCreateWithFlags(&os->join2, cudaEventDisableTiming));
   }
-  // S: products on s, reconstruction on the helper stream (overlaps Hs's
-  // products, which write their own slabs); join before returning.
-  if ((st = lanes_product(dev, os, ws, M, M, KP, L, true, &os->res_a, &os->mu_a, S, lds, alpha_s,
-                          beta_s, s, &os->partials, os->aux, bf)))
+  // Two streams (none of these kernels waits on another CTA, so they may
+  // share the machine in any proportion):
+  //   s:   norms(Psi) -> convert(Psi) -- wait(join) -> products(S, Hs) -> CRT(Hs)
+  //   aux: norms(HPsi) -> convert(HPsi) -> [join] -- wait(fork2) -> CRT(S) -> [join2]
+  // HPsi's norm pass and conversion overlap Psi's; one INT8 launch computes
+  // the products of both (pair_product); the two reconstructions overlap.
+  const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
+  SKG_CUDA(cudaEventRecord(os->fork, s));
+  SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork, 0));
+  int st_b = prep_norms<32>(M, K, KP, RA, HPsi, L, os->res_b, os->part_b, os->mu_b, os->aux, bf);
+  if (!st_b)
+    st_b = prep_convert<32>(dev, M, K, KP, RA, HPsi, L, os->res_b, os->mu_b, ws->err, os->aux, bf);
+  SKG_CUDA(cudaEventRecord(os->join, os->aux));  // recorded even when a B step failed
+  if (st_b) {
+    SKG_CUDA(cudaStreamWaitEvent(s, os->join, 0));
+    return st_b;
+  }
+  if ((st = prep_packed<16>(dev, M, K, KP, RA, Psi, L, os->res_a, os->part_a, os->mu_a, ws->err,
+                            s, bf))) {
+    SKG_CUDA(cudaStreamWaitEvent(s, os->join, 0));
     return st;
-  st = lanes_product(dev, os, ws, M, M, KP, L, false, &os->res_b, &os->mu_b, Hs, ldh, alpha_h,
-                     gamma_h, s, &os->partials2, nullptr, bf);
+  }
+  SKG_CUDA(cudaStreamWaitEvent(s, os->join, 0));
+  st = pair_product(dev, os, ws, M, KP, L, S, lds, alpha_s, beta_s, Hs, ldh, alpha_h, gamma_h, s,
+                    bf);
   SKG_CUDA(cudaStreamWaitEvent(s, os->join2, 0));
   if (st) return st;
   report(opts, L, gb, K);
@@ -1135,7 +1263,7 @@ namespace {
 // Scratch of one stream's Ozaki calls, per buffer of OzakiStream.
 struct OzakiNeed {
   size_t res_a = 0, res_b = 0, part_a = 0, part_b = 0, mu_a = 0, mu_b = 0, partials = 0,
-         partials2 = 0, rbytes = 0;
+         rbytes = 0;
   void max_with(const OzakiNeed& o) {
     res_a = std::max(res_a, o.res_a);
     res_b = std::max(res_b, o.res_b);
@@ -1144,11 +1272,10 @@ struct OzakiNeed {
     mu_a = std::max(mu_a, o.mu_a);
     mu_b = std::max(mu_b, o.mu_b);
     partials = std::max(partials, o.partials);
-    partials2 = std::max(partials2, o.partials2);
     rbytes = std::max(rbytes, o.rbytes);
   }
   size_t total() const {
-    return res_a + res_b + part_a + part_b + mu_a + mu_b + partials + partials2 + rbytes;
+    return res_a + res_b + part_a + part_b + mu_a + mu_b + partials + rbytes;
   }
 };
 
@@ -1161,12 +1288,13 @@ size_t norm_part_bytes(int64_t R, int T) {
 // Tiles and segment slots of the lane plan of (M, N, KB, L) (the counting
 // part of get_lane_plan).
 void lane_counts(int num_sms, int M, int N, int KB, int L, bool syrk, int seg_cap, int* T_out,
-                 int* slots_out) {
+                 int* slots_out, bool pair = false) {
   const int tiles_m = (M + kI8BM - 1) / kI8BM, tiles_n = (N + kI8BN - 1) / kI8BN;
   int T = 0;
   for (int tm = 0; tm < tiles_m; ++tm)
     for (int tn = 0; tn < tiles_n; ++tn)
-      if (!(syrk && tm * kI8BM > tn * kI8BN + kI8BN - 1)) ++T;
+      if (!((syrk || pair) && tm * kI8BM > tn * kI8BN + kI8BN - 1)) ++T;
+  if (pair) T += tiles_m * tiles_n;
   int Q = std::max(1, num_sms / T);
   const int64_t W = (int64_t)L * KB;
   if (Q > W) Q = (int)W;
@@ -1185,7 +1313,8 @@ void lane_counts(int num_sms, int M, int N, int KB, int L, bool syrk, int seg_ca
   *slots_out = slots;
 }
 
-OzakiNeed need_lanes(DeviceState* dev, int64_t M, int64_t N, int64_t K, int L, bool syrk) {
+OzakiNeed need_lanes(DeviceState* dev, int64_t M, int64_t N, int64_t K, int L, bool syrk,
+                     bool pair = false) {
   OzakiNeed n;
   const int64_t KP = (K + 127) / 128 * 128;
   const int KB = (int)(KP / 128);
@@ -1200,7 +1329,7 @@ OzakiNeed need_lanes(DeviceState* dev, int64_t M, int64_t N, int64_t K, int L, b
     n.mu_b = (size_t)RB * sizeof(int);
   }
   int T = 0, slots = 0;
-  lane_counts(dev->num_sms, (int)M, (int)N, KB, L, syrk, kSegKbCapSigned, &T, &slots);
+  lane_counts(dev->num_sms, (int)M, (int)N, KB, L, syrk, kSegKbCapSigned, &T, &slots, pair);
   n.partials = (size_t)slots * T * kI8BM * kI8BN * sizeof(int32_t);
   return n;
 }
@@ -1257,9 +1386,8 @@ int ozaki_reserve(DeviceState* dev, cudaStream_t s, int64_t Nd, int64_t nb, int 
   if ((st = choose_L(&o, nb, &Lr, &gb))) return st;
   OzakiNeed n = need_lanes(dev, nb, nb, Nd, Lk, false);
   n.max_with(need_lanes(dev, nb, nb, Nd, Lk, true));
+  n.max_with(need_lanes(dev, nb, nb, Nd, Lk, false, true));  // the fused subspace pair
   n.max_with(need_rot(Nd, nb, Lr));
-  // The subspace pair keeps S's slabs in `partials` while Hs's go to `partials2`.
-  n.partials2 = need_lanes(dev, nb, nb, Nd, Lk, false).partials;
   std::lock_guard<std::mutex> lk(g_oz_mu);
   if ((st = ensure_consts(dev))) return st;
   StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
@@ -1268,7 +1396,7 @@ int ozaki_reserve(DeviceState* dev, cudaStream_t s, int64_t Nd, int64_t nb, int 
   if ((st = os->res_a.ensure(n.res_a)) || (st = os->res_b.ensure(n.res_b)) ||
       (st = os->part_a.ensure(n.part_a)) || (st = os->part_b.ensure(n.part_b)) ||
       (st = os->mu_a.ensure(n.mu_a)) || (st = os->mu_b.ensure(n.mu_b)) ||
-      (st = os->partials.ensure(n.partials)) || (st = os->partials2.ensure(n.partials2)) ||
+      (st = os->partials.ensure(n.partials)) ||
       (st = os->rbytes.ensure(n.rbytes)))
     return st;
   return SKGEMM_OK;
@@ -1292,7 +1420,7 @@ int ozaki_release_stream(DeviceState* dev, cudaStream_t s) {
     cudaEventDestroy(os->join2);
   }
   for (DeviceBuffer* b : {&os->res_a, &os->res_b, &os->part_a, &os->part_b, &os->mu_a, &os->mu_b,
-                          &os->partials, &os->partials2, &os->rbytes})
+                          &os->partials, &os->rbytes})
     b->release();
   delete os;
   m.erase(it);
@@ -1306,7 +1434,7 @@ size_t ozaki_stream_bytes(DeviceState* dev, cudaStream_t s) {
   if (it == g_oz[dev->device].streams.end()) return 0;
   const OzakiStream* os = it->second;
   return os->res_a.bytes + os->res_b.bytes + os->part_a.bytes + os->part_b.bytes +
-         os->mu_a.bytes + os->mu_b.bytes + os->partials.bytes + os->partials2.bytes +
+         os->mu_a.bytes + os->mu_b.bytes + os->partials.bytes +
          os->rbytes.bytes;
 }
 
