@@ -3,9 +3,11 @@
 // blocking host-pointer entry points, TMA descriptor encoding, status strings.
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "skg_common.cuh"
 #include "skg_fp64_types.h"
@@ -537,16 +539,70 @@ SKG_EXPORT int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A, cons
   return ozaki_rot(Nd, nb, A, Q, D, opts, reinterpret_cast<cudaStream_t>(stream));
 }
 
+// Blocking host-pointer rotation, pipelined over row chunks of Psi: chunk c's
+// grid-packed rows go up on one copy stream, its rotation runs on the compute
+// stream into a chunk-local band-packed buffer, and its nb/16 band segments
+// come back (one strided copy) on a second copy stream, so the upload of
+// chunk c + 1 and the download of chunk c - 1 overlap (PCIe is full duplex)
+// and the compute hides under both.
 SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double* Q,
                            double* D) {
   int st = check_rot(Nd, nb);
   if (st) return st;
   if (Nd == 0 || nb == 0) return SKGEMM_OK;
   if (!A || !Q || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
-  HostIO in[2] = {{A, (size_t)Nd * nb * 8}, {Q, (size_t)nb * nb * 8}};
-  return run_host(2, in, D, (size_t)Nd * nb * 8, false, [&](void** d, cudaStream_t s) {
-    return skgemm_drot_dev(Nd, nb, (const double*)d[0], (const double*)d[1], (double*)d[3], s);
-  });
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  std::lock_guard<std::mutex> lk(dev->host_mu);
+  for (cudaStream_t* ps : {&dev->host_stream, &dev->host_h2d, &dev->host_d2h})
+    if (!*ps) SKG_CUDA(cudaStreamCreateWithFlags(ps, cudaStreamNonBlocking));
+  cudaStream_t sc = dev->host_stream, si = dev->host_h2d, so = dev->host_d2h;
+  const size_t bytes = (size_t)Nd * nb * 8;
+  if ((st = dev->stage[0].ensure(bytes)) || (st = dev->stage[1].ensure((size_t)nb * nb * 8)) ||
+      (st = dev->stage[3].ensure(bytes)))
+    return st;
+  double* dA = (double*)dev->stage[0].ptr;
+  double* dQ = (double*)dev->stage[1].ptr;
+  double* dD = (double*)dev->stage[3].ptr;
+  const int64_t panels = Nd / 16;
+  const int C = (int)std::min<int64_t>(8, panels);
+  std::vector<cudaEvent_t> ev(2 * C, nullptr);
+  for (auto& e : ev) SKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  SKG_CUDA(cudaMemcpyAsync(dQ, Q, (size_t)nb * nb * 8, cudaMemcpyHostToDevice, si));
+  for (int c = 0; c < C && st == SKGEMM_OK; ++c) {
+    const int64_t p0 = panels * c / C, p1 = panels * (c + 1) / C;
+    const int64_t g0 = p0 * 16, rows = (p1 - p0) * 16;
+    const size_t off = (size_t)g0 * nb;  // doubles: grid-packed rows and the chunk's output block
+    cudaError_t e = cudaMemcpyAsync(dA + off, A + off, (size_t)rows * nb * 8,
+                                    cudaMemcpyHostToDevice, si);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2 * c], si);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, ev[2 * c], 0);
+    if (e != cudaSuccess) {
+      st = cuda_fail(e, "rotation upload");
+      break;
+    }
+    if ((st = skgemm_drot_dev(rows, nb, dA + off, dQ, dD + off, sc)) != SKGEMM_OK) break;
+    e = cudaEventRecord(ev[2 * c + 1], sc);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(so, ev[2 * c + 1], 0);
+    // Band b of the chunk (rows x 16 doubles at dD + off + b rows 16) goes to
+    // D + b Nd 16 + g0 16.
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(D + g0 * 16, (size_t)Nd * 16 * 8, dD + off, (size_t)rows * 16 * 8,
+                            (size_t)rows * 16 * 8, (size_t)(nb / 16), cudaMemcpyDeviceToHost, so);
+    if (e != cudaSuccess) st = cuda_fail(e, "rotation download");
+  }
+  cudaStreamSynchronize(si);
+  cudaStreamSynchronize(sc);
+  cudaStreamSynchronize(so);
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (st) return st;
+  StreamWorkspace* ws = nullptr;
+  {
+    std::lock_guard<std::mutex> lk2(dev->mu);
+    auto it = dev->ws.find(sc);
+    if (it != dev->ws.end()) ws = it->second;
+  }
+  return consume_device_error(ws, sc);
 }
 
 // ------------------------------------------------------ layout converters

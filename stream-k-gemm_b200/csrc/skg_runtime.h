@@ -55,6 +55,9 @@ struct DeviceState {
   std::mutex host_mu;
   DeviceBuffer stage[4];
   cudaStream_t host_stream = nullptr;
+  // Copy streams of the pipelined host-pointer rotation (H2D and D2H run
+  // concurrently with each other and with the compute on host_stream).
+  cudaStream_t host_h2d = nullptr, host_d2h = nullptr;
 };
 
 // Current device's state (initialises on first use). Returns nullptr and
