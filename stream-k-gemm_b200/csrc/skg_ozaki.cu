@@ -1010,17 +1010,13 @@ int launch_local(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* s
   SKG_DISPATCH_L(L, (launch_local_L<LL, false>(R, K, KP, Rpad, src, panel_stride, ks, res, mu, s)))
 }
 
-// Shared body of the Ozaki GEMM and SYRK: residues of A (packed16) and B
-// (packed16 for SYRK, packed32 for GEMM), lane-scheduled INT8 products,
-// reconstruction.
-// Lane-scheduled INT8 products of prepared residues (A: os->res_a / mu_a,
+// Lane-scheduled INT8 (or BF16) products of prepared residues (A: os->res_a / mu_a,
 // B: resB / muB) and their reconstruction into D: SYRK (upper triangle of
 // the column-major M x M C = alpha A^T A + beta C) or GEMM (row-major
 // D = alpha A B + gamma).
 int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t M, int64_t N,
                   int64_t KP, int L, bool syrk, const DeviceBuffer* resB, const DeviceBuffer* muB,
                   double* D, int64_t ldd, double alpha, double gamma, cudaStream_t s,
-                  DeviceBuffer* slabs = nullptr, cudaStream_t crt_stream = nullptr,
                   bool bf = false) {
   int st;
   // Residue rows are KP * es bytes; a k-block is 128 bytes (128 INT8 or 64
@@ -1030,7 +1026,7 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   const int KB = (int)(KPb / 128);
   const int64_t RA = (M + kI8BN - 1) / kI8BN * kI8BN;
   const int64_t RB = (N + kI8BN - 1) / kI8BN * kI8BN;
-  DeviceBuffer& part = slabs ? *slabs : os->partials;
+  DeviceBuffer& part = os->partials;
   LanePlan* pl = nullptr;
   if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk,
                           bf ? kSegKbCapBf16 : kSegKbCapSigned, &pl,
@@ -1056,21 +1052,12 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   p.partials = (int32_t*)part.ptr;
   p.err = ws->err;
   if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s, bf))) return st;
-  // The reconstruction runs on `crt_stream` (forked after the products) when
-  // given, so that it can overlap the caller's next launch on `s`.
-  cudaStream_t cs = s;
-  if (crt_stream) {
-    SKG_CUDA(cudaEventRecord(os->fork2, s));
-    SKG_CUDA(cudaStreamWaitEvent(crt_stream, os->fork2, 0));
-    cs = crt_stream;
-  }
   const int64_t n = M * N;
-  crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, cs>>>(
+  crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       (int)M, (int)N, L, (const int32_t*)part.ptr, pl->T, pl->tile_index, pl->tiles_n,
       pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)muB->ptr,
       syrk ? 1 : 0, D, ldd, alpha, gamma, (syrk && gamma == 0.0) ? 1 : 0);
   SKG_CUDA(cudaGetLastError());
-  if (crt_stream) SKG_CUDA(cudaEventRecord(os->join2, crt_stream));
   return SKGEMM_OK;
 }
 
@@ -1189,7 +1176,7 @@ int ozaki_lanes(int64_t M, int64_t N, int64_t K, const double* Ap, const double*
   const DeviceBuffer* resB = syrk ? &os->res_a : &os->res_b;
   const DeviceBuffer* muB = syrk ? &os->mu_a : &os->mu_b;
   if ((st = lanes_product(dev, os, ws, M, N, KP, L, syrk, resB, muB, D, ldd, alpha, gamma, s,
-                          nullptr, nullptr, bf)))
+                          bf)))
     return st;
   report(opts, L, gb, K);
   return SKGEMM_OK;
