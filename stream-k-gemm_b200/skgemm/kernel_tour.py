@@ -1,0 +1,92 @@
+"""One launch of every auxiliary kernel of the library on a representative
+workload, for profiling (ncu) and as a quick end-to-end exercise:
+
+    python -m skgemm.kernel_tour
+
+Kernels and workloads (inputs larger than L2 where the kernel is HBM-bound):
+  pack_kernel<16>, pack_kernel<32>   dense 110592 x 512 -> band-packed (453 MB)
+  band_grid_kernel (both ways)       110592 x 512 band <-> grid packed (453 MB)
+  k0_kernel                          GEMM with K = 0 (D = gamma), 4096 x 4096
+  noalloc_fill_kernel                the allocation-free GEMM with K = 0
+  i8_gemm_kernel + sum_partials      the public exact int8 GEMM, 4096 x 4096 x 4096
+  BF16 Ozaki kernels                 GEMM 512 x 512 x 110592, rotation 110592 x 512
+  gen_normal / gen_uniform           a two-request serving trace (inputs made on
+                                     the device from seeds)
+  dmma_peak_kernel, i8_peak_kernel   the peak probes
+Every result is checked for a device-side error; nothing here is timed."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+import skgemm
+
+
+def main() -> None:
+    assert torch.cuda.is_available(), "the kernel tour needs a GPU"
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = torch.Generator(device=dev).manual_seed(5)
+    nd, nb = 110592, 512
+
+    # Layout kernels (HBM-bound).
+    dense = torch.randn(nd, nb, generator=g, dtype=torch.float64, device=dev) / nd ** 0.5
+    band16 = torch.empty(nd * nb, dtype=torch.float64, device=dev)
+    band32 = torch.empty_like(band16)
+    grid = torch.empty_like(band16)
+    back = torch.empty_like(band16)
+    skgemm.pack_dev(nb, nd, dense, 1, nb, 16, band16)
+    skgemm.pack_dev(nb, nd, dense, 1, nb, 32, band32)
+    skgemm.band_to_grid_dev(nd, nb, band16, grid)
+    skgemm.grid_to_band_dev(nd, nb, grid, back)
+    skgemm.stream_status()
+    assert torch.equal(back, band16)
+
+    # K = 0 epilogues.
+    n = 4096
+    d = torch.empty(n * n, dtype=torch.float64, device=dev)
+    a0 = torch.zeros(16, dtype=torch.float64, device=dev)
+    skgemm.dgemm_packed_dev(n, n, 0, a0, a0, d, n, 1.0, 2.5)
+    skgemm.stream_status()
+    assert bool((d == 2.5).all())
+    skgemm.dgemm_packed_dev_noalloc(n, n, 0, a0, a0, d, n, 1.0, -1.5)
+    assert bool((d == -1.5).all())
+
+    # Exact int8 GEMM (lane-scheduled tcgen05 kernel + slab sum).
+    ai = torch.randint(-128, 128, (n, n), generator=g, dtype=torch.int8, device=dev)
+    bi = torch.randint(-128, 128, (n, n), generator=g, dtype=torch.int8, device=dev)
+    ci = torch.empty(n, n, dtype=torch.int32, device=dev)
+    skgemm.igemm_s8_dev(n, n, n, ai, n, bi, n, ci, n)
+    skgemm.stream_status()
+    rows = torch.randint(0, n, (64,), generator=g, device=dev)
+    ref = ai[rows].to(torch.float64) @ bi.to(torch.float64).T
+    assert torch.equal(ci[rows].to(torch.float64), ref)
+
+    # BF16 Ozaki kernels (results equal the INT8 variant's).
+    h = torch.empty(nd * nb, dtype=torch.float64, device=dev)
+    skgemm.pack_dev(nb, nd, torch.randn(nd, nb, generator=g, dtype=torch.float64, device=dev)
+                    / nd ** 0.5, 1, nb, 32, h)
+    hs_b = torch.empty(nb * nb, dtype=torch.float64, device=dev)
+    hs_i = torch.empty_like(hs_b)
+    skgemm.dgemm_packed_dev(nb, nb, nd, band16, h, hs_b, nb, precision=skgemm.PREC_OZAKI_BF16)
+    skgemm.dgemm_packed_dev(nb, nb, nd, band16, h, hs_i, nb, precision=skgemm.PREC_OZAKI_I8)
+    q = torch.rand(nb * nb, generator=g, dtype=torch.float64, device=dev) * 2 - 1
+    skgemm.drot_dev(nd, nb, grid, q, back, precision=skgemm.PREC_OZAKI_BF16)
+    skgemm.stream_status()
+    assert torch.equal(hs_b, hs_i)
+
+    # Serving input generators.
+    trace = [(0.0, 65536, 256, 1), (0.0, 20000, 128, 2)]
+    rows_, _ = skgemm.serve(trace, precision=skgemm.PREC_NATIVE, hbm_budget=20e9,
+                            realtime=False)
+    assert len(rows_) == 2
+
+    # Peak probes.
+    fp64 = skgemm.probe_fp64_peak()
+    i8 = skgemm.probe_i8_peak()
+    print(f"kernel tour ok: FP64 DMMA peak {fp64:.1f} TFLOP/s, INT8 peak {i8:.0f} TOP/s")
+
+
+if __name__ == "__main__":
+    np.seterr(all="ignore")
+    main()
