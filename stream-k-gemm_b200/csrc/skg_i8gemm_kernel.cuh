@@ -29,10 +29,13 @@
 //
 // Schedules:
 //  kSchedLanes   (huge K, small M x N: S = Psi^T Psi, Hs = Psi^T H Psi)
-//     CTA c -> tile t = c % T, lane q = c / T. Lane q owns a contiguous range
-//     of the (modulus, k-block) space; all T CTAs of a lane walk the same
-//     range in lockstep, so each (modulus, k-range) panel of A and B is read
-//     from HBM about once and served to the other tiles from L2. Each
+//     T x Q items (tile t, lane q), persistent: CTA c takes items
+//     c, c + grid, ... with t = item mod T, q = item / T. Lane q owns a
+//     contiguous range of the (modulus, k-block) space; the T CTAs working on
+//     one lane at a time walk the same range in lockstep, so each
+//     (modulus, k-range) panel of A and B is read from HBM about once and
+//     served to the other tiles from L2. The host picks Q so that T x Q items
+//     fill whole waves of the grid (lanes_for). Each
 //     segment (one modulus, <= seg_kb_cap k-blocks) ends in an int32 partial
 //     slab written to `partials[seg_slot][t]` (plan-built slot table).
 //  kSchedUnits   (huge M, small K: Psi' = Psi Q)
@@ -126,27 +129,46 @@ struct I8Item {
   int l, tm, tn, kb0, kb1, slot, t;
 };
 
-__device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cursor,
+// Position of one role in the CTA's item sequence: the persistent item
+// (lanes: (tile, lane) pair; units: work unit) and, for lanes, the segment
+// within that lane.
+struct I8Cursor {
+  int item = 0;
+  int seg = 0;
+};
+
+__device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, I8Cursor& cur,
                                              I8Item& it) {
   if (p.sched == kSchedLanes) {
-    const int q = cta / p.T, t = cta - q * p.T;
-    if (q >= p.Q) return false;
-    const int idx = p.lane_seg_off[q] + cursor;
-    if (idx >= p.lane_seg_off[q + 1]) return false;
-    const I8Segment s = p.segs[idx];
-    const int2 tt = p.tiles[t];
-    it.l = s.l;
-    it.kb0 = s.kb0;
-    it.kb1 = s.kb1;
-    it.slot = s.slot * p.T + t;
-    it.t = t;
-    it.tm = tt.x;
-    it.tn = tt.y;
-    ++cursor;
-    return true;
+    // Persistent over the T x Q items w = cta + j * grid (tile t = w mod T,
+    // lane q = w / T): consecutive CTAs take the tiles of one lane, which
+    // read the same (modulus, k) panels at the same time.
+    const int total = p.T * p.Q;
+    for (;;) {
+      const int w = cta + cur.item * (int)gridDim.x;
+      if (w >= total) return false;
+      const int q = w / p.T, t = w - q * p.T;
+      const int idx = p.lane_seg_off[q] + cur.seg;
+      if (idx >= p.lane_seg_off[q + 1]) {
+        ++cur.item;
+        cur.seg = 0;
+        continue;
+      }
+      const I8Segment s = p.segs[idx];
+      const int2 tt = p.tiles[t];
+      it.l = s.l;
+      it.kb0 = s.kb0;
+      it.kb1 = s.kb1;
+      it.slot = s.slot * p.T + t;
+      it.t = t;
+      it.tm = tt.x;
+      it.tn = tt.y;
+      ++cur.seg;
+      return true;
+    }
   }
-  // kSchedUnits: u = cta + cursor * grid, order (tm, l, tn)
-  const int64_t u = (int64_t)cta + (int64_t)cursor * gridDim.x;
+  // kSchedUnits: u = cta + item * grid, order (tm, l, tn)
+  const int64_t u = (int64_t)cta + (int64_t)cur.item * gridDim.x;
   const int64_t total = (int64_t)p.tiles_m * p.L * p.tiles_n;
   if (u >= total) return false;
   const int tn = (int)(u % p.tiles_n);
@@ -158,7 +180,7 @@ __device__ __forceinline__ bool i8_next_item(const I8Params& p, int cta, int& cu
   it.kb1 = p.KB;
   it.slot = 0;
   it.t = 0;
-  ++cursor;
+  ++cur.item;
   return true;
 }
 
@@ -229,7 +251,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
 
   // Idle CTAs (no work at all) leave before touching TMEM.
   {
-    int cur = 0;
+    I8Cursor cur;
     I8Item probe;
     if (!i8_next_item(p, cta, cur, probe)) return;
   }
@@ -263,7 +285,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
       if (p.T1 > 0) tma_prefetch_desc(&mapB2);
       int stage = 0;
       uint32_t phase = 0;
-      int cur = 0;
+      I8Cursor cur;
       int64_t issued = 0;
       I8Item it;
       while (!*abort_flag && i8_next_item(p, cta, cur, it)) {
@@ -307,7 +329,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
       uint32_t phase = 0;
       int acc = 0;
       uint32_t acc_phase = 0;
-      int cur = 0;
+      I8Cursor cur;
       I8Item it;
       while (!*abort_flag && i8_next_item(p, cta, cur, it)) {
         if (!mbar_wait(&tempty_bar[acc], acc_phase ^ 1, p.err)) {
@@ -357,7 +379,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
     const int c_begin = ((warp - 2) >> 2) * (kI8BN / 64), c_end = c_begin + kI8BN / 64;
     int acc = 0;
     uint32_t acc_phase = 0;
-    int cur = 0;
+    I8Cursor cur;
     I8Item it;
     int32_t run[BF ? 128 : 1];  // BF16 lanes: int32 sums of this slot's sub-segments
 #pragma unroll
@@ -389,7 +411,7 @@ __global__ void __launch_bounds__(kI8Threads, 1)
           if (lane == 0) mbar_arrive(&tempty_bar[acc]);
           released = true;
           I8Item nx;
-          int peek = cur;
+          I8Cursor peek = cur;
           if (!i8_next_item(p, cta, peek, nx) || nx.slot != it.slot) {
 #pragma unroll
             for (int cc = 0; cc < 4; ++cc) {

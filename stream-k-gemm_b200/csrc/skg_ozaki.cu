@@ -707,6 +707,20 @@ OzakiStream* ozaki_stream(DeviceState* dev, cudaStream_t s) {
   return o;
 }
 
+// Lanes per tile for T tiles over a (modulus, k-block) space of W blocks on
+// `sms` persistent CTAs: the T x Q equal items take ceil(T Q / sms) waves of
+// W / Q blocks each, so Q minimises ceil(T Q / sms) / Q; among Q within 2%
+// of the best the smallest (fewer slabs) wins. A lane keeps >= 64 k-blocks.
+int lanes_for(int sms, int T, int64_t W) {
+  const int qmax = (int)std::max<int64_t>(1, std::min<int64_t>(64, W / 64));
+  double best = 1e300;
+  for (int Q = 1; Q <= qmax; ++Q)
+    best = std::min(best, (double)(((int64_t)T * Q + sms - 1) / sms) / Q);
+  for (int Q = 1; Q <= qmax; ++Q)
+    if ((double)(((int64_t)T * Q + sms - 1) / sms) / Q <= best * 1.02) return Q;
+  return 1;
+}
+
 // Lane schedule: T tiles x Q lanes, each lane a contiguous range of the
 // (modulus, k-block) space, cut into segments at modulus boundaries and at
 // seg_cap k-blocks (INT32 exactness).
@@ -747,9 +761,8 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
       }
   }
   pl->T = (int)tiles.size();
-  pl->Q = std::max(1, dev->num_sms / pl->T);
   const int64_t W = (int64_t)L * KB;
-  if (pl->Q > W) pl->Q = (int)W;
+  pl->Q = lanes_for(dev->num_sms, pl->T, W);
   std::vector<int> lane_off(pl->Q + 1, 0);
   std::vector<I8Segment> segs;
   int nslots = 0;
@@ -1051,7 +1064,7 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   p.segs = pl->segs;
   p.partials = (int32_t*)part.ptr;
   p.err = ws->err;
-  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s, bf))) return st;
+  if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s, bf))) return st;
   const int64_t n = M * N;
   crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       (int)M, (int)N, L, (const int32_t*)part.ptr, pl->T, pl->tile_index, pl->tiles_n,
@@ -1099,7 +1112,7 @@ int pair_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t
   p.segs = pl->segs;
   p.partials = (int32_t*)part.ptr;
   p.err = ws->err;
-  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s, bf, &mB2))) return st;
+  if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s, bf, &mB2))) return st;
   SKG_CUDA(cudaEventRecord(os->fork2, s));
   SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork2, 0));
   const int64_t n = M * M;
@@ -1282,9 +1295,8 @@ void lane_counts(int num_sms, int M, int N, int KB, int L, bool syrk, int seg_ca
     for (int tn = 0; tn < tiles_n; ++tn)
       if (!((syrk || pair) && tm * kI8BM > tn * kI8BN + kI8BN - 1)) ++T;
   if (pair) T += tiles_m * tiles_n;
-  int Q = std::max(1, num_sms / T);
   const int64_t W = (int64_t)L * KB;
-  if (Q > W) Q = (int)W;
+  const int Q = lanes_for(num_sms, T, W);
   int slots = 0;
   for (int q = 0; q < Q; ++q) {
     int64_t it = (int64_t)q * W / Q, end = (int64_t)(q + 1) * W / Q;
@@ -1647,7 +1659,7 @@ int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, cons
   p.segs = pl->segs;
   p.partials = (int32_t*)os->partials.ptr;
   p.err = ws->err;
-  if ((st = launch_i8(dev, mA, mB, p, pl->T * pl->Q, s))) return st;
+  if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s))) return st;
   const int64_t n = M * N;
   sum_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       (int)M, (int)N, (const int32_t*)os->partials.ptr, pl->T, pl->tile_index, pl->tiles_n,
