@@ -444,11 +444,13 @@ def run_reference(args):
     sample = (f"each step: the three ops on {ks} of {ND} grid points, reference kernels "
               f"(oracle/_ref) with {cores} OpenMP threads")
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "TFLOP/s",
-            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(tot / len(times) * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "Nd": ND, "nb": NB,
-                       "ops": ["syrk", "gemm", "rotation"], "sample_grid_points": ks},
+                       "ops": ["syrk", "gemm", "rotation"], "sample_grid_points": ks,
+                       "device": f"host CPU, {cores} cores (the arm launched for {args.gpus} "
+                                 f"GPU(s); rank 0 alone runs)"},
             "cpu_baseline": {"value": round(v, 6), "unit": "TFLOP/s", "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": round(v, 6), "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
