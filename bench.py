@@ -149,16 +149,22 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ distributed
-def dist_setup(n):
+def dist_setup(n, backend="nccl"):
+    """One process per GPU (torchrun env): (rank, world, torch.distributed or
+    None). The replicas exchange only their timings; `backend` "gloo" runs
+    the same plumbing on CPU (tests)."""
     import torch
     if n <= 1 or "RANK" not in os.environ:
         return 0, 1, None
     import datetime
     import torch.distributed as dist
     local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                            device_id=torch.device("cuda", local))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return dist.get_rank(), dist.get_world_size(), dist
 
 
@@ -166,7 +172,8 @@ def max_over_ranks(x, dist):
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -175,7 +182,14 @@ def barrier(dist):
     import torch
     if dist is not None:
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+
+
+def job_throughput(flop_per_step, steps, world, max_ms):
+    """Whole-job TFLOP/s of `world` replicas that each ran `steps` steps,
+    timed as the maximum over ranks (weak scaling)."""
+    return flop_per_step * steps * world / (max_ms * 1e-3) / 1e12
 
 
 # ------------------------------------------------------------------ inputs
@@ -275,7 +289,7 @@ def run_gpu(args):
                  "rotation": round(FLOP_ROT / per_op[:, 2].mean() / 1e9, 3)}
 
     line = {
-        "metric": METRIC, "value": round(FLOP_STEP * args.steps * world / (total_ms * 1e-3) / 1e12, 3),
+        "metric": METRIC, "value": round(job_throughput(FLOP_STEP, args.steps, world, total_ms), 3),
         "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -524,7 +538,7 @@ def run_batched(args):
     achieved = flop / (per.mean() * 1e-3) / 1e12
     mem = sum(x.numel() * 8 for k in keep for x in k)
     line = {
-        "metric": METRIC, "value": round(flop * args.steps * world / (total_ms * 1e-3) / 1e12, 3),
+        "metric": METRIC, "value": round(job_throughput(flop, args.steps, world, total_ms), 3),
         "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
