@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--nb", type=int, default=NB, help="states (default 512)")
     ap.add_argument("--workload", default="subspace", choices=["subspace", "batched", "serving"])
     ap.add_argument("--requests", type=int, default=2000, help="serving: trace length")
+    ap.add_argument("--serve-policy", default="smallest", choices=["smallest", "fifo"],
+                    help="serving: admission order (aged least-work-first, or arrival order)")
     ap.add_argument("--instances", type=int, default=64, help="batched: k-point instances")
     ap.add_argument("--max-grid", type=int, default=0,
                     help="batched: cap on grid points per instance (smaller cases for profiling)")
@@ -584,7 +586,9 @@ def run_serving(args):
     clocks = ClockSampler(torch.cuda.current_device())
     barrier(dist)
     clocks.start()
-    rows, o = skgemm.serve(trace, precision=prec, hbm_budget=150e9, realtime=True)
+    policy = skgemm.SERVE_SMALLEST if args.serve_policy == "smallest" else skgemm.SERVE_FIFO
+    rows, o = skgemm.serve(trace, precision=prec, hbm_budget=150e9, realtime=True,
+                           policy=policy, aging_s=0.25)
     barrier(dist)
     clk = clocks.stop()
     lat = np.array([d - a for a, _, d in rows]) * 1e3
@@ -598,6 +602,8 @@ def run_serving(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"serving_poisson200_{args.requests}req",
                    "precision": args.precision, "arrival_rate_per_s": 200.0,
+                   "admission": ("least work first, aged (wait / 0.25 s)"
+                                 if args.serve_policy == "smallest" else "arrival order"),
                    "grid_points": "log-uniform [1e4, 4e5], multiple of 16",
                    "states": "log-uniform [32, 2048], multiple of 16",
                    "hbm_budget_bytes": 150e9, "flop": o.flop,

@@ -323,6 +323,9 @@ typedef struct skgemm_serve_request {
   double done_s;  /* out: completion time (device clock, CUDA events) */
 } skgemm_serve_request_t;
 
+#define SKGEMM_SERVE_FIFO 0
+#define SKGEMM_SERVE_SMALLEST 1
+
 typedef struct skgemm_serve_options {
   int precision;           /* SKGEMM_PREC_NATIVE or SKGEMM_PREC_OZAKI_I8 */
   int slices;              /* Ozaki moduli, 0 = automatic */
@@ -331,6 +334,11 @@ typedef struct skgemm_serve_options {
   int ozaki_streams;       /* Ozaki: concurrent request streams (0 = 2) */
   double max_batch_tflop;  /* native: work cap of one grouped launch (0 = 2 TFLOP) */
   int realtime;            /* 1: release requests at arrival_s (wall clock); 0: all at 0 */
+  int policy;              /* admission order among waiting requests:
+                              SKGEMM_SERVE_FIFO (0, arrival order) or
+                              SKGEMM_SERVE_SMALLEST (least work first, aged) */
+  double aging_s;          /* SMALLEST: a request's work counts / (1 + wait / aging_s),
+                              so a long wait always ends (0 = 0.25 s) */
   /* skgemm_serve_simulate only: throughput model (0 = defaults) */
   double sim_native_tflops, sim_ozaki_tflops, sim_gen_gbs;
   /* out */

@@ -504,9 +504,25 @@ int schedule(skgemm_serve_request_t* io, int n, skgemm_serve_options_t& o, Exec&
         }
       }
     }
-    // Admission, in arrival order, while a slot and a contiguous block are free.
+    // Admission while a slot and a contiguous block are free: the request at
+    // the head of the queue (FIFO), or the waiting request with the least
+    // work, its work discounted by its wait (SMALLEST: small requests stop
+    // queueing behind large ones; the discount bounds any request's wait).
     while (!queue.empty()) {
-      Req& r = R[queue.front()];
+      auto pick = queue.begin();
+      if (o.policy == SKGEMM_SERVE_SMALLEST) {
+        const double tau = o.aging_s > 0 ? o.aging_s : 0.25;
+        double best = 1e300;
+        for (auto it = queue.begin(); it != queue.end(); ++it) {
+          const Req& c = R[*it];
+          const double key = c.flop / (1.0 + std::max(0.0, t - c.arrival) / tau);
+          if (key < best) {
+            best = key;
+            pick = it;
+          }
+        }
+      }
+      Req& r = R[*pick];
       int k = -1;
       if (native) {
         if (inflight >= max_inflight) break;
@@ -516,7 +532,7 @@ int schedule(skgemm_serve_request_t* io, int n, skgemm_serve_options_t& o, Exec&
         if (k < 0) break;
       }
       if (!arena.alloc(r.lay.total, &r.off)) break;
-      queue.pop_front();
+      queue.erase(pick);
       ++inflight;
       r.admit = t;
       if (native) {
@@ -587,6 +603,9 @@ int serve_run(skgemm_serve_request_t* io, int n, skgemm_serve_options_t* opts, b
   skgemm_serve_options_t& o = *opts;
   if (o.precision != SKGEMM_PREC_NATIVE && o.precision != SKGEMM_PREC_OZAKI_I8)
     return fail(SKGEMM_ERR_INVALID_ARG, "serve: unknown precision");
+  if (o.policy != SKGEMM_SERVE_FIFO && o.policy != SKGEMM_SERVE_SMALLEST)
+    return fail(SKGEMM_ERR_INVALID_ARG, "serve: unknown admission policy");
+  if (o.aging_s < 0) return fail(SKGEMM_ERR_INVALID_ARG, "serve: aging_s must be >= 0");
   int64_t max_ng = 0, max_nb = 0;
   for (int i = 0; i < n; ++i) {
     if (io[i].Ng <= 0 || io[i].nb <= 0 || io[i].Ng % 16 || io[i].nb % 16)

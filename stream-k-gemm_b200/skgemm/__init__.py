@@ -92,7 +92,8 @@ class ServeOptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("slices", ctypes.c_int),
                 ("hbm_budget_bytes", ctypes.c_double), ("max_inflight", ctypes.c_int),
                 ("ozaki_streams", ctypes.c_int), ("max_batch_tflop", ctypes.c_double),
-                ("realtime", ctypes.c_int), ("sim_native_tflops", ctypes.c_double),
+                ("realtime", ctypes.c_int), ("policy", ctypes.c_int), ("aging_s", ctypes.c_double),
+                ("sim_native_tflops", ctypes.c_double),
                 ("sim_ozaki_tflops", ctypes.c_double), ("sim_gen_gbs", ctypes.c_double),
                 ("makespan_s", ctypes.c_double), ("flop", ctypes.c_double),
                 ("batches", ctypes.c_int), ("mean_batch_problems", ctypes.c_double),
@@ -447,9 +448,13 @@ def serve_trace(n, rate=200.0, ng_range=(1e4, 4e5), nb_range=(32, 2048), seed=0)
     return [(float(t[i]), int(ng[i]), int(nb[i]), int(seed * 1000003 + i)) for i in range(n)]
 
 
+SERVE_FIFO = 0
+SERVE_SMALLEST = 1  # least work first among waiting requests, aged
+
+
 def serve(trace, precision=PREC_NATIVE, slices=0, hbm_budget=150e9, max_inflight=0,
           ozaki_streams=0, max_batch_tflop=0.0, realtime=True, simulate=False, keep=None,
-          sim=(0.0, 0.0, 0.0)):
+          sim=(0.0, 0.0, 0.0), policy=SERVE_FIFO, aging_s=0.0):
     """Runs (or simulates) a request trace; returns (per-request rows, options).
 
     ``keep``: optional dict index -> dict of host numpy buffers to fill
@@ -472,6 +477,7 @@ def serve(trace, precision=PREC_NATIVE, slices=0, hbm_budget=150e9, max_inflight
     o.precision, o.slices, o.hbm_budget_bytes = precision, slices, hbm_budget
     o.max_inflight, o.ozaki_streams, o.max_batch_tflop = max_inflight, ozaki_streams, max_batch_tflop
     o.realtime = 1 if realtime else 0
+    o.policy, o.aging_s = policy, aging_s
     o.sim_native_tflops, o.sim_ozaki_tflops, o.sim_gen_gbs = sim
     f = lib().skgemm_serve_simulate if simulate else lib().skgemm_serve_run
     _check(f(reqs, n, ctypes.byref(o)))

@@ -66,9 +66,10 @@ def _unpack32(buf, ng, nb):
 
 
 @pytest.mark.parametrize("precision", [NATIVE, OZAKI])
-def test_serve_results_same_alone_and_in_mix(cuda, precision):
+@pytest.mark.parametrize("policy", [skgemm.SERVE_FIFO, skgemm.SERVE_SMALLEST])
+def test_serve_results_same_alone_and_in_mix(cuda, precision, policy):
     trace = small_trace(10, seed=1)
-    mix, rows, o = run(trace, precision, realtime=False)
+    mix, rows, o = run(trace, precision, realtime=False, policy=policy)
     assert o.makespan_s > 0 and o.flop > 0
     if precision == NATIVE:
         assert o.batches >= 2 and o.mean_batch_problems > 2  # requests shared launches
