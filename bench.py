@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--nb", type=int, default=NB, help="states (default 512)")
     ap.add_argument("--workload", default="subspace", choices=["subspace", "batched", "serving"])
     ap.add_argument("--requests", type=int, default=2000, help="serving: trace length")
+    ap.add_argument("--ozaki-streams", type=int, default=2,
+                    help="serving, Ozaki: requests running concurrently (each stream holds "
+                         "scratch for the largest request)")
     ap.add_argument("--serve-policy", default="smallest", choices=["smallest", "fifo"],
                     help="serving: admission order (aged least-work-first, or arrival order)")
     ap.add_argument("--instances", type=int, default=64, help="batched: k-point instances")
@@ -104,9 +107,20 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+        self.gpu = self.smi_id(gpu_index)
         self.proc = None
         self.path = None
+
+    @staticmethod
+    def smi_id(index: int) -> str:
+        """nvidia-smi's id of CUDA device `index`: its PCI bus id, which stays
+        right when CUDA_VISIBLE_DEVICES remaps the ordinals."""
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(index)
+            return f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        except Exception:
+            return str(index)
 
     def start(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -588,7 +602,7 @@ def run_serving(args):
     clocks.start()
     policy = skgemm.SERVE_SMALLEST if args.serve_policy == "smallest" else skgemm.SERVE_FIFO
     rows, o = skgemm.serve(trace, precision=prec, hbm_budget=150e9, realtime=True,
-                           policy=policy, aging_s=0.25)
+                           policy=policy, aging_s=0.25, ozaki_streams=args.ozaki_streams)
     barrier(dist)
     clk = clocks.stop()
     lat = np.array([d - a for a, _, d in rows]) * 1e3
@@ -602,6 +616,7 @@ def run_serving(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"serving_poisson200_{args.requests}req",
                    "precision": args.precision, "arrival_rate_per_s": 200.0,
+                   "ozaki_streams": args.ozaki_streams if args.precision == "ozaki" else None,
                    "admission": ("least work first, aged (wait / 0.25 s)"
                                  if args.serve_policy == "smallest" else "arrival order"),
                    "grid_points": "log-uniform [1e4, 4e5], multiple of 16",
