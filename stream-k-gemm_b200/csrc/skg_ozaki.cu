@@ -371,20 +371,28 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     uint8_t* dst = res + ((g * 16 + r) * KP + kb * 32 + 16 * h) * ES;
     const int64_t lstride = Rpad * KP * ES;
     if (ok && BF) {
-      const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
+      // BF16 rows take 64 bytes per 32-k block: lane h converts k = 8h .. 8h+7
+      // and 16+8h .. 16+8h+7, so that each of its two 16-byte stores and the
+      // other half-lane's together fill one whole 32-byte sector.
+      const double* col = buf + s * kConvTile + r;
       Digits d[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) d[j] = digits_of<L>(blk[j * 16], s1, s2);
+      for (int j = 0; j < 8; ++j) {
+        d[j] = digits_of<L>(col[(8 * h + j) * 16], s1, s2);
+        d[8 + j] = digits_of<L>(col[(16 + 8 * h + j) * 16], s1, s2);
+      }
+      uint8_t* row = res + ((g * 16 + r) * KP + kb * 32) * 2;
 #pragma unroll
       for (int l = 0; l < L; ++l) {
         uint32_t b[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) b[j] = residue_bf16<L>(d[j], l);
-        uint4* d4 = reinterpret_cast<uint4*>(dst + l * lstride);
-        d4[0] = make_uint4(pack2(b[0], b[1]), pack2(b[2], b[3]), pack2(b[4], b[5]),
-                           pack2(b[6], b[7]));
-        d4[1] = make_uint4(pack2(b[8], b[9]), pack2(b[10], b[11]), pack2(b[12], b[13]),
-                           pack2(b[14], b[15]));
+        uint8_t* base = row + l * lstride;
+        *reinterpret_cast<uint4*>(base + 16 * h) =
+            make_uint4(pack2(b[0], b[1]), pack2(b[2], b[3]), pack2(b[4], b[5]), pack2(b[6], b[7]));
+        *reinterpret_cast<uint4*>(base + 32 + 16 * h) =
+            make_uint4(pack2(b[8], b[9]), pack2(b[10], b[11]), pack2(b[12], b[13]),
+                       pack2(b[14], b[15]));
       }
     } else if (ok) {
       const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
