@@ -406,3 +406,25 @@ def test_plan_ozaki_subspace_pairs(cuda):
         assert oracle.rel_frobenius(got[2].cpu().numpy().reshape(M, M),
                                     oracle.dot2_matmul(Psi.T, H2)) <= TOL
     plan.close()
+
+
+def test_plan_bf16_equals_int8(cuda):
+    """A plan with BF16 residues runs the same items as the INT8 plan and
+    gives the same results bit for bit (rotations with nb <= 1024)."""
+    items = mixed_batch(720)
+    p8 = skgemm.Plan([it.item() for it in items], tune=False, precision=skgemm.PREC_OZAKI_I8)
+    p8.run()
+    p8.status()
+    out8 = [it.dD.clone() for it in items]
+    for it in items:
+        it.reset()
+    torch.cuda.synchronize()
+    pb = skgemm.Plan([it.item() for it in items], tune=False, precision=skgemm.PREC_OZAKI_BF16)
+    assert pb.precisions().count(skgemm.PREC_OZAKI_BF16) == p8.config["ozaki_problems"]
+    pb.run()
+    pb.status()
+    for it, o in zip(items, out8):
+        assert torch.equal(it.dD, o)
+        it.check()
+    p8.close()
+    pb.close()
