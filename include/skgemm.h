@@ -59,8 +59,10 @@ extern "C" {
  * FP64 reconstruction. */
 #define SKGEMM_PREC_NATIVE 0
 #define SKGEMM_PREC_OZAKI_I8 1
-/* Batched plans only: per problem, whichever of the two is faster (cost
- * model, confirmed by timing when the plan tunes). */
+/* Per problem, whichever of native and Ozaki INT8 is faster: in batched
+ * plans by the cost model, confirmed by timing when the plan tunes; in the
+ * single-problem _opt entries and skgemm_dsubspace_packed_dev by the cost
+ * model (slices_used_out = 0 reports that native ran). */
 #define SKGEMM_PREC_AUTO 2
 /* SKGEMM_PREC_OZAKI_BF16: the same Ozaki scheme II with the residues stored
  * as BF16 and kind::f16 products (FP32 accumulation over at most 1024

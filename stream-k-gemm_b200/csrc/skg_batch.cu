@@ -484,6 +484,12 @@ double native_estimate(const Fp64Problem& p) {
   return std::min(i128 / 16e12, i64 / (0.9 * 16e12));
 }
 
+}  // namespace
+
+double batch_native_estimate(const Fp64Problem& p) { return native_estimate(p); }
+
+namespace {
+
 // Items run through the Ozaki split: none (native), every one the Ozaki path
 // takes (Ozaki), or those whose estimate is below 0.8 of native (auto).
 std::vector<char> assign_precision(const BatchPlan& P, int precision, int slices) {

@@ -22,6 +22,10 @@ int build_group_tables(const std::vector<Fp64Problem>& probs, int tile, int orde
                        GroupTables* T);
 // Cost-model tile shape (128 or 64) for a set of problems.
 int model_tile(const std::vector<Fp64Problem>& probs);
+// Cost-model device time (s) of `p` on the FP64 Stream-K kernels (issued
+// MACs at the sustained DMMA rate); compared with ozaki_time_estimate to
+// resolve SKGEMM_PREC_AUTO.
+double batch_native_estimate(const Fp64Problem& p);
 
 // A ring of `depth` grouped-launch workspaces for a stream of batches.
 struct GroupRing;

@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "skg_batch.h"
 #include "skg_common.cuh"
 #include "skg_fp64_types.h"
 #include "skg_ozaki.h"
@@ -250,6 +251,25 @@ int check_dims(int64_t a, int64_t b, int64_t c) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+// SKGEMM_PREC_AUTO on one call: the Ozaki split (INT8) when its cost-model
+// time is below 0.8 of the native kernels' (the batched plans' rule), native
+// otherwise. `t_ozaki` < 0 means the split does not take the shape.
+int auto_precision(double t_ozaki, double t_native) {
+  return (t_ozaki >= 0.0 && t_ozaki < 0.8 * t_native) ? SKGEMM_PREC_OZAKI_I8 : SKGEMM_PREC_NATIVE;
+}
+
+// Runs `call` with a copy of `opts` whose precision AUTO is resolved; the
+// caller's options get the outputs (slices_used_out = 0: native ran).
+template <typename Call>
+int run_resolved(skgemm_options_t* opts, int precision, Call call) {
+  skgemm_options_t o = *opts;
+  o.precision = precision;
+  const int st = call(&o);
+  opts->err_bound_out = o.err_bound_out;
+  opts->slices_used_out = precision == SKGEMM_PREC_NATIVE ? 0 : o.slices_used_out;
+  return st;
+}
+
 namespace {
 
 // Blocking host-pointer execution: copies `nin` inputs to device staging
@@ -409,6 +429,14 @@ SKG_EXPORT int skgemm_dgemm_packed_dev_opt(int64_t M, int64_t N, int64_t K, cons
                                            const double* Bp, double* D, int64_t ldd,
                                            double alpha, double gamma, skgemm_options_t* opts,
                                            void* stream) {
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const int pr = auto_precision(
+        ozaki_time_estimate(SKGEMM_OP_GEMM_PACKED, M, N, K, opts->slices),
+        batch_native_estimate(gemm_packed_problem(M, N, K, Ap, Bp, D, ldd, alpha, gamma)));
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return skgemm_dgemm_packed_dev_opt(M, N, K, Ap, Bp, D, ldd, alpha, gamma, o, stream);
+    });
+  }
   if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
     if (opts) {
       opts->err_bound_out = 0.0;
@@ -463,6 +491,14 @@ SKG_EXPORT int skgemm_dsyrk_packed_dev(int64_t K, int64_t M, const double* Ap, d
 SKG_EXPORT int skgemm_dsyrk_packed_dev_opt(int64_t K, int64_t M, const double* Ap, double* C,
                                            int64_t ldc, double alpha, double beta,
                                            skgemm_options_t* opts, void* stream) {
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const int pr = auto_precision(
+        ozaki_time_estimate(SKGEMM_OP_SYRK_PACKED, M, M, K, opts->slices),
+        batch_native_estimate(syrk_problem(K, M, Ap, C, ldc, alpha, beta)));
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return skgemm_dsyrk_packed_dev_opt(K, M, Ap, C, ldc, alpha, beta, o, stream);
+    });
+  }
   if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
     if (opts) {
       opts->err_bound_out = 0.0;
@@ -484,6 +520,15 @@ SKG_EXPORT int skgemm_dsubspace_packed_dev(int64_t K, int64_t M, const double* P
   if (st) return st;
   if (lds < M || ldh < M) return fail(SKGEMM_ERR_INVALID_ARG, "lds or ldh < M");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const double tn = batch_native_estimate(syrk_problem(K, M, Psi, S, lds, 1.0, 0.0)) +
+                      batch_native_estimate(gemm_packed_problem(M, M, K, Psi, HPsi, Hs, ldh,
+                                                                1.0, 0.0));
+    const int pr = auto_precision(ozaki_pair_time_estimate(K, M, opts->slices), tn);
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return skgemm_dsubspace_packed_dev(K, M, Psi, HPsi, S, lds, Hs, ldh, o, stream);
+    });
+  }
   if (!opts || opts->precision == SKGEMM_PREC_NATIVE || K == 0) {
     // Native FP64 (an empty reduction needs no split either).
     if (opts) {
@@ -527,6 +572,13 @@ SKG_EXPORT int skgemm_drot_dev(int64_t Nd, int64_t nb, const double* A, const do
 
 SKG_EXPORT int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A, const double* Q,
                                    double* D, skgemm_options_t* opts, void* stream) {
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const int pr = auto_precision(ozaki_time_estimate(SKGEMM_OP_ROT, Nd, nb, nb, opts->slices),
+                                  batch_native_estimate(rot_problem(Nd, nb, A, Q, D)));
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return skgemm_drot_dev_opt(Nd, nb, A, Q, D, o, stream);
+    });
+  }
   if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
     if (opts) {
       opts->err_bound_out = 0.0;

@@ -1502,6 +1502,7 @@ double ozaki_pair_time_estimate(int64_t K, int64_t M, int slices) {
   if (ts < 0.0 || tg < 0.0) return -1.0;
   skgemm_options_t o;
   memset(&o, 0, sizeof(o));
+  o.precision = SKGEMM_PREC_OZAKI_I8;
   o.slices = slices;
   int L, gb;
   if (choose_L(&o, K, &L, &gb)) return -1.0;

@@ -286,3 +286,55 @@ def test_ozaki_bf16_rot_rejects_large_nb(cuda):
     with pytest.raises(skgemm.SkgemmError) as e:
         skgemm.drot_dev(Nd, nb, A, q, D, precision=BF)
     assert e.value.code == skgemm.ERR_UNSUPPORTED
+
+
+def test_auto_precision_single_calls(cuda):
+    """SKGEMM_PREC_AUTO on the single-problem entries and the subspace pair:
+    a long reduction on 512 states runs through the split (moduli reported),
+    a short one on 64 states runs native (slices_used_out = 0); both agree
+    with the explicit precision's result bit for bit and with Dot2 within
+    1e-13."""
+    AUTO = skgemm.PREC_AUTO
+    for K, M, expect_split in ((65536, 512, True), (3000, 64, False)):
+        Psi = gaussian((K, M), 90 + M, 1.0 / np.sqrt(K))
+        H = gaussian((K, M), 91 + M, 1.0 / np.sqrt(K))
+        P16 = dev(oracle.pack(np.ascontiguousarray(Psi.T), 16))
+        H32 = dev(oracle.pack(np.ascontiguousarray(H.T), 32))
+        D = torch.zeros(M * M, dtype=torch.float64, device="cuda")
+        D_ref = torch.zeros_like(D)
+        o = skgemm.dgemm_packed_dev(M, M, K, P16, H32, D, M, precision=AUTO)
+        explicit = OZ if expect_split else None
+        skgemm.dgemm_packed_dev(M, M, K, P16, H32, D_ref, M, precision=explicit)
+        C = torch.zeros(M * M, dtype=torch.float64, device="cuda")
+        os_ = skgemm.dsyrk_packed_dev(K, M, P16, C, M, precision=AUTO)
+        S = torch.zeros(M * M, dtype=torch.float64, device="cuda")
+        Hs = torch.zeros_like(S)
+        op = skgemm.dsubspace_packed_dev(K, M, P16, H32, S, Hs, precision=AUTO)
+        skgemm.stream_status()
+        assert (o.slices_used_out > 0) == expect_split
+        assert (os_.slices_used_out > 0) == expect_split
+        assert (op.slices_used_out > 0) == expect_split
+        assert torch.equal(D, D_ref)
+        assert torch.equal(Hs, D_ref)
+        rng = np.random.default_rng(M)
+        ii, jj = rng.integers(0, M, 2048), rng.integers(0, M, 2048)
+        ref = oracle.dot2_sampled(Psi.T, H, ii, jj)
+        assert oracle.rel_frobenius(D.cpu().numpy().reshape(M, M)[ii, jj], ref) <= TOL
+
+
+def test_auto_precision_rotation(cuda):
+    """AUTO on the rotation: 64 states (conversion-bound) run native, 512
+    states run the split."""
+    for Nd, nb, expect_split in ((8192, 64, False), (65536, 512, True)):
+        Psi = gaussian((Nd, nb), 7, 1.0 / np.sqrt(Nd))
+        Q = uniform((nb, nb), 8)
+        D = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+        o = skgemm.drot_dev(Nd, nb, dev(oracle.grid_pack(Psi)), dev(Q), D,
+                            precision=skgemm.PREC_AUTO)
+        skgemm.stream_status()
+        assert (o.slices_used_out > 0) == expect_split
+        got = oracle.band_unpack(D.cpu().numpy().reshape(nb // 16, Nd, 16), Nd)
+        rng = np.random.default_rng(Nd)
+        ii, jj = rng.integers(0, Nd, 4096), rng.integers(0, nb, 4096)
+        ref = oracle.dot2_sampled(Psi, Q, ii, jj)
+        assert oracle.rel_frobenius(got[ii, jj], ref) <= TOL
