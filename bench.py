@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--precision", default="native",
                     choices=["native", "ozaki", "ozaki_bf16", "auto"],
                     help="ozaki: INT8 residues; ozaki_bf16: BF16 residues (same results); "
-                         "auto: batched workload only (the plan picks per problem)")
+                         "auto: per call (subspace) or per problem (batched), the faster path")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nd", type=int, default=ND,
@@ -235,12 +235,10 @@ def run_gpu(args):
     import torch
     import skgemm
 
-    if args.precision == "auto":
-        raise SystemExit("--precision auto applies to --workload batched")
     rank, world, dist = dist_setup(args.gpus)
     dev = torch.device("cuda", torch.cuda.current_device())
     prec = {"native": None, "ozaki": skgemm.PREC_OZAKI_I8,
-            "ozaki_bf16": skgemm.PREC_OZAKI_BF16}[args.precision]
+            "ozaki_bf16": skgemm.PREC_OZAKI_BF16, "auto": skgemm.PREC_AUTO}[args.precision]
     band, h32, grid, q = make_inputs(dev)
     S = torch.zeros(NB, NB, dtype=torch.float64, device=dev)
     Hs = torch.zeros_like(S)
