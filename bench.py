@@ -321,7 +321,11 @@ def run_gpu(args):
                      "Ozaki split (i8_gemm_kernel + residue conversion), FP64-equivalent flops",
                      "traffic": read_profile_traffic() if prec is None else None},
         "clocks": clk,
-        "gpu_launches": (3 if prec is None else 16) * args.steps,
+        # Ozaki step (ncu launch list): S+Hs = 2 x (norm partials + row
+        # exponents + conversion) + fused products + 2 reconstructions; the
+        # rotation = norms + exponents + conversion + Q's residues + products
+        # + reconstruction.
+        "gpu_launches": (3 if prec is None else 15) * args.steps,
     }
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, band, h32, grid, q, dist)
