@@ -89,6 +89,14 @@ int skgemm_stream_status(void* stream);
  * TFLOP/s, from a register-resident peak loop; the analogue of the
  * reference's FMOPA peak probe (sme_peak_microbench.cpp:16-61). */
 int skgemm_probe_fp64_peak(double* tflops_out);
+/* Diagnostic of the failure path: enqueues on `stream` one CTA whose bounded
+ * device wait (an mbarrier nothing arrives on) runs out after budget_ms
+ * (0 < budget_ms <= 1000), the same mechanism every kernel wait uses (their
+ * budgets are 4-8 s): the kernel records the timeout in the stream's device
+ * error word and returns, the GPU context stays usable, and the next
+ * skgemm_stream_status(stream) returns SKGEMM_ERR_DEVICE_TIMEOUT (and clears
+ * the word). No counterpart in the reference. */
+int skgemm_diag_expire_wait(double budget_ms, void* stream);
 /* Measured INT8 tensor-core (tcgen05.mma kind::i8, 128x256x32) throughput of
  * the current device, TOP/s; the roofline denominator of the Ozaki path. */
 int skgemm_probe_i8_peak(double* tops_out);

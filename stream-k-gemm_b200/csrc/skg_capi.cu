@@ -361,6 +361,13 @@ SKG_EXPORT int skgemm_stream_release(void* stream) {
   return ozaki_release_stream(dev, s);
 }
 
+SKG_EXPORT int skgemm_diag_expire_wait(double budget_ms, void* stream) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  return expire_wait(dev, budget_ms, reinterpret_cast<cudaStream_t>(stream));
+}
+
 SKG_EXPORT int skgemm_probe_fp64_peak(double* tflops_out) {
   int st;
   DeviceState* dev = current_device(&st);

@@ -81,16 +81,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: returns false (and records the error) when the budget runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err) {
+// Bounded wait: returns false (and records the error) when `budget_ns` of
+// device time or kMbarSpinCap polls run out.
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, uint32_t* err,
+                                             uint64_t budget_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t it = 1; it < kMbarSpinCap; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0 && globaltimer_ns() - t0 > kMbarBudgetNs) break;
+    if ((it & 255u) == 0 && globaltimer_ns() - t0 > budget_ns) break;
   }
   if (err) atomicOr(err, kDevErrMbarTimeout);
   return false;
+}
+// The kernels' wait: the 8 s budget.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err) {
+  return mbar_wait_ns(bar, parity, err, kMbarBudgetNs);
 }
 
 // --------------------------------------------------------------------------

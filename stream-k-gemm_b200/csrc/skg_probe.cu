@@ -29,7 +29,30 @@ __global__ void __launch_bounds__(256) dmma_peak_kernel(int iters, double* sink)
   if (s == 1.0e300) sink[0] = s;  // keeps the loop live; never true
 }
 
+// One thread waits on an mbarrier that nothing arrives on, with the same
+// bounded wait the kernels use (a shorter budget): the wait gives up, the
+// timeout lands in the stream's device error word, the kernel returns.
+__global__ void expire_wait_kernel(uint32_t* err, uint64_t budget_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_wait_ns(&bar, 0, err, budget_ns);  // phase 0 never completes
+  }
+}
+
 }  // namespace
+
+int expire_wait(DeviceState* dev, double budget_ms, cudaStream_t s) {
+  if (!(budget_ms > 0.0 && budget_ms <= 1000.0))
+    return fail(SKGEMM_ERR_INVALID_ARG, "budget_ms must be in (0, 1000]");
+  int st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  expire_wait_kernel<<<1, 32, 0, s>>>(ws->err, (uint64_t)(budget_ms * 1e6));
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
 
 int probe_fp64_peak(DeviceState* dev, double* tflops) {
   if (!tflops) return fail(SKGEMM_ERR_INVALID_ARG, "null output");

@@ -130,6 +130,9 @@ int launch_grid_to_band(int64_t Nd, int64_t nb, const double* src, double* dst,
 
 // Peak probe.
 int probe_fp64_peak(DeviceState* dev, double* tflops);
+// Diagnostic: one bounded device wait that runs out after budget_ms
+// (recorded in stream s's device error word).
+int expire_wait(DeviceState* dev, double budget_ms, cudaStream_t s);
 
 // Device-side failures of one-shot batched launches on `s` (read and cleared;
 // `s` already synchronised).

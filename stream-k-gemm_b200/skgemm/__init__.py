@@ -109,6 +109,7 @@ _lib: Optional[ctypes.CDLL] = None
 _SIGS = {
     "skgemm_stream_status": [_vp],
     "skgemm_probe_fp64_peak": [ctypes.POINTER(ctypes.c_double)],
+    "skgemm_diag_expire_wait": [ctypes.c_double, _vp],
     "skgemm_probe_i8_peak": [ctypes.POINTER(ctypes.c_double)],
     "skgemm_igemm_s8_dev": [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp],
     "skgemm_dgemm": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d],
@@ -341,6 +342,12 @@ def igemm_s8_dev(M, N, K, A, lda, B, ldb, C, ldc, stream=None):
     """Exact int8 x int8 -> int32 GEMM, both operands K-major (device)."""
     _check(lib().skgemm_igemm_s8_dev(M, N, K, _dptr(A), lda, _dptr(B), ldb, _dptr(C), ldc,
                                      _stream(stream)))
+
+
+def diag_expire_wait(budget_ms, stream=None) -> None:
+    """Enqueue one bounded device wait that runs out after budget_ms; the next
+    stream_status(stream) raises SkgemmError(ERR_DEVICE_TIMEOUT)."""
+    _check(lib().skgemm_diag_expire_wait(float(budget_ms), _stream(stream)))
 
 
 def probe_i8_peak() -> float:
