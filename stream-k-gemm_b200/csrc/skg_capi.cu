@@ -458,12 +458,104 @@ SKG_EXPORT int skgemm_dgemm_packed_dev_opt(int64_t M, int64_t N, int64_t K, cons
                            reinterpret_cast<cudaStream_t>(stream));
 }
 
+// ------------------------------------------- K-chunked blocking host calls
+// Long reductions (K >= 2 * kHostChunkK) are uploaded in k-chunks: chunk c + 1
+// goes up on the copy stream while chunk c is multiplied on the compute
+// stream, so the products hide under the upload. A packed-T operand
+// [ceil(R/T)][K][T] gives chunk [k0, k0 + kc) as one strided copy (ceil(R/T)
+// rows of kc*T doubles) into a compact [ceil(R/T)][kc][T] buffer; the chunks
+// sit one after another in the staging buffer, so no chunk overwrites another.
+constexpr int64_t kHostChunkK = 8192;
+constexpr int kHostChunks = 4;
+
+int host_chunks(int64_t K) {
+  return (int)std::min<int64_t>(kHostChunks, std::max<int64_t>(1, K / kHostChunkK));
+}
+
+cudaError_t upload_packed_chunk(double* dst, const double* src, int T, int64_t R, int64_t K,
+                                int64_t k0, int64_t kc, cudaStream_t s) {
+  const int64_t panels = (R + T - 1) / T;
+  return cudaMemcpy2DAsync(dst, (size_t)kc * T * 8, src + k0 * T, (size_t)K * T * 8,
+                           (size_t)kc * T * 8, (size_t)panels, cudaMemcpyHostToDevice, s);
+}
+
+struct HostPipe {
+  DeviceState* dev = nullptr;
+  cudaStream_t sc = nullptr, si = nullptr;
+  std::vector<cudaEvent_t> ev;
+  int init(DeviceState* d, int n) {
+    dev = d;
+    for (cudaStream_t* ps : {&dev->host_stream, &dev->host_h2d, &dev->host_d2h})
+      if (!*ps) SKG_CUDA(cudaStreamCreateWithFlags(ps, cudaStreamNonBlocking));
+    sc = dev->host_stream;
+    si = dev->host_h2d;
+    ev.assign(n, nullptr);
+    for (auto& e : ev) SKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return SKGEMM_OK;
+  }
+  // Waits for both streams, frees the events, reports device-side errors.
+  int finish(int st) {
+    cudaStreamSynchronize(si);
+    cudaStreamSynchronize(sc);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    ev.clear();
+    if (st) return st;
+    StreamWorkspace* ws = nullptr;
+    {
+      std::lock_guard<std::mutex> lk2(dev->mu);
+      auto it = dev->ws.find(sc);
+      if (it != dev->ws.end()) ws = it->second;
+    }
+    return consume_device_error(ws, sc);
+  }
+};
+
 SKG_EXPORT int skgemm_dgemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap,
                                    const double* Bp, double* D, double alpha, double gamma) {
   int st = check_dims(M, N, K);
   if (st) return st;
   if (M == 0 || N == 0) return SKGEMM_OK;
   if (!Ap || !Bp || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  const int C = host_chunks(K);
+  if (C > 1) {
+    // Chunk c: D_c = alpha A_c B_c into its own M x N buffer, then
+    // D = sum_c D_c + gamma (the GEMM contract has no accumulate form).
+    DeviceState* dev = current_device(&st);
+    if (!dev) return st;
+    std::lock_guard<std::mutex> lk(dev->host_mu);
+    HostPipe hp;
+    if ((st = hp.init(dev, C))) return hp.finish(st);
+    const int64_t PA = (M + 15) / 16, PB = (N + 31) / 32;
+    if ((st = dev->stage[0].ensure((size_t)PA * 16 * K * 8)) ||
+        (st = dev->stage[1].ensure((size_t)PB * 32 * K * 8)) ||
+        (st = dev->stage[3].ensure((size_t)C * M * N * 8)))
+      return hp.finish(st);
+    double* dA = (double*)dev->stage[0].ptr;
+    double* dB = (double*)dev->stage[1].ptr;
+    double* dD = (double*)dev->stage[3].ptr;
+    for (int c = 0; c < C && st == SKGEMM_OK; ++c) {
+      const int64_t k0 = K * c / C, kc = K * (c + 1) / C - k0;
+      double* a = dA + PA * 16 * k0;
+      double* b = dB + PB * 32 * k0;
+      cudaError_t e = upload_packed_chunk(a, Ap, 16, M, K, k0, kc, hp.si);
+      if (e == cudaSuccess) e = upload_packed_chunk(b, Bp, 32, N, K, k0, kc, hp.si);
+      if (e == cudaSuccess) e = cudaEventRecord(hp.ev[c], hp.si);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.sc, hp.ev[c], 0);
+      if (e != cudaSuccess) {
+        st = cuda_fail(e, "GEMM chunk upload");
+        break;
+      }
+      st = skgemm_dgemm_packed_dev(M, N, kc, a, b, dD + (size_t)c * M * N, N, alpha, 0.0, hp.sc);
+    }
+    if (!st) st = launch_sum_parts(dD, C, M * N, gamma, dD, hp.sc);
+    if (!st) {
+      const cudaError_t e = cudaMemcpyAsync(D, dD, (size_t)M * N * 8, cudaMemcpyDeviceToHost,
+                                            hp.sc);
+      if (e != cudaSuccess) st = cuda_fail(e, "GEMM download");
+    }
+    return hp.finish(st);
+  }
   HostIO in[2] = {{Ap, (size_t)((M + 15) / 16) * 16 * K * 8},
                   {Bp, (size_t)((N + 31) / 32) * 32 * K * 8}};
   return run_host(2, in, D, (size_t)M * N * 8, false, [&](void** d, cudaStream_t s) {
@@ -554,6 +646,43 @@ SKG_EXPORT int skgemm_dsyrk_packed(int64_t K, int64_t M, const double* Ap, doubl
   if (st) return st;
   if (M == 0) return SKGEMM_OK;
   if (!Ap || !C) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  const int nch = host_chunks(K);
+  if (nch > 1) {
+    // Chunk c accumulates into C through the SYRK contract: beta for the
+    // first chunk, 1 for the others (alpha on every chunk).
+    DeviceState* dev = current_device(&st);
+    if (!dev) return st;
+    std::lock_guard<std::mutex> lk(dev->host_mu);
+    HostPipe hp;
+    if ((st = hp.init(dev, nch))) return hp.finish(st);
+    const int64_t PA = (M + 15) / 16;
+    if ((st = dev->stage[0].ensure((size_t)PA * 16 * K * 8)) ||
+        (st = dev->stage[3].ensure((size_t)M * M * 8)))
+      return hp.finish(st);
+    double* dA = (double*)dev->stage[0].ptr;
+    double* dC = (double*)dev->stage[3].ptr;
+    // C goes up whole: beta != 0 reads it, and its strict lower triangle
+    // returns as the caller passed it.
+    cudaError_t e = cudaMemcpyAsync(dC, C, (size_t)M * M * 8, cudaMemcpyHostToDevice, hp.si);
+    if (e != cudaSuccess) return hp.finish(cuda_fail(e, "SYRK upload"));
+    for (int c = 0; c < nch && st == SKGEMM_OK; ++c) {
+      const int64_t k0 = K * c / nch, kc = K * (c + 1) / nch - k0;
+      double* a = dA + PA * 16 * k0;
+      e = upload_packed_chunk(a, Ap, 16, M, K, k0, kc, hp.si);
+      if (e == cudaSuccess) e = cudaEventRecord(hp.ev[c], hp.si);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.sc, hp.ev[c], 0);
+      if (e != cudaSuccess) {
+        st = cuda_fail(e, "SYRK chunk upload");
+        break;
+      }
+      st = skgemm_dsyrk_packed_dev(kc, M, a, dC, M, alpha, c == 0 ? beta : 1.0, hp.sc);
+    }
+    if (!st) {
+      e = cudaMemcpyAsync(C, dC, (size_t)M * M * 8, cudaMemcpyDeviceToHost, hp.sc);
+      if (e != cudaSuccess) st = cuda_fail(e, "SYRK download");
+    }
+    return hp.finish(st);
+  }
   HostIO in[1] = {{Ap, (size_t)((M + 15) / 16) * 16 * K * 8}};
   // C is copied in and out whole: the strict lower triangle is returned as the
   // caller passed it, and beta != 0 reads the upper triangle.

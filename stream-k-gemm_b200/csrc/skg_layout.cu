@@ -3,6 +3,8 @@
 // band-packed <-> grid-packed transposition of a block of states
 // (sme_pack<double>::band_to_grid_tile / grid_to_band_tile,
 // include/sme_pack.hpp:232-313).
+#include <algorithm>
+
 #include "skg_common.cuh"
 #include "skg_runtime.h"
 
@@ -78,7 +80,29 @@ __global__ void __launch_bounds__(256) band_grid_kernel(int64_t Nd, int64_t nb,
   }
 }
 
+// out[i] = gamma + sum over p < nparts of parts[p * n + i] (out may be parts).
+__global__ void __launch_bounds__(256) sum_parts_kernel(const double* parts, int nparts, int64_t n,
+                                                        double gamma, double* out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double v = parts[i];
+    for (int p = 1; p < nparts; ++p) v += parts[p * n + i];
+    out[i] = v + gamma;
+  }
+}
+
 }  // namespace
+
+// Sum of `nparts` partial outputs of n doubles each plus gamma (the K-chunked
+// host GEMM's combine step).
+int launch_sum_parts(const double* parts, int nparts, int64_t n, double gamma, double* out,
+                     cudaStream_t s) {
+  if (n <= 0) return SKGEMM_OK;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 8);
+  sum_parts_kernel<<<(unsigned)blocks, 256, 0, s>>>(parts, nparts, n, gamma, out);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
 
 int launch_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, int T,
                 double* Xp, cudaStream_t s) {

@@ -121,6 +121,8 @@ int run_k0(int mode, int64_t M, int64_t N, double* D, int64_t ld, double gamma, 
            cudaStream_t s);
 
 // Layout kernels.
+int launch_sum_parts(const double* parts, int nparts, int64_t n, double gamma, double* out,
+                     cudaStream_t s);
 int launch_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, int T,
                 double* Xp, cudaStream_t s);
 int launch_band_to_grid(int64_t Nd, int64_t nb, const double* src, double* dst,

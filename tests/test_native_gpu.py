@@ -293,3 +293,30 @@ def test_config2_subspace_ops_full_size(cuda):
     skgemm.drot_dev(Nd, nb, grid, dQ * 2.0, P2)
     skgemm.stream_status()
     assert np.array_equal(host(P2), 2.0 * P_h)
+
+
+@pytest.mark.parametrize("K", [40000, 16384])
+def test_host_calls_with_chunked_upload(cuda, K):
+    """Host-pointer GEMM and SYRK with long reductions upload their operands
+    in k-chunks and multiply chunk c while chunk c + 1 is copied (GEMM:
+    partial outputs summed at the end; SYRK: beta on the first chunk, 1 after).
+    Results within 1e-13 of Dot2; SYRK's strict lower triangle comes back as
+    passed."""
+    M, N = 200, 136
+    A, B = uniform((M, K), 5), uniform((K, N), 6)
+    D = np.zeros(M * N)
+    skgemm.gemm.compute_packed(M, N, K, oracle.pack(A, 16).ravel(),
+                               oracle.pack(np.ascontiguousarray(B.T), 32).ravel(), D, 1.5, -0.25)
+    ref = oracle.dot2_matmul(A, B, 1.5, -0.25)
+    assert oracle.rel_frobenius(D.reshape(M, N), ref) <= TOL
+    X = gaussian((K, M), 7, 1.0 / np.sqrt(K))
+    C0 = uniform((M, M), 8)                     # column-major C: C0[j, i] = C(i, j)
+    C = C0.ravel().copy()
+    skgemm.sme_syrk.compute(K, M, oracle.pack(X.T, 16).ravel(), C, 2.0, 0.5)
+    Cm = C.reshape(M, M)
+    S = oracle.dot2_matmul(X.T, X)
+    iu = np.triu_indices(M)
+    want = 2.0 * S[iu] + 0.5 * C0[iu[1], iu[0]]
+    assert oracle.rel_frobenius(Cm[iu[1], iu[0]], want) <= TOL
+    il = np.tril_indices(M, -1)
+    assert np.array_equal(Cm[il[1], il[0]], C0[il[1], il[0]])
