@@ -7,6 +7,7 @@ Kernels and workloads (inputs larger than L2 where the kernel is HBM-bound):
   pack_kernel<16>, pack_kernel<32>   dense 110592 x 512 -> band-packed (453 MB)
   band_grid_kernel (both ways)       110592 x 512 band <-> grid packed (453 MB)
   k0_kernel                          GEMM with K = 0 (D = gamma), 4096 x 4096
+  sum_parts_kernel                   the host GEMM's k-chunk combine, 2048 x 2048 x 32768
   noalloc_fill_kernel                the allocation-free GEMM with K = 0
   i8_gemm_kernel + sum_partials      the public exact int8 GEMM, 4096 x 4096 x 4096
   BF16 Ozaki kernels                 GEMM 512 x 512 x 110592, rotation 110592 x 512
@@ -51,6 +52,15 @@ def main() -> None:
     assert bool((d == 2.5).all())
     skgemm.dgemm_packed_dev_noalloc(n, n, 0, a0, a0, d, n, 1.0, -1.5)
     assert bool((d == -1.5).all())
+
+    # Host-pointer GEMM with a long reduction: k-chunked upload, partial
+    # outputs combined by sum_parts_kernel.
+    m2, k2 = 2048, 32768
+    ah = np.random.default_rng(3).uniform(-1, 1, (m2 // 16) * 16 * k2)
+    bh = np.random.default_rng(4).uniform(-1, 1, (m2 // 32) * 32 * k2)
+    dh = np.zeros(m2 * m2)
+    skgemm.gemm.compute_packed(m2, m2, k2, ah, bh, dh, 1.0, 0.5)
+    assert np.isfinite(dh).all()
 
     # Exact int8 GEMM (lane-scheduled tcgen05 kernel + slab sum).
     ai = torch.randint(-128, 128, (n, n), generator=g, dtype=torch.int8, device=dev)
