@@ -71,6 +71,11 @@ struct ResidueConsts {
   float inv[kI8MaxModuli];   // fl(1/m)
   float m[kI8MaxModuli];
   uint32_t mi[kI8MaxModuli];
+  // The same constants as {x, x} pairs for the packed FP32x2 pipe: pc[j] is
+  // cs[j] (L <= kShortDigitsMaxL) or c[j]; pinv = inv, pnm = -m.
+  float2 pc[4][kI8MaxModuli];
+  float2 pinv[kI8MaxModuli];
+  float2 pnm[kI8MaxModuli];
 };
 
 struct CrtConsts {  // for one moduli count L
@@ -211,36 +216,44 @@ __device__ __forceinline__ Digits digits_of(double v, double s1, double s2) {
   return d;
 }
 
-// Symmetric residue of the digits modulo odd kModuli[l] as an exact float
-// (|r| <= 127).
-template <int L>
-__device__ __forceinline__ float residue_float(const Digits& d, int l) {
-  const ResidueConsts& rc = c_res[L];
-  float S;
-  if constexpr (L <= kShortDigitsMaxL)
-    S = fmaf(d.f3, rc.cs[2][l], fmaf(d.f2, rc.cs[1][l], fmaf(d.f1, rc.cs[0][l], d.f0)));
-  else
-    S = fmaf(d.f4, rc.c[3][l],
-             fmaf(d.f3, rc.c[2][l], fmaf(d.f2, rc.c[1][l], fmaf(d.f1, rc.c[0][l], d.f0))));
-  const float q = fmaf(S, rc.inv[l], kMagic) - kMagic;
-  return fmaf(-q, rc.m[l], S);
-}
-
-// BF16 bits of residue l of the digits (l = 0: X mod 256 as a signed byte).
-// Integers of magnitude <= 128 are exact in BF16: the top half of the FP32.
-template <int L>
-__device__ __forceinline__ uint32_t residue_bf16(const Digits& d, int l) {
-  const float r = (l == 0) ? (float)((int)(d.lo << 24) >> 24) : residue_float<L>(d, l);
-  return __float_as_uint(r) >> 16;
+// BF16 bits of residue 0, X mod 256 as a signed byte. Integers of magnitude
+// <= 128 are exact in BF16: the top half of the FP32.
+__device__ __forceinline__ uint32_t low_byte_bf16(const Digits& d) {
+  return __float_as_uint((float)((int)(d.lo << 24) >> 24)) >> 16;
 }
 
 __device__ __forceinline__ uint32_t pack2(uint32_t a, uint32_t b) { return a | (b << 16); }
 
-// Symmetric residue of the digits modulo odd kModuli[l], as the low byte of
-// the returned word.
+// Symmetric residues modulo odd kModuli[l] of two elements a (x) and b (y),
+// as exact floats (|r| <= 127): S = d0 + sum_j d_j c_j, q = rint(S fl(1/m))
+// through the 1.5 2^23 shift, r = S - q m. Computed on the packed FP32x2
+// pipe (__ffma2_rn / __fadd2_rn: each lane rounds to nearest like fmaf), two
+// elements per issue slot — the conversion is issue-bound.
 template <int L>
-__device__ __forceinline__ uint32_t residue_byte(const Digits& d, int l) {
-  return __float_as_uint(residue_float<L>(d, l) + kMagic);
+__device__ __forceinline__ float2 residue_float2(const Digits& a, const Digits& b, int l) {
+  const ResidueConsts& rc = c_res[L];
+  float2 S = __ffma2_rn(make_float2(a.f1, b.f1), rc.pc[0][l], make_float2(a.f0, b.f0));
+  S = __ffma2_rn(make_float2(a.f2, b.f2), rc.pc[1][l], S);
+  S = __ffma2_rn(make_float2(a.f3, b.f3), rc.pc[2][l], S);
+  if constexpr (L > kShortDigitsMaxL) S = __ffma2_rn(make_float2(a.f4, b.f4), rc.pc[3][l], S);
+  const float2 q = __fadd2_rn(__ffma2_rn(S, rc.pinv[l], make_float2(kMagic, kMagic)),
+                              make_float2(-kMagic, -kMagic));
+  return __ffma2_rn(q, rc.pnm[l], S);
+}
+
+// The residues of two elements as the low bytes of the returned words.
+template <int L>
+__device__ __forceinline__ uint2 residue_byte2(const Digits& a, const Digits& b, int l) {
+  const float2 r = __fadd2_rn(residue_float2<L>(a, b, l), make_float2(kMagic, kMagic));
+  return make_uint2(__float_as_uint(r.x), __float_as_uint(r.y));
+}
+
+// BF16 bits of the residues l >= 1 of two elements, packed into one word (a
+// in the low half): the top halves of the two FP32 residues.
+template <int L>
+__device__ __forceinline__ uint32_t residue_bf16x2(const Digits& a, const Digits& b, int l) {
+  const float2 r = residue_float2<L>(a, b, l);
+  return __byte_perm(__float_as_uint(r.x), __float_as_uint(r.y), 0x7632);
 }
 
 // ------------------------------------------------- packed-T operand prep
@@ -294,12 +307,14 @@ __global__ void row_exponents_kernel(int64_t R, int64_t Rpad, int C, const doubl
 // rows x 32 k (group g = 16-row group, kb = 32-k block, g-major): a TMA box
 // {16 rows, 32 k} of the operand lands as [32 k][16 rows] doubles in one of
 // the warp's three 4 KB stages (zero-filled past K and past the operand's
-// panels), the tile two ahead already in flight. Lane (r = lane % 16,
-// h = lane / 16) converts k = 16 h .. 16 h + 15 of row r: its shared-memory
-// reads are conflict-free (16 consecutive rows per k) and each residue
-// leaves as one 16-byte store, the warp covering 16 rows x 32 bytes (whole
-// sectors). No CTA-wide barrier. Row exponents mu[row] are read from the
-// exponent pass.
+// panels), the tile two ahead already in flight. INT8: lanes 2r and 2r + 1
+// convert k = 0 .. 15 and 16 .. 31 of row r, so that each residue leaves as
+// one 16-byte store per lane whose quarter-warp phases (8 lanes) fill the
+// whole 32-byte sectors of 4 rows (8 rows of half sectors in lane order
+// r + 16 h took twice the L1 store wavefronts); the stage is 128B-swizzled so
+// that the two k-rows a half-warp reads fall on disjoint banks. BF16 (64-byte
+// rows): lane r + 16 h, unswizzled stage. No CTA-wide barrier. Row exponents
+// mu[row] are read from the exponent pass.
 constexpr int kConvStages = 3;
 constexpr int kConvWarps = 8;
 constexpr int kConvTile = 16 * 32;  // doubles per warp tile
@@ -353,7 +368,7 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     if (lane == 0 && st < nmine) issue(gi, ki, st);
     advance(gi, ki);
   }
-  const int r = lane & 15, h = lane >> 4;
+  const int r = BF ? (lane & 15) : (lane >> 1), h = BF ? (lane >> 4) : (lane & 1);
   double s1 = 1.0, s2 = 1.0;
   int64_t cur_g = -1;
   uint32_t phase = 0;  // bit s: parity of stage s's next completion
@@ -384,33 +399,46 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
       uint8_t* row = res + ((g * 16 + r) * KP + kb * 32) * 2;
 #pragma unroll
       for (int l = 0; l < L; ++l) {
-        uint32_t b[16];
+        uint32_t w[8];  // w[i]: elements 2i, 2i + 1
 #pragma unroll
-        for (int j = 0; j < 16; ++j) b[j] = residue_bf16<L>(d[j], l);
+        for (int i = 0; i < 8; ++i)
+          w[i] = l == 0 ? pack2(low_byte_bf16(d[2 * i]), low_byte_bf16(d[2 * i + 1]))
+                        : residue_bf16x2<L>(d[2 * i], d[2 * i + 1], l);
         uint8_t* base = row + l * lstride;
-        *reinterpret_cast<uint4*>(base + 16 * h) =
-            make_uint4(pack2(b[0], b[1]), pack2(b[2], b[3]), pack2(b[4], b[5]), pack2(b[6], b[7]));
-        *reinterpret_cast<uint4*>(base + 32 + 16 * h) =
-            make_uint4(pack2(b[8], b[9]), pack2(b[10], b[11]), pack2(b[12], b[13]),
-                       pack2(b[14], b[15]));
+        *reinterpret_cast<uint4*>(base + 16 * h) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(base + 32 + 16 * h) = make_uint4(w[4], w[5], w[6], w[7]);
       }
     } else if (ok) {
-      const double* blk = buf + s * kConvTile + (16 * h) * 16 + r;
+      // Swizzled stage: 16-byte chunk c of k-row k at c ^ (k % 8). At step j
+      // lane (r, h) reads k = 16 h + (j ^ 4 h), whose chunk (r / 2) ^ (j % 8)
+      // ^ 4 h differs from the other half-lane's in bit 2, so a half-warp
+      // touches 8 distinct chunks (all 32 banks once). d[j] then holds
+      // k = 16 h + (j ^ 4 h): for h = 1 the packed words are in the order
+      // 1, 0, 3, 2, and put() swaps them back.
+      const double* stage = buf + s * kConvTile;
+      const int z = 320 * h | (((r >> 1) ^ (4 * h)) << 1) | (r & 1);
       Digits d[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) d[j] = digits_of<L>(blk[j * 16], s1, s2);
-      *reinterpret_cast<uint4*>(dst) =
-          make_uint4(pack4(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pack4(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
-                     pack4(d[8].lo, d[9].lo, d[10].lo, d[11].lo),
-                     pack4(d[12].lo, d[13].lo, d[14].lo, d[15].lo));
+      for (int j = 0; j < 16; ++j)
+        d[j] = digits_of<L>(stage[((j << 4) | ((j & 7) << 1)) ^ z], s1, s2);
+      auto put = [&](uint8_t* p, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3) {
+        *reinterpret_cast<uint4*>(p) =
+            h ? make_uint4(w1, w0, w3, w2) : make_uint4(w0, w1, w2, w3);
+      };
+      put(dst, pack4(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pack4(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
+          pack4(d[8].lo, d[9].lo, d[10].lo, d[11].lo),
+          pack4(d[12].lo, d[13].lo, d[14].lo, d[15].lo));
 #pragma unroll
       for (int l = 1; l < L; ++l) {
         uint32_t b[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) b[j] = residue_byte<L>(d[j], l);
-        *reinterpret_cast<uint4*>(dst + l * lstride) =
-            make_uint4(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]),
-                       pack4(b[8], b[9], b[10], b[11]), pack4(b[12], b[13], b[14], b[15]));
+        for (int j = 0; j < 16; j += 2) {
+          const uint2 v = residue_byte2<L>(d[j], d[j + 1], l);
+          b[j] = v.x;
+          b[j + 1] = v.y;
+        }
+        put(dst + l * lstride, pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]),
+            pack4(b[8], b[9], b[10], b[11]), pack4(b[12], b[13], b[14], b[15]));
       }
     } else {
 #pragma unroll
@@ -472,11 +500,13 @@ __global__ void __launch_bounds__(256) convert_local_kernel(
       uint8_t* dst = res + ((p * 16 + r) * KP + k0 + 8 * kk) * 2;
 #pragma unroll
       for (int l = 0; l < L; ++l) {
-        uint32_t b[8];
+        uint32_t w[4];  // w[i]: elements 2i, 2i + 1
 #pragma unroll
-        for (int j = 0; j < 8; ++j) b[j] = residue_bf16<L>(d[j], l);
+        for (int i = 0; i < 4; ++i)
+          w[i] = l == 0 ? pack2(low_byte_bf16(d[2 * i]), low_byte_bf16(d[2 * i + 1]))
+                        : residue_bf16x2<L>(d[2 * i], d[2 * i + 1], l);
         *reinterpret_cast<uint4*>(dst + (int64_t)l * Rpad * KP * 2) =
-            make_uint4(pack2(b[0], b[1]), pack2(b[2], b[3]), pack2(b[4], b[5]), pack2(b[6], b[7]));
+            make_uint4(w[0], w[1], w[2], w[3]);
       }
       continue;
     }
@@ -487,7 +517,11 @@ __global__ void __launch_bounds__(256) convert_local_kernel(
     for (int l = 1; l < L; ++l) {
       uint32_t b[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) b[j] = residue_byte<L>(d[j], l);
+      for (int j = 0; j < 8; j += 2) {
+        const uint2 v = residue_byte2<L>(d[j], d[j + 1], l);
+        b[j] = v.x;
+        b[j + 1] = v.y;
+      }
       *reinterpret_cast<uint2*>(dst + (int64_t)l * Rpad * KP) =
           make_uint2(pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]));
     }
@@ -688,6 +722,12 @@ int ensure_consts(DeviceState* dev) {
       rc[L].inv[l] = 1.0f / (float)m;
       rc[L].m[l] = (float)m;
       rc[L].mi[l] = (uint32_t)m;
+      for (int j = 0; j < 4; ++j) {
+        const float c = L <= kShortDigitsMaxL ? (j < 3 ? rc[L].cs[j][l] : 0.0f) : rc[L].c[j][l];
+        rc[L].pc[j][l] = make_float2(c, c);
+      }
+      rc[L].pinv[l] = make_float2(rc[L].inv[l], rc[L].inv[l]);
+      rc[L].pnm[l] = make_float2(-rc[L].m[l], -rc[L].m[l]);
     }
   }
   for (int l = 0; l < kI8MaxModuli; ++l) {
@@ -993,7 +1033,7 @@ int prep_convert(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpa
   const uint32_t box[3] = {16, 32, 1};
   int st;
   if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                         CU_TENSOR_MAP_SWIZZLE_NONE)))
+                         bf ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B)))
     return st;
   const int* mp = (const int*)mu.ptr;
   uint8_t* rp = (uint8_t*)res.ptr;
