@@ -206,6 +206,19 @@ int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A_gridpacked,
                         const double* Q_rowmajor, double* D_bandpacked,
                         skgemm_options_t* opts, void* stream);
 
+/* The rotation on band-packed Psi, A_band[(b/16)*Nd*16 + g*16 + b%16] (the
+ * layout SYRK and GEMM read), so a CheFSI step keeps one copy of Psi: the
+ * band -> grid transposition that skgemm_drot_dev's input needs
+ * (sme_pack<double>::band_to_grid_tile, include/sme_pack.hpp:232-249) is
+ * folded into the operand loads. Output and options as skgemm_drot_dev /
+ * skgemm_drot_dev_opt, and equal to them on the grid-packed copy, bit for
+ * bit. Nd and nb multiples of 16. */
+int skgemm_drot_band_dev(int64_t Nd, int64_t nb, const double* A_bandpacked,
+                         const double* Q_rowmajor, double* D_bandpacked, void* stream);
+int skgemm_drot_band_dev_opt(int64_t Nd, int64_t nb, const double* A_bandpacked,
+                             const double* Q_rowmajor, double* D_bandpacked,
+                             skgemm_options_t* opts, void* stream);
+
 /* ------------------------------------------------------ layout converters */
 /* Device-side packing, the B200 counterpart of gemm<double>::pack_A / pack_B
  * (gemm_opt.cpp:342-371): strided dense X(r, k) = X[r*sr + k*sk] ->
@@ -213,6 +226,21 @@ int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A_gridpacked,
  * r >= R. */
 int skgemm_pack_dev(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk,
                     int T, double* X_packed, void* stream);
+/* The inverse: packed-T panels -> strided dense X(r, k) = X[r*sr + k*sk] for
+ * r < R (sme_pack<double>::unpack_c16 / unpack_r16 generalised,
+ * include/sme_pack.hpp:109-156). */
+int skgemm_unpack_dev(int64_t R, int64_t K, const double* X_packed, int T, double* X,
+                      int64_t sr, int64_t sk, void* stream);
+/* The reference's C converters linalg_pack_c16_f64 / linalg_pack_r16_f64 /
+ * linalg_unpack_c16_f64 / linalg_unpack_r16_f64 (include/sme_pack.hpp:
+ * 319-329) on device pointers: column-major [Nd, nb] (src[g + b*Nd]; the
+ * row-major [nb, Nd] of the r16 names is the same bytes) <-> grid-packed
+ * [Nd/16][nb][16]. Nd must be a multiple of 16 (the reference drops the
+ * remainder rows; these return SKGEMM_ERR_INVALID_ARG). */
+int skgemm_pack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, void* stream);
+int skgemm_pack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, void* stream);
+int skgemm_unpack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, void* stream);
+int skgemm_unpack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, void* stream);
 /* Band-packed <-> grid-packed conversion of an Nd x nb block of states
  * (sme_pack<double>::band_to_grid_tile / grid_to_band_tile,
  * include/sme_pack.hpp:232-313). */

@@ -227,9 +227,10 @@ Fp64Problem syrk_problem(int64_t K, int64_t M, const double* Ap, double* C, int6
   return p;
 }
 
-Fp64Problem rot_problem(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D) {
+Fp64Problem rot_problem(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
+                        bool a_band) {
   Fp64Problem p;
-  p.a = {A, kOpPacked16, Nd, 0};
+  p.a = {A, a_band ? kOpBandK : kOpPacked16, Nd, 0};
   p.b = {Q, kOpDense, nb, nb};
   p.M = Nd;
   p.N = nb;
@@ -727,6 +728,42 @@ SKG_EXPORT int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A, cons
   return ozaki_rot(Nd, nb, A, Q, D, opts, reinterpret_cast<cudaStream_t>(stream));
 }
 
+// The rotation reading band-packed Psi ([nb/16][Nd][16], the layout of SYRK's
+// and GEMM's A): the band -> grid transposition of the grid-packed entry's
+// input (sme_pack<double>::band_to_grid_tile, include/sme_pack.hpp:232-249)
+// folded into the operand loads (FP64: K-major TMA boxes; Ozaki: the
+// residue conversion's reads). Results equal skgemm_drot_dev /
+// skgemm_drot_dev_opt on the grid-packed copy, bit for bit.
+SKG_EXPORT int skgemm_drot_band_dev(int64_t Nd, int64_t nb, const double* A_band,
+                                    const double* Q, double* D, void* stream) {
+  int st = check_rot(Nd, nb);
+  if (st) return st;
+  return run_native(rot_problem(Nd, nb, A_band, Q, D, true),
+                    reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_drot_band_dev_opt(int64_t Nd, int64_t nb, const double* A_band,
+                                        const double* Q, double* D, skgemm_options_t* opts,
+                                        void* stream) {
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const int pr = auto_precision(ozaki_time_estimate(SKGEMM_OP_ROT, Nd, nb, nb, opts->slices),
+                                  batch_native_estimate(rot_problem(Nd, nb, A_band, Q, D)));
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return skgemm_drot_band_dev_opt(Nd, nb, A_band, Q, D, o, stream);
+    });
+  }
+  if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
+    if (opts) {
+      opts->err_bound_out = 0.0;
+      opts->slices_used_out = 0;
+    }
+    return skgemm_drot_band_dev(Nd, nb, A_band, Q, D, stream);
+  }
+  int st = check_rot(Nd, nb);
+  if (st) return st;
+  return ozaki_rot(Nd, nb, A_band, Q, D, opts, reinterpret_cast<cudaStream_t>(stream), true);
+}
+
 // Blocking host-pointer rotation, pipelined over row chunks of Psi: chunk c's
 // grid-packed rows go up on one copy stream, its rotation runs on the compute
 // stream into a chunk-local band-packed buffer, and its nb/16 band segments
@@ -797,6 +834,44 @@ SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double
 SKG_EXPORT int skgemm_pack_dev(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk,
                                int T, double* Xp, void* stream) {
   return launch_pack(R, K, X, sr, sk, T, Xp, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_unpack_dev(int64_t R, int64_t K, const double* X_packed, int T, double* X,
+                                 int64_t sr, int64_t sk, void* stream) {
+  return launch_unpack(R, K, X_packed, T, X, sr, sk, reinterpret_cast<cudaStream_t>(stream));
+}
+
+// The reference's extern "C" converters (include/sme_pack.hpp:319-329): grid
+// g, band b; column-major [Nd, nb] and row-major [nb, Nd] are the same bytes
+// src[g + b*Nd], and the packed side is grid-packed [Nd/16][nb][16].
+namespace {
+int c16_check(int64_t Nd, int64_t nb) {
+  if (Nd < 0 || nb < 0 || Nd % 16)
+    return skg::fail(SKGEMM_ERR_INVALID_ARG, "grid packing needs Nd >= 0 a multiple of 16");
+  return SKGEMM_OK;
+}
+}  // namespace
+
+SKG_EXPORT int skgemm_pack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
+                                   void* stream) {
+  if (int st = c16_check(Nd, nb)) return st;
+  return launch_pack(Nd, nb, src, 1, Nd, 16, dst, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_pack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
+                                   void* stream) {
+  return skgemm_pack_c16_dev(Nd, nb, src, dst, stream);
+}
+
+SKG_EXPORT int skgemm_unpack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
+                                     void* stream) {
+  if (int st = c16_check(Nd, nb)) return st;
+  return launch_unpack(Nd, nb, src, 16, dst, 1, Nd, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_unpack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
+                                     void* stream) {
+  return skgemm_unpack_c16_dev(Nd, nb, src, dst, stream);
 }
 
 SKG_EXPORT int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src, double* dst,

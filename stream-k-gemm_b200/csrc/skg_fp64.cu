@@ -25,6 +25,13 @@ int make_operand_map(CUtensorMap* map, const Fp64Operand& op, int64_t K, int row
     uint32_t box[3] = {16, (uint32_t)kBK, (uint32_t)(rows_per_tile / 32)};
     return encode_tiled(map, 3, op.ptr, dims, strides, box, dt, sw);
   }
+  if (op.kind == kOpBandK) {
+    if (K % 16) return fail(SKGEMM_ERR_INVALID_ARG, "K-major operand needs K a multiple of 16");
+    uint64_t dims[3] = {16, (uint64_t)op.rows, (uint64_t)(K / 16)};
+    uint64_t strides[2] = {16 * 8, (uint64_t)op.rows * 16 * 8};
+    uint32_t box[3] = {16, (uint32_t)rows_per_tile, 1};
+    return encode_tiled(map, 3, op.ptr, dims, strides, box, dt, sw);
+  }
   if (op.kind == kOpDense) {
     if (op.ld < op.rows || ((op.ld * 8) % 16) != 0)
       return fail(SKGEMM_ERR_INVALID_ARG, "dense operand leading dimension must be even and >= rows");
@@ -76,12 +83,12 @@ int single_tile(DeviceState* dev, const Fp64Problem& prob) {
   return (i64 == i128 && t128 >= 4.0 * dev->num_sms) ? 64 : 128;
 }
 
-// CTAs per SM of the single-problem kernel of `tile` (its shared-memory
-// attribute set once per device).
+// CTAs per SM of the single-problem kernel of `tile` and A layout (its
+// shared-memory attribute set once per device).
 template <class TS>
-int single_setup(int device, const void* kernel, int* per_sm) {
-  static int occ[2][64] = {};
-  int& o = occ[TS::BM == 64 ? 1 : 0][device];
+int single_setup(int device, const void* kernel, bool akm, int* per_sm) {
+  static int occ[2][2][64] = {};
+  int& o = occ[TS::BM == 64 ? 1 : 0][akm ? 1 : 0][device];
   if (!o) {
     SKG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TS::kSmem));
@@ -118,11 +125,16 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
   }
   if (tile == 0) tile = single_tile(dev, prob);
   if (tile != 128 && tile != 64) return fail(SKGEMM_ERR_INVALID_ARG, "tile must be 128 or 64");
-  const void* kernel = tile == 64 ? (const void*)fp64_streamk_kernel64
-                                  : (const void*)fp64_streamk_kernel;
+  const bool akm = prob.a.kind == kOpBandK;
+  if (prob.b.kind == kOpBandK || (akm && prob.b.kind == kOpPacked32))
+    return fail(SKGEMM_ERR_INVALID_ARG, "operand layouts not supported together");
+  const void* kernel = tile == 64 ? (akm ? (const void*)fp64_streamk_kernel64_ak
+                                         : (const void*)fp64_streamk_kernel64)
+                                  : (akm ? (const void*)fp64_streamk_kernel_ak
+                                         : (const void*)fp64_streamk_kernel);
   int per_sm = 1, st = SKGEMM_OK;
-  if ((st = tile == 64 ? single_setup<Tile64>(dev->device, kernel, &per_sm)
-                       : single_setup<Tile128>(dev->device, kernel, &per_sm)))
+  if ((st = tile == 64 ? single_setup<Tile64>(dev->device, kernel, akm, &per_sm)
+                       : single_setup<Tile128>(dev->device, kernel, akm, &per_sm)))
     return st;
   Schedule sc = make_schedule(dev, prob, tile, per_sm);
   if ((int64_t)sc.num_tiles * sc.ipt > ((int64_t)1 << 40))
@@ -173,9 +185,11 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (tile == 64)
-    SKG_CUDA(cudaLaunchKernelEx(&cfg, fp64_streamk_kernel64, mapA, mapB, p));
+    SKG_CUDA(cudaLaunchKernelEx(&cfg, akm ? fp64_streamk_kernel64_ak : fp64_streamk_kernel64,
+                                mapA, mapB, p));
   else
-    SKG_CUDA(cudaLaunchKernelEx(&cfg, fp64_streamk_kernel, mapA, mapB, p));
+    SKG_CUDA(cudaLaunchKernelEx(&cfg, akm ? fp64_streamk_kernel_ak : fp64_streamk_kernel, mapA,
+                                mapB, p));
   return SKGEMM_OK;
 }
 

@@ -70,6 +70,8 @@ __device__ __forceinline__ void load_operand(int kind, const CUtensorMap* map, u
                                              int k0) {
   if (kind == kOpPacked16) {
     tma_load_3d(dst, map, bar, 0, k0, tile_idx * (rows_per_tile / 16));
+  } else if (kind == kOpBandK) {
+    tma_load_3d(dst, map, bar, 0, tile_idx * rows_per_tile, k0 / 16);
   } else if (kind == kOpPacked32) {
     const int per = rows_per_tile / 32;
     tma_load_3d(dst, map, bar, 0, k0, tile_idx * per);
@@ -190,7 +192,7 @@ __device__ __forceinline__ Seg locate_seg(const Sched& S, int64_t it, int64_t it
   return sg;
 }
 
-template <class TS, class Sched>
+template <class TS, bool AKM = false, class Sched>
 __device__ __forceinline__ void streamk_body(const Sched& S) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -265,6 +267,16 @@ __device__ __forceinline__ void streamk_body(const Sched& S) {
   // unit g is XOR-swizzled with the row index (TMA SWIZZLE_128B).
   const uint32_t off_r0 = (2 * t) * 128 + ((g ^ (2 * t)) << 4);
   const uint32_t off_r1 = (2 * t + 1) * 128 + ((g ^ (2 * t + 1)) << 4);
+  // K-major A (AKM): output row r holds its 16 k in one 128-byte row, the
+  // 16-byte unit u at u ^ (r mod 8). MMA rows g and g + 8 are fed from tile
+  // rows q(g) and 8 + q(g), q(g) = 4 (g % 2) + g / 2 (the epilogue stores
+  // them there): the two g of a quarter-warp then differ in bit 2 of the
+  // swizzle, so its 16-byte loads of unit 4s + t (k = 8s + 2t, 8s + 2t + 1)
+  // hit 8 distinct units (conflict-free). Each load holds (a0, a2) or
+  // (a1, a3) of the fragment and is transposed into its order. Step s's
+  // unit is step 0's with bit 2 flipped: offset ^ (s << 6).
+  const int qg = 4 * (g & 1) + (g >> 1);
+  const uint32_t offk0 = qg * 128 + ((t ^ qg) << 4);
   const uint32_t smem_base = smem_u32(smem);
   __shared__ int fixup_ok;
 
@@ -290,7 +302,7 @@ __device__ __forceinline__ void streamk_body(const Sched& S) {
     // A packed32 operand lands as [half][tile32][BK][16]: logical chunk c
     // sits at (c % 2) * (BN/32) + c / 2.
     uint32_t b_chunk[NQ];
-    const bool b32 = (q.b_kind == kOpPacked32);
+    const bool b32 = !AKM && (q.b_kind == kOpPacked32);  // AKM: B never packed32
 #pragma unroll
     for (int qq = 0; qq < NQ; ++qq) {
       const int c = wn * NQ + qq;
@@ -311,8 +323,15 @@ __device__ __forceinline__ void streamk_body(const Sched& S) {
         double2 a_lo[MI], a_hi[MI], b_lo[NQ], b_hi[NQ];
 #pragma unroll
         for (int i = 0; i < MI; ++i) {
-          a_lo[i] = lds128(sa + i * kChunkBytes + ks + off_r0);
-          a_hi[i] = lds128(sa + i * kChunkBytes + ks + off_r1);
+          if constexpr (AKM) {
+            const uint32_t o = sa + i * kChunkBytes + (offk0 ^ (s << 6));
+            const double2 r0 = lds128(o), r1 = lds128(o + 8 * 128);
+            a_lo[i] = make_double2(r0.x, r1.x);
+            a_hi[i] = make_double2(r0.y, r1.y);
+          } else {
+            a_lo[i] = lds128(sa + i * kChunkBytes + ks + off_r0);
+            a_hi[i] = lds128(sa + i * kChunkBytes + ks + off_r1);
+          }
         }
 #pragma unroll
         for (int qq = 0; qq < NQ; ++qq) {
@@ -402,13 +421,15 @@ __device__ __forceinline__ void streamk_body(const Sched& S) {
       if (!syrk_skip) {
 #pragma unroll
         for (int i = 0; i < MI; ++i) {
-          const int64_t m0 = mbase + i * 16 + 2 * g;
+          // MMA rows g, g + 8 sit at tile rows 2g, 2g + 1 (AKM: q(g), 8 + q(g)).
+          const int64_t m0 = mbase + i * 16 + (AKM ? qg : 2 * g);
+          const int64_t m1 = m0 + (AKM ? 8 : 1);
 #pragma unroll
           for (int qq = 0; qq < NQ; ++qq) {
             const int64_t n0 = nbase + qq * 16 + 4 * t;
             store_row4(q, m0, n0, acc[i][2 * qq][0], acc[i][2 * qq + 1][0], acc[i][2 * qq][1],
                        acc[i][2 * qq + 1][1]);
-            store_row4(q, m0 + 1, n0, acc[i][2 * qq][2], acc[i][2 * qq + 1][2],
+            store_row4(q, m1, n0, acc[i][2 * qq][2], acc[i][2 * qq + 1][2],
                        acc[i][2 * qq][3], acc[i][2 * qq + 1][3]);
           }
         }
@@ -439,6 +460,24 @@ __global__ void __launch_bounds__(kThreads, Tile64::kMinBlocks)
                           const __grid_constant__ Fp64Params p) {
   const SingleSched S{p, &mapA, &mapB};
   streamk_body<Tile64>(S);
+}
+
+// The same two kernels on a K-major A (kOpBandK: the rotation reading
+// band-packed Psi, the band -> grid transposition folded into the loads).
+__global__ void __launch_bounds__(kThreads, 1)
+    fp64_streamk_kernel_ak(const __grid_constant__ CUtensorMap mapA,
+                           const __grid_constant__ CUtensorMap mapB,
+                           const __grid_constant__ Fp64Params p) {
+  const SingleSched S{p, &mapA, &mapB};
+  streamk_body<Tile128, true>(S);
+}
+
+__global__ void __launch_bounds__(kThreads, Tile64::kMinBlocks)
+    fp64_streamk_kernel64_ak(const __grid_constant__ CUtensorMap mapA,
+                             const __grid_constant__ CUtensorMap mapB,
+                             const __grid_constant__ Fp64Params p) {
+  const SingleSched S{p, &mapA, &mapB};
+  streamk_body<Tile64, true>(S);
 }
 
 template <class TS>

@@ -49,6 +49,11 @@ enum OperandKind : int {
   kOpPacked32 = 1,  // [ceil(R/32)][K][32]; 3-D map {32, K, tiles}, two half-width boxes
                     // per stage -> shared memory [half][tile][BK][16]
   kOpDense = 2,     // R contiguous, k stride ld; 2-D map {R, K}, one box per 16-chunk
+  kOpBandK = 3,     // K-major [K/16][R][16] (band-packed Psi as the rotation's A:
+                    // element (r, k) at (k/16)*R*16 + r*16 + k%16); 3-D map
+                    // {16, R, K/16}, one box {16, BM, 1} per stage (BK = 16) ->
+                    // shared memory [BM][16 k]; A operand of the single-problem
+                    // kernels only, K % 16 == 0
 };
 
 enum OutKind : int { kOutRowMajor = 0, kOutSyrkUpper = 1, kOutBand16 = 2 };

@@ -44,6 +44,31 @@ __global__ void __launch_bounds__(256) pack_kernel(int64_t R, int64_t K, const d
   }
 }
 
+// The inverse of pack_kernel: X[r*sr + k*sk] = Xp[(r/T)*K*T + k*T + r%T] for
+// r < R. Reads are coalesced along r%T (T contiguous doubles per panel row),
+// writes along whichever of r / k is contiguous in X.
+template <int T>
+__global__ void __launch_bounds__(256) unpack_kernel(int64_t R, int64_t K,
+                                                     const double* __restrict__ Xp,
+                                                     double* __restrict__ X, int64_t sr,
+                                                     int64_t sk) {
+  __shared__ double tile[32][33];
+  const int64_t r0 = (int64_t)blockIdx.x * 32;
+  const int64_t k0 = (int64_t)blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t k = k0 + i, r = r0 + tx;
+    tile[i][tx] = (k < K && r < R) ? Xp[(r / T) * K * T + k * T + (r % T)] : 0.0;  // [k][r]
+  }
+  __syncthreads();
+  const bool r_contig = (sr == 1);
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t r = r_contig ? r0 + tx : r0 + i;
+    const int64_t k = r_contig ? k0 + i : k0 + tx;
+    if (r < R && k < K) X[r * sr + k * sk] = r_contig ? tile[i][tx] : tile[tx][i];
+  }
+}
+
 // One 16 x 16 block per warp-pair: src[(b/16)*Nd*16 + g*16 + b%16] (band) ->
 // dst[(g/16)*nb*16 + b*16 + g%16] (grid), or the reverse.
 template <bool kBandToGrid>
@@ -116,6 +141,23 @@ int launch_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, i
     pack_kernel<16><<<grid, 256, 0, s>>>(R, K, X, sr, sk, Xp);
   else if (T == 32)
     pack_kernel<32><<<grid, 256, 0, s>>>(R, K, X, sr, sk, Xp);
+  else
+    return fail(SKGEMM_ERR_INVALID_ARG, "pack width must be 16 or 32");
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+int launch_unpack(int64_t R, int64_t K, const double* Xp, int T, double* X, int64_t sr,
+                  int64_t sk, cudaStream_t s) {
+  if (R < 0 || K < 0) return fail(SKGEMM_ERR_INVALID_ARG, "negative unpack extent");
+  if (R == 0 || K == 0) return SKGEMM_OK;
+  if (!X || !Xp) return fail(SKGEMM_ERR_INVALID_ARG, "null unpack pointer");
+  dim3 grid((unsigned)((R + 31) / 32), (unsigned)((K + 31) / 32));
+  if (grid.y > 65535u) return fail(SKGEMM_ERR_INVALID_ARG, "unpack: K too large for one launch");
+  if (T == 16)
+    unpack_kernel<16><<<grid, 256, 0, s>>>(R, K, Xp, X, sr, sk);
+  else if (T == 32)
+    unpack_kernel<32><<<grid, 256, 0, s>>>(R, K, Xp, X, sr, sk);
   else
     return fail(SKGEMM_ERR_INVALID_ARG, "pack width must be 16 or 32");
   SKG_CUDA(cudaGetLastError());

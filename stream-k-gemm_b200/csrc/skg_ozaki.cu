@@ -259,22 +259,34 @@ __device__ __forceinline__ uint32_t residue_bf16x2(const Digits& a, const Digits
 // ------------------------------------------------- packed-T operand prep
 // Partial sums of squares of each row of a packed-T operand
 // ([ceil(R/T)][K][T]): part[(p*C + c)*T + r] over k-chunk c.
-template <int T>
+template <int T, bool KM = false>
 __global__ void __launch_bounds__(256) norm_partials_kernel(int64_t R, int64_t K,
                                                            const double* __restrict__ X,
                                                            int C, double* __restrict__ part) {
   __shared__ double red[256];
   const int p = blockIdx.x, c = blockIdx.y;
-  const int r = threadIdx.x % T, kl = threadIdx.x / T;
+  // KM: thread (kl = tid % 16, r = tid / 16), so that a warp reads two rows'
+  // whole 128-byte k-blocks; each (r, kl) sum is the packed layout's, and
+  // red[] is indexed as there, so the result is the same bit for bit.
+  const int r = KM ? (int)threadIdx.x / 16 : (int)threadIdx.x % T;
+  const int kl = KM ? (int)threadIdx.x % 16 : (int)threadIdx.x / T;
+  const int slot = kl * T + r;  // = threadIdx.x for the packed layout
   constexpr int KL = 256 / T;
   const int64_t k0 = (int64_t)c * K / C, k1 = (int64_t)(c + 1) * K / C;
   const double* src = X + (int64_t)p * K * T;
+  // KM (T = 16): a K-major [K/16][R][16] operand, row p*16 + r read at
+  // X[(k/16)*R*16 + (p*16 + r)*16 + k%16]; the same sums in the same order.
+  const int64_t row_r = (int64_t)p * T + r;
   double acc = 0.0;
   for (int64_t k = k0 + kl; k < k1; k += KL) {
-    const double v = src[k * T + r];
+    double v;
+    if constexpr (KM)
+      v = row_r < R ? X[(k >> 4) * R * 16 + row_r * 16 + (k & 15)] : 0.0;
+    else
+      v = src[k * T + r];
     acc = fma(v, v, acc);
   }
-  red[threadIdx.x] = acc;
+  red[slot] = acc;
   __syncthreads();
   if (threadIdx.x < T) {
     double s = 0.0;
@@ -320,7 +332,12 @@ constexpr int kConvWarps = 8;
 constexpr int kConvTile = 16 * 32;  // doubles per warp tile
 constexpr int kConvSmem = kConvWarps * (kConvStages * kConvTile * 8 + kConvStages * 8);
 
-template <int T, int L, bool BF>
+// KM: the operand is K-major, [K/16][R][16] (band-packed Psi as the
+// rotation's A: the band -> grid transposition happens here, in the reads).
+// Its box {16 k, 16 rows, 2 k-blocks} lands as [2][16 rows][16 k], 128B-
+// swizzled per 128-byte row: element (k, r) at row R = 16 (k / 16) + r, unit
+// ((k % 16) / 2) ^ (R % 8), half k % 2.
+template <int T, int L, bool BF, bool KM = false>
 __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     const __grid_constant__ CUtensorMap map, int64_t KP, int64_t Rpad,
     const int* __restrict__ mu, uint8_t* __restrict__ res, uint32_t* __restrict__ err) {
@@ -349,8 +366,11 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
   auto issue = [&](int64_t g, int64_t kb, int st) {
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&bar[st], kConvTile * 8);
-    tma_load_3d(buf + st * kConvTile, &map, &bar[st], (int)(16 * (g % (T / 16))), (int)(kb * 32),
-                (int)(g / (T / 16)));
+    if constexpr (KM)
+      tma_load_3d(buf + st * kConvTile, &map, &bar[st], 0, (int)(16 * g), (int)(2 * kb));
+    else
+      tma_load_3d(buf + st * kConvTile, &map, &bar[st], (int)(16 * (g % (T / 16))),
+                  (int)(kb * 32), (int)(g / (T / 16)));
   };
   auto advance = [&](int64_t& g, int64_t& kb) {
     g += dq;
@@ -390,11 +410,18 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
       // and 16+8h .. 16+8h+7, so that each of its two 16-byte stores and the
       // other half-lane's together fill one whole 32-byte sector.
       const double* col = buf + s * kConvTile + r;
+      auto at = [&](int k) {  // element (k, r) of the stage
+        if constexpr (KM)
+          return buf[s * kConvTile + (16 * (k >> 4) + r) * 16 +
+                     (((((k & 15) >> 1) ^ (r & 7))) << 1) + (k & 1)];
+        else
+          return col[k * 16];
+      };
       Digits d[16];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        d[j] = digits_of<L>(col[(8 * h + j) * 16], s1, s2);
-        d[8 + j] = digits_of<L>(col[(16 + 8 * h + j) * 16], s1, s2);
+        d[j] = digits_of<L>(at(8 * h + j), s1, s2);
+        d[8 + j] = digits_of<L>(at(16 + 8 * h + j), s1, s2);
       }
       uint8_t* row = res + ((g * 16 + r) * KP + kb * 32) * 2;
 #pragma unroll
@@ -415,19 +442,27 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
       // touches 8 distinct chunks (all 32 banks once). d[j] then holds
       // k = 16 h + (j ^ 4 h): for h = 1 the packed words are in the order
       // 1, 0, 3, 2, and put() swaps them back.
+      // KM: lane h = 1 walks its k in the order j ^ 1 instead, so that the
+      // half-warp's two k-blocks read opposite halves of each 16-byte unit
+      // (conflict-free); its pairs come out swapped, which the byte-permute
+      // selector of pk() undoes, and put() keeps the word order.
       const double* stage = buf + s * kConvTile;
-      const int z = 320 * h | (((r >> 1) ^ (4 * h)) << 1) | (r & 1);
+      const int z = KM ? 256 * h + 16 * r + ((r & 7) << 1) + h
+                       : 320 * h | (((r >> 1) ^ (4 * h)) << 1) | (r & 1);
       Digits d[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j)
-        d[j] = digits_of<L>(stage[((j << 4) | ((j & 7) << 1)) ^ z], s1, s2);
+        d[j] = digits_of<L>(stage[(KM ? j : ((j << 4) | ((j & 7) << 1))) ^ z], s1, s2);
+      const uint32_t sel = (KM && h) ? 0x0004u : 0x0040u;
+      auto pk = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t e) {
+        return __byte_perm(__byte_perm(a, b, sel), __byte_perm(c, e, sel), 0x5410);
+      };
       auto put = [&](uint8_t* p, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3) {
         *reinterpret_cast<uint4*>(p) =
-            h ? make_uint4(w1, w0, w3, w2) : make_uint4(w0, w1, w2, w3);
+            (!KM && h) ? make_uint4(w1, w0, w3, w2) : make_uint4(w0, w1, w2, w3);
       };
-      put(dst, pack4(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pack4(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
-          pack4(d[8].lo, d[9].lo, d[10].lo, d[11].lo),
-          pack4(d[12].lo, d[13].lo, d[14].lo, d[15].lo));
+      put(dst, pk(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pk(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
+          pk(d[8].lo, d[9].lo, d[10].lo, d[11].lo), pk(d[12].lo, d[13].lo, d[14].lo, d[15].lo));
 #pragma unroll
       for (int l = 1; l < L; ++l) {
         uint32_t b[16];
@@ -437,8 +472,8 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
           b[j] = v.x;
           b[j + 1] = v.y;
         }
-        put(dst + l * lstride, pack4(b[0], b[1], b[2], b[3]), pack4(b[4], b[5], b[6], b[7]),
-            pack4(b[8], b[9], b[10], b[11]), pack4(b[12], b[13], b[14], b[15]));
+        put(dst + l * lstride, pk(b[0], b[1], b[2], b[3]), pk(b[4], b[5], b[6], b[7]),
+            pk(b[8], b[9], b[10], b[11]), pk(b[12], b[13], b[14], b[15]));
       }
     } else {
 #pragma unroll
@@ -972,16 +1007,16 @@ void report(skgemm_options_t* opts, int L, int gamma_bits, int64_t K) {
     default: return fail(SKGEMM_ERR_INVALID_ARG, "moduli count out of range");   \
   }
 
-template <int T, int L, bool BF>
+template <int T, int L, bool BF, bool KM = false>
 int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t Rpad,
                    const int* mu, uint8_t* res, uint32_t* err, cudaStream_t s) {
   static int occ[64] = {0};
   if (!occ[dev->device]) {
-    SKG_CUDA(cudaFuncSetAttribute(convert_tma_kernel<T, L, BF>,
+    SKG_CUDA(cudaFuncSetAttribute(convert_tma_kernel<T, L, BF, KM>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
     int n = 0;
-    SKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, convert_tma_kernel<T, L, BF>, 256,
-                                                           kConvSmem));
+    SKG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, convert_tma_kernel<T, L, BF, KM>,
+                                                           256, kConvSmem));
     occ[dev->device] = n > 0 ? n : 1;
   }
   const int64_t ntiles = (Rpad / 16) * (KP / 32);
@@ -989,8 +1024,8 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
                                            (int64_t)dev->num_sms * occ[dev->device]);
   // (every warp of the grid gets at least one tile only if ntiles >= warps;
   // warps without a tile return at once)
-  convert_tma_kernel<T, L, BF><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, KP, Rpad, mu, res,
-                                                                        err);
+  convert_tma_kernel<T, L, BF, KM><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, KP, Rpad, mu,
+                                                                            res, err);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
 }
@@ -1002,7 +1037,7 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
 template <int T>
 int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, int L,
                DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu, cudaStream_t s,
-               bool bf = false) {
+               bool bf = false, bool km = false) {
   if ((reinterpret_cast<uintptr_t>(X) & 15) != 0)
     return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
   if (K > ((int64_t)1 << 31) - 128) return fail(SKGEMM_ERR_INVALID_ARG, "K too large");
@@ -1012,8 +1047,14 @@ int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, 
   if ((st = res.ensure((size_t)L * Rpad * KP * (bf ? 2 : 1))) != SKGEMM_OK) return st;
   if ((st = part.ensure((size_t)P_in * C * T * sizeof(double))) != SKGEMM_OK) return st;
   if ((st = mu.ensure((size_t)Rpad * sizeof(int))) != SKGEMM_OK) return st;
-  norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
-                                                                  (double*)part.ptr);
+  if (km && T == 16)
+    norm_partials_kernel<16, true><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
+                                                                          (double*)part.ptr);
+  else if (km)
+    return fail(SKGEMM_ERR_INVALID_ARG, "K-major operand with 32-wide panels");
+  else
+    norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
+                                                                    (double*)part.ptr);
   SKG_CUDA(cudaGetLastError());
   row_exponents_kernel<T><<<(unsigned)((Rpad + 255) / 256), 256, 0, s>>>(
       R, Rpad, C, (const double*)part.ptr, gamma_for(L), (int*)mu.ptr);
@@ -1024,10 +1065,28 @@ int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, 
 template <int T>
 int prep_convert(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
                  const double* X, int L, DeviceBuffer& res, DeviceBuffer& mu, uint32_t* err,
-                 cudaStream_t s, bool bf = false) {
+                 cudaStream_t s, bool bf = false, bool km = false) {
+  CUtensorMap map;
+  const int* mp = (const int*)mu.ptr;
+  uint8_t* rp = (uint8_t*)res.ptr;
+  if (km) {
+    // K-major [K/16][R][16] (T = 16, K % 16 == 0): boxes {16 k, 16 rows, 2
+    // k-blocks}, zero fill past R and past the last k-block.
+    if (T != 16 || K % 16) return fail(SKGEMM_ERR_INVALID_ARG, "K-major operand layout");
+    const uint64_t dims[3] = {16, (uint64_t)R, (uint64_t)(K / 16)};
+    const uint64_t strides[2] = {16 * 8, (uint64_t)R * 16 * 8};
+    const uint32_t box[3] = {16, 16, 2};
+    int st;
+    if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                           CU_TENSOR_MAP_SWIZZLE_128B)))
+      return st;
+    if (bf) {
+      SKG_DISPATCH_L(L, (launch_convert<16, LL, true, true>(dev, map, KP, Rpad, mp, rp, err, s)))
+    }
+    SKG_DISPATCH_L(L, (launch_convert<16, LL, false, true>(dev, map, KP, Rpad, mp, rp, err, s)))
+  }
   // [P_in][K][T] doubles; boxes of 16 rows x 32 k (zero fill past K / P_in).
   const int64_t P_in = (R + T - 1) / T;
-  CUtensorMap map;
   const uint64_t dims[3] = {(uint64_t)T, (uint64_t)K, (uint64_t)P_in};
   const uint64_t strides[2] = {(uint64_t)T * 8, (uint64_t)K * T * 8};
   const uint32_t box[3] = {16, 32, 1};
@@ -1035,8 +1094,6 @@ int prep_convert(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpa
   if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                          bf ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B)))
     return st;
-  const int* mp = (const int*)mu.ptr;
-  uint8_t* rp = (uint8_t*)res.ptr;
   if (bf) {
     SKG_DISPATCH_L(L, (launch_convert<T, LL, true>(dev, map, KP, Rpad, mp, rp, err, s)))
   }
@@ -1046,10 +1103,10 @@ int prep_convert(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpa
 template <int T>
 int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
                 const double* X, int L, DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu,
-                uint32_t* err, cudaStream_t s, bool bf = false) {
+                uint32_t* err, cudaStream_t s, bool bf = false, bool km = false) {
   int st;
-  if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s, bf))) return st;
-  return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s, bf);
+  if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s, bf, km))) return st;
+  return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s, bf, km);
 }
 
 template <int L, bool BF>
@@ -1562,7 +1619,7 @@ int ozaki_syrk_packed(int64_t K, int64_t M, const double* Ap, double* C, int64_t
 }
 
 int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
-              skgemm_options_t* opts, cudaStream_t s) {
+              skgemm_options_t* opts, cudaStream_t s, bool a_band) {
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -1588,9 +1645,10 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   if ((st = os->res_b.ensure((size_t)L * RB * KPb))) return st;
   if ((st = os->mu_b.ensure((size_t)RB * sizeof(int)))) return st;
   if ((st = os->rbytes.ensure((size_t)L * Nd * nb))) return st;
-  // Grid-packed Psi is a packed16 operand with rows = grid points, K = bands.
+  // Grid-packed Psi is a packed16 operand with rows = grid points, K = bands;
+  // band-packed Psi (a_band) the K-major form of the same operand.
   if ((st = prep_packed<16>(dev, Nd, nb, KP, RA, A, L, os->res_a, os->part_a, os->mu_a, ws->err,
-                            s, bf)))
+                            s, bf, a_band)))
     return st;
   if ((st = launch_local(nb, nb, KP, RB, Q, 16, nb, L, (uint8_t*)os->res_b.ptr,
                          (int*)os->mu_b.ptr, s, bf)))

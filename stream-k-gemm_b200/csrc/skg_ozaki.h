@@ -16,8 +16,9 @@ int ozaki_syrk_packed(int64_t K, int64_t M, const double* Ap, double* C, int64_t
 int ozaki_subspace(int64_t K, int64_t M, const double* Psi, const double* HPsi, double* S,
                    int64_t lds, double alpha_s, double beta_s, double* Hs, int64_t ldh,
                    double alpha_h, double gamma_h, skgemm_options_t* opts, cudaStream_t s);
+// A grid-packed, or band-packed when a_band (read K-major by the conversion).
 int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
-              skgemm_options_t* opts, cudaStream_t s);
+              skgemm_options_t* opts, cudaStream_t s, bool a_band = false);
 int ozaki_consume_error(DeviceState* dev, cudaStream_t s);
 // Estimated device time (s) of an Ozaki call (op = SKGEMM_OP_*), < 0 if the
 // shape is not eligible.

@@ -115,7 +115,9 @@ Fp64Problem gemm_packed_problem(int64_t M, int64_t N, int64_t K, const double* A
                                 double gamma);
 Fp64Problem syrk_problem(int64_t K, int64_t M, const double* Ap, double* C, int64_t ldc,
                          double alpha, double beta);
-Fp64Problem rot_problem(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D);
+// a_band: A band-packed (read K-major), else grid-packed.
+Fp64Problem rot_problem(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
+                        bool a_band = false);
 // Result of an empty reduction (K == 0): D = gamma (GEMM), C = beta*C (SYRK).
 int run_k0(int mode, int64_t M, int64_t N, double* D, int64_t ld, double gamma, bool beta_zero,
            cudaStream_t s);
@@ -125,6 +127,8 @@ int launch_sum_parts(const double* parts, int nparts, int64_t n, double gamma, d
                      cudaStream_t s);
 int launch_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, int T,
                 double* Xp, cudaStream_t s);
+int launch_unpack(int64_t R, int64_t K, const double* Xp, int T, double* X, int64_t sr,
+                  int64_t sk, cudaStream_t s);
 int launch_band_to_grid(int64_t Nd, int64_t nb, const double* src, double* dst,
                         cudaStream_t s);
 int launch_grid_to_band(int64_t Nd, int64_t nb, const double* src, double* dst,

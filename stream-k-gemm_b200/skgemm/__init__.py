@@ -128,7 +128,14 @@ _SIGS = {
     "skgemm_drot": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_drot_dev": [_i64, _i64, _vp, _vp, _vp, _vp],
     "skgemm_drot_dev_opt": [_i64, _i64, _vp, _vp, _vp, ctypes.POINTER(Options), _vp],
+    "skgemm_drot_band_dev": [_i64, _i64, _vp, _vp, _vp, _vp],
+    "skgemm_drot_band_dev_opt": [_i64, _i64, _vp, _vp, _vp, ctypes.POINTER(Options), _vp],
     "skgemm_pack_dev": [_i64, _i64, _vp, _i64, _i64, ctypes.c_int, _vp, _vp],
+    "skgemm_unpack_dev": [_i64, _i64, _vp, ctypes.c_int, _vp, _i64, _i64, _vp],
+    "skgemm_pack_c16_dev": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_pack_r16_dev": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_unpack_c16_dev": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_unpack_r16_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_band_to_grid_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_grid_to_band_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_plan_create": [ctypes.POINTER(BatchItem), ctypes.c_int,
@@ -321,8 +328,46 @@ def drot_dev(Nd, nb, A_grid, Q, D_band, stream=None, precision=None, slices=0):
     return o
 
 
+def drot_band_dev(Nd, nb, A_band, Q, D_band, stream=None, precision=None, slices=0):
+    """The rotation on band-packed Psi (the layout SYRK and GEMM read); equals
+    drot_dev on the grid-packed copy, bit for bit."""
+    o = _opts(precision, slices)
+    if o is None:
+        _check(lib().skgemm_drot_band_dev(Nd, nb, _dptr(A_band), _dptr(Q), _dptr(D_band),
+                                          _stream(stream)))
+        return None
+    _check(lib().skgemm_drot_band_dev_opt(Nd, nb, _dptr(A_band), _dptr(Q), _dptr(D_band),
+                                          ctypes.byref(o), _stream(stream)))
+    return o
+
+
 def pack_dev(R, K, X, sr, sk, T, X_packed, stream=None):
     _check(lib().skgemm_pack_dev(R, K, _dptr(X), sr, sk, T, _dptr(X_packed), _stream(stream)))
+
+
+def unpack_dev(R, K, X_packed, T, X, sr, sk, stream=None):
+    """Packed-T panels -> strided dense X[r*sr + k*sk] (rows r < R)."""
+    _check(lib().skgemm_unpack_dev(R, K, _dptr(X_packed), T, _dptr(X), sr, sk, _stream(stream)))
+
+
+def pack_c16_dev(Nd, nb, src, dst, stream=None):
+    """linalg_pack_c16_f64 (sme_pack.hpp:319): column-major [Nd, nb] -> grid-packed."""
+    _check(lib().skgemm_pack_c16_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
+
+
+def pack_r16_dev(Nd, nb, src, dst, stream=None):
+    """linalg_pack_r16_f64 (sme_pack.hpp:322): row-major [nb, Nd] -> grid-packed."""
+    _check(lib().skgemm_pack_r16_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
+
+
+def unpack_c16_dev(Nd, nb, src, dst, stream=None):
+    """linalg_unpack_c16_f64 (sme_pack.hpp:325): grid-packed -> column-major [Nd, nb]."""
+    _check(lib().skgemm_unpack_c16_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
+
+
+def unpack_r16_dev(Nd, nb, src, dst, stream=None):
+    """linalg_unpack_r16_f64 (sme_pack.hpp:328): grid-packed -> row-major [nb, Nd]."""
+    _check(lib().skgemm_unpack_r16_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
 
 
 def band_to_grid_dev(Nd, nb, src, dst, stream=None):

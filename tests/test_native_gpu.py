@@ -211,6 +211,33 @@ def test_rot_shapes(cuda, Nd, nb):
     assert oracle.rel_frobenius(host(dD), ref) <= TOL
 
 
+@pytest.mark.parametrize("Nd,nb", [(16, 16), (48, 80), (1024, 528), (4096, 512), (2000, 400),
+                                   (20000, 512), (4096, 1024)])
+def test_rot_band_equals_grid(cuda, Nd, nb):
+    """skgemm_drot_band_dev on band-packed Psi (the transposition folded into
+    the K-major loads) equals skgemm_drot_dev on the grid-packed copy, bit for
+    bit (same tiles, schedule and k order), and Dot2 within the gate. The
+    shapes cover both tile kernels (128 x 128 for few tiles, 64 x 64)."""
+    Psi = gaussian((Nd, nb), Nd + 3 * nb, 1 / np.sqrt(Nd))
+    Q = dev(uniform((nb, nb), 12))
+    grid = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+    band = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+    skgemm.drot_dev(Nd, nb, dev(oracle.grid_pack(Psi)), Q, grid)
+    skgemm.drot_band_dev(Nd, nb, dev(oracle.band_pack(Psi)), Q, band)
+    skgemm.stream_status()
+    assert torch.equal(band, grid)
+    ref = oracle.band_pack(oracle.dot2_matmul(Psi, host(Q).reshape(nb, nb))).ravel()
+    assert oracle.rel_frobenius(host(band), ref) <= TOL
+
+
+def test_rot_band_rejects_ragged(cuda):
+    A = torch.zeros(48 * 40, dtype=torch.float64, device="cuda")
+    q = torch.zeros(40 * 40, dtype=torch.float64, device="cuda")
+    with pytest.raises(skgemm.SkgemmError) as e:
+        skgemm.drot_band_dev(48, 40, A, q, torch.zeros_like(A))
+    assert e.value.code == skgemm.ERR_INVALID_ARG
+
+
 # --------------------------------------------------------- layout kernels
 def test_band_grid_roundtrip_device(cuda):
     Nd, nb = 272, 96
@@ -234,6 +261,38 @@ def test_pack_device_matches_oracle(cuda):
         out2 = torch.zeros_like(out)
         skgemm.pack_dev(R, K, dev(np.ascontiguousarray(X.T)), 1, R, T, out2)  # column-major
         assert np.array_equal(host(out2), oracle.pack(X, T).ravel())
+
+
+def test_unpack_device_inverts_pack(cuda):
+    R, K = 45, 70
+    X = uniform((R, K), 9)
+    for T in (16, 32):
+        P = dev(oracle.pack(X, T))
+        out = torch.full((R * K,), np.nan, dtype=torch.float64, device="cuda")
+        skgemm.unpack_dev(R, K, P, T, out, K, 1)   # row-major destination
+        assert np.array_equal(host(out).reshape(R, K), oracle.unpack(oracle.pack(X, T), R))
+        out2 = torch.full((R * K,), np.nan, dtype=torch.float64, device="cuda")
+        skgemm.unpack_dev(R, K, P, T, out2, 1, R)  # column-major destination
+        assert np.array_equal(host(out2).reshape(K, R).T, X)
+
+
+def test_linalg_c16_r16_converters(cuda):
+    """linalg_pack_c16/r16 and unpack_c16/r16 (sme_pack.hpp:319-329): column-major
+    [Nd, nb] = row-major [nb, Nd] bytes <-> grid-packed [Nd/16][nb][16]."""
+    Nd, nb = 96, 40
+    Psi = uniform((Nd, nb), 10)
+    colmajor = dev(np.ascontiguousarray(Psi.T))  # src[g + b*Nd]
+    for pack, unpack in ((skgemm.pack_c16_dev, skgemm.unpack_c16_dev),
+                         (skgemm.pack_r16_dev, skgemm.unpack_r16_dev)):
+        grid = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+        pack(Nd, nb, colmajor, grid)
+        assert np.array_equal(host(grid), oracle.grid_pack(Psi).ravel())
+        back = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+        unpack(Nd, nb, grid, back)
+        assert np.array_equal(host(back), host(colmajor).ravel())
+    with pytest.raises(skgemm.SkgemmError) as e:
+        skgemm.pack_c16_dev(Nd + 8, nb, colmajor, grid)
+    assert e.value.code == skgemm.ERR_INVALID_ARG
 
 
 # ------------------------------------------------- full-size configuration

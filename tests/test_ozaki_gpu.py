@@ -21,6 +21,10 @@ TOL = 1e-13
 OZ = skgemm.PREC_OZAKI_I8
 
 
+def host_np(t):
+    return t.detach().cpu().numpy()
+
+
 def dev(x, dtype=torch.float64):
     return torch.from_numpy(np.ascontiguousarray(x)).to(dtype=dtype, device="cuda")
 
@@ -115,6 +119,41 @@ def test_ozaki_rot_accuracy(cuda, Nd, nb, kind):
     skgemm.stream_status()
     ref = oracle.band_pack(oracle.dot2_matmul(Psi, Q)).ravel()
     assert oracle.rel_frobenius(D.cpu().numpy(), ref) <= TOL
+
+
+@pytest.mark.parametrize("Nd,nb,prec", [(4096, 512, "i8"), (2000, 400, "i8"), (48, 80, "i8"),
+                                        (1024, 576, "i8"), (4096, 256, "bf"), (144, 496, "bf")])
+def test_ozaki_rot_band_equals_grid(cuda, Nd, nb, prec):
+    """The Ozaki rotation on band-packed Psi (norms and residues read K-major)
+    equals the grid-packed call bit for bit: same exponents, same residues."""
+    precision = OZ if prec == "i8" else skgemm.PREC_OZAKI_BF16
+    Psi = gaussian((Nd, nb), 5 * Nd + nb, 1 / np.sqrt(Nd))
+    Psi[::7, 3] *= 2.0 ** 30  # rows of very different scale
+    Q = dev(uniform((nb, nb), 9))
+    grid = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+    band = torch.full((Nd * nb,), np.nan, dtype=torch.float64, device="cuda")
+    og = skgemm.drot_dev(Nd, nb, dev(oracle.grid_pack(Psi)), Q, grid, precision=precision)
+    ob = skgemm.drot_band_dev(Nd, nb, dev(oracle.band_pack(Psi)), Q, band, precision=precision)
+    skgemm.stream_status()
+    assert ob.slices_used_out == og.slices_used_out and ob.err_bound_out == og.err_bound_out
+    assert torch.equal(band, grid)
+    ref = oracle.band_pack(oracle.dot2_matmul(Psi, host_np(Q).reshape(nb, nb))).ravel()
+    assert oracle.rel_frobenius(band.cpu().numpy(), ref) <= TOL
+
+
+def test_rot_band_auto_precision(cuda):
+    Nd, nb = 110592, 512
+    Psi = torch.randn(Nd * nb, dtype=torch.float64, device="cuda") / Nd ** 0.5
+    Q = torch.rand(nb * nb, dtype=torch.float64, device="cuda") * 2 - 1
+    grid = torch.empty_like(Psi)
+    skgemm.band_to_grid_dev(Nd, nb, Psi, grid)
+    a = torch.empty_like(Psi)
+    b = torch.empty_like(Psi)
+    oa = skgemm.drot_dev(Nd, nb, grid, Q, a, precision=skgemm.PREC_AUTO)
+    ob = skgemm.drot_band_dev(Nd, nb, Psi, Q, b, precision=skgemm.PREC_AUTO)
+    skgemm.stream_status()
+    assert oa.slices_used_out == ob.slices_used_out
+    assert torch.equal(a, b)
 
 
 def test_ozaki_deterministic(cuda):
