@@ -70,6 +70,10 @@ def parse():
                     help="grid points (default 110592 = 48^3; smaller values for profiling)")
     ap.add_argument("--nb", type=int, default=NB, help="states (default 512)")
     ap.add_argument("--workload", default="subspace", choices=["subspace", "batched", "serving"])
+    ap.add_argument("--rot-layout", default="grid", choices=["grid", "band"],
+                    help="subspace: the rotation reads grid-packed Psi (the reference's "
+                         "sme_gemm_trp_3d input) or the band-packed Psi of SYRK/GEMM "
+                         "(skgemm_drot_band_dev, no grid-packed copy)")
     ap.add_argument("--requests", type=int, default=2000, help="serving: trace length")
     ap.add_argument("--ozaki-streams", type=int, default=2,
                     help="serving, Ozaki: requests running concurrently (each stream holds "
@@ -263,7 +267,10 @@ def run_gpu(args):
                 evs[1].record(stream)
         if evs:
             evs[2].record(stream)
-        skgemm.drot_dev(ND, NB, grid, q, Pn, stream=stream, precision=prec)
+        if args.rot_layout == "band":
+            skgemm.drot_band_dev(ND, NB, band, q, Pn, stream=stream, precision=prec)
+        else:
+            skgemm.drot_dev(ND, NB, grid, q, Pn, stream=stream, precision=prec)
         if evs:
             evs[3].record(stream)
 
@@ -308,7 +315,8 @@ def run_gpu(args):
         "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "Nd": ND, "nb": NB, "ops": ["syrk", "gemm", "rotation"],
-                   "precision": args.precision, "parallelism": f"replicas{world}",
+                   "precision": args.precision, "rot_layout": args.rot_layout,
+                   "parallelism": f"replicas{world}",
                    "flop_per_step": FLOP_STEP, "l2": "inputs larger than L2 (453 MB each)"},
         "latency_ms": dict({"p50": round(float(np.percentile(step_ms, 50)), 4),
                             "p99": round(float(np.percentile(step_ms, 99)), 4)}, **op_ms),

@@ -6,6 +6,9 @@ workload, for profiling (ncu) and as a quick end-to-end exercise:
 Kernels and workloads (inputs larger than L2 where the kernel is HBM-bound):
   pack_kernel<16>, pack_kernel<32>   dense 110592 x 512 -> band-packed (453 MB)
   band_grid_kernel (both ways)       110592 x 512 band <-> grid packed (453 MB)
+  unpack_kernel<16>                  grid-packed -> column-major (linalg_unpack_c16)
+  fp64_streamk_kernel64_ak,          the rotation on band-packed Psi, 110592 x 512,
+  norm_partials / convert_tma (KM)   native and Ozaki (K-major operand reads)
   k0_kernel                          GEMM with K = 0 (D = gamma), 4096 x 4096
   sum_parts_kernel                   the host GEMM's k-chunk combine, 2048 x 2048 x 32768
   noalloc_fill_kernel                the allocation-free GEMM with K = 0
@@ -42,6 +45,20 @@ def main() -> None:
     skgemm.grid_to_band_dev(nd, nb, grid, back)
     skgemm.stream_status()
     assert torch.equal(back, band16)
+    colmajor = torch.empty_like(band16)
+    skgemm.unpack_c16_dev(nd, nb, grid, colmajor)
+    skgemm.stream_status()
+    assert torch.equal(colmajor.view(nb, nd).t(), dense)
+
+    # The rotation on band-packed Psi (no grid-packed copy), native and Ozaki.
+    q = torch.rand(nb * nb, generator=g, dtype=torch.float64, device=dev) * 2 - 1
+    rot_g = torch.empty_like(band16)
+    rot_b = torch.empty_like(band16)
+    for prec in (None, skgemm.PREC_OZAKI_I8):
+        skgemm.drot_dev(nd, nb, grid, q, rot_g, precision=prec)
+        skgemm.drot_band_dev(nd, nb, band16, q, rot_b, precision=prec)
+        skgemm.stream_status()
+        assert torch.equal(rot_b, rot_g)
 
     # K = 0 epilogues.
     n = 4096
