@@ -11,6 +11,9 @@
 //   sme_syrk<double>::compute      (include/sme_syrk.hpp:137, syrk_crsp.cpp:306)
 //   sme_gemm_trp_3d<double>::compute, sme_gemm_trp<double>
 //                                  (include/sme_trp_3d.hpp:194, :218-220)
+//   sme_pack<double>::pack_c16 / pack_r16 / unpack_c16 / unpack_r16 /
+//       band_to_grid_tile / grid_to_band_tile (include/sme_pack.hpp:85-313;
+//       host-side layout converters)
 //
 // Like the reference these return void; a failing call throws
 // skgemm::error (the reference has no error channel at all). Define
@@ -40,6 +43,16 @@ inline void check(int status) {
   std::abort();
 #else
   throw error(status, skgemm_last_error());
+#endif
+}
+
+inline void require(bool ok, const char* msg) {
+  if (ok) return;
+#ifdef SKGEMM_NO_EXCEPTIONS
+  std::fprintf(stderr, "skgemm error %d: %s\n", SKGEMM_ERR_INVALID_ARG, msg);
+  std::abort();
+#else
+  throw error(SKGEMM_ERR_INVALID_ARG, msg);
 #endif
 }
 
@@ -112,3 +125,57 @@ class sme_gemm_trp_3d {
 
 template <typename T>
 using sme_gemm_trp = sme_gemm_trp_3d<T>;
+
+// The reference's host-side layout converters (sme_pack<double>,
+// include/sme_pack.hpp:30-313) under the same names, as plain loops; the
+// device forms are skgemm_{pack,unpack}_{c16,r16}_dev and
+// skgemm_band_to_grid_dev / skgemm_grid_to_band_dev. Grid point g, band b:
+//   column-major [Nd, nb] (= row-major [nb, Nd]): X[g + b*Nd]
+//   grid-packed [Nd/16][nb][16]:                 P[(g/16)*nb*16 + b*16 + g%16]
+//   band-packed [nb/16][Nd][16]:                 B[(b/16)*Nd*16 + g*16 + b%16]
+// Nd (and nb for the band form) must be multiples of 16: the reference drops
+// the remainder tiles, these throw skgemm::error.
+template <typename T>
+class sme_pack {
+ public:
+  static constexpr int PACK_G = 16;
+
+  static void pack_c16(const int Nd, const int nb, const T* src, T* dst) {
+    skgemm::require(Nd >= 0 && nb >= 0 && Nd % 16 == 0, "pack_c16: Nd must be a multiple of 16");
+    for (int gt = 0; gt < Nd / 16; ++gt)
+      for (int b = 0; b < nb; ++b)
+        for (int i = 0; i < 16; ++i)
+          dst[((int64_t)gt * nb + b) * 16 + i] = src[gt * 16 + i + (int64_t)b * Nd];
+  }
+  static void pack_r16(const int Nd, const int nb, const T* src, T* dst) {
+    pack_c16(Nd, nb, src, dst);  // row-major [nb, Nd] is the same bytes
+  }
+  static void unpack_c16(const int Nd, const int nb, const T* src, T* dst) {
+    skgemm::require(Nd >= 0 && nb >= 0 && Nd % 16 == 0, "unpack_c16: Nd must be a multiple of 16");
+    for (int gt = 0; gt < Nd / 16; ++gt)
+      for (int b = 0; b < nb; ++b)
+        for (int i = 0; i < 16; ++i)
+          dst[gt * 16 + i + (int64_t)b * Nd] = src[((int64_t)gt * nb + b) * 16 + i];
+  }
+  static void unpack_r16(const int Nd, const int nb, const T* src, T* dst) {
+    unpack_c16(Nd, nb, src, dst);
+  }
+  static void band_to_grid_tile(const int Nd, const int nb, const T* src, T* dst) {
+    skgemm::require(Nd >= 0 && nb >= 0 && Nd % 16 == 0 && nb % 16 == 0,
+                    "band_to_grid_tile: Nd and nb must be multiples of 16");
+    for (int gt = 0; gt < Nd / 16; ++gt)
+      for (int b = 0; b < nb; ++b)
+        for (int i = 0; i < 16; ++i)
+          dst[((int64_t)gt * nb + b) * 16 + i] =
+              src[((int64_t)(b / 16) * Nd + gt * 16 + i) * 16 + b % 16];
+  }
+  static void grid_to_band_tile(const int Nd, const int nb, const T* src, T* dst) {
+    skgemm::require(Nd >= 0 && nb >= 0 && Nd % 16 == 0 && nb % 16 == 0,
+                    "grid_to_band_tile: Nd and nb must be multiples of 16");
+    for (int bt = 0; bt < nb / 16; ++bt)
+      for (int g = 0; g < Nd; ++g)
+        for (int i = 0; i < 16; ++i)
+          dst[((int64_t)bt * Nd + g) * 16 + i] =
+              src[((int64_t)(g / 16) * nb + bt * 16 + i) * 16 + g % 16];
+  }
+};
