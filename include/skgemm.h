@@ -249,6 +249,34 @@ int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src_band,
 int skgemm_grid_to_band_dev(int64_t Nd, int64_t nb, const double* src_grid,
                             double* dst_band, void* stream);
 
+/* ----------------------------------------------- H Psi producer (stencil) */
+/* The 6th-order finite-difference stencil of the kinetic part of H on
+ * extended (halo-padded) band-packed Psi: calc_laplacian_extended_packed_16to32
+ * (out_tile 32: the 32-band-packed B operand of skgemm_dgemm_packed, so that
+ * Hs = Psi^T (H Psi) follows on the device) and _16to16 (out_tile 16),
+ * include/stencil_extended_packed.hpp:47-181, :276-. Grid point
+ * g = i + j*ni + k*ni*nj, extended index g_ex = (i+FDn) + (j+FDn)*ni_ex +
+ * (k+FDn)*ni_ex*nj_ex with ni_ex = ni + 2*FDn (likewise nj_ex, nk_ex):
+ *   out[g, b] = ext[g_ex, b]*(A_diag[g] + coef_0)
+ *             + sum_{r=1..FDn} coef_x[r]*(ext[g_ex+r, b] + ext[g_ex-r, b])
+ *             + the same along y (stride ni_ex) and z (stride ni_ex*nj_ex),
+ * in the reference's SVE operation order (the results equal it bit for bit).
+ * psi_ext16: [ceil(nb/16)][ni_ex*nj_ex*nk_ex][16]; A_diag: [ni*nj*nk];
+ * coef_x/y/z: host arrays of FDn + 1 doubles (entry 0 unused); out:
+ * [ceil(nb/T)][ni*nj*nk][T], T = out_tile, lanes b >= nb left untouched.
+ * FDn must be 6 (the reference's kernels); other radii return
+ * SKGEMM_ERR_UNSUPPORTED. */
+int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                           const double* psi_ext16, const double* A_diag,
+                           const double* coef_x, const double* coef_y, const double* coef_z,
+                           double coef_0, double* out, int out_tile, void* stream);
+/* Single-rank periodic extension of band-packed Psi [ceil(nb/16)][ni*nj*nk][16]
+ * into that extended array: the interior copy (copy_interior_to_extended_packed,
+ * include/halo_packed.hpp:93-124) and the no-MPI periodic wrap (:350-393).
+ * FDn <= ni, nj, nk. */
+int skgemm_halo_periodic_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                             const double* psi_local16, double* psi_ext16, void* stream);
+
 /* ------------------------------------------------------ batched (grouped) */
 /* Many independent GEMM / SYRK / rotation problems of uneven sizes (k-points,
  * spin blocks) in ONE persistent Stream-K launch: the MAC-loop iterations of

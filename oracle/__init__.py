@@ -60,9 +60,13 @@ def lib() -> ctypes.CDLL:
                                           ctypes.c_double, ctypes.c_int]
         L.oracle_pack.argtypes = [_i64, _i64, _f64p, _i64, _i64, ctypes.c_int, _f64p]
         L.oracle_init_A_packed_rand.argtypes = [_i64, _i64, _f64p, ctypes.c_int]
+        L.oracle_stencil_ext.argtypes = [_i64, _i64, _i64, _i64, ctypes.c_int, _f64p, _f64p,
+                                         _f64p, _f64p, _f64p, ctypes.c_double, _f64p,
+                                         ctypes.c_int, ctypes.c_int]
+        L.oracle_halo_periodic.argtypes = [_i64, _i64, _i64, _i64, ctypes.c_int, _f64p, _f64p]
         for f in ("oracle_gemm_naive", "oracle_syrk_naive", "oracle_rot_naive",
                   "oracle_dot2_gemm", "oracle_dot2_sampled", "oracle_pack",
-                  "oracle_init_A_packed_rand"):
+                  "oracle_init_A_packed_rand", "oracle_stencil_ext", "oracle_halo_periodic"):
             getattr(L, f).restype = None
         _lib = L
     return _lib
@@ -80,7 +84,7 @@ def ref(name: str) -> ctypes.CDLL:
 
 def have_ref() -> bool:
     return all(os.path.exists(os.path.join(REF_DIR, f"libref_{n}.so"))
-               for n in ("gemm_opt", "gemm_crsp", "sme_syrk", "syrk_crsp", "trp_3d"))
+               for n in ("gemm_opt", "gemm_crsp", "sme_syrk", "syrk_crsp", "trp_3d", "stencil"))
 
 
 def ptr(a: np.ndarray):
@@ -142,6 +146,45 @@ def rot_naive(A_grid: np.ndarray, Q: np.ndarray, Nd, nb, threads: int = 1) -> np
     D = np.zeros(Nd * nb)
     lib().oracle_rot_naive(Nd, nb, ptr(A_grid), ptr(Q), ptr(D), threads)
     return D
+
+
+def ext_size(ni, nj, nk, nb, FDn=6):
+    """Doubles in an extended band-packed array [ceil(nb/16)][K_ex][16]."""
+    return (nb + 15) // 16 * (ni + 2 * FDn) * (nj + 2 * FDn) * (nk + 2 * FDn) * 16
+
+
+def stencil_ext(ext, A, ni, nj, nk, nb, cx, cy, cz, c0, out_tile=32, FDn=6, threads=1):
+    """H Psi from extended band-packed Psi in the reference SVE kernels' order
+    (stencil_extended_packed.hpp:47-181): [ceil(nb/T)][K][T] doubles."""
+    K = ni * nj * nk
+    out = np.zeros((nb + out_tile - 1) // out_tile * K * out_tile)
+    lib().oracle_stencil_ext(ni, nj, nk, nb, FDn, ptr(ext), ptr(A), ptr(np.asarray(cx, float)),
+                             ptr(np.asarray(cy, float)), ptr(np.asarray(cz, float)), c0,
+                             ptr(out), out_tile, threads)
+    return out
+
+
+def stencil_naive(S_ex, A, ni, nj, nk, nb, cx, cy, cz, c0, FDn=6):
+    """stencil_extended_test.cpp:200-236 restated with numpy: S_ex[b][k_ex][j_ex][i_ex]
+    extended unpacked input, result [b][k][j][i]; x, then y, then z sums (not
+    fused), the test's naive reference."""
+    c = (slice(FDn, FDn + nk), slice(FDn, FDn + nj), slice(FDn, FDn + ni))
+    res = S_ex[(slice(None),) + c] * (A.reshape(nk, nj, ni) + c0)
+    for ax, coef in ((3, cx), (2, cy), (1, cz)):
+        for r in range(1, FDn + 1):
+            sp = [slice(None)] + list(c)
+            sm = [slice(None)] + list(c)
+            sp[ax] = slice(c[ax - 1].start + r, c[ax - 1].stop + r)
+            sm[ax] = slice(c[ax - 1].start - r, c[ax - 1].stop - r)
+            res = res + coef[r] * (S_ex[tuple(sp)] + S_ex[tuple(sm)])
+    return res
+
+
+def halo_periodic(local, ni, nj, nk, nb, FDn=6):
+    """Single-rank periodic extension of band-packed Psi (halo_packed.hpp:93-124, :350-393)."""
+    ext = np.zeros(ext_size(ni, nj, nk, nb, FDn))
+    lib().oracle_halo_periodic(ni, nj, nk, nb, FDn, ptr(local), ptr(ext))
+    return ext
 
 
 def dot2_matmul(X: np.ndarray, Y: np.ndarray, alpha=1.0, gamma=0.0) -> np.ndarray:

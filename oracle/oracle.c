@@ -135,3 +135,44 @@ void oracle_init_A_packed_rand(int64_t K, int64_t M, double* A, int seed) {
         A[(tm * K + k) * 16 + ml] = m < M ? (double)(rand() % 100) / 100.0 : 0.0;
       }
 }
+
+/* ------------------------------------------------------------- stencil */
+void oracle_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                        const double* ext, const double* A, const double* cx, const double* cy,
+                        const double* cz, double c0, double* out, int out_tile, int nthreads) {
+  const int64_t K = ni * nj * nk;
+  const int64_t ni_ex = ni + 2 * FDn, nj_ex = nj + 2 * FDn, nk_ex = nk + 2 * FDn;
+  const int64_t K_ex = ni_ex * nj_ex * nk_ex;
+  const int64_t sj = ni_ex, sk = ni_ex * nj_ex;
+#pragma omp parallel for schedule(static) num_threads(clamp_threads(nthreads))
+  for (int64_t g = 0; g < K; ++g) {
+    const int64_t i = g % ni, j = (g / ni) % nj, k = g / (ni * nj);
+    const int64_t gx = (i + FDn) + (j + FDn) * sj + (k + FDn) * sk;
+    const double a = A[g] + c0;
+    for (int64_t b = 0; b < nb; ++b) {
+      const double* s = ext + (b / 16) * K_ex * 16 + b % 16;
+      double res = s[gx * 16] * a;
+      for (int r = 1; r <= FDn; ++r) {
+        res = fma(s[(gx + r) * 16] + s[(gx - r) * 16], cx[r], res);
+        res = fma(s[(gx + r * sj) * 16] + s[(gx - r * sj) * 16], cy[r], res);
+        res = fma(s[(gx + r * sk) * 16] + s[(gx - r * sk) * 16], cz[r], res);
+      }
+      out[((b / out_tile) * K + g) * out_tile + b % out_tile] = res;
+    }
+  }
+}
+
+static inline int64_t wrap(int64_t x, int64_t n) { return ((x % n) + n) % n; }
+
+void oracle_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                          const double* local, double* ext) {
+  const int64_t K = ni * nj * nk;
+  const int64_t ni_ex = ni + 2 * FDn, nj_ex = nj + 2 * FDn, nk_ex = nk + 2 * FDn;
+  const int64_t K_ex = ni_ex * nj_ex * nk_ex, tiles = (nb + 15) / 16;
+  for (int64_t t = 0; t < tiles; ++t)
+    for (int64_t gx = 0; gx < K_ex; ++gx) {
+      const int64_t ix = gx % ni_ex, jx = (gx / ni_ex) % nj_ex, kx = gx / (ni_ex * nj_ex);
+      const int64_t g = wrap(ix - FDn, ni) + wrap(jx - FDn, nj) * ni + wrap(kx - FDn, nk) * ni * nj;
+      for (int l = 0; l < 16; ++l) ext[(t * K_ex + gx) * 16 + l] = local[(t * K + g) * 16 + l];
+    }
+}

@@ -67,6 +67,28 @@ void oracle_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, 
  * in [tm][k][ml] order, zero for padding rows (host C library rand()). */
 void oracle_init_A_packed_rand(int64_t K, int64_t M, double* A_packed, int seed);
 
+/* H Psi stencil on extended (halo-padded) band-packed Psi, restating
+ * calc_laplacian_extended_packed_16to32 / _16to16
+ * (include/stencil_extended_packed.hpp:47-181, :276-): grid point
+ * g = i + j*ni + k*ni*nj, g_ex its extended index (offset FDn per axis),
+ * per band b < nb:
+ *   res = ext[g_ex] * (A[g] + c0);
+ *   for r = 1..FDn: res = fma(ext[g_ex+r] + ext[g_ex-r], cx[r], res),
+ *                   then the same along y (stride ni_ex) and z (ni_ex*nj_ex),
+ * the SVE kernels' operation order (x, y, z for each r; svmla is fused).
+ * ext: [ceil(nb/16)][K_ex][16]; out: [ceil(nb/T)][K][T], T = out_tile (16
+ * or 32); lanes b >= nb of out are left untouched. */
+void oracle_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                        const double* ext, const double* A, const double* cx, const double* cy,
+                        const double* cz, double c0, double* out, int out_tile, int nthreads);
+
+/* Single-rank periodic halo: copy_interior_to_extended_packed
+ * (include/halo_packed.hpp:93-124) plus the periodic wrap of the no-MPI path
+ * (:350-393): ext[(t*K_ex + g_ex)*16 + l] = local[(t*K + g)*16 + l] with
+ * g = ((i_ex - FDn) mod ni) + ((j_ex - FDn) mod nj)*ni + ((k_ex - FDn) mod nk)*ni*nj. */
+void oracle_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                          const double* local, double* ext);
+
 #ifdef __cplusplus
 }
 #endif

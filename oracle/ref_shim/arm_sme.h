@@ -166,6 +166,26 @@ inline svfloat64_t svmla_f64_x(svbool_t pg, svfloat64_t acc, svfloat64_t a,
     r.v[i] = std::fma(a.v[i], b.v[i], acc.v[i]);
   return r;
 }
+// The overloaded (type-generic) names of the same operations.
+inline svfloat64_t svadd_x(svbool_t pg, svfloat64_t a, svfloat64_t b) {
+  return svadd_f64_x(pg, a, b);
+}
+inline svfloat64_t svmul_x(svbool_t pg, svfloat64_t a, svfloat64_t b) {
+  (void)pg;
+  svfloat64_t r;
+  for (int i = 0; i < skgemm_sme_emul::kLanesD; ++i) r.v[i] = a.v[i] * b.v[i];
+  return r;
+}
+inline svfloat64_t svmla_x(svbool_t pg, svfloat64_t acc, svfloat64_t a, svfloat64_t b) {
+  return svmla_f64_x(pg, acc, a, b);
+}
+// WHILELT: 64-bit lane i active while a + i < b.
+inline svbool_t svwhilelt_b64(uint64_t a, uint64_t b) {
+  svbool_t r;
+  std::memset(r.p, 0, sizeof(r.p));
+  for (int i = 0; i < skgemm_sme_emul::kLanesD; ++i) r.p[i * 8] = (a + (uint64_t)i < b) ? 1 : 0;
+  return r;
+}
 
 // ---------------------------------------------------------------- ZA (f64)
 inline void svzero_za() {

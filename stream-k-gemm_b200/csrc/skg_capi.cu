@@ -874,6 +874,26 @@ SKG_EXPORT int skgemm_unpack_r16_dev(int64_t Nd, int64_t nb, const double* src, 
   return skgemm_unpack_c16_dev(Nd, nb, src, dst, stream);
 }
 
+SKG_EXPORT int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                                      const double* psi_ext16, const double* A_diag,
+                                      const double* coef_x, const double* coef_y,
+                                      const double* coef_z, double coef_0, double* out,
+                                      int out_tile, void* stream) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  return launch_stencil_ext(ni, nj, nk, nb, FDn, psi_ext16, A_diag, coef_x, coef_y, coef_z,
+                            coef_0, out, out_tile, dev->num_sms,
+                            reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT int skgemm_halo_periodic_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                                        const double* psi_local16, double* psi_ext16,
+                                        void* stream) {
+  return launch_halo_periodic(ni, nj, nk, nb, FDn, psi_local16, psi_ext16,
+                              reinterpret_cast<cudaStream_t>(stream));
+}
+
 SKG_EXPORT int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                        void* stream) {
   return launch_band_to_grid(Nd, nb, src, dst, reinterpret_cast<cudaStream_t>(stream));

@@ -129,6 +129,14 @@ int launch_pack(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk, i
                 double* Xp, cudaStream_t s);
 int launch_unpack(int64_t R, int64_t K, const double* Xp, int T, double* X, int64_t sr,
                   int64_t sk, cudaStream_t s);
+// H Psi stencil on extended band-packed Psi (skg_stencil.cu) and the
+// single-rank periodic halo that builds that extended array.
+int launch_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                       const double* ext, const double* A, const double* cx, const double* cy,
+                       const double* cz, double c0, double* out, int out_tile, int num_sms,
+                       cudaStream_t s);
+int launch_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
+                         const double* local, double* ext, cudaStream_t s);
 int launch_band_to_grid(int64_t Nd, int64_t nb, const double* src, double* dst,
                         cudaStream_t s);
 int launch_grid_to_band(int64_t Nd, int64_t nb, const double* src, double* dst,

@@ -136,6 +136,11 @@ _SIGS = {
     "skgemm_pack_r16_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_unpack_c16_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_unpack_r16_dev": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_stencil_ext_dev": [_i64, _i64, _i64, _i64, ctypes.c_int, _vp, _vp,
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), ctypes.c_double, _vp,
+                               ctypes.c_int, _vp],
+    "skgemm_halo_periodic_dev": [_i64, _i64, _i64, _i64, ctypes.c_int, _vp, _vp, _vp],
     "skgemm_band_to_grid_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_grid_to_band_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_plan_create": [ctypes.POINTER(BatchItem), ctypes.c_int,
@@ -368,6 +373,26 @@ def unpack_c16_dev(Nd, nb, src, dst, stream=None):
 def unpack_r16_dev(Nd, nb, src, dst, stream=None):
     """linalg_unpack_r16_f64 (sme_pack.hpp:328): grid-packed -> row-major [nb, Nd]."""
     _check(lib().skgemm_unpack_r16_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
+
+
+def _coef(c):
+    a = (ctypes.c_double * len(c))(*[float(x) for x in c])
+    return a
+
+
+def stencil_ext_dev(ni, nj, nk, nb, ext16, A_diag, coef_x, coef_y, coef_z, coef_0, out,
+                    out_tile=32, FDn=6, stream=None):
+    """H Psi = stencil(extended band-packed Psi) into 32- (or 16-) band-packed
+    out (calc_laplacian_extended_packed_16to32 / _16to16)."""
+    _check(lib().skgemm_stencil_ext_dev(ni, nj, nk, nb, FDn, _dptr(ext16), _dptr(A_diag),
+                                        _coef(coef_x), _coef(coef_y), _coef(coef_z),
+                                        float(coef_0), _dptr(out), out_tile, _stream(stream)))
+
+
+def halo_periodic_dev(ni, nj, nk, nb, local16, ext16, FDn=6, stream=None):
+    """Single-rank periodic extension of band-packed Psi (halo_packed.hpp)."""
+    _check(lib().skgemm_halo_periodic_dev(ni, nj, nk, nb, FDn, _dptr(local16), _dptr(ext16),
+                                          _stream(stream)))
 
 
 def band_to_grid_dev(Nd, nb, src, dst, stream=None):

@@ -9,6 +9,8 @@ Kernels and workloads (inputs larger than L2 where the kernel is HBM-bound):
   unpack_kernel<16>                  grid-packed -> column-major (linalg_unpack_c16)
   fp64_streamk_kernel64_ak,          the rotation on band-packed Psi, 110592 x 512,
   norm_partials / convert_tma (KM)   native and Ozaki (K-major operand reads)
+  halo_periodic_kernel,              H Psi on the 48^3 grid (= 110592 points) x 512:
+  stencil_ext_kernel<32>             periodic halo, then the 6th-order stencil
   k0_kernel                          GEMM with K = 0 (D = gamma), 4096 x 4096
   sum_parts_kernel                   the host GEMM's k-chunk combine, 2048 x 2048 x 32768
   noalloc_fill_kernel                the allocation-free GEMM with K = 0
@@ -59,6 +61,20 @@ def main() -> None:
         skgemm.drot_band_dev(nd, nb, band16, q, rot_b, precision=prec)
         skgemm.stream_status()
         assert torch.equal(rot_b, rot_g)
+
+    # H Psi producer: periodic halo of band-packed Psi (48^3 grid points, the
+    # nd above), then the 6th-order stencil into the GEMM's 32-band-packed B.
+    n = 48
+    assert n ** 3 == nd
+    cx = [0.0, -1.0 / 12, 2.0 / 3, -2.5, 8.0 / 3, -1.0 / 4, 1.0 / 30]
+    ext = torch.empty((nb + 15) // 16 * (n + 12) ** 3 * 16, dtype=torch.float64, device=dev)
+    a_diag = torch.rand(nd, generator=g, dtype=torch.float64, device=dev)
+    hpsi = torch.empty_like(band16)
+    skgemm.halo_periodic_dev(n, n, n, nb, band16, ext)
+    skgemm.stencil_ext_dev(n, n, n, nb, ext, a_diag, cx, cx, cx, -0.5, hpsi, 32)
+    skgemm.stream_status()
+    assert bool(torch.isfinite(hpsi).all())
+    del ext, hpsi
 
     # K = 0 epilogues.
     n = 4096
