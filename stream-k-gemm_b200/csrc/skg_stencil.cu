@@ -100,7 +100,8 @@ __global__ void __launch_bounds__(256, 2) stencil_ext_kernel(
 }
 
 // One CTA per extended row (tile t, k_ex, j_ex): ext[(t K_ex + g_ex) 16 + l] =
-// local[(t K + g) 16 + l], g the periodic image of g_ex's interior point.
+// local[(t K + g) 16 + l], g the periodic image of g_ex's interior point;
+// 16-byte lane pairs (the copy is bound by its index arithmetic).
 __global__ void __launch_bounds__(256) halo_periodic_kernel(int ni, int nj, int nk, int FDn,
                                                             const double* __restrict__ local,
                                                             double* __restrict__ ext) {
@@ -111,12 +112,13 @@ __global__ void __launch_bounds__(256) halo_periodic_kernel(int ni, int nj, int 
   jl += jl < 0 ? nj : (jl >= nj ? -nj : 0);
   kl += kl < 0 ? nk : (kl >= nk ? -nk : 0);
   const int64_t K = (int64_t)ni * nj * nk;
-  const double* src = local + (t * K + (int64_t)jl * ni + (int64_t)kl * ni * nj) * 16;
-  double* dst = ext + row * nix * 16;
-  for (int64_t e = threadIdx.x; e < nix * 16; e += blockDim.x) {
-    int il = (int)(e >> 4) - FDn;
+  const double2* src = reinterpret_cast<const double2*>(local) +
+                       (t * K + (int64_t)jl * ni + (int64_t)kl * ni * nj) * 8;
+  double2* dst = reinterpret_cast<double2*>(ext) + row * nix * 8;
+  for (int e = threadIdx.x; e < (int)nix * 8; e += blockDim.x) {
+    int il = (e >> 3) - FDn;
     il += il < 0 ? ni : (il >= ni ? -ni : 0);
-    dst[e] = src[(int64_t)il * 16 + (e & 15)];
+    dst[e] = src[il * 8 + (e & 7)];
   }
 }
 
@@ -170,6 +172,8 @@ int launch_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn
   if (FDn > ni || FDn > nj || FDn > nk)
     return fail(SKGEMM_ERR_INVALID_ARG, "periodic halo wider than the domain");
   if (!local || !ext) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  if ((reinterpret_cast<uintptr_t>(local) | reinterpret_cast<uintptr_t>(ext)) & 15)
+    return fail(SKGEMM_ERR_INVALID_ARG, "halo arrays must be 16-byte aligned");
   if (ni > (1 << 20) || nj > (1 << 20) || nk > (1 << 20))
     return fail(SKGEMM_ERR_INVALID_ARG, "grid too large");
   const int64_t rows = ((nb + 15) / 16) * (nk + 2 * FDn) * (nj + 2 * FDn);
