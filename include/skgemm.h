@@ -277,6 +277,31 @@ int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int F
 int skgemm_halo_periodic_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                              const double* psi_local16, double* psi_ext16, void* stream);
 
+/* ------------------------------------------ nonlocal projector (V_nloc) */
+/* The nonlocal part of H (Hamiltonian::nloc_project_vectors_packed and
+ * _16to16, include/nloc_packed_opt2.hpp:226-445) on the device. A handle
+ * holds the projector set, the reference's Effective_potential_nloc:
+ * projector p has nrow[p] grid rows (its entries of `index`, concatenated in
+ * projector order, each < K), coefficients chi (column-major nrow x ncol,
+ * concatenated), gamma (ncol values, concatenated), atom index atom[p] and a
+ * coefficient block at column offsets[p] (offsets[P] = total columns;
+ * projectors sharing a block — the periodic images of one atom — accumulate
+ * into it and must have the same ncol). Host arrays, copied at creation. */
+typedef struct skgemm_nloc* skgemm_nloc_t;
+int skgemm_nloc_create(int64_t P, const uint32_t* nrow, const uint32_t* ncol,
+                       const int32_t* atom, const uint32_t* offsets, const uint32_t* index,
+                       const double* chi, const double* gamma, int64_t K, skgemm_nloc_t* out);
+/* out += V_nloc psi: psi 16-band-packed [ceil(nb/16)][K][16]; out
+ * 32-band-packed (out_tile 32: H Psi, the GEMM's B operand) or 16-band-packed
+ * (out_tile 16). Device pointers; dv the grid volume element. Per projector:
+ * gather, C += dv chi^T psi; gamma scaling on every change of atom index in
+ * projector order; scatter-add of chi C. The single-rank all-reduce is the
+ * identity. Results equal the reference's bit for bit. A handle's calls must
+ * not run concurrently on two streams (they share its scratch). */
+int skgemm_nloc_apply_dev(skgemm_nloc_t h, int64_t nb, double dv, const double* psi16,
+                          double* out, int out_tile, void* stream);
+void skgemm_nloc_destroy(skgemm_nloc_t h);
+
 /* ------------------------------------------------------ batched (grouped) */
 /* Many independent GEMM / SYRK / rotation problems of uneven sizes (k-points,
  * spin blocks) in ONE persistent Stream-K launch: the MAC-loop iterations of

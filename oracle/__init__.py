@@ -64,9 +64,16 @@ def lib() -> ctypes.CDLL:
                                          _f64p, _f64p, _f64p, ctypes.c_double, _f64p,
                                          ctypes.c_int, ctypes.c_int]
         L.oracle_halo_periodic.argtypes = [_i64, _i64, _i64, _i64, ctypes.c_int, _f64p, _f64p]
+        _u32p = ctypes.POINTER(ctypes.c_uint32)
+        _i32p = ctypes.POINTER(ctypes.c_int32)
+        _i64p = ctypes.POINTER(ctypes.c_int64)
+        L.oracle_nloc_project.argtypes = [_i64, _u32p, _u32p, _i32p, _u32p, _u32p, _i64p, _f64p,
+                                          _i64p, _f64p, _i64p, _i64, _i64, ctypes.c_double,
+                                          _f64p, _f64p, ctypes.c_int]
         for f in ("oracle_gemm_naive", "oracle_syrk_naive", "oracle_rot_naive",
                   "oracle_dot2_gemm", "oracle_dot2_sampled", "oracle_pack",
-                  "oracle_init_A_packed_rand", "oracle_stencil_ext", "oracle_halo_periodic"):
+                  "oracle_init_A_packed_rand", "oracle_stencil_ext", "oracle_halo_periodic",
+                  "oracle_nloc_project"):
             getattr(L, f).restype = None
         _lib = L
     return _lib
@@ -84,7 +91,8 @@ def ref(name: str) -> ctypes.CDLL:
 
 def have_ref() -> bool:
     return all(os.path.exists(os.path.join(REF_DIR, f"libref_{n}.so"))
-               for n in ("gemm_opt", "gemm_crsp", "sme_syrk", "syrk_crsp", "trp_3d", "stencil"))
+               for n in ("gemm_opt", "gemm_crsp", "sme_syrk", "syrk_crsp", "trp_3d", "stencil",
+                         "nloc"))
 
 
 def ptr(a: np.ndarray):
@@ -185,6 +193,69 @@ def halo_periodic(local, ni, nj, nk, nb, FDn=6):
     ext = np.zeros(ext_size(ni, nj, nk, nb, FDn))
     lib().oracle_halo_periodic(ni, nj, nk, nb, FDn, ptr(local), ptr(ext))
     return ext
+
+
+class NlocProjectors:
+    """A flattened nonlocal projector set: projector p has nrow[p] grid rows
+    index[row_off[p]:], coefficients chi[chi_off[p]:] (column-major nrow x
+    ncol), gamma[gam_off[p]:] (ncol), atom index atom[p] and its coefficient
+    block at offsets[p] (offsets[P] = total columns) — the fields of the
+    reference's Nloc_projector / Effective_potential_nloc."""
+
+    def __init__(self, nrow, ncol, atom, offsets, index, chi, gamma):
+        self.nrow = np.ascontiguousarray(nrow, dtype=np.uint32)
+        self.ncol = np.ascontiguousarray(ncol, dtype=np.uint32)
+        self.atom = np.ascontiguousarray(atom, dtype=np.int32)
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        self.index = np.ascontiguousarray(index, dtype=np.uint32)
+        self.chi = np.ascontiguousarray(chi, dtype=np.float64)
+        self.gamma = np.ascontiguousarray(gamma, dtype=np.float64)
+        P = len(self.nrow)
+        self.row_off = np.concatenate([[0], np.cumsum(self.nrow.astype(np.int64))])[:P]
+        self.chi_off = np.concatenate(
+            [[0], np.cumsum(self.nrow.astype(np.int64) * self.ncol)])[:P].astype(np.int64)
+        self.gam_off = np.concatenate([[0], np.cumsum(self.ncol.astype(np.int64))])[:P]
+        self.row_off = np.ascontiguousarray(self.row_off, dtype=np.int64)
+        self.gam_off = np.ascontiguousarray(self.gam_off, dtype=np.int64)
+
+    def args(self):
+        c = ctypes
+        return (len(self.nrow), self.nrow.ctypes.data_as(c.POINTER(c.c_uint32)),
+                self.ncol.ctypes.data_as(c.POINTER(c.c_uint32)),
+                self.atom.ctypes.data_as(c.POINTER(c.c_int32)),
+                self.offsets.ctypes.data_as(c.POINTER(c.c_uint32)),
+                self.index.ctypes.data_as(c.POINTER(c.c_uint32)),
+                self.row_off.ctypes.data_as(c.POINTER(c.c_int64)), ptr(self.chi),
+                self.chi_off.ctypes.data_as(c.POINTER(c.c_int64)), ptr(self.gamma),
+                self.gam_off.ctypes.data_as(c.POINTER(c.c_int64)))
+
+
+def nloc_random(K, nrow, ncol, P, seed, images=1):
+    """P atoms, each with `images` projectors that share its coefficient block
+    (periodic images), unique grid rows per projector, chi ~ U[-1, 1), gamma ~
+    0.5 U[-1, 1) (as nloc_packed_opt2_test.cpp:242-269 draws them)."""
+    rng = np.random.default_rng(seed)
+    nr, nc, at, off, idx, chi, gam = [], [], [], [], [], [], []
+    col = 0
+    for a in range(P):
+        for _ in range(images):
+            nr.append(nrow)
+            nc.append(ncol)
+            at.append(a + 1)
+            off.append(col)
+            idx.append(rng.permutation(K)[:nrow])
+            chi.append(rng.uniform(-1, 1, nrow * ncol))
+            gam.append(rng.uniform(-1, 1, ncol) * 0.5)
+        col += ncol
+    off.append(col)
+    return NlocProjectors(nr, nc, at, off, np.concatenate(idx), np.concatenate(chi),
+                          np.concatenate(gam))
+
+
+def nloc_project(pj: NlocProjectors, psi16, nb, K, dv, out, out_tile=32):
+    """out += V_nloc psi in the reference's order (oracle_nloc_project)."""
+    lib().oracle_nloc_project(*pj.args(), nb, K, dv, ptr(psi16), ptr(out), out_tile)
+    return out
 
 
 def dot2_matmul(X: np.ndarray, Y: np.ndarray, alpha=1.0, gamma=0.0) -> np.ndarray:

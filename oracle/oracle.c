@@ -176,3 +176,59 @@ void oracle_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FD
       for (int l = 0; l < 16; ++l) ext[(t * K_ex + gx) * 16 + l] = local[(t * K + g) * 16 + l];
     }
 }
+
+/* ----------------------------------------------------------- projector */
+/* Rounding as the reference compiles (g++ contracts a*b + c in C++ by
+ * default; determined against the in-place build): the forward dot products
+ * unfused, the block update fma(dv, sum, C), the backward products fused. */
+void oracle_nloc_project(int64_t P, const uint32_t* nrow, const uint32_t* ncol,
+                         const int32_t* atom, const uint32_t* offsets, const uint32_t* index,
+                         const int64_t* row_off, const double* chi, const int64_t* chi_off,
+                         const double* gamma, const int64_t* gam_off, int64_t nb, int64_t K,
+                         double dv, const double* psi16, double* out, int out_tile) {
+  if (P <= 0 || offsets[P] == 0) return;
+  double* C = (double*)calloc((size_t)offsets[P] * nb, sizeof(double));
+  for (int64_t p = 0; p < P; ++p) { /* gather + C += dv chi^T filtered */
+    const int64_t nr = nrow[p], nc = ncol[p];
+    if (nr == 0 || nc == 0) continue;
+    const uint32_t* idx = index + row_off[p];
+    const double* X = chi + chi_off[p];
+    double* Cb = C + (int64_t)offsets[p] * nb;
+    for (int64_t n = 0; n < nb; ++n)
+      for (int64_t m = 0; m < nc; ++m) {
+        double sum = 0.0;
+        for (int64_t k = 0; k < nr; ++k)
+          sum = sum + X[k + m * nr] * psi16[((n / 16) * K + idx[k]) * 16 + n % 16];
+        Cb[m + n * nc] = fma(dv, sum, 1.0 * Cb[m + n * nc]);
+      }
+  }
+  int32_t a = atom[0] - 1; /* gamma on each change of atom index */
+  for (int64_t p = 0; p < P; ++p) {
+    if (a == atom[p]) continue;
+    a = atom[p];
+    double* Cb = C + (int64_t)offsets[p] * nb;
+    const double* gm = gamma + gam_off[p];
+    for (int64_t b = 0; b < nb; ++b)
+      for (int64_t j = 0; j < ncol[p]; ++j) Cb[j + b * ncol[p]] *= gm[j];
+  }
+  for (int64_t p = 0; p < P; ++p) { /* temp = chi C, scatter-add */
+    const int64_t nr = nrow[p], nc = ncol[p];
+    if (nr == 0 || nc == 0) continue;
+    const uint32_t* idx = index + row_off[p];
+    const double* X = chi + chi_off[p];
+    const double* Cb = C + (int64_t)offsets[p] * nb;
+    double* t = (double*)malloc((size_t)nr * nb * sizeof(double));
+    for (int64_t n = 0; n < nb; ++n) {
+      for (int64_t m = 0; m < nr; ++m) t[m + n * nr] = 0.0;
+      for (int64_t k = 0; k < nc; ++k) {
+        const double bv = 1.0 * Cb[k + n * nc];
+        for (int64_t m = 0; m < nr; ++m) t[m + n * nr] = fma(X[m + k * nr], bv, t[m + n * nr]);
+      }
+    }
+    for (int64_t b = 0; b < nb; ++b)
+      for (int64_t r = 0; r < nr; ++r)
+        out[((b / out_tile) * K + idx[r]) * out_tile + b % out_tile] += t[r + b * nr];
+    free(t);
+  }
+  free(C);
+}

@@ -89,6 +89,22 @@ void oracle_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
 void oracle_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                           const double* local, double* ext);
 
+/* Nonlocal projector, restating Hamiltonian::nloc_project_vectors_packed /
+ * _16to16 (include/nloc_packed_opt2.hpp:226-445, the sequential form) in its
+ * loop and rounding order, without fused multiply-adds: per projector p (rows
+ * index[row_off[p] ..], coefficients chi col-major nrow x ncol at chi_off[p],
+ * block at offsets[p]): C_p[j + b*ncol] = C_p + dv * sum_r chi[r + j*nrow] *
+ * psi(index[r], b) (gemm_aTb, :143-176); then, on every change of atom index
+ * in projector order, C_p *= gamma_p per column; then temp = chi * C_p (gemm_ab,
+ * :181-224) scatter-added into out[(b/T)*K + index[r]][b%T] (:85-135).
+ * Rounding of the reference as compiled (C++ contracts a*b + c): forward
+ * sums unfused, the block update fma(dv, sum, C), backward sums fused. */
+void oracle_nloc_project(int64_t P, const uint32_t* nrow, const uint32_t* ncol,
+                         const int32_t* atom, const uint32_t* offsets, const uint32_t* index,
+                         const int64_t* row_off, const double* chi, const int64_t* chi_off,
+                         const double* gamma, const int64_t* gam_off, int64_t nb, int64_t K,
+                         double dv, const double* psi16, double* out, int out_tile);
+
 #ifdef __cplusplus
 }
 #endif

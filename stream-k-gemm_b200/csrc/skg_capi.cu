@@ -894,6 +894,21 @@ SKG_EXPORT int skgemm_halo_periodic_dev(int64_t ni, int64_t nj, int64_t nk, int6
                               reinterpret_cast<cudaStream_t>(stream));
 }
 
+SKG_EXPORT int skgemm_nloc_create(int64_t P, const uint32_t* nrow, const uint32_t* ncol,
+                                  const int32_t* atom, const uint32_t* offsets,
+                                  const uint32_t* index, const double* chi, const double* gamma,
+                                  int64_t K, skgemm_nloc_t* out) {
+  return nloc_create(P, nrow, ncol, atom, offsets, index, chi, gamma, K, out);
+}
+
+SKG_EXPORT int skgemm_nloc_apply_dev(skgemm_nloc_t h, int64_t nb, double dv,
+                                     const double* psi16, double* out, int out_tile,
+                                     void* stream) {
+  return nloc_apply(h, nb, dv, psi16, out, out_tile, reinterpret_cast<cudaStream_t>(stream));
+}
+
+SKG_EXPORT void skgemm_nloc_destroy(skgemm_nloc_t h) { nloc_destroy(h); }
+
 SKG_EXPORT int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                        void* stream) {
   return launch_band_to_grid(Nd, nb, src, dst, reinterpret_cast<cudaStream_t>(stream));

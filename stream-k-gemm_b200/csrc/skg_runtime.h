@@ -137,6 +137,13 @@ int launch_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                        cudaStream_t s);
 int launch_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                          const double* local, double* ext, cudaStream_t s);
+// Nonlocal projector set on the device (skg_nloc.cu).
+int nloc_create(int64_t P, const uint32_t* nrow, const uint32_t* ncol, const int32_t* atom,
+                const uint32_t* offsets, const uint32_t* index, const double* chi,
+                const double* gamma, int64_t K, skgemm_nloc** out);
+int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, double* out,
+               int out_tile, cudaStream_t s);
+void nloc_destroy(skgemm_nloc* h);
 int launch_band_to_grid(int64_t Nd, int64_t nb, const double* src, double* dst,
                         cudaStream_t s);
 int launch_grid_to_band(int64_t Nd, int64_t nb, const double* src, double* dst,

@@ -141,6 +141,11 @@ _SIGS = {
                                ctypes.POINTER(ctypes.c_double), ctypes.c_double, _vp,
                                ctypes.c_int, _vp],
     "skgemm_halo_periodic_dev": [_i64, _i64, _i64, _i64, ctypes.c_int, _vp, _vp, _vp],
+    "skgemm_nloc_create": [_i64, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                           ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint32),
+                           ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_double), _i64, ctypes.POINTER(ctypes.c_void_p)],
+    "skgemm_nloc_apply_dev": [_vp, _i64, ctypes.c_double, _vp, _vp, ctypes.c_int, _vp],
     "skgemm_band_to_grid_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_grid_to_band_dev": [_i64, _i64, _vp, _vp, _vp],
     "skgemm_plan_create": [ctypes.POINTER(BatchItem), ctypes.c_int,
@@ -177,13 +182,16 @@ def lib() -> ctypes.CDLL:
         L.skgemm_last_error.restype = ctypes.c_char_p
         L.skgemm_last_error.argtypes = []
         L.skgemm_plan_destroy.restype = None
+        L.skgemm_nloc_destroy.restype = None
+        L.skgemm_nloc_destroy.argtypes = [ctypes.c_void_p]
         L.skgemm_plan_destroy.argtypes = [_vp]
         _lib = L
     return _lib
 
 
 def exported_symbols() -> list:
-    return ["skgemm_version", "skgemm_last_error", "skgemm_plan_destroy"] + list(_SIGS)
+    return ["skgemm_version", "skgemm_last_error", "skgemm_plan_destroy",
+            "skgemm_nloc_destroy"] + list(_SIGS)
 
 
 def version() -> str:
@@ -393,6 +401,43 @@ def halo_periodic_dev(ni, nj, nk, nb, local16, ext16, FDn=6, stream=None):
     """Single-rank periodic extension of band-packed Psi (halo_packed.hpp)."""
     _check(lib().skgemm_halo_periodic_dev(ni, nj, nk, nb, FDn, _dptr(local16), _dptr(ext16),
                                           _stream(stream)))
+
+
+class NlocProjector:
+    """A nonlocal projector set on the device (skgemm_nloc_create): the
+    reference's Effective_potential_nloc. Arrays as numpy (host); `apply`
+    adds V_nloc psi into out (16- or 32-band-packed, device tensors)."""
+
+    def __init__(self, nrow, ncol, atom, offsets, index, chi, gamma, K):
+        arr = lambda a, t: np.ascontiguousarray(a, dtype=t)
+        self._keep = [arr(nrow, np.uint32), arr(ncol, np.uint32), arr(atom, np.int32),
+                      arr(offsets, np.uint32), arr(index, np.uint32), arr(chi, np.float64),
+                      arr(gamma, np.float64)]
+        nr, nc, at, off, idx, ch, gm = self._keep
+        c = ctypes
+        h = c.c_void_p()
+        _check(lib().skgemm_nloc_create(
+            len(nr), nr.ctypes.data_as(c.POINTER(c.c_uint32)),
+            nc.ctypes.data_as(c.POINTER(c.c_uint32)), at.ctypes.data_as(c.POINTER(c.c_int32)),
+            off.ctypes.data_as(c.POINTER(c.c_uint32)), idx.ctypes.data_as(c.POINTER(c.c_uint32)),
+            ch.ctypes.data_as(c.POINTER(c.c_double)), gm.ctypes.data_as(c.POINTER(c.c_double)),
+            K, c.byref(h)))
+        self._h = h
+
+    def apply(self, nb, dv, psi16, out, out_tile=32, stream=None):
+        _check(lib().skgemm_nloc_apply_dev(self._h, nb, float(dv), _dptr(psi16), _dptr(out),
+                                           out_tile, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().skgemm_nloc_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def band_to_grid_dev(Nd, nb, src, dst, stream=None):

@@ -11,6 +11,8 @@ Kernels and workloads (inputs larger than L2 where the kernel is HBM-bound):
   norm_partials / convert_tma (KM)   native and Ozaki (K-major operand reads)
   halo_periodic_kernel,              H Psi on the 48^3 grid (= 110592 points) x 512:
   stencil_ext_kernel<32>             periodic halo, then the 6th-order stencil
+  nloc_forward / nloc_chi_c /        the nonlocal projector on the same Psi: 64 atoms
+  nloc_backward<32>                  x 2 periodic images, 800 rows x 16 columns each
   k0_kernel                          GEMM with K = 0 (D = gamma), 4096 x 4096
   sum_parts_kernel                   the host GEMM's k-chunk combine, 2048 x 2048 x 32768
   noalloc_fill_kernel                the allocation-free GEMM with K = 0
@@ -74,6 +76,20 @@ def main() -> None:
     skgemm.stencil_ext_dev(n, n, n, nb, ext, a_diag, cx, cx, cx, -0.5, hpsi, 32)
     skgemm.stream_status()
     assert bool(torch.isfinite(hpsi).all())
+
+    # Nonlocal projector: H Psi += V_nloc Psi (64 atoms x 2 images).
+    rng = np.random.default_rng(8)
+    atoms, images, nrow, ncol = 64, 2, 800, 16
+    nproj = atoms * images
+    proj = skgemm.NlocProjector(
+        np.full(nproj, nrow), np.full(nproj, ncol), np.repeat(np.arange(1, atoms + 1), images),
+        np.append(np.repeat(np.arange(atoms) * ncol, images), atoms * ncol),
+        np.concatenate([rng.permutation(nd)[:nrow] for _ in range(nproj)]),
+        rng.uniform(-1, 1, nproj * nrow * ncol), rng.uniform(-0.5, 0.5, nproj * ncol), nd)
+    proj.apply(nb, 0.01, band16, hpsi, 32)
+    skgemm.stream_status()
+    assert bool(torch.isfinite(hpsi).all())
+    proj.close()
     del ext, hpsi
 
     # K = 0 epilogues.
