@@ -64,18 +64,19 @@ namespace skg {
 namespace {
 
 // Forward CTA: (block q, 32 bands, 16 columns); thread (band bl = tid % 32,
-// column j = tid / 32). For each projector of the block, in order, the CTA
-// gathers 64 rows x 32 bands of psi into shared memory (all 512 threads
-// loading: many gathers in flight), then every thread adds its column's
+// columns 4 jq .. 4 jq + 3, jq = tid / 32). For each projector of the block,
+// in order, the CTA stages 64 gathered rows x 32 bands of psi and the
+// matching 64 rows x 16 columns of chi in shared memory (all 128 threads
+// loading: many gathers in flight), then every thread adds its four columns'
 // products over those rows in row order — the reference's order, so the
-// sums are exact to it — and folds the projector's sum into the block
-// coefficient with fma(dv, sum, C). The coefficients are stored
-// [column][band] (band fastest).
+// sums are exact to it — and folds each projector's sum into the block
+// coefficient with fma(dv, sum, C). Coefficients stored [column][band].
 constexpr int kNlocBands = 32;
 constexpr int kNlocCols = 16;
 constexpr int kNlocRows = 64;
+constexpr int kNlocThreads = kNlocBands * kNlocCols / 4;
 
-__global__ void __launch_bounds__(kNlocBands * kNlocCols) nloc_forward_kernel(
+__global__ void __launch_bounds__(kNlocThreads) nloc_forward_kernel(
     int64_t nb, int64_t K, double dv, const int64_t* __restrict__ blk,
     const int64_t* __restrict__ blk_end, const int32_t* __restrict__ blk_proj,
     const int64_t* __restrict__ blk_scale, const uint32_t* __restrict__ nrow,
@@ -84,21 +85,23 @@ __global__ void __launch_bounds__(kNlocBands * kNlocCols) nloc_forward_kernel(
     const double* __restrict__ gamma, const double* __restrict__ psi16,
     double* __restrict__ coef) {
   __shared__ double rows[kNlocRows][kNlocBands];
+  __shared__ double xs[kNlocCols][kNlocRows];
   const int64_t q = blockIdx.x;
   const int64_t b0 = (int64_t)blockIdx.y * kNlocBands;
+  const int64_t jb = (int64_t)blockIdx.z * kNlocCols;  // the CTA's first column
   const int bl = threadIdx.x % kNlocBands;
-  const int64_t j = (int64_t)blockIdx.z * kNlocCols + threadIdx.x / kNlocBands;
+  const int jq = threadIdx.x / kNlocBands;
   const int64_t col0 = blk[4 * q], nc = blk[4 * q + 1];
+  if (jb >= nc) return;  // the whole CTA past the block
+  const int ncc = (int)min((int64_t)kNlocCols, nc - jb);  // columns of this CTA
   const int64_t b = b0 + bl;
-  const bool mine = j < nc && b < nb;
-  if ((int64_t)blockIdx.z * kNlocCols >= nc) return;  // the whole CTA past the block
-  double acc = 0.0;
+  double acc[4] = {};
   for (int64_t e = blk[4 * q + 2]; e < blk_end[2 * q]; ++e) {
     const int p = blk_proj[e];
     const int64_t nr = nrow[p];
-    const double* x = chi + chi_off[p] + (mine ? j : 0) * nr;
+    const double* x = chi + chi_off[p] + jb * nr;
     const uint32_t* idx = index + row_off[p];
-    double sum = 0.0;
+    double sum[4] = {};
     for (int64_t r0 = 0; r0 < nr; r0 += kNlocRows) {
       const int nrr = (int)min((int64_t)kNlocRows, nr - r0);
       __syncthreads();  // the previous chunk is consumed
@@ -110,17 +113,31 @@ __global__ void __launch_bounds__(kNlocBands * kNlocCols) nloc_forward_kernel(
           v = __ldg(psi16 + ((bb / 16) * K + (int64_t)__ldg(idx + r0 + rr)) * 16 + (bb % 16));
         rows[rr][cb] = v;
       }
+      for (int i = threadIdx.x; i < kNlocCols * kNlocRows; i += blockDim.x) {
+        const int jj = i / kNlocRows, rr = i % kNlocRows;
+        xs[jj][rr] = (jj < ncc && rr < nrr) ? __ldg(x + jj * nr + r0 + rr) : 0.0;
+      }
       __syncthreads();
-      if (mine)
-        for (int rr = 0; rr < nrr; ++rr)
-          sum = __dadd_rn(sum, __dmul_rn(__ldg(x + r0 + rr), rows[rr][bl]));
+      for (int rr = 0; rr < nrr; ++rr) {
+        const double v = rows[rr][bl];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+          sum[jj] = __dadd_rn(sum[jj], __dmul_rn(xs[4 * jq + jj][rr], v));
+      }
     }
-    acc = fma(dv, sum, acc);
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) acc[jj] = fma(dv, sum[jj], acc[jj]);
   }
-  if (!mine) return;
-  for (int64_t e = blk[4 * q + 3]; e < blk_end[2 * q + 1]; ++e)
-    acc = __dmul_rn(acc, __ldg(gamma + blk_scale[e] + j));
-  coef[(col0 + j) * nb + b] = acc;
+  if (b >= nb) return;
+#pragma unroll
+  for (int jj = 0; jj < 4; ++jj) {
+    const int64_t j = jb + 4 * jq + jj;
+    if (j >= nc) break;
+    double a = acc[jj];
+    for (int64_t e = blk[4 * q + 3]; e < blk_end[2 * q + 1]; ++e)
+      a = __dmul_rn(a, __ldg(gamma + blk_scale[e] + j));
+    coef[(col0 + j) * nb + b] = a;
+  }
 }
 
 // Back-projection, step 1: temp_p[r, b] = sum_k chi_p[r, k] C_p[k, b] (fused,
@@ -158,15 +175,31 @@ __global__ void __launch_bounds__(256) nloc_chi_c_kernel(
     xs[rr * (nc + 1) + k] = rr < nrr ? x[k * nr + rr] : 0.0;
   }
   __syncthreads();
-  const int bl = threadIdx.x % kNlocTileB;
-  const int64_t b = b0 + bl;
-  if (b >= nb) return;
-  double* out = temp + (row_off[p] + r0) * nb + b;
-  for (int rr = threadIdx.x / kNlocTileB; rr < nrr; rr += blockDim.x / kNlocTileB) {
-    const double* xr = xs + rr * (nc + 1);
-    double tt = 0.0;
-    for (int k = 0; k < nc; ++k) tt = fma(xr[k], cs[k * kNlocTileB + bl], tt);
-    out[(int64_t)rr * nb] = tt;
+  // Thread: bands 4 q4 .. 4 q4 + 3 of the tile (q4 = tid % 16) and rows
+  // rg, rg + 16, rg + 32, rg + 48 (rg = tid / 16): per column, four chi and
+  // four C values feed 16 multiply-adds, each output's sum over the columns
+  // in order.
+  const int q4 = threadIdx.x % 16, rg = threadIdx.x / 16;
+  double tt[4][4] = {};
+  for (int k = 0; k < nc; ++k) {
+    double cv[4], xv[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) cv[jj] = cs[k * kNlocTileB + 4 * q4 + jj];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) xv[i] = xs[(rg + 16 * i) * (nc + 1) + k];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) tt[i][jj] = fma(xv[i], cv[jj], tt[i][jj]);
+  }
+  double* out = temp + (row_off[p] + r0) * nb + b0 + 4 * q4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int rr = rg + 16 * i;
+    if (rr >= nrr) break;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+      if (b0 + 4 * q4 + jj < nb) out[(int64_t)rr * nb + jj] = tt[i][jj];
   }
 }
 
@@ -383,7 +416,7 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
               (unsigned)((maxw + kNlocCols - 1) / kNlocCols));
     if (grid.y > 65535u || grid.z > 65535u)
       return fail(SKGEMM_ERR_INVALID_ARG, "too many bands or projector columns");
-    nloc_forward_kernel<<<grid, kNlocBands * kNlocCols, 0, s>>>(
+    nloc_forward_kernel<<<grid, kNlocThreads, 0, s>>>(
         nb, h->K, dv, h->d_blk, h->d_blk_end, h->d_blk_proj, h->d_blk_scale, h->d_nrow,
         h->d_row_off, h->d_chi_off, h->d_index, h->d_chi, h->d_gamma, psi16, h->d_coef);
     SKG_CUDA(cudaGetLastError());
