@@ -7,6 +7,8 @@ Kernels and workloads (inputs larger than L2 where the kernel is HBM-bound):
   pack_kernel<16>, pack_kernel<32>   dense 110592 x 512 -> band-packed (453 MB)
   band_grid_kernel (both ways)       110592 x 512 band <-> grid packed (453 MB)
   unpack_kernel<16>                  grid-packed -> column-major (linalg_unpack_c16)
+  fp64_streamk_kernel_ak             the rotation on band-packed Psi, 8192 x 1024
+                                     (512 tiles of 128 x 128: the 128-row kernel)
   fp64_streamk_kernel64_ak,          the rotation on band-packed Psi, 110592 x 512,
   norm_partials / convert_tma (KM)   native and Ozaki (K-major operand reads)
   halo_periodic_kernel,              H Psi on the 48^3 grid (= 110592 points) x 512:
@@ -35,6 +37,18 @@ def main() -> None:
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     g = torch.Generator(device=dev).manual_seed(5)
+
+    # The rotation's 128 x 128 K-major kernel (fewer than 4 tiles per SM),
+    # first, while little memory is held: Psi 67 MB, Q 8 MB.
+    nd, nb = 8192, 1024
+    psi = torch.randn(nd * nb, generator=g, dtype=torch.float64, device=dev) / nd ** 0.5
+    q = torch.rand(nb * nb, generator=g, dtype=torch.float64, device=dev) * 2 - 1
+    rot = torch.empty_like(psi)
+    skgemm.drot_band_dev(nd, nb, psi, q, rot)
+    skgemm.stream_status()
+    assert bool(torch.isfinite(rot).all())
+    del psi, q, rot
+
     nd, nb = 110592, 512
 
     # Layout kernels (HBM-bound).
