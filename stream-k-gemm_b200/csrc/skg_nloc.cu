@@ -55,6 +55,7 @@ struct skgemm_nloc {
   // the back-projection rows (total_rows x nb)
   double* d_coef = nullptr;
   int64_t coef_cap = 0;
+  bool chi_c_smem_set = false;  // the chi*C kernel's shared-memory attribute
   std::vector<int64_t> blk_width;  // host copy of each block's ncol
   std::mutex mu;
 };
@@ -247,7 +248,7 @@ int nloc_create(int64_t P, const uint32_t* nrow, const uint32_t* ncol, const int
                 const double* gamma, int64_t K, skgemm_nloc** out) {
   if (!out) return fail(SKGEMM_ERR_INVALID_ARG, "null handle pointer");
   *out = nullptr;
-  if (P < 0 || K <= 0 || K > ((int64_t)1 << 32))
+  if (P < 0 || P > INT32_MAX || K <= 0 || K > ((int64_t)1 << 32))
     return fail(SKGEMM_ERR_INVALID_ARG, "projector count or grid size out of range");
   if (P > 0 && (!nrow || !ncol || !atom || !offsets))
     return fail(SKGEMM_ERR_INVALID_ARG, "null projector array");
@@ -406,6 +407,7 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
       SKG_CUDA(cudaStreamSynchronize(s));
       cudaFree(h->d_coef);
       h->d_coef = nullptr;
+      h->coef_cap = 0;
     }
     SKG_CUDA(cudaMalloc(&h->d_coef, need * sizeof(double)));
     h->coef_cap = need;
@@ -427,11 +429,10 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
     if (h->ntiles > INT32_MAX || grid.y > 65535u)
       return fail(SKGEMM_ERR_INVALID_ARG, "too many projector rows or bands");
     const size_t smem = (kNlocMaxCols * kNlocTileB + kNlocTileR * (kNlocMaxCols + 1)) * 8;
-    static bool attr_set[64] = {};
-    if (!attr_set[h->device]) {
+    if (!h->chi_c_smem_set) {  // per handle: a handle belongs to one device
       SKG_CUDA(cudaFuncSetAttribute(nloc_chi_c_kernel,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr_set[h->device] = true;
+      h->chi_c_smem_set = true;
     }
     nloc_chi_c_kernel<<<grid, 256, smem, s>>>(nb, h->d_tile_proj, h->d_tile_r0, h->d_nrow,
                                               h->d_ncol, h->d_row_off, h->d_chi_off,
@@ -440,6 +441,8 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
   }
   const int64_t nbk = h->ntouch * nb;
   if (nbk > 0) {
+    if ((nbk + 255) / 256 > INT32_MAX)
+      return fail(SKGEMM_ERR_INVALID_ARG, "too many touched points x bands");
     if (out_tile == 32)
       nloc_backward_kernel<32><<<(unsigned)((nbk + 255) / 256), 256, 0, s>>>(
           h->ntouch, nb, h->K, h->d_touch, h->d_touch_off, h->d_ent_proj, h->d_ent_row,

@@ -33,6 +33,27 @@ def test_nloc_equals_oracle(cuda, K, nb, nrow, ncol, P, images, T):
     h.close()
 
 
+def test_nloc_handle_reused_across_band_counts(cuda):
+    """One handle applied at growing band counts (its scratch regrows) and
+    twice at the same count (out accumulates): each call equals the oracle."""
+    K = 5000
+    pj = oracle.nloc_random(K, 300, 9, 6, seed=77, images=2)
+    h = handle(pj, K)
+    rng = np.random.default_rng(5)
+    for nb in (16, 200, 40, 200):
+        psi16 = rng.uniform(-1, 1, (nb + 15) // 16 * K * 16)
+        base = rng.uniform(-1, 1, (nb + 31) // 32 * K * 32)
+        want = oracle.nloc_project(pj, psi16, nb, K, 0.03, base.copy(), 32)
+        want = oracle.nloc_project(pj, psi16, nb, K, 0.03, want, 32)
+        out = torch.from_numpy(base.copy()).cuda()
+        p = torch.from_numpy(psi16).cuda()
+        h.apply(nb, 0.03, p, out, 32)
+        h.apply(nb, 0.03, p, out, 32)
+        skgemm.stream_status()
+        assert np.array_equal(out.cpu().numpy(), want), nb
+    h.close()
+
+
 def test_nloc_repeated_atoms_and_empty_projectors(cuda):
     """Atoms that come back after another atom (scaled again, as the
     reference's change-of-atom rule does) and projectors without rows."""
