@@ -414,6 +414,14 @@ class NlocProjector:
                       arr(offsets, np.uint32), arr(index, np.uint32), arr(chi, np.float64),
                       arr(gamma, np.float64)]
         nr, nc, at, off, idx, ch, gm = self._keep
+        P = len(nr)
+        if len(nc) != P or len(at) != P or len(off) != P + 1:
+            raise SkgemmError(ERR_INVALID_ARG, "ncol and atom take one entry per projector, "
+                                               "offsets one more")
+        if (len(idx) < int(nr.sum(dtype=np.int64))
+                or len(ch) < int((nr.astype(np.int64) * nc).sum())
+                or len(gm) < int(nc.sum(dtype=np.int64))):
+            raise SkgemmError(ERR_INVALID_ARG, "index, chi or gamma shorter than the projectors")
         c = ctypes
         h = c.c_void_p()
         _check(lib().skgemm_nloc_create(

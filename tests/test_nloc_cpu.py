@@ -35,3 +35,20 @@ def test_oracle_equals_reference(K, nb, nrow, ncol, P, images, T):
     mine = oracle.nloc_project(pj, psi16, nb, K, 0.01, base.copy(), T)
     ref = ref_project(pj, psi16, nb, K, 0.01, base.copy(), T)
     assert np.array_equal(mine, ref)
+
+
+def test_projector_host_arrays_checked():
+    """The binding rejects host arrays shorter than the set they describe
+    before the library reads them (no device needed)."""
+    import skgemm
+
+    pj = oracle.nloc_random(100, 10, 4, 2, seed=3)
+    args = [pj.nrow, pj.ncol, pj.atom, pj.offsets, pj.index, pj.chi, pj.gamma]
+    bad = [(3, pj.offsets[:-1]), (4, pj.index[:-1]), (5, pj.chi[:-1]), (6, pj.gamma[:-1]),
+           (1, pj.ncol[:-1]), (2, pj.atom[:-1])]
+    for pos, arr in bad:
+        a = list(args)
+        a[pos] = arr
+        with pytest.raises(skgemm.SkgemmError) as e:
+            skgemm.NlocProjector(*a, 100)
+        assert e.value.code == skgemm.ERR_INVALID_ARG
