@@ -383,9 +383,11 @@ def unpack_r16_dev(Nd, nb, src, dst, stream=None):
     _check(lib().skgemm_unpack_r16_dev(Nd, nb, _dptr(src), _dptr(dst), _stream(stream)))
 
 
-def _coef(c):
-    a = (ctypes.c_double * len(c))(*[float(x) for x in c])
-    return a
+def _coef(c, n):
+    """The first n stencil coefficients (index 0 .. FDn) as a C array."""
+    if len(c) < n:
+        raise SkgemmError(ERR_INVALID_ARG, f"stencil coefficients need {n} values (0 .. FDn)")
+    return (ctypes.c_double * n)(*[float(x) for x in c[:n]])
 
 
 def stencil_ext_dev(ni, nj, nk, nb, ext16, A_diag, coef_x, coef_y, coef_z, coef_0, out,
@@ -393,7 +395,9 @@ def stencil_ext_dev(ni, nj, nk, nb, ext16, A_diag, coef_x, coef_y, coef_z, coef_
     """H Psi = stencil(extended band-packed Psi) into 32- (or 16-) band-packed
     out (calc_laplacian_extended_packed_16to32 / _16to16)."""
     _check(lib().skgemm_stencil_ext_dev(ni, nj, nk, nb, FDn, _dptr(ext16), _dptr(A_diag),
-                                        _coef(coef_x), _coef(coef_y), _coef(coef_z),
+                                        _coef(coef_x, max(FDn + 1, 0)),
+                                        _coef(coef_y, max(FDn + 1, 0)),
+                                        _coef(coef_z, max(FDn + 1, 0)),
                                         float(coef_0), _dptr(out), out_tile, _stream(stream)))
 
 

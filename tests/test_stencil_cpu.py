@@ -67,3 +67,13 @@ def test_halo_periodic_oracle_is_a_wrap():
     ext = oracle.halo_periodic(local, ni, nj, nk, nb)
     want = np.pad(X, ((0, 0), (F, F), (F, F), (F, F)), mode="wrap").reshape(nb, -1)
     assert np.array_equal(oracle.unpack(ext.reshape(-1, want.shape[1], 16), nb), want)
+
+
+def test_binding_rejects_short_coefficient_lists():
+    """The binding checks that each axis has FDn + 1 coefficients before the
+    library reads them (raised before any device work; null pointers)."""
+    import skgemm
+
+    with pytest.raises(skgemm.SkgemmError) as e:
+        skgemm.stencil_ext_dev(8, 8, 8, 16, 0, 0, CX, CX[:6], CX, C0, 0)
+    assert e.value.code == skgemm.ERR_INVALID_ARG
