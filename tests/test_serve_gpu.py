@@ -121,3 +121,45 @@ def test_serve_rejects_oversized_request(cuda):
     with pytest.raises(skgemm.SkgemmError) as e:
         skgemm.serve([(0.0, 16000, 512, 1)], hbm_budget=200e6)
     assert e.value.code == skgemm.ERR_OOM
+
+
+@pytest.mark.parametrize("precision", [NATIVE, OZAKI])
+def test_serve_largest_request_matches_oracle(cuda, precision):
+    """A trace holding config 5's largest request (Ng = 4e5 grid points, 2048
+    states: K crosses the Ozaki path's 1023-k-block segments, the rotation
+    runs with 2048 states) between small ones, under the 150 GB budget. The
+    large request's S, Hs and Psi' are checked against Dot2 on sampled
+    entries: 48 states (all their pairs) for S and Hs, 64 grid points x 64
+    states for the rotation."""
+    big = (0.0, 400000, 2048, 99)
+    trace = [(0.0, 1024, 64, 1), big, (0.0, 2048, 128, 2), (0.0, 4096, 96, 3)]
+    keep = {1: buffers(big[1], big[2])}
+    rows, o = skgemm.serve(trace, precision=precision, hbm_budget=150e9, keep=keep,
+                           realtime=False)
+    assert o.flop > 0
+    k = keep[1]
+    ng, nb = big[1], big[2]
+    rng = np.random.default_rng(5)
+    st = np.sort(rng.choice(nb, 48, replace=False))
+    P16 = k["Psi_in"].reshape(nb // 16, ng, 16)
+    P32 = k["HPsi_in"].reshape(nb // 32, ng, 32)
+    X = np.ascontiguousarray(P16[st // 16, :, st % 16])    # (48, Ng): states over the grid
+    Y = np.ascontiguousarray(P32[st // 32, :, st % 32])
+    a, b = np.meshgrid(np.arange(48), np.arange(48), indexing="ij")
+    a, b = a.ravel(), b.ravel()
+    ref_h = oracle.dot2_sampled(X, Y, a, b, x_strides=(ng, 1), y_strides=(1, ng), K=ng)
+    Hs = k["Hs"].reshape(nb, nb)
+    assert oracle.rel_frobenius(Hs[st[a], st[b]], ref_h) <= TOL
+    u = a <= b
+    ref_s = oracle.dot2_sampled(X, X, a[u], b[u], x_strides=(ng, 1), y_strides=(1, ng), K=ng)
+    C = k["S"].reshape(nb, nb)                            # row j = column j of C
+    assert oracle.rel_frobenius(C[st[b[u]], st[a[u]]], ref_s) <= TOL
+    gs = np.sort(rng.choice(ng, 64, replace=False))
+    R = np.ascontiguousarray(P16[:, gs, :].transpose(1, 0, 2).reshape(64, nb))  # Psi rows
+    Q = k["Q"].reshape(nb, nb)
+    bs = rng.integers(0, nb, 64)
+    g2, b2 = np.meshgrid(np.arange(64), bs, indexing="ij")
+    g2, b2 = g2.ravel(), b2.ravel()
+    ref_r = oracle.dot2_sampled(R, Q, g2, b2)
+    Po = k["Psi"].reshape(nb // 16, ng, 16)
+    assert oracle.rel_frobenius(Po[b2 // 16, gs[g2], b2 % 16], ref_r) <= TOL
