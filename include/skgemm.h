@@ -241,6 +241,20 @@ int skgemm_pack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, 
 int skgemm_pack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, void* stream);
 int skgemm_unpack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, void* stream);
 int skgemm_unpack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst, void* stream);
+/* The same four converters under the reference's own names and signatures
+ * (include/sme_pack.hpp:316-352: `void f(const int Nd, const int nb, const
+ * double* src, double* dst)`), for callers linked against those names. Host
+ * pointers; blocking (staged through device memory, converted on the GPU).
+ * As in the reference, only the first 16 * floor(Nd/16) grid points are
+ * converted (its g_tiles = Nd / 16) and the dense side keeps the column
+ * stride Nd; unpacking leaves the remaining rows of dst unchanged. They
+ * return nothing, like the reference: a refused call (negative sizes, a null
+ * pointer, no usable device) leaves dst unchanged and its reason is read
+ * with skgemm_last_error(), which is empty after a call that succeeded. */
+void linalg_pack_c16_f64(const int Nd, const int nb, const double* src, double* dst);
+void linalg_pack_r16_f64(const int Nd, const int nb, const double* src, double* dst);
+void linalg_unpack_c16_f64(const int Nd, const int nb, const double* src, double* dst);
+void linalg_unpack_r16_f64(const int Nd, const int nb, const double* src, double* dst);
 /* Band-packed <-> grid-packed conversion of an Nd x nb block of states
  * (sme_pack<double>::band_to_grid_tile / grid_to_band_tile,
  * include/sme_pack.hpp:232-313). */

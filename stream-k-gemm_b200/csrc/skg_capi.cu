@@ -874,6 +874,58 @@ SKG_EXPORT int skgemm_unpack_r16_dev(int64_t Nd, int64_t nb, const double* src, 
   return skgemm_unpack_c16_dev(Nd, nb, src, dst, stream);
 }
 
+// The reference's extern "C" converters under their own names and signatures
+// (include/sme_pack.hpp:316-352): host pointers, blocking, no status (the
+// reference returns void; a refused call leaves dst as it was and records
+// the reason for skgemm_last_error, which a successful call clears). As in
+// the reference, only the first 16 * floor(Nd / 16) grid points are
+// converted (its g_tiles = Nd / 16); the dense side keeps its column stride Nd.
+namespace {
+void linalg_convert(int Nd, int nb, const double* src, double* dst, bool pack) {
+  g_last_error.clear();  // no status to return: an empty message means success
+  if (Nd < 0 || nb < 0) {
+    skg::fail(SKGEMM_ERR_INVALID_ARG, "linalg converters: Nd and nb must be >= 0");
+    return;
+  }
+  const int64_t R = (int64_t)Nd / 16 * 16;
+  if (R == 0 || nb == 0) return;
+  if (!src || !dst) {
+    skg::fail(SKGEMM_ERR_INVALID_ARG, "linalg converters: null pointer");
+    return;
+  }
+  const size_t dense = (size_t)Nd * nb * 8, packed = (size_t)R * nb * 8;
+  const HostIO in{src, pack ? dense : packed};
+  // Unpacking a ragged Nd writes only the first R rows of each column: the
+  // rest of dst must come back unchanged, so it goes up first.
+  const bool keep = !pack && R != Nd;
+  run_host(1, &in, dst, pack ? packed : dense, keep, [&](void** d, cudaStream_t s) {
+    return pack ? launch_pack(R, nb, (const double*)d[0], 1, Nd, 16, (double*)d[3], s)
+                : launch_unpack(R, nb, (const double*)d[0], 16, (double*)d[3], 1, Nd, s);
+  });
+}
+}  // namespace
+
+SKG_EXPORT void linalg_pack_c16_f64(const int Nd, const int nb, const double* src,
+                                    double* dst) {
+  linalg_convert(Nd, nb, src, dst, true);
+}
+
+// Row-major [nb, Nd] (src[b*Nd + g]) is the same bytes as column-major [Nd, nb].
+SKG_EXPORT void linalg_pack_r16_f64(const int Nd, const int nb, const double* src,
+                                    double* dst) {
+  linalg_convert(Nd, nb, src, dst, true);
+}
+
+SKG_EXPORT void linalg_unpack_c16_f64(const int Nd, const int nb, const double* src,
+                                      double* dst) {
+  linalg_convert(Nd, nb, src, dst, false);
+}
+
+SKG_EXPORT void linalg_unpack_r16_f64(const int Nd, const int nb, const double* src,
+                                      double* dst) {
+  linalg_convert(Nd, nb, src, dst, false);
+}
+
 SKG_EXPORT int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                                       const double* psi_ext16, const double* A_diag,
                                       const double* coef_x, const double* coef_y,

@@ -165,6 +165,12 @@ _SIGS = {
 }
 
 
+# The reference's own extern "C" converter names (include/sme_pack.hpp:316-352):
+# void f(int Nd, int nb, const double* src, double* dst), host pointers.
+LINALG = ("linalg_pack_c16_f64", "linalg_pack_r16_f64", "linalg_unpack_c16_f64",
+          "linalg_unpack_r16_f64")
+
+
 def lib() -> ctypes.CDLL:
     """Loads libskgemm.so (raises if it has not been built)."""
     global _lib
@@ -185,13 +191,17 @@ def lib() -> ctypes.CDLL:
         L.skgemm_nloc_destroy.restype = None
         L.skgemm_nloc_destroy.argtypes = [ctypes.c_void_p]
         L.skgemm_plan_destroy.argtypes = [_vp]
+        for name in LINALG:
+            f = getattr(L, name)
+            f.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp]
+            f.restype = None
         _lib = L
     return _lib
 
 
 def exported_symbols() -> list:
     return ["skgemm_version", "skgemm_last_error", "skgemm_plan_destroy",
-            "skgemm_nloc_destroy"] + list(_SIGS)
+            "skgemm_nloc_destroy"] + list(_SIGS) + list(LINALG)
 
 
 def version() -> str:
@@ -361,6 +371,37 @@ def pack_dev(R, K, X, sr, sk, T, X_packed, stream=None):
 def unpack_dev(R, K, X_packed, T, X, sr, sk, stream=None):
     """Packed-T panels -> strided dense X[r*sr + k*sk] (rows r < R)."""
     _check(lib().skgemm_unpack_dev(R, K, _dptr(X_packed), T, _dptr(X), sr, sk, _stream(stream)))
+
+
+class sme_pack:
+    """The reference's C converters by their own names (sme_pack.hpp:316-352),
+    host numpy arrays, blocking: ``pack_c16(Nd, nb, src, dst)`` etc. Like the
+    reference they convert the first 16 * (Nd // 16) grid points; a refused
+    call raises here (the C functions return nothing and leave the reason in
+    skgemm_last_error)."""
+
+    @staticmethod
+    def _call(name, Nd, nb, src, dst):
+        getattr(lib(), name)(Nd, nb, _hptr(src), _hptr(dst, True))
+        msg = lib().skgemm_last_error().decode(errors="replace")
+        if msg:
+            raise SkgemmError(ERR_INVALID_ARG, msg)
+
+    @staticmethod
+    def pack_c16(Nd, nb, src, dst):
+        sme_pack._call("linalg_pack_c16_f64", Nd, nb, src, dst)
+
+    @staticmethod
+    def pack_r16(Nd, nb, src, dst):
+        sme_pack._call("linalg_pack_r16_f64", Nd, nb, src, dst)
+
+    @staticmethod
+    def unpack_c16(Nd, nb, src, dst):
+        sme_pack._call("linalg_unpack_c16_f64", Nd, nb, src, dst)
+
+    @staticmethod
+    def unpack_r16(Nd, nb, src, dst):
+        sme_pack._call("linalg_unpack_r16_f64", Nd, nb, src, dst)
 
 
 def pack_c16_dev(Nd, nb, src, dst, stream=None):

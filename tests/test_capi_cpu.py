@@ -42,7 +42,20 @@ def test_only_the_abi_is_exported():
     out = subprocess.run(["nm", "-D", "--defined-only", skgemm.LIB_PATH], capture_output=True,
                          text=True, check=True).stdout
     text_syms = re.findall(r"\bT (\S+)", out)
-    assert all(s.startswith("skgemm_") for s in text_syms), text_syms
+    assert all(s.startswith("skgemm_") or s in skgemm.LINALG for s in text_syms), text_syms
+
+
+def test_reference_converter_names_exported():
+    """The reference's own extern "C" names (include/sme_pack.hpp:316-352) are
+    declared in the header with the reference's signature and exported, so a
+    caller linked against them resolves."""
+    src = open(os.path.join(REPO, "include", "skgemm.h")).read()
+    out = subprocess.run(["nm", "-D", "--defined-only", skgemm.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    for name in skgemm.LINALG:
+        assert re.search(rf"\bvoid {name}\(const int Nd, const int nb, const double\* src, "
+                         rf"double\* dst\);", src), name
+        assert re.search(rf"\bT {name}\b", out), name
 
 
 @pytest.mark.parametrize("call", [
