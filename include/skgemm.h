@@ -141,16 +141,23 @@ int skgemm_dgemm_packed_dev(int64_t M, int64_t N, int64_t K, const double* A_pac
  * fixed after start-up, or loops that cannot take the synchronisation of
  * cudaMalloc / cudaFree. No counterpart in the reference (whose drivers
  * allocate every buffer themselves).
- * Same contract and result as skgemm_dgemm_packed_dev (native FP64). Its
- * Stream-K scratch is a static device array of 148 partial-tile slots
- * (19.4 MB) that exists on every GPU that loads the library until the process
- * exits; a launch that needs more slots (a device with more than 148 SMs) is
- * rejected with SKGEMM_ERR_INVALID_ARG. The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) with that device current,
- * so make that first call before any stream capture. Every call shares the
- * array, so calls are serialised by a process-wide lock and each call returns
- * only after its kernel has finished (it synchronises `stream`); a device-side
- * wait that ran out is reported as SKGEMM_ERR_DEVICE_TIMEOUT. */
+ * Same contract as skgemm_dgemm_packed_dev (native FP64, 128 x 128 tiles);
+ * the result agrees with it within FP64 rounding (relative Frobenius error
+ * <= 1e-13), not bit for bit, since the regular entry may pick 64 x 64 tiles
+ * and so a different Stream-K split. Its Stream-K scratch is a static device
+ * array of 148 partial-tile slots (19.4 MB), held on each GPU where the
+ * library's no-alloc code has been loaded until the process exits; a launch
+ * that needs more slots (a device with more than 148 SMs) is rejected with
+ * SKGEMM_ERR_INVALID_ARG. With CUDA's lazy module loading (the default) the
+ * first call on a device loads that array and the kernel's code, taking
+ * their device memory then: make that first call (an empty one, M = 0 or
+ * N = 0, is enough) before reserving the rest of the device's memory. The
+ * first call also looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current. Every call on a device shares its array, so calls
+ * on one device are serialised by a per-device lock, and each call returns
+ * only after its kernel has finished (it synchronises `stream`): it cannot be
+ * issued while `stream` is being captured. A device-side wait that ran out is
+ * reported as SKGEMM_ERR_DEVICE_TIMEOUT. */
 int skgemm_dgemm_packed_dev_noalloc(int64_t M, int64_t N, int64_t K,
                                     const double* A_packed16, const double* B_packed32,
                                     double* D, int64_t ldd, double alpha, double gamma,

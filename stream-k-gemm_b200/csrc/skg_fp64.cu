@@ -103,6 +103,11 @@ int single_setup(int device, const void* kernel, bool akm, int* per_sm) {
 
 }  // namespace
 
+int fp64_preload(DeviceState* dev) {
+  int per_sm = 0;
+  return single_setup<Tile128>(dev->device, (const void*)fp64_streamk_kernel, false, &per_sm);
+}
+
 int fp64_grid_for(DeviceState* dev, const Fp64Problem& prob) {
   if (prob.M <= 0 || prob.N <= 0 || prob.K <= 0) return 0;
   return make_schedule(dev, prob, 128, 1).grid;

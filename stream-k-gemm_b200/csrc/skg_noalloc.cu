@@ -11,20 +11,26 @@
 //
 // Its scratch (one partial-tile slot per persistent CTA, the CTAs' fixup
 // flags and a device error word) is the file-scope array below: 148 slots of
-// 128 x 128 doubles plus flags, 19.4 MB in all. The array exists on every GPU
-// that loads this library and stays allocated until the process exits.
+// 128 x 128 doubles plus flags, 19.4 MB in all. With CUDA's lazy module
+// loading (the default) the array, like the kernel code it feeds, takes its
+// device memory when this file's module is first used on a device, not when
+// the library is loaded: the first call on a device — an empty call with
+// M = 0 or N = 0 will do — loads both, and should come before the caller
+// reserves the rest of the device's memory. From then on the array stays
+// allocated on that device until the process exits.
 //
 // The array's name in host code is only a host-side stand-in, not a device
 // address, so the first call on a device (with that device current) looks up
 // the real address once with cudaGetSymbolAddress and passes it to the
-// kernel. That first call should therefore come before any stream capture.
+// kernel.
 //
 // Every call uses the same array and finds the previous call's contents in
 // it. The flags carry a per-call epoch, so stale flags never match; the error
 // word is cleared at the start of each call; partial slots are written before
-// they are read. Two calls running on the GPU at the same time would race on
-// the slots and flags, so calls are serialised by a process-wide lock and a
-// call returns only after its kernel has finished (it synchronises `stream`).
+// they are read. Two calls running on the same GPU at the same time would
+// race on the slots and flags, so calls on one device are serialised by that
+// device's lock and a call returns only after its kernel has finished (it
+// synchronises `stream`; it therefore cannot be issued under stream capture).
 #include <cstdio>
 #include <mutex>
 
@@ -43,17 +49,21 @@ static_assert(kNoAllocSlots * sizeof(uint32_t) <= kNoAllocFlagBytes, "flag area 
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
+constexpr int kNoAllocDevices = 64;
+
 struct NoAllocDevice {
+  std::mutex mu;  // serialises the calls on this device (they share its array)
   bool ready = false;
   StreamWorkspace ws;  // views into g_noalloc_scratch; never allocates
 };
 
-std::mutex g_noalloc_mu;
-NoAllocDevice g_noalloc_dev[64];
+NoAllocDevice g_noalloc_dev[kNoAllocDevices];
 
-// Once per device, with that device current.
-int noalloc_setup(NoAllocDevice& d) {
+// Once per device, with that device current (caller holds d.mu): the
+// array's device address, and the GEMM kernel's code loaded.
+int noalloc_setup(DeviceState* dev, NoAllocDevice& d) {
   if (d.ready) return SKGEMM_OK;
+  if (int st = fp64_preload(dev)) return st;
   void* base = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
@@ -65,11 +75,6 @@ int noalloc_setup(NoAllocDevice& d) {
   d.ws.epoch = 0;  // the array starts zeroed: first epoch used is 1
   d.ready = true;
   return SKGEMM_OK;
-}
-
-__global__ void noalloc_fill_kernel(int64_t M, int64_t N, double* D, int64_t ldd, double v) {
-  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx < M * N) D[(idx / N) * ldd + idx % N] = v;
 }
 
 }  // namespace
@@ -85,17 +90,20 @@ extern "C" __attribute__((visibility("default"))) int skgemm_dgemm_packed_dev_no
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
+  if (dev->device < 0 || dev->device >= kNoAllocDevices)
+    return fail(SKGEMM_ERR_UNSUPPORTED, "no-alloc GEMM: device ordinal beyond 63");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+
+  NoAllocDevice& nd = g_noalloc_dev[dev->device];
+  std::lock_guard<std::mutex> lk(nd.mu);
+  // Set-up before the empty-shape return, so that an empty call loads the
+  // array and the kernel on this device ahead of the caller's own pool.
+  if ((st = noalloc_setup(dev, nd)) != SKGEMM_OK) return st;
   if (M == 0 || N == 0) return SKGEMM_OK;
   if (!D) return fail(SKGEMM_ERR_INVALID_ARG, "null output pointer");
 
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  NoAllocDevice& nd = g_noalloc_dev[dev->device];
-  if ((st = noalloc_setup(nd)) != SKGEMM_OK) return st;
-
   if (K == 0) {  // empty reduction: D = alpha * 0 + gamma
-    noalloc_fill_kernel<<<(unsigned)((M * N + 255) / 256), 256, 0, s>>>(M, N, D, ldd, gamma);
-    SKG_CUDA(cudaGetLastError());
+    if ((st = run_k0(kOutRowMajor, M, N, D, ldd, gamma, false, s)) != SKGEMM_OK) return st;
     SKG_CUDA(cudaStreamSynchronize(s));
     return SKGEMM_OK;
   }

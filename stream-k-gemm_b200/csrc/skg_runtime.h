@@ -98,6 +98,11 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
 // Number of Stream-K partial slots the 128 x 128-tile launch of `prob` uses
 // (= its grid).
 int fp64_grid_for(DeviceState* dev, const Fp64Problem& prob);
+// Loads the 128 x 128 single-problem kernel's code on the current device and
+// sets its shared-memory attribute, without launching it (with lazy module
+// loading the code would otherwise be loaded, and its memory taken, at the
+// first launch).
+int fp64_preload(DeviceState* dev);
 // Grouped launch (batched path): CTAs per SM the grouped kernel of `tile`
 // (128 or 64) fits, and the launch itself (flag reset + kernel, no cooperative
 // attribute so that the pair can be captured into a CUDA graph; the grid must

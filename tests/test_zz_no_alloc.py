@@ -4,10 +4,12 @@ skgemm_dgemm_packed_dev_noalloc serves callers that cannot allocate device
 memory when they call the GEMM (their memory is reserved in their own pool,
 or their device footprint must stay fixed after start-up): its Stream-K
 scratch is a static device array instead of a workspace allocated on first
-use. These tests check that it returns what the regular entry point
-(skgemm_dgemm_packed_dev) returns, on two calls in a row with different
-shapes (the second finds the first's leftovers in the shared scratch), and
-that a call on a fresh stream leaves the device's free memory unchanged.
+use. These tests check that it agrees with the regular entry point
+(skgemm_dgemm_packed_dev) and with the Dot2 oracle within the parity
+tolerance, on two calls in a row (the second finds the first's leftovers in
+the shared scratch); that K = 0 writes gamma and leaves the row padding
+alone; and that, once an empty call has primed a fresh process's device, a
+call on a new stream takes no device memory.
 
 This file is collected last so that a run stopping at the first failure has
 run every other test; it also passes on its own in a fresh process.
@@ -33,28 +35,89 @@ def _noalloc(M, N, K, Ap, Bp, D, ldd, alpha, gamma, stream=0):
         raise skgemm.SkgemmError(rc, skgemm.lib().skgemm_last_error().decode())
 
 
-def _operands(M, N, K, seed):
+def _operands(M, N, K, seed, host=False):
     rng = np.random.default_rng(seed)
     A = rng.standard_normal((M, K))
     B = rng.standard_normal((K, N))
     Ap = torch.from_numpy(oracle.pack(A, 16)).cuda()
     Bp = torch.from_numpy(oracle.pack(np.ascontiguousarray(B.T), 32)).cuda()
-    return Ap, Bp
+    return (Ap, Bp, A, B) if host else (Ap, Bp)
 
 
 @pytest.mark.parametrize("M,N,K,alpha,gamma", [(512, 512, 65536, 1.0, 0.0),
                                                (333, 129, 4099, -1.5, 0.25)])
 def test_noalloc_matches_regular_entry_two_calls(cuda, M, N, K, alpha, gamma):
-    Ap, Bp = _operands(M, N, K, M + K)
+    Ap, Bp, A, B = _operands(M, N, K, M + K, host=True)
     ref = torch.full((M, N), np.nan, dtype=torch.float64, device="cuda")
     skgemm.dgemm_packed_dev(M, N, K, Ap, Bp, ref, N, alpha, gamma)
     skgemm.stream_status()
+    rng = np.random.default_rng(K)
+    ii, jj = rng.integers(0, M, 2048), rng.integers(0, N, 2048)
+    exact = oracle.dot2_sampled(A, B, ii, jj, alpha, gamma)
     for _ in range(2):
         out = torch.full((M, N), np.nan, dtype=torch.float64, device="cuda")
         _noalloc(M, N, K, Ap, Bp, out, N, alpha, gamma)
         torch.cuda.synchronize()
-        assert oracle.rel_frobenius(out.cpu().numpy(), ref.cpu().numpy()) <= TOL
-        assert not torch.isnan(out).any()
+        o = out.cpu().numpy()
+        assert not np.isnan(o).any()
+        assert oracle.rel_frobenius(o, ref.cpu().numpy()) <= TOL
+        assert oracle.rel_frobenius(o[ii, jj], exact) <= TOL
+
+
+def test_noalloc_k0_writes_gamma_and_keeps_padding(cuda):
+    """K = 0: D = alpha * 0 + gamma on the M x N block of a padded D (ldd > N);
+    the padding columns keep their values. Empty shapes return at once."""
+    M, N, ldd = 37, 20, 23
+    d = torch.zeros(1, dtype=torch.float64, device="cuda")
+    D = torch.full((M, ldd), 5.0, dtype=torch.float64, device="cuda")
+    _noalloc(M, N, 0, d, d, D, ldd, 2.0, -0.75)
+    out = D.cpu().numpy()
+    assert np.all(out[:, :N] == -0.75)
+    assert np.all(out[:, N:] == 5.0)
+    _noalloc(0, 0, 16, d, d, d, 0, 1.0, 0.0)
+    _noalloc(0, 8, 16, d, d, d, 8, 1.0, 0.0)
+
+
+_FRESH = r"""
+import ctypes, sys
+import numpy as np, torch
+sys.path[:0] = sys.argv[1:3]
+import skgemm
+L = skgemm.lib()
+f = L.skgemm_dgemm_packed_dev_noalloc
+vp = ctypes.c_void_p
+M, N, K = 256, 384, 20000
+Ap = torch.randn(((M + 15) // 16) * 16 * K, dtype=torch.float64, device="cuda")
+Bp = torch.randn(((N + 31) // 32) * 32 * K, dtype=torch.float64, device="cuda")
+D = torch.zeros(M * N, dtype=torch.float64, device="cuda")
+torch.cuda.synchronize()
+assert f(0, 0, 0, None, None, None, 0, 1.0, 0.0, None) == 0      # primes this device
+s = torch.cuda.Stream()
+torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info()[0]
+for _ in range(2):
+    assert f(M, N, K, vp(Ap.data_ptr()), vp(Bp.data_ptr()), vp(D.data_ptr()), N, 1.0, 0.0,
+             vp(s.cuda_stream)) == 0
+torch.cuda.synchronize()
+free1 = torch.cuda.mem_get_info()[0]
+print("free before", free0, "after", free1)
+assert free1 == free0, (free0, free1)
+print("OK")
+"""
+
+
+def test_noalloc_primed_by_empty_call_allocates_nothing_fresh_process(cuda):
+    """In a fresh process: after one empty call (which loads the static array
+    and the kernel code on the device), two full calls on a new stream leave
+    the device's free memory unchanged."""
+    import os
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _FRESH, repo,
+                        os.path.join(repo, "stream-k-gemm_b200")],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stdout + r.stderr
 
 
 def test_noalloc_new_stream_allocates_nothing(cuda):
