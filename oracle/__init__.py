@@ -32,10 +32,12 @@ _lib: Optional[ctypes.CDLL] = None
 _refs: dict = {}
 
 
-def build(reference_root: str = "/root/reference") -> None:
-    """make liboracle.so, and oracle/_ref when the reference tree is present."""
+def build(reference_root: Optional[str] = None) -> None:
+    """make liboracle.so, and oracle/_ref from the reference source tree at
+    `reference_root` (or $SKGEMM_REFERENCE_ROOT) when one is given and exists."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if os.path.isdir(reference_root):
+    reference_root = reference_root or os.environ.get("SKGEMM_REFERENCE_ROOT")
+    if reference_root and os.path.isdir(reference_root):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}"], check=True)
 
 
@@ -84,7 +86,7 @@ def ref(name: str) -> ctypes.CDLL:
     if name not in _refs:
         path = os.path.join(REF_DIR, f"libref_{name}.so")
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref REF=<reference source tree>`")
         _refs[name] = ctypes.CDLL(path)
     return _refs[name]
 

@@ -1,7 +1,7 @@
 """Generates the golden vectors in this directory from the reference itself.
 
 Runs the reference's own kernel files, compiled in place from the reference
-tree by ``make -C oracle ref`` (oracle/_ref), on the reference's own
+tree by ``make -C oracle ref REF=<reference tree>`` (oracle/_ref), on the reference's own
 known-answer inputs:
 
 * gemm_opt.cpp / gemm_crsp.cpp test_gemm cases (M,N,K,alpha,gamma) =

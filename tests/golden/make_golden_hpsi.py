@@ -1,6 +1,6 @@
 """Generates reference_hpsi.npz: golden outputs of the H Psi producers from the
 reference itself. Uses the reference's own kernels, compiled in place from the
-reference tree by ``make -C oracle ref`` (oracle/_ref):
+reference tree by ``make -C oracle ref REF=<reference tree>`` (oracle/_ref):
 
 * calc_laplacian_extended_packed_16to32 / _16to16
   (include/stencil_extended_packed.hpp, through oracle/_ref/libref_stencil.so);
