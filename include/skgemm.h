@@ -97,6 +97,13 @@ int skgemm_probe_fp64_peak(double* tflops_out);
  * skgemm_stream_status(stream) returns SKGEMM_ERR_DEVICE_TIMEOUT (and clears
  * the word). No counterpart in the reference. */
 int skgemm_diag_expire_wait(double budget_ms, void* stream);
+/* The same for the Stream-K fixup's flag wait (the wait of the CTA that
+ * finishes a tile for the partial tiles of the CTAs after it; budget 4 s in
+ * the kernels): one thread runs that wait, with budget_ms (0 < budget_ms <=
+ * 1000), on a flag nothing sets; the timeout is recorded, the kernel returns
+ * and the next skgemm_stream_status(stream) returns
+ * SKGEMM_ERR_DEVICE_TIMEOUT. No counterpart in the reference. */
+int skgemm_diag_expire_fixup_wait(double budget_ms, void* stream);
 /* Measured INT8 tensor-core (tcgen05.mma kind::i8, 128x256x32) throughput of
  * the current device, TOP/s; the roofline denominator of the Ozaki path. */
 int skgemm_probe_i8_peak(double* tops_out);

@@ -369,6 +369,13 @@ SKG_EXPORT int skgemm_diag_expire_wait(double budget_ms, void* stream) {
   return expire_wait(dev, budget_ms, reinterpret_cast<cudaStream_t>(stream));
 }
 
+SKG_EXPORT int skgemm_diag_expire_fixup_wait(double budget_ms, void* stream) {
+  int st;
+  DeviceState* dev = current_device(&st);
+  if (!dev) return st;
+  return expire_fixup_wait(dev, budget_ms, reinterpret_cast<cudaStream_t>(stream));
+}
+
 SKG_EXPORT int skgemm_probe_fp64_peak(double* tflops_out) {
   int st;
   DeviceState* dev = current_device(&st);

@@ -199,4 +199,22 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
   return v;
 }
 
+// The Stream-K fixup's wait for a later CTA's partial tile: spin (acquire)
+// until *flag == want, bounded by budget_ns of %globaltimer and
+// kFixupSpinCap polls. On expiry the timeout is ORed into *err and false is
+// returned; the caller skips that partial and finishes normally.
+__device__ __forceinline__ bool fixup_flag_wait(const uint32_t* flag, uint32_t want,
+                                                uint32_t* err, uint64_t budget_ns) {
+  const uint64_t t0 = globaltimer_ns();
+  uint32_t spins = 0;
+  while (ld_acquire_gpu(flag) != want) {
+    __nanosleep(128);
+    if (++spins > kFixupSpinCap || globaltimer_ns() - t0 > budget_ns) {
+      atomicOr(err, kDevErrFixupTimeout);
+      return false;
+    }
+  }
+  return true;
+}
+
 }  // namespace skg

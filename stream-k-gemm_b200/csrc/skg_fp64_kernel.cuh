@@ -386,20 +386,8 @@ __device__ __forceinline__ void streamk_body(const Sched& S) {
         for (int c2 = cta + 1; c2 < S.grid(); ++c2) {
           const int64_t s2 = (int64_t)c2 * S.total() / S.grid();
           if (s2 >= tile_end) break;
-          if (ctid == 0) {
-            const uint64_t t0 = globaltimer_ns();
-            uint32_t spins = 0;
-            int ok = 1;
-            while (ld_acquire_gpu(S.flags() + c2) != pubval) {
-              __nanosleep(128);
-              if (++spins > kFixupSpinCap || globaltimer_ns() - t0 > kFixupBudgetNs) {
-                atomicOr(S.err(), kDevErrFixupTimeout);
-                ok = 0;
-                break;
-              }
-            }
-            fixup_ok = ok;
-          }
+          if (ctid == 0)
+            fixup_ok = fixup_flag_wait(S.flags() + c2, pubval, S.err(), kFixupBudgetNs) ? 1 : 0;
           asm volatile("bar.sync 1, %0;" ::"n"(kConsumerThreads));
           const bool have = fixup_ok != 0;
           asm volatile("bar.sync 1, %0;" ::"n"(kConsumerThreads));

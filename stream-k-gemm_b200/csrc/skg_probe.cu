@@ -41,7 +41,27 @@ __global__ void expire_wait_kernel(uint32_t* err, uint64_t budget_ns) {
   }
 }
 
+// One thread runs the Stream-K fixup's flag wait on a flag that is never
+// set to the awaited value (the stream's first partial-tile flag holds call
+// epochs, which count up from 1 and never reach 0xffffffff): the wait gives
+// up after its budget, records the fixup timeout, and the kernel returns.
+__global__ void expire_fixup_wait_kernel(const uint32_t* flag, uint32_t* err,
+                                         uint64_t budget_ns) {
+  if (threadIdx.x == 0) fixup_flag_wait(flag, 0xffffffffu, err, budget_ns);
+}
+
 }  // namespace
+
+int expire_fixup_wait(DeviceState* dev, double budget_ms, cudaStream_t s) {
+  if (!(budget_ms > 0.0 && budget_ms <= 1000.0))
+    return fail(SKGEMM_ERR_INVALID_ARG, "budget_ms must be in (0, 1000]");
+  int st;
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
+  expire_fixup_wait_kernel<<<1, 32, 0, s>>>(ws->flags, ws->err, (uint64_t)(budget_ms * 1e6));
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
 
 int expire_wait(DeviceState* dev, double budget_ms, cudaStream_t s) {
   if (!(budget_ms > 0.0 && budget_ms <= 1000.0))

@@ -159,6 +159,7 @@ int probe_fp64_peak(DeviceState* dev, double* tflops);
 // Diagnostic: one bounded device wait that runs out after budget_ms
 // (recorded in stream s's device error word).
 int expire_wait(DeviceState* dev, double budget_ms, cudaStream_t s);
+int expire_fixup_wait(DeviceState* dev, double budget_ms, cudaStream_t s);
 
 // Device-side failures of one-shot batched launches on `s` (read and cleared;
 // `s` already synchronised).

@@ -110,6 +110,7 @@ _SIGS = {
     "skgemm_stream_status": [_vp],
     "skgemm_probe_fp64_peak": [ctypes.POINTER(ctypes.c_double)],
     "skgemm_diag_expire_wait": [ctypes.c_double, _vp],
+    "skgemm_diag_expire_fixup_wait": [ctypes.c_double, _vp],
     "skgemm_probe_i8_peak": [ctypes.POINTER(ctypes.c_double)],
     "skgemm_igemm_s8_dev": [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp],
     "skgemm_dgemm": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d],
@@ -516,6 +517,12 @@ def diag_expire_wait(budget_ms, stream=None) -> None:
     """Enqueue one bounded device wait that runs out after budget_ms; the next
     stream_status(stream) raises SkgemmError(ERR_DEVICE_TIMEOUT)."""
     _check(lib().skgemm_diag_expire_wait(float(budget_ms), _stream(stream)))
+
+
+def diag_expire_fixup_wait(budget_ms, stream=None) -> None:
+    """Enqueue the Stream-K fixup's flag wait on a flag nothing sets, with
+    budget_ms; the next stream_status(stream) raises ERR_DEVICE_TIMEOUT."""
+    _check(lib().skgemm_diag_expire_fixup_wait(float(budget_ms), _stream(stream)))
 
 
 def probe_i8_peak() -> float:
