@@ -214,6 +214,23 @@ int skgemm_dsubspace_packed_dev(int64_t K, int64_t M, const double* Psi_packed16
  * Replaces sme_gemm_trp_3d<double>::compute (include/sme_trp_3d.hpp:194-215). */
 int skgemm_drot(int64_t Nd, int64_t nb, const double* A_gridpacked,
                 const double* Q_rowmajor, double* D_bandpacked);
+/* Host-pointer forms of the three reference calls with a precision selector
+ * (skgemm_options_t, NULL = native): the reference's blocking, host-memory
+ * interface on the Ozaki path. Native runs the same pipelined copies as the
+ * calls without `_opt`. Ozaki GEMM and SYRK upload their operands whole (the
+ * split scales each row by its norm over all of K) and run one device call;
+ * the Ozaki rotation keeps the row-chunked pipeline (each grid row is scaled
+ * by its own norm, so chunks give the same bits). Results equal the `_dev_opt`
+ * entries' bit for bit; AUTO is resolved once per call. Same references as
+ * skgemm_dgemm_packed, skgemm_dsyrk_packed and skgemm_drot. */
+int skgemm_dgemm_packed_opt(int64_t M, int64_t N, int64_t K, const double* A_packed16,
+                            const double* B_packed32, double* D_rowmajor, double alpha,
+                            double gamma, skgemm_options_t* opts);
+int skgemm_dsyrk_packed_opt(int64_t K, int64_t M, const double* A_packed16,
+                            double* C_colmajor, double alpha, double beta,
+                            skgemm_options_t* opts);
+int skgemm_drot_opt(int64_t Nd, int64_t nb, const double* A_gridpacked,
+                    const double* Q_rowmajor, double* D_bandpacked, skgemm_options_t* opts);
 int skgemm_drot_dev(int64_t Nd, int64_t nb, const double* A_gridpacked,
                     const double* Q_rowmajor, double* D_bandpacked, void* stream);
 int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A_gridpacked,

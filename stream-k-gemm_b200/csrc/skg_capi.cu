@@ -777,10 +777,25 @@ SKG_EXPORT int skgemm_drot_band_dev_opt(int64_t Nd, int64_t nb, const double* A_
 // come back (one strided copy) on a second copy stream, so the upload of
 // chunk c + 1 and the download of chunk c - 1 overlap (PCIe is full duplex)
 // and the compute hides under both.
-SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double* Q,
-                           double* D) {
+// `opts` (optional) selects the precision of every chunk; AUTO is resolved
+// once for the whole Nd, so all chunks take the same path. The Ozaki split
+// scales each grid row by its own norm and each column of Q by its norm over
+// the same nb, so a chunk of rows gets exactly the bits the whole call would.
+static int host_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* D,
+                    skgemm_options_t* opts) {
   int st = check_rot(Nd, nb);
   if (st) return st;
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const int pr = auto_precision(ozaki_time_estimate(SKGEMM_OP_ROT, Nd, nb, nb, opts->slices),
+                                  batch_native_estimate(rot_problem(Nd, nb, A, Q, D)));
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return host_rot(Nd, nb, A, Q, D, o);
+    });
+  }
+  if (opts) {
+    opts->err_bound_out = 0.0;
+    opts->slices_used_out = 0;
+  }
   if (Nd == 0 || nb == 0) return SKGEMM_OK;
   if (!A || !Q || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
   DeviceState* dev = current_device(&st);
@@ -813,7 +828,8 @@ SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double
       st = cuda_fail(e, "rotation upload");
       break;
     }
-    if ((st = skgemm_drot_dev(rows, nb, dA + off, dQ, dD + off, sc)) != SKGEMM_OK) break;
+    if ((st = skgemm_drot_dev_opt(rows, nb, dA + off, dQ, dD + off, opts, sc)) != SKGEMM_OK)
+      break;
     e = cudaEventRecord(ev[2 * c + 1], sc);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(so, ev[2 * c + 1], 0);
     // Band b of the chunk (rows x 16 doubles at dD + off + b rows 16) goes to
@@ -835,6 +851,79 @@ SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double
     if (it != dev->ws.end()) ws = it->second;
   }
   return consume_device_error(ws, sc);
+}
+
+SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double* Q,
+                           double* D) {
+  return host_rot(Nd, nb, A, Q, D, nullptr);
+}
+
+SKG_EXPORT int skgemm_drot_opt(int64_t Nd, int64_t nb, const double* A, const double* Q,
+                               double* D, skgemm_options_t* opts) {
+  return host_rot(Nd, nb, A, Q, D, opts);
+}
+
+// Host-pointer GEMM and SYRK with a precision selector. Native runs the
+// k-chunked pipelines of skgemm_dgemm_packed / skgemm_dsyrk_packed. The Ozaki
+// split scales every row by its norm over the whole K, so its operands go up
+// whole and one device call runs them: the result is the device entry's bit
+// for bit (its products are a small fraction of the upload time).
+SKG_EXPORT int skgemm_dgemm_packed_opt(int64_t M, int64_t N, int64_t K, const double* Ap,
+                                       const double* Bp, double* D, double alpha, double gamma,
+                                       skgemm_options_t* opts) {
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const int pr = auto_precision(
+        ozaki_time_estimate(SKGEMM_OP_GEMM_PACKED, M, N, K, opts->slices),
+        batch_native_estimate(gemm_packed_problem(M, N, K, Ap, Bp, D, N, alpha, gamma)));
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return skgemm_dgemm_packed_opt(M, N, K, Ap, Bp, D, alpha, gamma, o);
+    });
+  }
+  if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
+    if (opts) {
+      opts->err_bound_out = 0.0;
+      opts->slices_used_out = 0;
+    }
+    return skgemm_dgemm_packed(M, N, K, Ap, Bp, D, alpha, gamma);
+  }
+  int st = check_dims(M, N, K);
+  if (st) return st;
+  if (M == 0 || N == 0) return SKGEMM_OK;
+  if (!Ap || !Bp || !D) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  HostIO in[2] = {{Ap, (size_t)((M + 15) / 16) * 16 * K * 8},
+                  {Bp, (size_t)((N + 31) / 32) * 32 * K * 8}};
+  return run_host(2, in, D, (size_t)M * N * 8, false, [&](void** d, cudaStream_t s) {
+    return skgemm_dgemm_packed_dev_opt(M, N, K, (const double*)d[0], (const double*)d[1],
+                                       (double*)d[3], N, alpha, gamma, opts, s);
+  });
+}
+
+SKG_EXPORT int skgemm_dsyrk_packed_opt(int64_t K, int64_t M, const double* Ap, double* C,
+                                       double alpha, double beta, skgemm_options_t* opts) {
+  if (opts && opts->precision == SKGEMM_PREC_AUTO) {
+    const int pr = auto_precision(
+        ozaki_time_estimate(SKGEMM_OP_SYRK_PACKED, M, M, K, opts->slices),
+        batch_native_estimate(syrk_problem(K, M, Ap, C, M, alpha, beta)));
+    return run_resolved(opts, pr, [&](skgemm_options_t* o) {
+      return skgemm_dsyrk_packed_opt(K, M, Ap, C, alpha, beta, o);
+    });
+  }
+  if (!opts || opts->precision == SKGEMM_PREC_NATIVE) {
+    if (opts) {
+      opts->err_bound_out = 0.0;
+      opts->slices_used_out = 0;
+    }
+    return skgemm_dsyrk_packed(K, M, Ap, C, alpha, beta);
+  }
+  int st = check_dims(K, M, 0);
+  if (st) return st;
+  if (M == 0) return SKGEMM_OK;
+  if (!Ap || !C) return fail(SKGEMM_ERR_INVALID_ARG, "null pointer");
+  HostIO in[1] = {{Ap, (size_t)((M + 15) / 16) * 16 * K * 8}};
+  return run_host(1, in, C, (size_t)M * M * 8, true, [&](void** d, cudaStream_t s) {
+    return skgemm_dsyrk_packed_dev_opt(K, M, (const double*)d[0], (double*)d[3], M, alpha, beta,
+                                       opts, s);
+  });
 }
 
 // ------------------------------------------------------ layout converters

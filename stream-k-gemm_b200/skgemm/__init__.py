@@ -127,6 +127,10 @@ _SIGS = {
     "skgemm_dsubspace_packed_dev": [_i64, _i64, _vp, _vp, _vp, _i64, _vp, _i64,
                                     ctypes.POINTER(Options), _vp],
     "skgemm_drot": [_i64, _i64, _vp, _vp, _vp],
+    "skgemm_drot_opt": [_i64, _i64, _vp, _vp, _vp, ctypes.POINTER(Options)],
+    "skgemm_dgemm_packed_opt": [_i64, _i64, _i64, _vp, _vp, _vp, _d, _d,
+                                ctypes.POINTER(Options)],
+    "skgemm_dsyrk_packed_opt": [_i64, _i64, _vp, _vp, _d, _d, ctypes.POINTER(Options)],
     "skgemm_drot_dev": [_i64, _i64, _vp, _vp, _vp, _vp],
     "skgemm_drot_dev_opt": [_i64, _i64, _vp, _vp, _vp, ctypes.POINTER(Options), _vp],
     "skgemm_drot_band_dev": [_i64, _i64, _vp, _vp, _vp, _vp],
@@ -252,9 +256,18 @@ class gemm:
                                   _hptr(D, True), alpha, gamma))
 
     @staticmethod
-    def compute_packed(M, N, K, A_packed, B_packed, D, alpha=1.0, gamma=0.0):
-        _check(lib().skgemm_dgemm_packed(M, N, K, _hptr(A_packed), _hptr(B_packed),
-                                         _hptr(D, True), alpha, gamma))
+    def compute_packed(M, N, K, A_packed, B_packed, D, alpha=1.0, gamma=0.0, precision=None,
+                       slices=0):
+        """``precision`` (an addition, default native) routes the host call
+        through the Ozaki split; returns the options (moduli used, bound)."""
+        o = _opts(precision, slices)
+        if o is None:
+            _check(lib().skgemm_dgemm_packed(M, N, K, _hptr(A_packed), _hptr(B_packed),
+                                             _hptr(D, True), alpha, gamma))
+            return None
+        _check(lib().skgemm_dgemm_packed_opt(M, N, K, _hptr(A_packed), _hptr(B_packed),
+                                             _hptr(D, True), alpha, gamma, ctypes.byref(o)))
+        return o
 
     compute_streamk_packed = compute_packed
 
@@ -264,8 +277,14 @@ class sme_syrk:
     C = alpha*A^T*A + beta*C, upper triangle, column-major C."""
 
     @staticmethod
-    def compute(K, M, A_packed, C, alpha=1.0, beta=0.0):
-        _check(lib().skgemm_dsyrk_packed(K, M, _hptr(A_packed), _hptr(C, True), alpha, beta))
+    def compute(K, M, A_packed, C, alpha=1.0, beta=0.0, precision=None, slices=0):
+        o = _opts(precision, slices)
+        if o is None:
+            _check(lib().skgemm_dsyrk_packed(K, M, _hptr(A_packed), _hptr(C, True), alpha, beta))
+            return None
+        _check(lib().skgemm_dsyrk_packed_opt(K, M, _hptr(A_packed), _hptr(C, True), alpha, beta,
+                                             ctypes.byref(o)))
+        return o
 
 
 class sme_gemm_trp_3d:
@@ -273,8 +292,14 @@ class sme_gemm_trp_3d:
     with A grid-packed, B row-major, D band-packed."""
 
     @staticmethod
-    def compute(Nd, nb, A_grid, B, D_band):
-        _check(lib().skgemm_drot(Nd, nb, _hptr(A_grid), _hptr(B), _hptr(D_band, True)))
+    def compute(Nd, nb, A_grid, B, D_band, precision=None, slices=0):
+        o = _opts(precision, slices)
+        if o is None:
+            _check(lib().skgemm_drot(Nd, nb, _hptr(A_grid), _hptr(B), _hptr(D_band, True)))
+            return None
+        _check(lib().skgemm_drot_opt(Nd, nb, _hptr(A_grid), _hptr(B), _hptr(D_band, True),
+                                     ctypes.byref(o)))
+        return o
 
 
 sme_gemm_trp = sme_gemm_trp_3d

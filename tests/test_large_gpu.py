@@ -28,6 +28,18 @@ NS = 2048  # sampled entries per result
 I8, BF, NAT = skgemm.PREC_OZAKI_I8, skgemm.PREC_OZAKI_BF16, skgemm.PREC_NATIVE
 
 
+@pytest.fixture(autouse=True)
+def _release_device_memory():
+    """These cases hold several GB each: return torch's cached blocks and the
+    library's per-stream scratch after every case, so that later tests in the
+    same process find the device's memory free."""
+    yield
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    skgemm.stream_release(torch.cuda.current_stream())
+    skgemm.stream_release(None)
+
+
 def draw(kind, rows, cols, seed):
     """rows x cols float64 on the device: Gaussian N(0,1)/sqrt(rows) or the
     exponent stress sign * 2^e * m (e integer in [-20, 20], m in [1, 2))."""

@@ -383,3 +383,49 @@ def test_auto_precision_rotation(cuda):
         ii, jj = rng.integers(0, Nd, 4096), rng.integers(0, nb, 4096)
         ref = oracle.dot2_sampled(Psi, Q, ii, jj)
         assert oracle.rel_frobenius(got[ii, jj], ref) <= TOL
+
+
+@pytest.mark.parametrize("prec", [OZ, BF, skgemm.PREC_AUTO])
+def test_host_pointer_opt_entries_equal_device_calls(cuda, prec):
+    """skgemm_dgemm_packed_opt / skgemm_dsyrk_packed_opt / skgemm_drot_opt (the
+    reference's blocking host-memory calls with a precision selector) return
+    the device entries' results bit for bit, report the same moduli, and meet
+    the 1e-13 gate against Dot2. K = 40000 is long enough for the native host
+    GEMM to pipeline k-chunks; the Ozaki host calls must not."""
+    K, M, Nd, nb = 40000, 192, 4096, 256
+    Psi = gaussian((K, M), 61, 1 / np.sqrt(K))
+    H = gaussian((K, M), 62, 1 / np.sqrt(K))
+    A16 = np.ascontiguousarray(oracle.pack(np.ascontiguousarray(Psi.T), 16).ravel())
+    B32 = np.ascontiguousarray(oracle.pack(np.ascontiguousarray(H.T), 32).ravel())
+    D = np.zeros(M * M)
+    og = skgemm.gemm.compute_packed(M, M, K, A16, B32, D, 1.25, 0.5, precision=prec)
+    Dd = torch.zeros(M * M, dtype=torch.float64, device="cuda")
+    od = skgemm.dgemm_packed_dev(M, M, K, dev(A16), dev(B32), Dd, M, 1.25, 0.5, precision=prec)
+    C0 = uniform((M, M), 63)
+    C = np.ascontiguousarray(C0.ravel())
+    os_ = skgemm.sme_syrk.compute(K, M, A16, C, 1.0, 0.5, precision=prec)
+    Cd = dev(C0.ravel())
+    osd = skgemm.dsyrk_packed_dev(K, M, dev(A16), Cd, M, 1.0, 0.5, precision=prec)
+    P = gaussian((Nd, nb), 64, 1 / np.sqrt(Nd))
+    Q = uniform((nb, nb), 65)
+    G = np.ascontiguousarray(oracle.grid_pack(P).ravel())
+    R = np.zeros(Nd * nb)
+    orr = skgemm.sme_gemm_trp_3d.compute(Nd, nb, G, np.ascontiguousarray(Q.ravel()), R,
+                                         precision=prec)
+    Rd = torch.zeros(Nd * nb, dtype=torch.float64, device="cuda")
+    ord_ = skgemm.drot_dev(Nd, nb, dev(G), dev(Q), Rd, precision=prec)
+    skgemm.stream_status()
+    for a, b in ((og, od), (os_, osd), (orr, ord_)):
+        assert a.slices_used_out == b.slices_used_out
+    # Ozaki: bit for bit. Where AUTO picked native, the host GEMM and SYRK
+    # pipeline k-chunks (another summation order): within the tolerance.
+    for (host, devr), o in (((D, Dd), og), ((C, Cd), os_), ((R, Rd), orr)):
+        if o.slices_used_out > 0:
+            assert np.array_equal(host, devr.cpu().numpy())
+        else:
+            assert oracle.rel_frobenius(host, devr.cpu().numpy()) <= TOL
+    assert oracle.rel_frobenius(D.reshape(M, M), oracle.dot2_matmul(Psi.T, H, 1.25, 0.5)) <= TOL
+    iu = np.triu_indices(M)
+    S = oracle.dot2_matmul(Psi.T, Psi) + 0.5 * C0.T
+    assert oracle.rel_frobenius(C.reshape(M, M).T[iu], S[iu]) <= TOL
+    assert oracle.rel_frobenius(R, oracle.band_pack(oracle.dot2_matmul(P, Q)).ravel()) <= TOL
