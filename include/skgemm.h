@@ -104,6 +104,17 @@ int skgemm_diag_expire_wait(double budget_ms, void* stream);
  * and the next skgemm_stream_status(stream) returns
  * SKGEMM_ERR_DEVICE_TIMEOUT. No counterpart in the reference. */
 int skgemm_diag_expire_fixup_wait(double budget_ms, void* stream);
+/* Per-kernel timing, off by default. skgemm_kernel_timing(1) clears the
+ * record and starts recording: every launch of the FP64 Stream-K and Ozaki
+ * kernels is then bracketed by two CUDA events on its own stream (a few
+ * microseconds each, so time the workload itself with timing off).
+ * skgemm_kernel_timing(0) stops recording. skgemm_kernel_timing_report
+ * synchronises the recorded events, writes one line per kernel name,
+ * "<name> <launches> <total_ms>\n", into buf (NUL-terminated), clears the
+ * record and returns the number of lines (negative: a status). No
+ * counterpart in the reference. */
+int skgemm_kernel_timing(int enable);
+int skgemm_kernel_timing_report(char* buf, int64_t len);
 /* Measured INT8 tensor-core (tcgen05.mma kind::i8, 128x256x32) throughput of
  * the current device, TOP/s; the roofline denominator of the Ozaki path. */
 int skgemm_probe_i8_peak(double* tops_out);

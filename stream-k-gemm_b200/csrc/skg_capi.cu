@@ -120,6 +120,53 @@ int consume_device_error(StreamWorkspace* ws, cudaStream_t s) {
   return fail(SKGEMM_ERR_DEVICE_TIMEOUT, buf);
 }
 
+// ------------------------------------------------------- kernel timing
+bool g_ktimer_on = false;
+namespace {
+struct KtRecord {
+  const char* name;
+  cudaEvent_t start, stop;
+};
+std::mutex g_kt_mu;
+std::vector<KtRecord> g_kt_records;
+std::vector<cudaEvent_t> g_kt_pool;
+std::map<cudaStream_t, std::pair<const char*, cudaEvent_t>> g_kt_open;
+
+cudaEvent_t kt_event() {
+  if (!g_kt_pool.empty()) {
+    cudaEvent_t e = g_kt_pool.back();
+    g_kt_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+}  // namespace
+
+void ktimer_record(cudaStream_t s, const char* name, bool start) {
+  std::lock_guard<std::mutex> lk(g_kt_mu);
+  cudaEvent_t e = kt_event();
+  if (!e) return;
+  if (cudaEventRecord(e, s) != cudaSuccess) {
+    g_kt_pool.push_back(e);
+    return;
+  }
+  if (start) {
+    auto it = g_kt_open.find(s);
+    if (it != g_kt_open.end()) g_kt_pool.push_back(it->second.second);  // unmatched start
+    g_kt_open[s] = {name, e};
+    return;
+  }
+  auto it = g_kt_open.find(s);
+  if (it == g_kt_open.end()) {
+    g_kt_pool.push_back(e);
+    return;
+  }
+  g_kt_records.push_back({name, it->second.second, e});
+  g_kt_open.erase(it);
+}
+
 // ------------------------------------------------------------------- TMA
 int encode_tiled(CUtensorMap* map, int rank, const void* base, const uint64_t* dims,
                  const uint64_t* strides_bytes, const uint32_t* box, CUtensorMapDataType dtype,
@@ -360,6 +407,56 @@ SKG_EXPORT int skgemm_stream_release(void* stream) {
     }
   }
   return ozaki_release_stream(dev, s);
+}
+
+SKG_EXPORT int skgemm_kernel_timing(int enable) {
+  std::lock_guard<std::mutex> lk(g_kt_mu);
+  if (enable) {
+    for (auto& r : g_kt_records) {
+      g_kt_pool.push_back(r.start);
+      g_kt_pool.push_back(r.stop);
+    }
+    g_kt_records.clear();
+    for (auto& o : g_kt_open) g_kt_pool.push_back(o.second.second);
+    g_kt_open.clear();
+  }
+  g_ktimer_on = enable != 0;
+  return SKGEMM_OK;
+}
+
+SKG_EXPORT int skgemm_kernel_timing_report(char* buf, int64_t len) {
+  std::lock_guard<std::mutex> lk(g_kt_mu);
+  std::map<std::string, std::pair<int64_t, double>> sum;
+  int st = SKGEMM_OK;
+  for (auto& r : g_kt_records) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventSynchronize(r.stop);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, r.start, r.stop);
+    if (e != cudaSuccess) {
+      st = cuda_fail(e, "kernel timing events");
+      break;
+    }
+    auto& v = sum[r.name];
+    v.first += 1;
+    v.second += ms;
+  }
+  for (auto& r : g_kt_records) {
+    g_kt_pool.push_back(r.start);
+    g_kt_pool.push_back(r.stop);
+  }
+  g_kt_records.clear();
+  if (st) return st;
+  std::string out;
+  char line[256];
+  for (auto& kv : sum) {
+    snprintf(line, sizeof(line), "%s %lld %.6f\n", kv.first.c_str(), (long long)kv.second.first,
+             kv.second.second);
+    out += line;
+  }
+  if (!buf || len <= (int64_t)out.size())
+    return fail(SKGEMM_ERR_INVALID_ARG, "kernel timing report: buffer too small");
+  memcpy(buf, out.c_str(), out.size() + 1);
+  return (int)sum.size();
 }
 
 SKG_EXPORT int skgemm_diag_expire_wait(double budget_ms, void* stream) {

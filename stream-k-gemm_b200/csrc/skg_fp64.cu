@@ -189,6 +189,8 @@ int launch_fp64(DeviceState* dev, const Fp64Problem& prob, cudaStream_t s,
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  KernelTimer kt_(s, tile == 64 ? (akm ? "fp64_streamk_kernel64_ak" : "fp64_streamk_kernel64")
+                                 : (akm ? "fp64_streamk_kernel_ak" : "fp64_streamk_kernel"));
   if (tile == 64)
     SKG_CUDA(cudaLaunchKernelEx(&cfg, akm ? fp64_streamk_kernel64_ak : fp64_streamk_kernel64,
                                 mapA, mapB, p));

@@ -677,6 +677,7 @@ template <int L>
 int launch_crt_band(int64_t Nd, int64_t nb, const uint8_t* res, const int* mu, const int* nu,
                     double* D, cudaStream_t s) {
   const int64_t n = Nd * (nb / 8);
+  KernelTimer kt_(s, "crt_residues_band_kernel");
   crt_residues_band_kernel<L><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(Nd, nb, res, nb, mu,
                                                                           nu, D);
   SKG_CUDA(cudaGetLastError());
@@ -934,6 +935,7 @@ int launch_i8_t(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
                                   kI8SmemBytes));
     attr_done[dev->device] = true;
   }
+  KernelTimer kt_(s, "i8_gemm_kernel");
   i8_gemm_kernel<BF><<<grid, kI8Threads, kI8SmemBytes, s>>>(mA, mB, mB2, p);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
@@ -955,6 +957,7 @@ int launch_i8_rot(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB
                                   kI8RotSmemBytes));
     attr_done[dev->device] = true;
   }
+  KernelTimer kt_(s, "i8_rot_kernel");
   i8_rot_kernel<<<grid, kI8Threads, kI8RotSmemBytes, s>>>(mA, mB, mR, p);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
@@ -1024,6 +1027,7 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
                                            (int64_t)dev->num_sms * occ[dev->device]);
   // (every warp of the grid gets at least one tile only if ntiles >= warps;
   // warps without a tile return at once)
+  KernelTimer kt_(s, "convert_tma_kernel");
   convert_tma_kernel<T, L, BF, KM><<<(unsigned)blocks, 256, kConvSmem, s>>>(map, KP, Rpad, mu,
                                                                             res, err);
   SKG_CUDA(cudaGetLastError());
@@ -1047,15 +1051,18 @@ int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, 
   if ((st = res.ensure((size_t)L * Rpad * KP * (bf ? 2 : 1))) != SKGEMM_OK) return st;
   if ((st = part.ensure((size_t)P_in * C * T * sizeof(double))) != SKGEMM_OK) return st;
   if ((st = mu.ensure((size_t)Rpad * sizeof(int))) != SKGEMM_OK) return st;
-  if (km && T == 16)
-    norm_partials_kernel<16, true><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
-                                                                          (double*)part.ptr);
-  else if (km)
-    return fail(SKGEMM_ERR_INVALID_ARG, "K-major operand with 32-wide panels");
-  else
-    norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
-                                                                    (double*)part.ptr);
+  if (km && T != 16) return fail(SKGEMM_ERR_INVALID_ARG, "K-major operand with 32-wide panels");
+  {
+    KernelTimer kt_(s, "norm_partials_kernel");
+    if (km)
+      norm_partials_kernel<16, true><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
+                                                                            (double*)part.ptr);
+    else
+      norm_partials_kernel<T><<<dim3((unsigned)P_in, C), 256, 0, s>>>(R, K, X, C,
+                                                                      (double*)part.ptr);
+  }
   SKG_CUDA(cudaGetLastError());
+  KernelTimer kt_(s, "row_exponents_kernel");
   row_exponents_kernel<T><<<(unsigned)((Rpad + 255) / 256), 256, 0, s>>>(
       R, Rpad, C, (const double*)part.ptr, gamma_for(L), (int*)mu.ptr);
   SKG_CUDA(cudaGetLastError());
@@ -1112,6 +1119,7 @@ int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad
 template <int L, bool BF>
 int launch_local_L(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* src,
                    int64_t panel_stride, int64_t ks, uint8_t* res, int* mu, cudaStream_t s) {
+  KernelTimer kt_(s, "convert_local_kernel");
   convert_local_kernel<L, BF><<<(unsigned)(Rpad / 16), 256, 0, s>>>(R, K, KP, Rpad, src,
                                                                     panel_stride, ks, res, mu);
   SKG_CUDA(cudaGetLastError());
@@ -1171,6 +1179,7 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   p.err = ws->err;
   if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s, bf))) return st;
   const int64_t n = M * N;
+  KernelTimer kt_(s, "crt_partials_kernel");
   crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       (int)M, (int)N, L, (const int32_t*)part.ptr, pl->T, pl->tile_index, pl->tiles_n,
       pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)muB->ptr,
@@ -1222,13 +1231,17 @@ int pair_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t
   SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork2, 0));
   const int64_t n = M * M;
   const unsigned blocks = (unsigned)((n + 255) / 256);
-  crt_partials_kernel<<<blocks, 256, 0, os->aux>>>(
-      (int)M, (int)M, L, (const int32_t*)part.ptr, pl->T, pl->tile_index, pl->tiles_n,
-      pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)os->mu_a.ptr, 1, S,
-      lds, alpha_s, beta_s, beta_s == 0.0 ? 1 : 0);
+  {
+    KernelTimer kt_(os->aux, "crt_partials_kernel");
+    crt_partials_kernel<<<blocks, 256, 0, os->aux>>>(
+        (int)M, (int)M, L, (const int32_t*)part.ptr, pl->T, pl->tile_index, pl->tiles_n,
+        pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)os->mu_a.ptr, 1, S,
+        lds, alpha_s, beta_s, beta_s == 0.0 ? 1 : 0);
+  }
   const cudaError_t e1 = cudaGetLastError();
   SKG_CUDA(cudaEventRecord(os->join2, os->aux));
   if (e1 != cudaSuccess) return cuda_fail(e1, "crt_partials_kernel");
+  KernelTimer kt_(s, "crt_partials_kernel");
   crt_partials_kernel<<<blocks, 256, 0, s>>>(
       (int)M, (int)M, L, (const int32_t*)part.ptr, pl->T, pl->tile_index2, pl->tiles_n,
       pl->mod_slot_off, pl->mod_slots, (const int*)os->mu_a.ptr, (const int*)os->mu_b.ptr, 0, Hs,
@@ -1768,6 +1781,7 @@ int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, cons
   p.err = ws->err;
   if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s))) return st;
   const int64_t n = M * N;
+  KernelTimer kt_(s, "sum_partials_kernel");
   sum_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       (int)M, (int)N, (const int32_t*)os->partials.ptr, pl->T, pl->tile_index, pl->tiles_n,
       pl->mod_slot_off, pl->mod_slots, C, ldc);

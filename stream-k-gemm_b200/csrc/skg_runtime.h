@@ -168,4 +168,22 @@ int batch_consume_error(DeviceState* dev, cudaStream_t s);
 // Reads and clears the error word of `ws` (synchronises `s`).
 int consume_device_error(StreamWorkspace* ws, cudaStream_t s);
 
+// Per-kernel timing (off by default; skgemm_kernel_timing). While it is on,
+// a KernelTimer around a launch records a CUDA event before and after it on
+// the launch's stream, under the kernel's name; skgemm_kernel_timing_report
+// sums the elapsed times per name. While it is off a KernelTimer only reads
+// one flag.
+extern bool g_ktimer_on;
+void ktimer_record(cudaStream_t s, const char* name, bool start);
+struct KernelTimer {
+  cudaStream_t s;
+  const char* name;
+  KernelTimer(cudaStream_t s_, const char* n) : s(s_), name(n) {
+    if (g_ktimer_on) ktimer_record(s, name, true);
+  }
+  ~KernelTimer() {
+    if (g_ktimer_on) ktimer_record(s, name, false);
+  }
+};
+
 }  // namespace skg

@@ -110,6 +110,8 @@ _SIGS = {
     "skgemm_stream_status": [_vp],
     "skgemm_probe_fp64_peak": [ctypes.POINTER(ctypes.c_double)],
     "skgemm_diag_expire_wait": [ctypes.c_double, _vp],
+    "skgemm_kernel_timing": [ctypes.c_int],
+    "skgemm_kernel_timing_report": [ctypes.c_char_p, _i64],
     "skgemm_diag_expire_fixup_wait": [ctypes.c_double, _vp],
     "skgemm_probe_i8_peak": [ctypes.POINTER(ctypes.c_double)],
     "skgemm_igemm_s8_dev": [_i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp],
@@ -548,6 +550,25 @@ def diag_expire_fixup_wait(budget_ms, stream=None) -> None:
     """Enqueue the Stream-K fixup's flag wait on a flag nothing sets, with
     budget_ms; the next stream_status(stream) raises ERR_DEVICE_TIMEOUT."""
     _check(lib().skgemm_diag_expire_fixup_wait(float(budget_ms), _stream(stream)))
+
+
+def kernel_timing(enable: bool) -> None:
+    """Start (clearing the record) or stop per-kernel event timing."""
+    _check(lib().skgemm_kernel_timing(1 if enable else 0))
+
+
+def kernel_timing_report() -> dict:
+    """{kernel name: (launches, total ms)} recorded since kernel_timing(True)
+    (synchronises; clears the record)."""
+    buf = ctypes.create_string_buffer(1 << 16)
+    n = lib().skgemm_kernel_timing_report(buf, len(buf))
+    if n < 0:
+        _check(n)
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, cnt, ms = line.split()
+        out[name] = (int(cnt), float(ms))
+    return out
 
 
 def probe_i8_peak() -> float:
