@@ -49,6 +49,7 @@ sys.path.insert(0, REPO)
 sys.path.insert(0, os.path.join(REPO, "stream-k-gemm_b200"))
 
 ND, NB = 110592, 512
+ND0, NB0 = ND, NB  # the configuration's shape (set_shape changes ND, NB)
 FLOP_SYRK = NB * (NB + 1) * ND
 FLOP_GEMM = 2 * NB * NB * ND
 FLOP_ROT = 2 * ND * NB * NB
@@ -63,10 +64,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="skgemm", choices=["skgemm", "reference"])
-    ap.add_argument("--precision", default="native",
-                    choices=["native", "ozaki", "ozaki_bf16", "auto"],
-                    help="ozaki: INT8 residues; ozaki_bf16: BF16 residues (same results); "
+    ap.add_argument("--precision", default="both",
+                    choices=["both", "native", "ozaki", "ozaki_bf16", "auto"],
+                    help="subspace: both (default) times native and Ozaki INT8 in one run; "
+                         "ozaki: INT8 residues; ozaki_bf16: BF16 residues (same results); "
                          "auto: per call (subspace) or per problem (batched), the faster path")
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="subspace: requests of the serving sub-object run after the step "
+                         "(native and Ozaki; 0 = skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nd", type=int, default=ND,
@@ -85,6 +90,9 @@ def parse():
                          "scratch for the largest request)")
     ap.add_argument("--serve-policy", default="smallest", choices=["smallest", "fifo"],
                     help="serving: admission order (aged least-work-first, or arrival order)")
+    ap.add_argument("--serve-aging", type=float, default=0.25,
+                    help="serving, least-work-first: seconds of waiting that count as one "
+                         "unit of priority")
     ap.add_argument("--instances", type=int, default=64, help="batched: k-point instances")
     ap.add_argument("--max-grid", type=int, default=0,
                     help="batched: cap on grid points per instance (smaller cases for profiling)")
@@ -218,8 +226,15 @@ def job_throughput(flop_per_step, steps, world, max_ms):
 
 
 # ------------------------------------------------------------------ inputs
+N_CHECK_STATES = 48    # states whose pairs sample S and Hs for the in-run error
+N_CHECK_ROWS = 64      # grid rows sampling the rotation's error
+FALLBACK_HBM_GBS = 6650.0
+
+
 def make_inputs(device):
-    """Seeded synthetic inputs of the workload, generated on the device."""
+    """Seeded synthetic inputs of the workload, generated on the device; also
+    the slices the in-run accuracy check needs (columns of Psi and H Psi for
+    N_CHECK_STATES states, N_CHECK_ROWS rows of Psi)."""
     import torch
     import skgemm
     g = torch.Generator(device=device).manual_seed(20240611)
@@ -233,55 +248,156 @@ def make_inputs(device):
     skgemm.pack_dev(NB, ND, psi, 1, NB, 16, band)   # band-packed Psi
     skgemm.pack_dev(NB, ND, hpsi, 1, NB, 32, h32)   # 32-band-packed H Psi
     skgemm.pack_dev(ND, NB, psi, NB, 1, 16, grid)   # grid-packed Psi
+    gc = torch.Generator().manual_seed(7)
+    st = torch.randperm(NB, generator=gc)[:min(N_CHECK_STATES, NB)].sort().values
+    gs = torch.randperm(ND, generator=gc)[:min(N_CHECK_ROWS, ND)].sort().values
+    check = {"st": st, "gs": gs, "psi_cols": psi[:, st.to(device)].contiguous(),
+             "hpsi_cols": hpsi[:, st.to(device)].contiguous(),
+             "psi_rows": psi[gs.to(device)].contiguous()}
     torch.cuda.synchronize()
     del psi, hpsi
-    return band, h32, grid, q
+    return band, h32, grid, q, check
+
+
+def dd_products(X, Y, chunk=8192):
+    """X^T Y for X (K, m), Y (K, n) on the device in double-double arithmetic:
+    Dekker's exact products (each factor split into 26-bit halves) and
+    Knuth's TwoSum in a pairwise tree, the error terms carried beside the sums;
+    every step is a separate elementwise torch operation, so nothing is fused
+    into an FMA. Accurate to about 2^-104 of sum |x y|: an independent
+    reference for the library's results (it uses none of the library's
+    kernels)."""
+    import torch
+    c = 134217729.0  # 2^27 + 1
+
+    def split(a):
+        t = a * c
+        hi = t - (t - a)
+        return hi, a - hi
+
+    def two_sum(a, b):
+        s = a + b
+        bb = s - a
+        return s, (a - (s - bb)) + (b - bb)
+
+    m, n = X.shape[1], Y.shape[1]
+    hi_tot = torch.zeros(m, n, dtype=torch.float64, device=X.device)
+    lo_tot = torch.zeros_like(hi_tot)
+    for k0 in range(0, X.shape[0], chunk):
+        x = X[k0:k0 + chunk, :, None]
+        y = Y[k0:k0 + chunk, None, :]
+        p = x * y
+        xh, xl = split(x)
+        yh, yl = split(y)
+        e = ((xh * yh - p) + xh * yl + xl * yh) + xl * yl    # p + e = x y exactly
+        while p.shape[0] > 1:
+            if p.shape[0] % 2:
+                p = torch.cat([p, torch.zeros_like(p[:1])])
+                e = torch.cat([e, torch.zeros_like(e[:1])])
+            s, err = two_sum(p[0::2], p[1::2])
+            e = e[0::2] + e[1::2] + err
+            p = s
+        hi_tot, err = two_sum(hi_tot, p[0])
+        lo_tot = lo_tot + e[0] + err
+    return hi_tot + lo_tot
+
+
+def subspace_errors(S, Hs, Pn, check):
+    """Relative Frobenius errors of S (upper triangle), Hs and Psi' on the
+    sampled entries against the double-double reference."""
+    import torch
+    st, gs = check["st"], check["gs"]
+    X, Y, R = check["psi_cols"], check["hpsi_cols"], check["psi_rows"]
+    dev = X.device
+    s_ref = dd_products(X, X)
+    h_ref = dd_products(X, Y)
+    q = check["q"]
+    r_ref = dd_products(R.t().contiguous(), q)            # (rows, NB)
+    sd, gd = st.to(dev), gs.to(dev)
+    a, b = torch.meshgrid(torch.arange(len(st), device=dev), torch.arange(len(st), device=dev),
+                          indexing="ij")
+    up = a <= b
+    # S is column-major: S[i + j*NB] = S(i, j), i <= j.
+    s_got = S.view(-1)[(sd[a] + sd[b] * NB)[up]]
+    h_got = Hs.view(-1)[sd[a] * NB + sd[b]].view(len(st), len(st))
+    bb = torch.arange(NB, device=dev)
+    P = Pn.view(NB // 16, ND, 16)
+    r_got = P[(bb // 16)[None, :], gd[:, None], (bb % 16)[None, :]]
+
+    def rel(x, r):
+        return float(torch.linalg.norm(x - r) / torch.linalg.norm(r))
+
+    return {"S": rel(s_got, s_ref[up]), "Hs": rel(h_got, h_ref), "Psi_Q": rel(r_got, r_ref)}
+
+
+def measured_peaks():
+    """HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json when present, else
+    the pool's fallback figure; returns (value, source)."""
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)"
+    except (OSError, KeyError, ValueError, TypeError):
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
 
 
 # ----------------------------------------------------------- GPU arm
-def run_gpu(args):
-    import numpy as np
-    import torch
-    import skgemm
+PREC_NAMES = ("native", "ozaki", "ozaki_bf16", "auto")
 
-    rank, world, dist = dist_setup(args.gpus)
-    dev = torch.device("cuda", torch.cuda.current_device())
-    prec = {"native": None, "ozaki": skgemm.PREC_OZAKI_I8,
-            "ozaki_bf16": skgemm.PREC_OZAKI_BF16, "auto": skgemm.PREC_AUTO}[args.precision]
-    band, h32, grid, q = make_inputs(dev)
-    S = torch.zeros(NB, NB, dtype=torch.float64, device=dev)
-    Hs = torch.zeros_like(S)
-    Pn = torch.empty_like(band)
-    stream = torch.cuda.current_stream()
-    peak = skgemm.probe_fp64_peak()
 
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+def _prec(skgemm, name):
+    return {"native": None, "ozaki": skgemm.PREC_OZAKI_I8,
+            "ozaki_bf16": skgemm.PREC_OZAKI_BF16, "auto": skgemm.PREC_AUTO}[name]
 
-    def step(evs=None):
+
+class Step:
+    """One subspace step (S, Hs, Psi') on device-resident inputs."""
+
+    def __init__(self, skgemm, prec, band, h32, grid, q, S, Hs, Pn, stream, rot_layout):
+        self.k, self.prec = skgemm, prec
+        self.band, self.h32, self.grid, self.q = band, h32, grid, q
+        self.S, self.Hs, self.Pn, self.stream = S, Hs, Pn, stream
+        self.rot_layout = rot_layout
+        self.opts = {}
+
+    def __call__(self, evs=None):
+        k, s = self.k, self.stream
         if evs:
-            evs[0].record(stream)
-        if prec is None:
-            skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, 1.0, 0.0, stream=stream)
+            evs[0].record(s)
+        if self.prec is None:
+            k.dsyrk_packed_dev(ND, NB, self.band, self.S, NB, 1.0, 0.0, stream=s)
             if evs:
-                evs[1].record(stream)
-            skgemm.dgemm_packed_dev(NB, NB, ND, band, h32, Hs, NB, 1.0, 0.0, stream=stream)
+                evs[1].record(s)
+            k.dgemm_packed_dev(NB, NB, ND, self.band, self.h32, self.Hs, NB, 1.0, 0.0, stream=s)
         else:
             # S and Hs share one split of Psi (skgemm_dsubspace_packed_dev).
-            skgemm.dsubspace_packed_dev(ND, NB, band, h32, S, Hs, stream=stream, precision=prec)
+            self.opts["pair"] = k.dsubspace_packed_dev(ND, NB, self.band, self.h32, self.S,
+                                                       self.Hs, stream=s, precision=self.prec)
             if evs:
-                evs[1].record(stream)
+                evs[1].record(s)
         if evs:
-            evs[2].record(stream)
-        if args.rot_layout == "band":
-            skgemm.drot_band_dev(ND, NB, band, q, Pn, stream=stream, precision=prec)
+            evs[2].record(s)
+        if self.rot_layout == "band":
+            o = k.drot_band_dev(ND, NB, self.band, self.q, self.Pn, stream=s, precision=self.prec)
         else:
-            skgemm.drot_dev(ND, NB, grid, q, Pn, stream=stream, precision=prec)
+            o = k.drot_dev(ND, NB, self.grid, self.q, self.Pn, stream=s, precision=self.prec)
+        self.opts["rot"] = o
         if evs:
-            evs[3].record(stream)
+            evs[3].record(s)
 
+
+def time_step(step, args, dist, torch):
+    """W untimed steps, then K steps bracketed by barriers and a device
+    synchronise, CUDA events on the launching stream; clocks sampled during
+    the timed region. Returns (max-over-ranks total ms, per-op ms array,
+    clocks)."""
+    import numpy as np
+    stream = step.stream
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     for _ in range(args.warmup):
         step()
-    skgemm.stream_status(stream)
+    step.k.stream_status(stream)
     clocks = ClockSampler(torch.cuda.current_device())
     barrier(dist)
     clocks.start()
@@ -293,55 +409,194 @@ def run_gpu(args):
     t1.record(stream)
     barrier(dist)
     clk = clocks.stop()
-    skgemm.stream_status(stream)
+    step.k.stream_status(stream)
     total_ms = max_over_ranks(t0.elapsed_time(t1), dist)
     per_op = np.array([[ev[i][j].elapsed_time(ev[i][j + 1]) for j in range(3)]
                        for i in range(args.steps)])
-    step_ms = per_op.sum(axis=1)
-    kernel_ms = float(per_op.sum())
-    achieved = FLOP_STEP * args.steps / (kernel_ms * 1e-3) / 1e12
-    if prec is None:
-        op_ms = {"syrk": round(float(per_op[:, 0].mean()), 4),
-                 "gemm": round(float(per_op[:, 1].mean()), 4),
-                 "rotation": round(float(per_op[:, 2].mean()), 4)}
-        op_tf = {"syrk": round(FLOP_SYRK / per_op[:, 0].mean() / 1e9, 3),
-                 "gemm": round(FLOP_GEMM / per_op[:, 1].mean() / 1e9, 3),
-                 "rotation": round(FLOP_ROT / per_op[:, 2].mean() / 1e9, 3)}
-    else:
-        pair = per_op[:, 0] + per_op[:, 1]
-        op_ms = {"syrk+gemm": round(float(pair.mean()), 4),
-                 "rotation": round(float(per_op[:, 2].mean()), 4)}
-        op_tf = {"syrk+gemm": round((FLOP_SYRK + FLOP_GEMM) / pair.mean() / 1e9, 3),
-                 "rotation": round(FLOP_ROT / per_op[:, 2].mean() / 1e9, 3)}
+    return total_ms, per_op, clk
 
+
+def time_calls(fn, stream, torch, reps=10, warm=2):
+    """Mean ms of fn() over reps calls (CUDA events on `stream`)."""
+    for _ in range(warm):
+        fn()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        fn()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def kernel_rooflines(skgemm, step, torch, steps, peaks):
+    """Per-kernel times of `steps` more steps with the library's event timer
+    on (outside the timed region), each kernel rated against its roofline:
+    FP64 Stream-K kernels against the FP64 DMMA peak, INT8 products against
+    the INT8 peak, conversions / norms / reconstructions against HBM.
+    Algorithmic work per launch: GEMM 2 M N K, SYRK M (M+1) K, rotation
+    2 Nd nb^2 (INT8 ops: the same times the moduli count L); conversion 8 + L
+    bytes per element (8 + 2 L with BF16 residues), norms 8 B per element,
+    rotation reconstruction L + 8 B per element."""
+    fp64_peak, i8_peak, hbm = peaks
+    skgemm.kernel_timing(True)
+    for _ in range(steps):
+        step()
+    skgemm.stream_status(step.stream)
+    rep = skgemm.kernel_timing_report()
+    skgemm.kernel_timing(False)
+    E = ND * NB
+    out = {}
+    if step.prec is None:
+        work = {"fp64_streamk_kernel64": (FLOP_SYRK + FLOP_ROT, "TFLOP/s", fp64_peak, "tensor"),
+                "fp64_streamk_kernel": (FLOP_GEMM, "TFLOP/s", fp64_peak, "tensor"),
+                "fp64_streamk_kernel64_ak": (FLOP_ROT, "TFLOP/s", fp64_peak, "tensor")}
+        if step.rot_layout == "band":
+            work["fp64_streamk_kernel64"] = (FLOP_SYRK, "TFLOP/s", fp64_peak, "tensor")
+    else:
+        Lp = step.opts["pair"].slices_used_out
+        Lr = step.opts["rot"].slices_used_out
+        rb = 2 if step.prec == skgemm.PREC_OZAKI_BF16 else 1
+        work = {"i8_gemm_kernel": (Lp * (FLOP_SYRK + FLOP_GEMM), "TOP/s", i8_peak, "tensor"),
+                "i8_rot_kernel": (Lr * FLOP_ROT, "TOP/s", i8_peak, "tensor"),
+                "convert_tma_kernel": (E * (3 * 8 + rb * (2 * Lp + Lr)), "GB/s", hbm, "hbm"),
+                "norm_partials_kernel": (3 * E * 8, "GB/s", hbm, "hbm"),
+                "crt_residues_band_kernel": (E * (rb * Lr + 8), "GB/s", hbm, "hbm")}
+    total = sum(ms for _, ms in rep.values()) or 1.0
+    for name, (n, ms) in sorted(rep.items(), key=lambda kv: -kv[1][1]):
+        row = {"launches_per_step": round(n / steps, 2), "ms_per_launch": round(ms / n, 4),
+               "share": round(ms / total, 4)}
+        if name in work:
+            w, unit, peak, bound = work[name]
+            scale = 1e12 if unit in ("TFLOP/s", "TOP/s") else 1e9
+            ach = w * steps / (ms * 1e-3) / scale
+            row.update({"bound": bound, "achieved": round(ach, 3), "peak": round(peak, 3),
+                        "unit": unit, "frac": round(ach / peak, 4),
+                        "work_per_step": w})
+        out[name] = row
+    return out
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import skgemm
+
+    rank, world, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    names = ["native", "ozaki"] if args.precision == "both" else [args.precision]
+    band, h32, grid, q, check = make_inputs(dev)
+    check["q"] = q
+    S = torch.zeros(NB, NB, dtype=torch.float64, device=dev)
+    Hs = torch.zeros_like(S)
+    Pn = torch.empty_like(band)
+    stream = torch.cuda.current_stream()
+    fp64_peak = skgemm.probe_fp64_peak()
+    i8_peak = skgemm.probe_i8_peak()
+    hbm, hbm_src = measured_peaks()
+
+    res = {}
+    for name in names:
+        step = Step(skgemm, _prec(skgemm, name), band, h32, grid, q, S, Hs, Pn, stream,
+                    args.rot_layout)
+        total_ms, per_op, clk = time_step(step, args, dist, torch)
+        step_ms = per_op.sum(axis=1)
+        r = {"tflops": round(job_throughput(FLOP_STEP, args.steps, world, total_ms), 3),
+             "ms_per_step": round(total_ms / args.steps, 4),
+             "latency_ms": {"p50": round(float(np.percentile(step_ms, 50)), 4),
+                            "p99": round(float(np.percentile(step_ms, 99)), 4)},
+             "clocks": clk}
+        if step.prec is None:
+            ops = {"syrk": (per_op[:, 0], FLOP_SYRK), "gemm": (per_op[:, 1], FLOP_GEMM),
+                   "rotation": (per_op[:, 2], FLOP_ROT)}
+        else:
+            ops = {"syrk+gemm": (per_op[:, 0] + per_op[:, 1], FLOP_SYRK + FLOP_GEMM),
+                   "rotation": (per_op[:, 2], FLOP_ROT)}
+        r["op_ms"] = {k: round(float(v.mean()), 4) for k, (v, _) in ops.items()}
+        r["op_tflops"] = {k: round(f / v.mean() / 1e9, 3) for k, (v, f) in ops.items()}
+        if step.prec is not None:
+            r["moduli"] = {"syrk+gemm": step.opts["pair"].slices_used_out,
+                           "rotation": step.opts["rot"].slices_used_out}
+        # Accuracy of this precision's results (the last timed step's outputs).
+        r["rel_frobenius_error"] = {k: float(f"{v:.3e}")
+                                    for k, v in subspace_errors(S, Hs, Pn, check).items()}
+        r["kernels"] = kernel_rooflines(skgemm, step, torch, 3, (fp64_peak, i8_peak, hbm))
+        res[name] = r
+
+    # Standalone SYRK and GEMM (the reference's one-call-at-a-time use).
+    alone = {}
+    if len(names) > 1 or names[0] != "native":
+        for name in names:
+            p = _prec(skgemm, name)
+            alone[name] = {
+                "syrk_ms": round(time_calls(lambda: skgemm.dsyrk_packed_dev(
+                    ND, NB, band, S, NB, stream=stream, precision=p), stream, torch), 4),
+                "gemm_ms": round(time_calls(lambda: skgemm.dgemm_packed_dev(
+                    NB, NB, ND, band, h32, Hs, NB, stream=stream, precision=p), stream, torch), 4),
+                "rotation_ms": round(time_calls(lambda: skgemm.drot_dev(
+                    ND, NB, grid, q, Pn, stream=stream, precision=p), stream, torch), 4)}
+        skgemm.stream_status(stream)
+
+    ok = {n: max(r["rel_frobenius_error"].values()) <= 1e-13 for n, r in res.items()}
+    head = "ozaki" if "ozaki" in res and ok["ozaki"] else names[0]
+    H = res[head]
+    per_kernel = H["kernels"]
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["share"])
+    dk = per_kernel[dom]
+    traffic = read_profile_traffic(dom)
     line = {
-        "metric": METRIC, "value": round(job_throughput(FLOP_STEP, args.steps, world, total_ms), 3),
-        "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": METRIC, "value": H["tflops"], "unit": "TFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": H["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "Nd": ND, "nb": NB, "ops": ["syrk", "gemm", "rotation"],
-                   "precision": args.precision, "rot_layout": args.rot_layout,
-                   "parallelism": f"replicas{world}",
+                   "precision": head,
+                   "value_is": (f"the {head} step (FP64-accurate: measured error <= 1e-13 on "
+                                f"every result)" if ok[head] else
+                                f"the {head} step (measured error above 1e-13)"),
+                   "rot_layout": args.rot_layout, "parallelism": f"replicas{world}",
                    "flop_per_step": FLOP_STEP, "l2": "inputs larger than L2 (453 MB each)"},
-        "latency_ms": dict({"p50": round(float(np.percentile(step_ms, 50)), 4),
-                            "p99": round(float(np.percentile(step_ms, 99)), 4)}, **op_ms),
-        "op_tflops": op_tf,
-        "roofline": {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
-                     "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
-                     "peak_source": "measured FP64 DMMA peak (skgemm_probe_fp64_peak, this run)",
-                     "kernel": "fp64_streamk_kernel64 (SYRK, rotation), fp64_streamk_kernel "
-                               "(GEMM)" if prec is None else
-                     "Ozaki split (i8_gemm_kernel + residue conversion), FP64-equivalent flops",
-                     "traffic": read_profile_traffic() if prec is None else None},
-        "clocks": clk,
-        # Ozaki step (ncu launch list): S+Hs = 2 x (norm partials + row
-        # exponents + conversion) + fused products + 2 reconstructions; the
-        # rotation = norms + exponents + conversion + Q's residues + products
-        # + reconstruction.
-        "gpu_launches": (3 if prec is None else 15) * args.steps,
+        "latency_ms": H["latency_ms"],
+        "roofline": {"bound": dk.get("bound"), "achieved": dk.get("achieved"),
+                     "peak": dk.get("peak"), "unit": dk.get("unit"), "frac": dk.get("frac"),
+                     "traffic": traffic, "kernel": dom, "share_of_step": dk["share"],
+                     "peak_source": {"tensor": "measured in this run (skgemm_probe_fp64_peak / "
+                                               "skgemm_probe_i8_peak)",
+                                     "hbm": hbm_src}.get(dk.get("bound"), None),
+                     "timing": "CUDA events around each launch on its stream (library kernel "
+                               "timer), 3 steps after the timed region"},
+        "clocks": H["clocks"],
+        "gpu_launches": 0,
     }
+    line["native"] = res.get("native")
+    line["ozaki"] = res.get("ozaki")
+    if args.precision not in ("both", "native", "ozaki"):
+        line[args.precision] = res[args.precision]
+    # Every kernel of the library in a step, counted by its event timer.
+    line["gpu_launches"] = int(round(sum(k["launches_per_step"] for k in per_kernel.values())
+                                     * args.steps))
+    if alone:
+        line["standalone_ms"] = alone
+        if "native" in alone and "ozaki" in alone:
+            a, o = alone["native"], alone["ozaki"]
+            line["speedup_ozaki_vs_native"] = {
+                "step": round(res["native"]["ms_per_step"] / res["ozaki"]["ms_per_step"], 3),
+                "syrk": round(a["syrk_ms"] / o["syrk_ms"], 3),
+                "gemm": round(a["gemm_ms"] / o["gemm_ms"], 3),
+                "rotation": round(a["rotation_ms"] / o["rotation_ms"], 3)}
+    del check
     if not args.no_e2e:
-        line["e2e"] = run_e2e(args, band, h32, grid, q, dist)
+        line["e2e"] = run_e2e(args, band, h32, grid, q, dist, _prec(skgemm, head), head)
+    del band, h32, grid, S, Hs, Pn
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    skgemm.stream_release(stream)
+    if world == 1 and args.serve_requests > 0:
+        line["serving"] = {
+            n: serve_measure(args, n, args.serve_requests, rank, None)
+            for n in ("native", "ozaki")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
@@ -350,24 +605,28 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-def read_profile_traffic():
-    """DRAM bytes (read + write) per launch of the dominant kernel, from the
-    committed ncu summary of the same workload (mean of its three launches)."""
-    path = os.path.join(REPO, "profiles", "fp64_streamk_kernel_dft_subspace.md")
-    if not os.path.exists(path):
+def read_profile_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` on this workload, from
+    the committed ncu summaries (their `traffic_bytes_per_launch <kernel>:`
+    lines), or None."""
+    pdir = os.path.join(REPO, "profiles")
+    if not os.path.isdir(pdir):
         return None
-    for line in open(path):
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
+    key = f"traffic_bytes_per_launch {kernel}:"
+    for fn in sorted(os.listdir(pdir)):
+        for line in open(os.path.join(pdir, fn)):
+            if line.startswith(key):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
     return None
 
 
-def run_e2e(args, band, h32, grid, q, dist):
+def run_e2e(args, band, h32, grid, q, dist, prec, name):
     """Same step through the blocking host-pointer C ABI (the reference-facing
-    call): inputs copied from pinned host memory and results read back every step."""
+    calls, with the precision selector of their `_opt` forms): inputs copied
+    from pinned host memory and results read back every step."""
     import torch
     import skgemm
     hb = band.cpu().pin_memory().numpy()
@@ -379,9 +638,9 @@ def run_e2e(args, band, h32, grid, q, dist):
     Pn = torch.zeros(ND * NB, dtype=torch.float64).pin_memory().numpy()
 
     def step():
-        skgemm.sme_syrk.compute(ND, NB, hb, S, 1.0, 0.0)
-        skgemm.gemm.compute_packed(NB, NB, ND, hb, hh, Hs, 1.0, 0.0)
-        skgemm.sme_gemm_trp_3d.compute(ND, NB, hg, hq, Pn)
+        skgemm.sme_syrk.compute(ND, NB, hb, S, 1.0, 0.0, precision=prec)
+        skgemm.gemm.compute_packed(NB, NB, ND, hb, hh, Hs, 1.0, 0.0, precision=prec)
+        skgemm.sme_gemm_trp_3d.compute(ND, NB, hg, hq, Pn, precision=prec)
 
     steps = max(2, min(args.steps, 5))
     for _ in range(2):
@@ -394,10 +653,14 @@ def run_e2e(args, band, h32, grid, q, dist):
     h2d = hb.nbytes * 2 + hh.nbytes + hg.nbytes + hq.nbytes + S.nbytes
     d2h = S.nbytes + Hs.nbytes + Pn.nbytes
     world = 1 if dist is None else dist.get_world_size()
+    api = ("skgemm_dsyrk_packed + skgemm_dgemm_packed + skgemm_drot (host pointers)"
+           if prec is None else
+           "skgemm_dsyrk_packed_opt + skgemm_dgemm_packed_opt + skgemm_drot_opt (host pointers, "
+           f"precision {name})")
     return {"value": round(FLOP_STEP * steps * world / el / 1e12, 4), "unit": "TFLOP/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "ms_per_step": round(el / steps * 1e3, 3), "steps": steps,
-            "api": "skgemm_dsyrk_packed + skgemm_dgemm_packed + skgemm_drot (host pointers)"}
+            "ms_per_step": round(el / steps * 1e3, 3), "steps": steps, "precision": name,
+            "api": api}
 
 
 # ------------------------------------------------------------ kernel tour
@@ -618,7 +881,89 @@ def cpu_baseline(sample_seconds=10.0, kslice=ND):
             "sample": f"{len(times)} passes of the three ops on {kslice} of {ND} grid points; "
                       f"reference kernels sme_syrk.hpp / gemm_opt.cpp / sme_trp_3d.hpp built "
                       f"-O3 (AVX2) with the host SME-intrinsic emulation, OpenMP {cores} threads",
-            "seconds": round(sum(times), 3)}
+            "seconds": round(sum(times), 3), "cpu_model": cpu_model(),
+            "host_has_sme": host_has_sme(),
+            "also": cpu_naive_baselines()}
+
+
+def host_has_sme() -> bool:
+    """Arm SME on this host (aarch64 `Features: ... sme`; the x86 `sme` flag
+    is AMD's memory encryption and does not count)."""
+    import platform
+    if platform.machine() not in ("aarch64", "arm64"):
+        return False
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("Features") and "sme" in line.split(":", 1)[1].split():
+                return True
+    except OSError:
+        pass
+    return False
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def naive_pass(L, kslice, threads, inputs):
+    """One pass of the reference's portable naive loops (gemm_opt.cpp:467-475,
+    syrk_crsp.cpp:355-373, trp_3d_test.cpp:55-66, as restated in the oracle)
+    on a K-slice of the workload; returns seconds."""
+    import oracle
+    A_col, B_row, A16, grid, q, D, C, P = inputs
+    p = oracle.ptr
+    t = time.perf_counter()
+    L.oracle_syrk_naive(kslice, NB, p(A16), p(C), 1.0, 0.0, threads)
+    L.oracle_gemm_naive(NB, NB, kslice, p(A_col), p(B_row), p(D), 1.0, 0.0, threads)
+    L.oracle_rot_naive(kslice, NB, p(grid), p(q), p(P), threads)
+    return time.perf_counter() - t
+
+
+def cpu_naive_baselines(target_s=6.0):
+    """The reference's portable naive loops built -O3 -march=native on this
+    host: serial on 1 core (as the reference runs them), and the same loops
+    with their outer loop split over all cores by OpenMP (a restatement, not
+    the reference's code). Each times a K-slice of the workload sized to about
+    target_s seconds; TFLOP/s are per flop of that slice (the loops' cost is
+    linear in K, so it extrapolates to the full 110592 grid points)."""
+    import numpy as np
+    import oracle
+    try:
+        L = oracle.naive_native()
+    except Exception as e:  # no compiler on this host
+        return [{"unavailable": f"naive loops not built: {e}"}]
+    cores = os.cpu_count() or 1
+    out = []
+    for threads, label in ((1, "reference portable naive loops, serial (1 core)"),
+                           (cores, f"OpenMP outer-loop restatement of the naive loops "
+                                   f"({cores} cores)")):
+        ks = 256
+        while True:
+            rng = np.random.default_rng(5)
+            X = rng.standard_normal((ks, NB)) / ND ** 0.5
+            Y = rng.standard_normal((ks, NB)) / ND ** 0.5
+            inputs = (np.ascontiguousarray(X).ravel(),    # A col-major: A[i + k M] = X[k, i]
+                      np.ascontiguousarray(Y).ravel(),    # B row-major: B[k N + j] = Y[k, j]
+                      oracle.pack(np.ascontiguousarray(X.T), 16).ravel(),
+                      oracle.grid_pack(X).ravel(), rng.uniform(-1, 1, NB * NB),
+                      np.zeros(NB * NB), np.zeros(NB * NB), np.zeros(ks * NB))
+            sec = naive_pass(L, ks, threads, inputs)
+            if sec >= target_s / 4 or ks >= ND:
+                break
+            ks = min(ND, int(ks * min(8.0, max(2.0, target_s / max(sec, 1e-3)))) // 16 * 16)
+        flops = (NB * (NB + 1) + 2 * NB * NB) * ks + 2 * ks * NB * NB
+        out.append({"value": round(flops / sec / 1e12, 6), "unit": "TFLOP/s", "cores": threads,
+                    "kind": "port", "label": label,
+                    "sample": f"the three ops on a {ks}-grid-point slice of {ND} "
+                              f"(per-flop rate; the loops are linear in K), -O3 -march=native",
+                    "seconds": round(sec, 3)})
+    return out
 
 
 def run_reference(args):
@@ -702,6 +1047,8 @@ def run_batched(args):
                   skgemm.batch_item(skgemm.OP_GEMM_PACKED, nb, nb, ng, p16, h32, Hs, nb)]
         flop += nb * nb * ng + 2.0 * nb * nb * ng
     stream = torch.cuda.current_stream()
+    if args.precision == "both":
+        args.precision = "native"
     prec = {"native": skgemm.PREC_NATIVE, "ozaki": skgemm.PREC_OZAKI_I8,
             "ozaki_bf16": skgemm.PREC_OZAKI_BF16,
             "auto": skgemm.PREC_AUTO}[args.precision]
@@ -760,15 +1107,16 @@ def run_batched(args):
 
 
 # ------------------------------------------------------------ serving arm
-def run_serving(args):
+def serve_measure(args, name, requests, rank, dist):
+    """One Poisson trace (200 requests/s, seeded per rank) through the serving
+    engine at precision `name`, after a small warm-up trace. Returns the
+    engine's throughput, p50/p99 latency (overall and per decile of request
+    work), the clocks and the engine's figures."""
     import numpy as np
     import torch
     import skgemm
-    if args.precision in ("auto", "ozaki_bf16"):
-        raise SystemExit("the serving workload runs --precision native or ozaki")
-    rank, world, dist = dist_setup(args.gpus)
-    prec = {"native": skgemm.PREC_NATIVE, "ozaki": skgemm.PREC_OZAKI_I8}[args.precision]
-    trace = skgemm.serve_trace(args.requests, rate=200.0, seed=11 + rank)
+    prec = {"native": skgemm.PREC_NATIVE, "ozaki": skgemm.PREC_OZAKI_I8}[name]
+    trace = skgemm.serve_trace(requests, rate=200.0, seed=11 + rank)
     warm = skgemm.serve_trace(8, rate=200.0, seed=99, nb_range=(32, 256), ng_range=(1e4, 5e4))
     skgemm.serve(warm, precision=prec, hbm_budget=150e9)
     clocks = ClockSampler(torch.cuda.current_device())
@@ -776,38 +1124,61 @@ def run_serving(args):
     clocks.start()
     policy = skgemm.SERVE_SMALLEST if args.serve_policy == "smallest" else skgemm.SERVE_FIFO
     rows, o = skgemm.serve(trace, precision=prec, hbm_budget=150e9, realtime=True,
-                           policy=policy, aging_s=0.25, ozaki_streams=args.ozaki_streams)
+                           policy=policy, aging_s=args.serve_aging,
+                           ozaki_streams=args.ozaki_streams)
     barrier(dist)
     clk = clocks.stop()
     lat = np.array([d - a for a, _, d in rows]) * 1e3
-    span = max_over_ranks(o.makespan_s, dist)
+    work = np.array([5.0 * nb * nb * ng for _, ng, nb, _ in trace])
+    dec = np.minimum(9, (np.argsort(np.argsort(work)) * 10) // len(work))
+    p99_dec = [round(float(np.percentile(lat[dec == d], 99)), 1) for d in range(10)
+               if np.any(dec == d)]
+    return {"precision": name, "requests": requests, "flop": o.flop,
+            "makespan_s": round(o.makespan_s, 3),
+            "tflops": round(o.flop / o.makespan_s / 1e12, 3),
+            "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 2),
+                           "p99": round(float(np.percentile(lat, 99)), 2),
+                           "mean": round(float(lat.mean()), 2),
+                           "p99_by_work_decile": p99_dec},
+            "admission": ("least work first, aged (wait / %g s)" % args.serve_aging
+                          if args.serve_policy == "smallest" else "arrival order"),
+            "ozaki_streams": args.ozaki_streams if name == "ozaki" else None,
+            "batches": o.batches, "mean_batch_problems": round(o.mean_batch_problems, 2),
+            "peak_admitted_bytes": o.peak_admitted_bytes, "scratch_bytes": o.scratch_bytes,
+            "clocks": clk}
+
+
+def run_serving(args):
+    import skgemm
+    if args.precision in ("auto", "ozaki_bf16"):
+        raise SystemExit("the serving workload runs --precision native or ozaki")
+    name = "native" if args.precision == "both" else args.precision
+    rank, world, dist = dist_setup(args.gpus)
+    r = serve_measure(args, name, args.requests, rank, dist)
+    span = max_over_ranks(r["makespan_s"], dist)
     peak = skgemm.probe_fp64_peak()
-    tf = o.flop / o.makespan_s / 1e12
+    tf = r["tflops"]
     line = {
-        "metric": METRIC, "value": round(o.flop * world / span / 1e12, 3), "unit": "TFLOP/s",
-        "n_gpus": world, "steps": args.requests, "warmup": len(warm),
+        "metric": METRIC, "value": round(r["flop"] * world / span / 1e12, 3), "unit": "TFLOP/s",
+        "n_gpus": world, "steps": args.requests, "warmup": 8,
         "ms_per_step": round(span / max(1, args.requests) * 1e3, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"serving_poisson200_{args.requests}req",
-                   "precision": args.precision, "arrival_rate_per_s": 200.0,
-                   "ozaki_streams": args.ozaki_streams if args.precision == "ozaki" else None,
-                   "admission": ("least work first, aged (wait / 0.25 s)"
-                                 if args.serve_policy == "smallest" else "arrival order"),
+                   "precision": name, "arrival_rate_per_s": 200.0,
+                   "ozaki_streams": r["ozaki_streams"], "admission": r["admission"],
                    "grid_points": "log-uniform [1e4, 4e5], multiple of 16",
                    "states": "log-uniform [32, 2048], multiple of 16",
-                   "hbm_budget_bytes": 150e9, "flop": o.flop,
-                   "batches": o.batches, "mean_batch_problems": round(o.mean_batch_problems, 2),
-                   "peak_admitted_bytes": o.peak_admitted_bytes,
-                   "scratch_bytes": o.scratch_bytes, "parallelism": f"replicas{world}"},
-        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 2),
-                       "p99": round(float(np.percentile(lat, 99)), 2),
-                       "mean": round(float(lat.mean()), 2)},
+                   "hbm_budget_bytes": 150e9, "flop": r["flop"],
+                   "batches": r["batches"], "mean_batch_problems": r["mean_batch_problems"],
+                   "peak_admitted_bytes": r["peak_admitted_bytes"],
+                   "scratch_bytes": r["scratch_bytes"], "parallelism": f"replicas{world}"},
+        "latency_ms": r["latency_ms"],
         "roofline": {"bound": "tensor", "achieved": round(tf, 3), "peak": round(peak, 3),
                      "unit": "TFLOP/s", "frac": round(tf / peak, 4),
                      "peak_source": "measured FP64 DMMA peak (skgemm_probe_fp64_peak, this run)",
-                     "kernel": "fp64_grouped_kernel" if prec == skgemm.PREC_NATIVE
-                     else "i8_gemm_kernel", "traffic": None},
-        "clocks": clk,
+                     "kernel": "fp64_grouped_kernel" if name == "native" else "i8_gemm_kernel",
+                     "traffic": None},
+        "clocks": r["clocks"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

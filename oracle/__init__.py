@@ -81,6 +81,24 @@ def lib() -> ctypes.CDLL:
     return _lib
 
 
+def naive_native() -> ctypes.CDLL:
+    """The naive loops (oracle_gemm_naive / _syrk_naive / _rot_naive) built
+    -O3 -march=native for this host (`make native`, built here on first use):
+    the reference's portable kernels as a CPU baseline."""
+    path = os.path.join(HERE, "_native", "liboracle_native.so")
+    if not os.path.exists(path):
+        subprocess.run(["make", "-s", "-C", HERE, "native"], check=True)
+    L = ctypes.CDLL(path)
+    L.oracle_gemm_naive.argtypes = [_i64, _i64, _i64, _f64p, _f64p, _f64p,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    L.oracle_syrk_naive.argtypes = [_i64, _i64, _f64p, _f64p, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int]
+    L.oracle_rot_naive.argtypes = [_i64, _i64, _f64p, _f64p, _f64p, ctypes.c_int]
+    for f in ("oracle_gemm_naive", "oracle_syrk_naive", "oracle_rot_naive"):
+        getattr(L, f).restype = None
+    return L
+
+
 def ref(name: str) -> ctypes.CDLL:
     """The reference's own kernel file ``name`` built in place (oracle/_ref)."""
     if name not in _refs:
