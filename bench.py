@@ -594,9 +594,12 @@ def run_gpu(args):
     torch.cuda.empty_cache()
     skgemm.stream_release(stream)
     if world == 1 and args.serve_requests > 0:
-        line["serving"] = {
-            n: serve_measure(args, n, args.serve_requests, rank, None)
-            for n in ("native", "ozaki")}
+        line["serving"] = {}
+        for n in ("native", "ozaki"):
+            try:
+                line["serving"][n] = serve_measure(args, n, args.serve_requests, rank, None)
+            except skgemm.SkgemmError as e:  # keep the step's line; say what failed
+                line["serving"][n] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
