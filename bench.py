@@ -431,51 +431,76 @@ def time_calls(fn, stream, torch, reps=10, warm=2):
     return a.elapsed_time(b) / reps
 
 
-def kernel_rooflines(skgemm, step, torch, steps, peaks):
-    """Per-kernel times of `steps` more steps with the library's event timer
-    on (outside the timed region), each kernel rated against its roofline:
-    FP64 Stream-K kernels against the FP64 DMMA peak, INT8 products against
-    the INT8 peak, conversions / norms / reconstructions against HBM.
-    Algorithmic work per launch: GEMM 2 M N K, SYRK M (M+1) K, rotation
-    2 Nd nb^2 (INT8 ops: the same times the moduli count L); conversion 8 + L
-    bytes per element (8 + 2 L with BF16 residues), norms 8 B per element,
-    rotation reconstruction L + 8 B per element."""
-    fp64_peak, i8_peak, hbm = peaks
+def _timed_kernels(skgemm, fn, stream, steps):
+    """{kernel: (launches, total ms)} of `steps` calls of fn() with the
+    library's event timer on."""
     skgemm.kernel_timing(True)
     for _ in range(steps):
-        step()
-    skgemm.stream_status(step.stream)
+        fn()
+    skgemm.stream_status(stream)
     rep = skgemm.kernel_timing_report()
     skgemm.kernel_timing(False)
-    E = ND * NB
-    out = {}
-    if step.prec is None:
-        work = {"fp64_streamk_kernel64": (FLOP_SYRK + FLOP_ROT, "TFLOP/s", fp64_peak, "tensor"),
-                "fp64_streamk_kernel": (FLOP_GEMM, "TFLOP/s", fp64_peak, "tensor"),
-                "fp64_streamk_kernel64_ak": (FLOP_ROT, "TFLOP/s", fp64_peak, "tensor")}
-        if step.rot_layout == "band":
-            work["fp64_streamk_kernel64"] = (FLOP_SYRK, "TFLOP/s", fp64_peak, "tensor")
-    else:
-        Lp = step.opts["pair"].slices_used_out
-        Lr = step.opts["rot"].slices_used_out
-        rb = 2 if step.prec == skgemm.PREC_OZAKI_BF16 else 1
-        work = {"i8_gemm_kernel": (Lp * (FLOP_SYRK + FLOP_GEMM), "TOP/s", i8_peak, "tensor"),
-                "i8_rot_kernel": (Lr * FLOP_ROT, "TOP/s", i8_peak, "tensor"),
-                "convert_tma_kernel": (E * (3 * 8 + rb * (2 * Lp + Lr)), "GB/s", hbm, "hbm"),
-                "norm_partials_kernel": (3 * E * 8, "GB/s", hbm, "hbm"),
-                "crt_residues_band_kernel": (E * (rb * Lr + 8), "GB/s", hbm, "hbm")}
+    return rep
+
+
+def kernel_rooflines(skgemm, step, torch, steps, peaks, band, grid, q, S, Pn):
+    """Per-kernel figures of this precision, measured with the library's
+    event timer outside the timed region.
+
+    `share` / `ms_in_step`: from `steps` more subspace steps (in the Ozaki
+    pair, H Psi's norms and conversion run on a helper stream beside Psi's,
+    so two kernels can share the GPU there). `achieved` / `frac`: from a
+    serial pass of standalone calls (SYRK, then the rotation, one stream,
+    one kernel at a time), each kernel rated against its roofline: FP64
+    Stream-K kernels against the FP64 DMMA peak, INT8 products against the
+    INT8 peak, conversions / norms / the rotation's reconstruction against
+    HBM. Algorithmic work per launch: SYRK M (M+1) K, rotation 2 Nd nb^2
+    flop (INT8 ops: the same times the moduli count L); a conversion 8 + L
+    bytes per element (8 + 2 L for BF16 residues), a norm pass 8 bytes per
+    element, the rotation's reconstruction L + 8 bytes per element (element
+    = one of the Nd x nb operand's)."""
+    fp64_peak, i8_peak, hbm = peaks
+    rep = _timed_kernels(skgemm, step, step.stream, steps)
     total = sum(ms for _, ms in rep.values()) or 1.0
-    for name, (n, ms) in sorted(rep.items(), key=lambda kv: -kv[1][1]):
-        row = {"launches_per_step": round(n / steps, 2), "ms_per_launch": round(ms / n, 4),
-               "share": round(ms / total, 4)}
+    out = {name: {"launches_per_step": round(n / steps, 2),
+                  "ms_in_step": round(ms / n, 4), "share": round(ms / total, 4)}
+           for name, (n, ms) in sorted(rep.items(), key=lambda kv: -kv[1][1])}
+    E = ND * NB
+    s = step.stream
+    opts = {}
+
+    def serial():
+        opts["syrk"] = skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, stream=s, precision=step.prec)
+        opts["rot"] = skgemm.drot_dev(ND, NB, grid, q, Pn, stream=s, precision=step.prec)
+
+    alone = _timed_kernels(skgemm, serial, s, steps)
+    if step.prec is None:
+        work = {"fp64_streamk_kernel64": (FLOP_SYRK + FLOP_ROT, "TFLOP/s", fp64_peak, "tensor")}
+    else:
+        Ls, Lr = opts["syrk"].slices_used_out, opts["rot"].slices_used_out
+        rb = 2 if step.prec == skgemm.PREC_OZAKI_BF16 else 1
+        work = {"i8_gemm_kernel": (Ls * FLOP_SYRK, "TOP/s", i8_peak, "tensor"),
+                "i8_rot_kernel": (Lr * FLOP_ROT, "TOP/s", i8_peak, "tensor"),
+                "convert_tma_kernel": (E * (16 + rb * (Ls + Lr)), "GB/s", hbm, "hbm"),
+                "norm_partials_kernel": (2 * E * 8, "GB/s", hbm, "hbm"),
+                "crt_residues_band_kernel": (E * (rb * Lr + 8), "GB/s", hbm, "hbm")}
+    if step.prec is None:
+        # the GEMM's kernel from the step itself (one launch per step, serial)
+        n, ms = rep.get("fp64_streamk_kernel", (0, 0.0))
+        if n:
+            ach = FLOP_GEMM * n / (ms * 1e-3) / 1e12
+            out["fp64_streamk_kernel"].update({
+                "bound": "tensor", "ms_alone": round(ms / n, 4), "achieved": round(ach, 3),
+                "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "frac": round(ach / fp64_peak, 4)})
+    for name, (n, ms) in alone.items():
+        row = out.setdefault(name, {"launches_per_step": 0, "ms_in_step": None, "share": 0.0})
+        row["ms_alone"] = round(ms / n, 4)
         if name in work:
             w, unit, peak, bound = work[name]
             scale = 1e12 if unit in ("TFLOP/s", "TOP/s") else 1e9
             ach = w * steps / (ms * 1e-3) / scale
             row.update({"bound": bound, "achieved": round(ach, 3), "peak": round(peak, 3),
-                        "unit": unit, "frac": round(ach / peak, 4),
-                        "work_per_step": w})
-        out[name] = row
+                        "unit": unit, "frac": round(ach / peak, 4)})
     return out
 
 
@@ -522,7 +547,8 @@ def run_gpu(args):
         # Accuracy of this precision's results (the last timed step's outputs).
         r["rel_frobenius_error"] = {k: float(f"{v:.3e}")
                                     for k, v in subspace_errors(S, Hs, Pn, check).items()}
-        r["kernels"] = kernel_rooflines(skgemm, step, torch, 3, (fp64_peak, i8_peak, hbm))
+        r["kernels"] = kernel_rooflines(skgemm, step, torch, 3, (fp64_peak, i8_peak, hbm),
+                                        band, grid, q, S, Pn)
         res[name] = r
 
     # Standalone SYRK and GEMM (the reference's one-call-at-a-time use).
@@ -566,7 +592,8 @@ def run_gpu(args):
                                                "skgemm_probe_i8_peak)",
                                      "hbm": hbm_src}.get(dk.get("bound"), None),
                      "timing": "CUDA events around each launch on its stream (library kernel "
-                               "timer), 3 steps after the timed region"},
+                               "timer), standalone SYRK + rotation calls after the timed "
+                               "region; share = of the step's kernel time"},
         "clocks": H["clocks"],
         "gpu_launches": 0,
     }

@@ -86,6 +86,7 @@ struct CrtConsts {  // for one moduli count L
 
 __constant__ ResidueConsts c_res[kI8MaxModuli + 1];
 __constant__ CrtConsts c_crt[kI8MaxModuli + 1];
+__constant__ double c_inv_mod[kI8MaxModuli];  // fl(1 / m_l) of the moduli
 
 typedef unsigned __int128 u128;
 
@@ -580,6 +581,10 @@ __device__ __forceinline__ double crt_value(const uint32_t (&r)[kI8MaxModuli], i
   return fma(-q, c.mh, sh) + fma(-q, c.ml, sl);
 }
 
+__device__ __forceinline__ double pow2i(int e) {  // 2^e, e in [-1022, 1023]
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
 // GEMM / SYRK: out(i, j) from the int32 partial slabs of the lane schedule.
 // mode 0: D[i*ldd + j] = alpha*v + gamma; mode 1 (SYRK, i <= j only):
 // C[i + j*ldd] = alpha*v + beta*C (beta_zero: no read).
@@ -602,13 +607,21 @@ __global__ void __launch_bounds__(256) crt_partials_kernel(
       int64_t s = 0;
       for (int q = mod_slot_off[l]; q < mod_slot_off[l + 1]; ++q)
         s += partials[((int64_t)mod_slots[q] * T + t) * (kI8BM * kI8BN) + off];
+      // s mod m without an integer division: |s| < 2^31 * (slots) is exact in
+      // a double, floor(s * fl(1/m)) is the true quotient or one off (the
+      // product's error is below 2^-20), and one correction step each way
+      // makes the remainder exact.
       const int64_t m = c_res[L].mi[l];
-      int64_t rr = s % m;
-      if (rr < 0) rr += m;
+      const int64_t q = (int64_t)floor((double)s * c_inv_mod[l]);
+      int64_t rr = s - q * m;
+      rr += rr < 0 ? m : 0;
+      rr -= rr >= m ? m : 0;
       r[l] = (uint32_t)rr;
     }
   }
-  const double v = ldexp(crt_value(r, L), -(mu[i] + nu[j]));
+  const double x = crt_value(r, L);
+  const int ex = -(mu[i] + nu[j]);
+  const double v = (ex >= -1022 && ex <= 1023) ? x * pow2i(ex) : ldexp(ldexp(x, -mu[i]), -nu[j]);
   if (mode == 0) {
     D[(int64_t)i * ldd + j] = alpha * v + gamma;
   } else {
@@ -623,9 +636,6 @@ __global__ void __launch_bounds__(256) crt_partials_kernel(
 // their latency otherwise); bytes widen to doubles exactly (2^52 + r - 2^52).
 // The scale 2^-(mu[g] + nu[b]) is built from exponent bits (four 16-byte
 // loads of nu per thread).
-__device__ __forceinline__ double pow2i(int e) {  // 2^e, e in [-1022, 1023]
-  return __longlong_as_double((long long)(e + 1023) << 52);
-}
 
 template <int L>
 __global__ void __launch_bounds__(128) crt_residues_band_kernel(
@@ -781,6 +791,9 @@ int ensure_consts(DeviceState* dev) {
   for (int L = kMinModuli; L <= kI8MaxModuli; ++L) cc[L] = make_crt(L, nullptr);
   SKG_CUDA(cudaMemcpyToSymbol(c_res, rc, sizeof(rc)));
   SKG_CUDA(cudaMemcpyToSymbol(c_crt, cc, sizeof(cc)));
+  double inv_mod[kI8MaxModuli];
+  for (int l = 0; l < kI8MaxModuli; ++l) inv_mod[l] = 1.0 / (double)kModuli[l];
+  SKG_CUDA(cudaMemcpyToSymbol(c_inv_mod, inv_mod, sizeof(inv_mod)));
   od.consts_ready = true;
   return SKGEMM_OK;
 }

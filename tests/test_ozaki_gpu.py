@@ -402,7 +402,7 @@ def test_host_pointer_opt_entries_equal_device_calls(cuda, prec):
     Dd = torch.zeros(M * M, dtype=torch.float64, device="cuda")
     od = skgemm.dgemm_packed_dev(M, M, K, dev(A16), dev(B32), Dd, M, 1.25, 0.5, precision=prec)
     C0 = uniform((M, M), 63)
-    C = np.ascontiguousarray(C0.ravel())
+    C = C0.ravel().copy()
     os_ = skgemm.sme_syrk.compute(K, M, A16, C, 1.0, 0.5, precision=prec)
     Cd = dev(C0.ravel())
     osd = skgemm.dsyrk_packed_dev(K, M, dev(A16), Cd, M, 1.0, 0.5, precision=prec)
