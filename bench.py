@@ -88,8 +88,9 @@ def parse():
     ap.add_argument("--ozaki-streams", type=int, default=2,
                     help="serving, Ozaki: requests running concurrently (each stream holds "
                          "scratch for the largest request)")
-    ap.add_argument("--serve-policy", default="smallest", choices=["smallest", "fifo"],
-                    help="serving: admission order (aged least-work-first, or arrival order)")
+    ap.add_argument("--serve-policy", default="smallest", choices=["smallest", "fifo", "ratio"],
+                    help="serving: admission order (aged least-work-first, arrival order, or "
+                         "highest response ratio next)")
     ap.add_argument("--serve-aging", type=float, default=0.25,
                     help="serving, least-work-first: seconds of waiting that count as one "
                          "unit of priority")
@@ -621,12 +622,19 @@ def run_gpu(args):
     torch.cuda.empty_cache()
     skgemm.stream_release(stream)
     if world == 1 and args.serve_requests > 0:
+        # Both precisions under the default admission policy and, on the same
+        # box, under arrival order (FIFO) for comparison.
         line["serving"] = {}
         for n in ("native", "ozaki"):
-            try:
-                line["serving"][n] = serve_measure(args, n, args.serve_requests, rank, None)
-            except skgemm.SkgemmError as e:  # keep the step's line; say what failed
-                line["serving"][n] = {"error": str(e)}
+            for pol in (args.serve_policy, "fifo"):
+                key = n if pol == args.serve_policy else f"{n}_fifo"
+                if key in line["serving"]:
+                    continue
+                try:
+                    line["serving"][key] = serve_measure(args, n, args.serve_requests, rank,
+                                                         None, pol)
+                except skgemm.SkgemmError as e:  # keep the step's line; say what failed
+                    line["serving"][key] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
@@ -1137,7 +1145,7 @@ def run_batched(args):
 
 
 # ------------------------------------------------------------ serving arm
-def serve_measure(args, name, requests, rank, dist):
+def serve_measure(args, name, requests, rank, dist, policy_name=None):
     """One Poisson trace (200 requests/s, seeded per rank) through the serving
     engine at precision `name`, after a small warm-up trace. Returns the
     engine's throughput, p50/p99 latency (overall and per decile of request
@@ -1152,7 +1160,8 @@ def serve_measure(args, name, requests, rank, dist):
     clocks = ClockSampler(torch.cuda.current_device())
     barrier(dist)
     clocks.start()
-    policy = skgemm.SERVE_SMALLEST if args.serve_policy == "smallest" else skgemm.SERVE_FIFO
+    policy = {"smallest": skgemm.SERVE_SMALLEST, "fifo": skgemm.SERVE_FIFO,
+              "ratio": skgemm.SERVE_RATIO}[policy_name or args.serve_policy]
     rows, o = skgemm.serve(trace, precision=prec, hbm_budget=150e9, realtime=True,
                            policy=policy, aging_s=args.serve_aging,
                            ozaki_streams=args.ozaki_streams)
@@ -1170,8 +1179,10 @@ def serve_measure(args, name, requests, rank, dist):
                            "p99": round(float(np.percentile(lat, 99)), 2),
                            "mean": round(float(lat.mean()), 2),
                            "p99_by_work_decile": p99_dec},
-            "admission": ("least work first, aged (wait / %g s)" % args.serve_aging
-                          if args.serve_policy == "smallest" else "arrival order"),
+            "admission": {"smallest": "least work first, aged (wait / %g s)" % args.serve_aging,
+                          "fifo": "arrival order",
+                          "ratio": "highest response ratio next (wait / work)"}[
+                              policy_name or args.serve_policy],
             "ozaki_streams": args.ozaki_streams if name == "ozaki" else None,
             "batches": o.batches, "mean_batch_problems": round(o.mean_batch_problems, 2),
             "peak_admitted_bytes": o.peak_admitted_bytes, "scratch_bytes": o.scratch_bytes,

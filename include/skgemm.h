@@ -472,6 +472,10 @@ typedef struct skgemm_serve_request {
 
 #define SKGEMM_SERVE_FIFO 0
 #define SKGEMM_SERVE_SMALLEST 1
+/* Highest response ratio next: the waiting request with the largest wait per
+ * unit of its own work (ties: least work). A large request ages in proportion
+ * to its size, so it cannot starve behind a stream of small ones. */
+#define SKGEMM_SERVE_RATIO 2
 
 typedef struct skgemm_serve_options {
   int precision;           /* SKGEMM_PREC_NATIVE or SKGEMM_PREC_OZAKI_I8 */
@@ -482,8 +486,9 @@ typedef struct skgemm_serve_options {
   double max_batch_tflop;  /* native: work cap of one grouped launch (0 = 2 TFLOP) */
   int realtime;            /* 1: release requests at arrival_s (wall clock); 0: all at 0 */
   int policy;              /* admission order among waiting requests:
-                              SKGEMM_SERVE_FIFO (0, arrival order) or
-                              SKGEMM_SERVE_SMALLEST (least work first, aged) */
+                              SKGEMM_SERVE_FIFO (0, arrival order),
+                              SKGEMM_SERVE_SMALLEST (least work first, aged) or
+                              SKGEMM_SERVE_RATIO (largest wait / work first) */
   double aging_s;          /* SMALLEST: a request's work counts / (1 + wait / aging_s),
                               so a long wait always ends (0 = 0.25 s) */
   /* skgemm_serve_simulate only: throughput model (0 = defaults) */

@@ -521,6 +521,19 @@ int schedule(skgemm_serve_request_t* io, int n, skgemm_serve_options_t& o, Exec&
             pick = it;
           }
         }
+      } else if (o.policy == SKGEMM_SERVE_RATIO) {
+        // Response ratio (wait + service) / service = 1 + wait / service, and
+        // service is proportional to work: the largest wait / work wins.
+        double best = -1.0, best_flop = 1e300;
+        for (auto it = queue.begin(); it != queue.end(); ++it) {
+          const Req& c = R[*it];
+          const double key = std::max(0.0, t - c.arrival) / std::max(c.flop, 1.0);
+          if (key > best || (key == best && c.flop < best_flop)) {
+            best = key;
+            best_flop = c.flop;
+            pick = it;
+          }
+        }
       }
       Req& r = R[*pick];
       int k = -1;
@@ -603,7 +616,8 @@ int serve_run(skgemm_serve_request_t* io, int n, skgemm_serve_options_t* opts, b
   skgemm_serve_options_t& o = *opts;
   if (o.precision != SKGEMM_PREC_NATIVE && o.precision != SKGEMM_PREC_OZAKI_I8)
     return fail(SKGEMM_ERR_INVALID_ARG, "serve: unknown precision");
-  if (o.policy != SKGEMM_SERVE_FIFO && o.policy != SKGEMM_SERVE_SMALLEST)
+  if (o.policy != SKGEMM_SERVE_FIFO && o.policy != SKGEMM_SERVE_SMALLEST &&
+      o.policy != SKGEMM_SERVE_RATIO)
     return fail(SKGEMM_ERR_INVALID_ARG, "serve: unknown admission policy");
   if (o.aging_s < 0) return fail(SKGEMM_ERR_INVALID_ARG, "serve: aging_s must be >= 0");
   int64_t max_ng = 0, max_nb = 0;

@@ -678,6 +678,7 @@ def serve_trace(n, rate=200.0, ng_range=(1e4, 4e5), nb_range=(32, 2048), seed=0)
 
 SERVE_FIFO = 0
 SERVE_SMALLEST = 1  # least work first among waiting requests, aged
+SERVE_RATIO = 2  # highest response ratio next (largest wait / work)
 
 
 def serve(trace, precision=PREC_NATIVE, slices=0, hbm_budget=150e9, max_inflight=0,

@@ -143,3 +143,37 @@ def test_sim_rejects_bad_policy():
         skgemm.serve(tr, precision=OZAKI, simulate=True, policy=7)
     with pytest.raises(skgemm.SkgemmError):
         skgemm.serve(tr, precision=OZAKI, simulate=True, policy=skgemm.SERVE_SMALLEST, aging_s=-1)
+
+
+def test_sim_ratio_policy_bounds_the_largest_requests_wait():
+    """Highest response ratio next (largest wait / work first) on the
+    2000-request trace at ~93% load: all work done, median far below arrival
+    order's, p99 at or below arrival order's, and the largest decile of
+    requests served sooner than under aged least-work-first (which lets a
+    stream of small requests hold the large ones back)."""
+    tr = skgemm.serve_trace(2000, rate=200.0, seed=11)
+    work = np.array([request_flop(ng, nb) for _, ng, nb, _ in tr])
+    top = work >= np.percentile(work, 90)
+    res = {}
+    for pol in (skgemm.SERVE_FIFO, skgemm.SERVE_SMALLEST, skgemm.SERVE_RATIO):
+        rows, o = skgemm.serve(tr, precision=OZAKI, simulate=True, sim=(30.0, 55.0, 3000.0),
+                               policy=pol, aging_s=0.25, ozaki_streams=2)
+        lat = np.array([d - a for a, _, d in rows])
+        res[pol] = (np.percentile(lat, 50), np.percentile(lat, 99),
+                    np.percentile(lat[top], 99), o.flop)
+    fifo, small, ratio = (res[p] for p in (skgemm.SERVE_FIFO, skgemm.SERVE_SMALLEST,
+                                           skgemm.SERVE_RATIO))
+    assert ratio[3] == fifo[3]
+    assert ratio[0] < 0.25 * fifo[0]
+    assert ratio[1] <= fifo[1]
+    assert ratio[2] < small[2]
+
+
+def test_sim_ratio_policy_picks_the_longest_relative_wait():
+    """Behind a busy slot: a small request that has waited admits before a
+    large one that waited longer in absolute terms but less per unit of work."""
+    tr = [(0.0, 400000, 2048, 1), (0.001, 400000, 1024, 2), (0.05, 16384, 64, 3)]
+    rows, _ = skgemm.serve(tr, precision=OZAKI, simulate=True, sim=(30.0, 50.0, 900.0),
+                           policy=skgemm.SERVE_RATIO, ozaki_streams=1)
+    admit = [a for _, a, _ in rows]
+    assert admit[2] < admit[1]
