@@ -91,7 +91,7 @@ def parse():
     ap.add_argument("--serve-policy", default="smallest", choices=["smallest", "fifo", "ratio"],
                     help="serving: admission order (aged least-work-first, arrival order, or "
                          "highest response ratio next)")
-    ap.add_argument("--serve-aging", type=float, default=0.25,
+    ap.add_argument("--serve-aging", type=float, default=1.0,
                     help="serving, least-work-first: seconds of waiting that count as one "
                          "unit of priority")
     ap.add_argument("--instances", type=int, default=64, help="batched: k-point instances")

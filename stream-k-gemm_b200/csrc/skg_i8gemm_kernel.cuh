@@ -89,6 +89,11 @@ struct I8Params {
   uint8_t* residues;            // [L][M][ldr]
   int64_t ldr;
   uint32_t* err;
+  // kSchedLanes on CTA pairs (i8_gemm2_kernel): T2 pair tiles, each two
+  // vertically adjacent 128 x 256 tiles {tm_lo, tn, t_lo, t_hi} (t_* index
+  // `tiles`, which then holds both halves of every pair).
+  int T2;
+  const int4* pairs;
 };
 
 // Moduli and the constants of an exact remainder by multiply-high: with

@@ -29,6 +29,7 @@
 #include <tuple>
 #include <vector>
 
+#include "skg_i8gemm2_kernel.cuh"
 #include "skg_i8gemm_kernel.cuh"
 #include "skg_ozaki.h"
 
@@ -713,6 +714,8 @@ __global__ void __launch_bounds__(256) sum_partials_kernel(
 // ------------------------------------------------------------- host side
 struct LanePlan {
   int T = 0, T1 = 0, Q = 0, slots = 0, L = 0, KB = 0, tiles_m = 0, tiles_n = 0;
+  int T2 = 0;              // CTA-pair plans: pair tiles (0: one-CTA plan)
+  int4* pairs = nullptr;   // [T2] {tm_lo, tn, t_lo, t_hi}
   // tiles | lane_seg_off | segs | tile_index | mod_slot_off | mod_slots | tile_index2
   DeviceBuffer buf;
   int2* tiles = nullptr;
@@ -824,11 +827,15 @@ int lanes_for(int sms, int T, int64_t W) {
 // With `pair` (M == N) the tile list is the SYRK's upper tiles (t < T1,
 // tile_index) followed by all tiles of the GEMM (tile_index2): one launch
 // computes S = A^T A and Hs = A^T B from the same A panels.
+// With `units` > 0 the plan is for the CTA-pair kernel (i8_gemm2_kernel) on
+// `units` co-resident clusters: the tile set is closed under pairing
+// (tiles 2p and 2p + 1 of a column), the pair list is built, and the lanes
+// are sized for the clusters.
 int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int seg_cap,
-                  LanePlan** out, int sub_cap = 0, bool pair = false) {
+                  LanePlan** out, int sub_cap = 0, bool pair = false, int units = 0) {
   OzakiDevice& od = g_oz[dev->device];
   auto key = std::make_tuple(M, N, KB, (L * 4096 + seg_cap) * 64 + sub_cap,
-                             (syrk ? 1 : 0) + (pair ? 2 : 0));
+                             (syrk ? 1 : 0) + (pair ? 2 : 0) + units * 4);
   auto itp = od.plans.find(key);
   if (itp != od.plans.end()) {
     *out = itp->second;
@@ -840,26 +847,51 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
   pl->tiles_m = (M + kI8BM - 1) / kI8BM;
   pl->tiles_n = (N + kI8BN - 1) / kI8BN;
   std::vector<int2> tiles;
+  std::vector<int4> pairs;
   std::vector<int> tile_index(pl->tiles_m * pl->tiles_n, -1), tile_index2;
-  for (int tm = 0; tm < pl->tiles_m; ++tm)
-    for (int tn = 0; tn < pl->tiles_n; ++tn) {
-      if ((syrk || pair) && tm * kI8BM > tn * kI8BN + kI8BN - 1) continue;  // strictly lower
-      tile_index[tm * pl->tiles_n + tn] = (int)tiles.size();
-      tiles.push_back(make_int2(tm, tn));
+  // Rows of tile tm: 128 tm ..; residue planes are padded to 256 rows, so a
+  // pair plan may use tile row tiles_m (padding) as the partner of the last.
+  const int tm_span = units > 0 ? (pl->tiles_m + 1) / 2 * 2 : pl->tiles_m;
+  auto add_set = [&](bool upper, std::vector<int>& index) {
+    if (units == 0) {  // one-CTA plan: row-major tile order
+      for (int tm = 0; tm < pl->tiles_m; ++tm)
+        for (int tn = 0; tn < pl->tiles_n; ++tn) {
+          if (upper && tm * kI8BM > tn * kI8BN + kI8BN - 1) continue;  // strictly lower
+          index[tm * pl->tiles_n + tn] = (int)tiles.size();
+          tiles.push_back(make_int2(tm, tn));
+        }
+      return;
     }
+    for (int tn = 0; tn < pl->tiles_n; ++tn)
+      for (int tm2 = 0; tm2 < tm_span; tm2 += 2) {
+        const int span = 2;
+        bool need = false;
+        for (int h = 0; h < span; ++h) {
+          const int tm = tm2 + h;
+          if (tm < pl->tiles_m && !(upper && tm * kI8BM > tn * kI8BN + kI8BN - 1)) need = true;
+        }
+        if (!need) continue;
+        int t[2] = {-1, -1};
+        for (int h = 0; h < span; ++h) {
+          const int tm = tm2 + h;
+          t[h] = (int)tiles.size();
+          if (tm < pl->tiles_m) index[tm * pl->tiles_n + tn] = t[h];
+          tiles.push_back(make_int2(tm, tn));
+        }
+        pairs.push_back(make_int4(tm2, tn, t[0], t[1]));
+      }
+  };
+  add_set(syrk || pair, tile_index);
   pl->T1 = 0;
   if (pair) {
     pl->T1 = (int)tiles.size();
     tile_index2.assign(pl->tiles_m * pl->tiles_n, -1);
-    for (int tm = 0; tm < pl->tiles_m; ++tm)
-      for (int tn = 0; tn < pl->tiles_n; ++tn) {
-        tile_index2[tm * pl->tiles_n + tn] = (int)tiles.size();
-        tiles.push_back(make_int2(tm, tn));
-      }
+    add_set(false, tile_index2);
   }
   pl->T = (int)tiles.size();
+  pl->T2 = (int)pairs.size();
   const int64_t W = (int64_t)L * KB;
-  pl->Q = lanes_for(dev->num_sms, pl->T, W);
+  pl->Q = units > 0 ? lanes_for(units, pl->T2, W) : lanes_for(dev->num_sms, pl->T, W);
   std::vector<int> lane_off(pl->Q + 1, 0);
   std::vector<I8Segment> segs;
   int nslots = 0;
@@ -900,14 +932,18 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
   const size_t s0 = al(tiles.size() * sizeof(int2)), s1 = al(lane_off.size() * sizeof(int)),
                s2 = al(segs.size() * sizeof(I8Segment)), s3 = al(tile_index.size() * sizeof(int)),
                s4 = al(mod_off.size() * sizeof(int)), s5 = al(mod_slots.size() * sizeof(int) + 4),
-               s6 = al(tile_index2.size() * sizeof(int) + 4);
+               s6 = al(tile_index2.size() * sizeof(int) + 4),
+               s7 = al(pairs.size() * sizeof(int4) + 16);
   int st;
-  if ((st = pl->buf.ensure(s0 + s1 + s2 + s3 + s4 + s5 + s6)) != SKGEMM_OK) {
+  if ((st = pl->buf.ensure(s0 + s1 + s2 + s3 + s4 + s5 + s6 + s7)) != SKGEMM_OK) {
     delete pl;
     return st;
   }
   uint8_t* b = static_cast<uint8_t*>(pl->buf.ptr);
-  std::vector<uint8_t> host(s0 + s1 + s2 + s3 + s4 + s5 + s6, 0);
+  std::vector<uint8_t> host(s0 + s1 + s2 + s3 + s4 + s5 + s6 + s7, 0);
+  if (!pairs.empty())
+    memcpy(host.data() + s0 + s1 + s2 + s3 + s4 + s5 + s6, pairs.data(),
+           pairs.size() * sizeof(int4));
   if (!tile_index2.empty())
     memcpy(host.data() + s0 + s1 + s2 + s3 + s4 + s5, tile_index2.data(),
            tile_index2.size() * sizeof(int));
@@ -925,6 +961,7 @@ int get_lane_plan(DeviceState* dev, int M, int N, int KB, int L, bool syrk, int 
   pl->mod_slot_off = reinterpret_cast<int*>(b + s0 + s1 + s2 + s3);
   pl->mod_slots = reinterpret_cast<int*>(b + s0 + s1 + s2 + s3 + s4);
   pl->tile_index2 = pair ? reinterpret_cast<int*>(b + s0 + s1 + s2 + s3 + s4 + s5) : nullptr;
+  pl->pairs = units > 0 ? reinterpret_cast<int4*>(b + s0 + s1 + s2 + s3 + s4 + s5 + s6) : nullptr;
   od.plans[key] = pl;
   *out = pl;
   return SKGEMM_OK;
@@ -954,12 +991,104 @@ int launch_i8_t(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
   return SKGEMM_OK;
 }
 
+// CTA-pair lanes kernel: on unless SKGEMM_LANES_PAIR=0 selects the one-CTA
+// kernel (same slabs, same results bit for bit; kept for comparison).
+bool lanes_pair_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("SKGEMM_LANES_PAIR");
+    v = (e && e[0] == '0') ? 0 : 1;
+  }
+  return v == 1;
+}
+
+cudaLaunchConfig_t pair_config(int grid, cudaStream_t s, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kI8Threads);
+  cfg.dynamicSmemBytes = kI8P2SmemBytes;
+  cfg.stream = s;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <bool BF>
+int pair_setup(DeviceState* dev, int* clusters) {
+  static int ncl[64] = {0};
+  if (!ncl[dev->device]) {
+    SKG_CUDA(cudaFuncSetAttribute(i8_gemm2_kernel<BF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kI8P2SmemBytes));
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = pair_config(2 * (dev->num_sms / 2), nullptr, attr);
+    int n = 0;
+    SKG_CUDA(cudaOccupancyMaxActiveClusters(&n, (const void*)i8_gemm2_kernel<BF>, &cfg));
+    if (n < 1) return fail(SKGEMM_ERR_CUDA, "INT8 pair kernel: no cluster of two fits");
+    ncl[dev->device] = n;
+  }
+  *clusters = ncl[dev->device];
+  return SKGEMM_OK;
+}
+
+// Co-resident clusters of the pair kernel on this device (0: pair kernel off).
+int lanes_pair_units(DeviceState* dev, bool bf) {
+  if (!lanes_pair_enabled()) return 0;
+  int n = 0;
+  if ((bf ? pair_setup<true>(dev, &n) : pair_setup<false>(dev, &n)) != SKGEMM_OK) return 0;
+  return n;
+}
+
+template <bool BF>
+int launch_i8_pair_t(const CUtensorMap& mA, const CUtensorMap& mB, const CUtensorMap& mB2,
+                     const I8Params& p, int clusters, cudaStream_t s) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = pair_config(2 * clusters, s, attr);
+  KernelTimer kt_(s, "i8_gemm2_kernel");
+  SKG_CUDA(cudaLaunchKernelEx(&cfg, i8_gemm2_kernel<BF>, mA, mB, mB2, p));
+  return SKGEMM_OK;
+}
+
 // INT8 (bf = false) or BF16 (bf = true) residue products.
 int launch_i8(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB, const I8Params& p,
               int grid, cudaStream_t s, bool bf = false, const CUtensorMap* mB2 = nullptr) {
   const CUtensorMap& b2 = mB2 ? *mB2 : mB;
   return bf ? launch_i8_t<true>(dev, mA, mB, b2, p, grid, s)
             : launch_i8_t<false>(dev, mA, mB, b2, p, grid, s);
+}
+
+// The lanes products of plan `pl`: the CTA-pair kernel when the plan was
+// built for it (B boxes of 128 rows), the one-CTA kernel otherwise (B boxes
+// of 256 rows). `p` holds everything but the plan's tile / pair fields.
+int launch_lanes(DeviceState* dev, const LanePlan* pl, const void* resA, int64_t KPb, int64_t RA,
+                 const void* resB, int64_t RB, const void* resB2, I8Params p, cudaStream_t s,
+                 bool bf) {
+  int st;
+  const bool pair_k = pl->T2 > 0;
+  CUtensorMap mA, mB, mB2;
+  if ((st = make_res_map(&mA, resA, KPb, RA, p.L, kI8BM))) return st;
+  if ((st = make_res_map(&mB, resB, KPb, RB, p.L, pair_k ? 128 : kI8BN))) return st;
+  if (resB2 && (st = make_res_map(&mB2, resB2, KPb, RB, p.L, pair_k ? 128 : kI8BN))) return st;
+  p.T = pl->T;
+  p.T1 = pl->T1;
+  p.Q = pl->Q;
+  p.tiles = pl->tiles;
+  p.lane_seg_off = pl->lane_seg_off;
+  p.segs = pl->segs;
+  p.T2 = pl->T2;
+  p.pairs = pl->pairs;
+  if (!pair_k)
+    return launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s, bf,
+                     resB2 ? &mB2 : nullptr);
+  int ncl = 0;
+  if ((st = bf ? pair_setup<true>(dev, &ncl) : pair_setup<false>(dev, &ncl))) return st;
+  ncl = std::min(ncl, pl->T2 * pl->Q);
+  const CUtensorMap& b2 = resB2 ? mB2 : mB;
+  return bf ? launch_i8_pair_t<true>(mA, mB, b2, p, ncl, s)
+            : launch_i8_pair_t<false>(mA, mB, b2, p, ncl, s);
 }
 
 int launch_i8_rot(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB,
@@ -1169,12 +1298,9 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   LanePlan* pl = nullptr;
   if ((st = get_lane_plan(dev, (int)M, (int)N, KB, L, syrk,
                           bf ? kSegKbCapBf16 : kSegKbCapSigned, &pl,
-                          bf ? kSubKbCapBf16 : 0)) != SKGEMM_OK)
+                          bf ? kSubKbCapBf16 : 0, false, lanes_pair_units(dev, bf))) != SKGEMM_OK)
     return st;
   if ((st = part.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t)))) return st;
-  CUtensorMap mA, mB;
-  if ((st = make_res_map(&mA, os->res_a.ptr, KPb, RA, L, kI8BM))) return st;
-  if ((st = make_res_map(&mB, resB->ptr, KPb, syrk ? RA : RB, L, kI8BN))) return st;
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedLanes;
@@ -1183,14 +1309,11 @@ int lanes_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_
   p.KB = KB;
   p.M = (int)M;
   p.N = (int)N;
-  p.T = pl->T;
-  p.Q = pl->Q;
-  p.tiles = pl->tiles;
-  p.lane_seg_off = pl->lane_seg_off;
-  p.segs = pl->segs;
   p.partials = (int32_t*)part.ptr;
   p.err = ws->err;
-  if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s, bf))) return st;
+  if ((st = launch_lanes(dev, pl, os->res_a.ptr, KPb, RA, resB->ptr, syrk ? RA : RB, nullptr, p,
+                         s, bf)))
+    return st;
   const int64_t n = M * N;
   KernelTimer kt_(s, "crt_partials_kernel");
   crt_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
@@ -1215,14 +1338,10 @@ int pair_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t
   LanePlan* pl = nullptr;
   if ((st = get_lane_plan(dev, (int)M, (int)M, KB, L, false,
                           bf ? kSegKbCapBf16 : kSegKbCapSigned, &pl, bf ? kSubKbCapBf16 : 0,
-                          true)) != SKGEMM_OK)
+                          true, lanes_pair_units(dev, bf))) != SKGEMM_OK)
     return st;
   DeviceBuffer& part = os->partials;
   if ((st = part.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t)))) return st;
-  CUtensorMap mA, mB, mB2;
-  if ((st = make_res_map(&mA, os->res_a.ptr, KPb, RA, L, kI8BM))) return st;
-  if ((st = make_res_map(&mB, os->res_a.ptr, KPb, RA, L, kI8BN))) return st;
-  if ((st = make_res_map(&mB2, os->res_b.ptr, KPb, RA, L, kI8BN))) return st;
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedLanes;
@@ -1231,15 +1350,11 @@ int pair_product(DeviceState* dev, OzakiStream* os, StreamWorkspace* ws, int64_t
   p.KB = KB;
   p.M = (int)M;
   p.N = (int)M;
-  p.T = pl->T;
-  p.T1 = pl->T1;
-  p.Q = pl->Q;
-  p.tiles = pl->tiles;
-  p.lane_seg_off = pl->lane_seg_off;
-  p.segs = pl->segs;
   p.partials = (int32_t*)part.ptr;
   p.err = ws->err;
-  if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s, bf, &mB2))) return st;
+  if ((st = launch_lanes(dev, pl, os->res_a.ptr, KPb, RA, os->res_a.ptr, RA, os->res_b.ptr, p, s,
+                         bf)))
+    return st;
   SKG_CUDA(cudaEventRecord(os->fork2, s));
   SKG_CUDA(cudaStreamWaitEvent(os->aux, os->fork2, 0));
   const int64_t n = M * M;
@@ -1769,14 +1884,11 @@ int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, cons
     SKG_CUDA(cudaMemcpy2DAsync(os->res_b.ptr, KP, B, ldb, K, N, cudaMemcpyDeviceToDevice, s));
   }
   LanePlan* pl = nullptr;
-  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, 1, false, kSegKbCapSigned, &pl)) !=
-      SKGEMM_OK)
+  if ((st = get_lane_plan(dev, (int)M, (int)N, KB, 1, false, kSegKbCapSigned, &pl, 0, false,
+                          lanes_pair_units(dev, false))) != SKGEMM_OK)
     return st;
   if ((st = os->partials.ensure((size_t)pl->slots * pl->T * kI8BM * kI8BN * sizeof(int32_t))))
     return st;
-  CUtensorMap mA, mB;
-  if ((st = make_res_map(&mA, os->res_a.ptr, KP, RA, 1, kI8BM))) return st;
-  if ((st = make_res_map(&mB, os->res_b.ptr, KP, RB, 1, kI8BN))) return st;
   I8Params p;
   memset(&p, 0, sizeof(p));
   p.sched = kSchedLanes;
@@ -1785,14 +1897,11 @@ int igemm_s8(int64_t M, int64_t N, int64_t K, const int8_t* A, int64_t lda, cons
   p.KB = KB;
   p.M = (int)M;
   p.N = (int)N;
-  p.T = pl->T;
-  p.Q = pl->Q;
-  p.tiles = pl->tiles;
-  p.lane_seg_off = pl->lane_seg_off;
-  p.segs = pl->segs;
   p.partials = (int32_t*)os->partials.ptr;
   p.err = ws->err;
-  if ((st = launch_i8(dev, mA, mB, p, std::min(dev->num_sms, pl->T * pl->Q), s))) return st;
+  if ((st = launch_lanes(dev, pl, os->res_a.ptr, KP, RA, os->res_b.ptr, RB, nullptr, p, s,
+                         false)))
+    return st;
   const int64_t n = M * N;
   KernelTimer kt_(s, "sum_partials_kernel");
   sum_partials_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(

@@ -511,7 +511,7 @@ int schedule(skgemm_serve_request_t* io, int n, skgemm_serve_options_t& o, Exec&
     while (!queue.empty()) {
       auto pick = queue.begin();
       if (o.policy == SKGEMM_SERVE_SMALLEST) {
-        const double tau = o.aging_s > 0 ? o.aging_s : 0.25;
+        const double tau = o.aging_s > 0 ? o.aging_s : 1.0;
         double best = 1e300;
         for (auto it = queue.begin(); it != queue.end(); ++it) {
           const Req& c = R[*it];
