@@ -77,8 +77,10 @@ def parse():
     ap.add_argument("--nd", type=int, default=ND,
                     help="grid points (default 110592 = 48^3; smaller values for profiling)")
     ap.add_argument("--nb", type=int, default=NB, help="states (default 512)")
+    ap.add_argument("--op", default="syrk", choices=["syrk", "gemm", "rotation", "pair"],
+                    help="--workload op: which call (one per step, standalone)")
     ap.add_argument("--workload", default="subspace",
-                    choices=["subspace", "batched", "serving", "tour"],
+                    choices=["subspace", "batched", "serving", "tour", "op"],
                     help="tour: one checked launch of every auxiliary kernel (for ncu), untimed")
     ap.add_argument("--rot-layout", default="grid", choices=["grid", "band"],
                     help="subspace: the rotation reads grid-packed Psi (the reference's "
@@ -701,6 +703,39 @@ def run_e2e(args, band, h32, grid, q, dist, prec, name):
             "api": api}
 
 
+# ------------------------------------------------------------ one op
+def run_op(args):
+    """One standalone call per step (the reference's one-call-at-a-time use)
+    on the subspace shapes: SYRK S = Psi^T Psi, GEMM Hs = Psi^T H Psi, the
+    rotation Psi Q, or the S + Hs pair; for profiling a single op and timing
+    it alone. Prints {"op", "precision", "ms", "tflops"}."""
+    import torch
+    import skgemm
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    band, h32, grid, q, _ = make_inputs(dev)
+    S = torch.zeros(NB * NB, dtype=torch.float64, device=dev)
+    Hs = torch.zeros_like(S)
+    Pn = torch.empty_like(band)
+    name = "native" if args.precision == "both" else args.precision
+    p = _prec(skgemm, name)
+    s = torch.cuda.current_stream()
+    calls = {
+        "syrk": (lambda: skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, stream=s, precision=p),
+                 FLOP_SYRK),
+        "gemm": (lambda: skgemm.dgemm_packed_dev(NB, NB, ND, band, h32, Hs, NB, stream=s,
+                                                 precision=p), FLOP_GEMM),
+        "rotation": (lambda: skgemm.drot_dev(ND, NB, grid, q, Pn, stream=s, precision=p),
+                     FLOP_ROT),
+        "pair": (lambda: skgemm.dsubspace_packed_dev(ND, NB, band, h32, S, Hs, stream=s,
+                                                     precision=p), FLOP_SYRK + FLOP_GEMM)}
+    fn, flop = calls[args.op]
+    ms = time_calls(fn, s, torch, reps=max(1, args.steps), warm=max(0, args.warmup))
+    skgemm.stream_status(s)
+    print(json.dumps({"workload": f"op_{args.op}_{WORKLOAD}", "op": args.op, "precision": name,
+                      "ms": round(ms, 4), "tflops": round(flop / ms / 1e9, 3)}), flush=True)
+
+
 # ------------------------------------------------------------ kernel tour
 def run_tour(args=None) -> None:
     """One launch of every auxiliary kernel of the library on a representative
@@ -1237,6 +1272,8 @@ def main():
         run_serving(args)
     elif args.workload == "tour":
         run_tour(args)
+    elif args.workload == "op":
+        run_op(args)
     else:
         run_gpu(args)
 
