@@ -1,6 +1,7 @@
-"""The CTA-pair (tcgen05 .cta_group::2) lanes kernel against the one-CTA
-kernel: both write the same int32 partial slabs, so every Ozaki GEMM, SYRK,
-subspace pair and the exact int8 GEMM must agree bit for bit. The one-CTA
+"""The CTA-pair (tcgen05 .cta_group::2) INT8 kernels against the one-CTA
+kernels: the lanes kernels write the same int32 partial slabs and the
+rotation kernels the same residue bytes, so every Ozaki GEMM, SYRK, subspace
+pair, rotation and the exact int8 GEMM must agree bit for bit. The one-CTA
 results come from a child process with SKGEMM_LANES_PAIR=0 (the switch is
 read once per process); this process runs the default (pair) kernel."""
 import os
@@ -46,6 +47,20 @@ def compute(prec):
             res += [S.cpu().numpy(), Hs.cpu().numpy()]
         skgemm.stream_status()
         out.append(res)
+    # Rotations (the B-resident products: CTA pairs of 256-row units), one of
+    # them with an odd number of 128-row tiles (the last pair half is padding).
+    for j, (Nd, nb) in enumerate([(4096, 512), (12288, 256), (1040, 208), (110592, 512)]):
+        g = torch.Generator(device="cuda").manual_seed(200 + j)
+        Psi = torch.randn(Nd, nb, generator=g, dtype=torch.float64, device="cuda") / Nd ** 0.5
+        Q = torch.rand(nb, nb, generator=g, dtype=torch.float64, device="cuda") * 2 - 1
+        G = torch.empty(Nd * nb, dtype=torch.float64, device="cuda")
+        skgemm.pack_dev(Nd, nb, Psi, nb, 1, 16, G)
+        R = torch.full((Nd * nb,), float("nan"), dtype=torch.float64, device="cuda")
+        if prec == skgemm.PREC_OZAKI_BF16 and nb > 1024:
+            continue
+        skgemm.drot_dev(Nd, nb, G, Q, R, precision=prec)
+        skgemm.stream_status()
+        out.append([R.cpu().numpy()])
     ai = torch.randint(-128, 128, (700, 3000), dtype=torch.int8, device="cuda",
                        generator=torch.Generator(device="cuda").manual_seed(7))
     bi = torch.randint(-128, 128, (333, 3000), dtype=torch.int8, device="cuda",
