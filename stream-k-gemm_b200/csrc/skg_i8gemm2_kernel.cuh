@@ -297,310 +297,4 @@ __global__ void __launch_bounds__(kI8Threads, 1)
   if (warp == 1) tmem_dealloc_pair(tmem_base, kI8TmemCols);
 }
 
-
-// ---------------------------------------------------------------------------
-// The rotation's products (Psi' = Psi Q, K = nb <= 512) on CTA pairs: the
-// B-resident schedule of i8_rot_kernel with 256-row units (l, tm2) per
-// cluster. Each CTA keeps its 128 rows (N / 2) of B_l[tn] for all k blocks
-// (64 KB instead of 128 KB), which leaves room for an 8-stage ring of 16 KB
-// A tiles (two units of look-ahead instead of one), and writes the residue
-// bytes of its own 128 rows through the same 32 x 128-byte TMA store boxes.
-// Rank 0 issues the pair MMAs. A loads of both CTAs count on rank 0's full
-// barriers; rank 1's B loads complete on its own barrier and a relay from
-// its producer arrives on rank 0's, so each CTA can wait for its own B loads
-// before it exits.
-constexpr int kI8R2Stages = 8;
-constexpr int kI8R2BBytes = kI8RotKbMax * kI8P2TileBytes;  // 64 KB
-constexpr int kI8R2SmemBytes = kI8R2BBytes + kI8R2Stages * kI8P2TileBytes +
-                               kI8EpiWarps * kI8RotBoxBytes + 1024 + 256;
-static_assert(kI8R2SmemBytes <= 232448, "pair rotation kernel exceeds 227 KB of shared memory");
-static_assert((2 * kI8R2Stages + 7) * 8 + 8 <= 256, "pair rotation kernel barrier area");
-
-// Units (l, tm2) of cluster `cl`: group q = cl / tiles_n with column tile
-// tn = cl % tiles_n walks [q V / G, (q+1) V / G) of V = L * tiles_m units,
-// l major; here tiles_m counts 256-row pair tiles.
-__device__ __forceinline__ bool rot2_next_item(const I8RotParams& p, int cl, int rank, int& cursor,
-                                               I8Item& it) {
-  const int q = cl / p.tiles_n;
-  if (q >= p.groups) return false;
-  const int64_t V = (int64_t)p.L * p.tiles_m;
-  const int64_t b = V * q / p.groups, e = V * (q + 1) / p.groups;
-  const int64_t v = b + cursor;
-  if (v >= e) return false;
-  it.l = (int)(v / p.tiles_m);
-  it.tm = 2 * (int)(v - (int64_t)it.l * p.tiles_m) + rank;  // this CTA's 128-row tile
-  it.tn = cl - q * p.tiles_n;
-  it.kb0 = 0;
-  it.kb1 = p.KB;
-  it.slot = 0;
-  ++cursor;
-  return true;
-}
-
-__global__ void __launch_bounds__(kI8Threads, 1)
-    i8_rot2_kernel(const __grid_constant__ CUtensorMap mapA,
-                   const __grid_constant__ CUtensorMap mapB,
-                   const __grid_constant__ CUtensorMap mapR, const I8RotParams p) {
-  extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
-                                             ~uintptr_t(1023));
-  uint8_t* sB = smem;
-  uint8_t* sA = smem + kI8R2BBytes;
-  uint8_t* sR = sA + kI8R2Stages * kI8P2TileBytes;
-  uint64_t* full_bar = reinterpret_cast<uint64_t*>(sR + kI8EpiWarps * kI8RotBoxBytes);
-  uint64_t* empty_bar = full_bar + kI8R2Stages;
-  uint64_t* bfull = empty_bar + kI8R2Stages;  // rank 0: both CTAs' B loaded
-  uint64_t* bown = bfull + 1;                 // this CTA's own B loads (rank 1)
-  uint64_t* bempty = bown + 1;
-  uint64_t* tfull_bar = bempty + 1;
-  uint64_t* tempty_bar = tfull_bar + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty_bar + 2);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int rank = (int)cluster_ctarank();
-  const int cl = blockIdx.x >> 1;
-
-  // Shapes outside the B region and clusters with no work leave together.
-  if (p.KB < 1 || p.KB > kI8RotKbMax) return;
-  {
-    int cur = 0;
-    I8Item probe;
-    if (!rot2_next_item(p, cl, rank, cur, probe)) return;
-  }
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kI8R2Stages; ++s) {
-      mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
-    }
-    mbar_init(bfull, 2);  // rank 0's arrive with its byte count + rank 1's relay
-    mbar_init(bown, 1);
-    mbar_init(bempty, 1);
-    for (int a = 0; a < 2; ++a) {
-      mbar_init(&tfull_bar[a], 1);
-      mbar_init(&tempty_bar[a], 2 * kI8EpiWarps);
-    }
-    *abort_flag = 0;
-    fence_mbar_init();
-  }
-  if (warp == 1) {
-    tmem_alloc_pair(tmem_slot, kI8TmemCols);
-    tmem_relinquish_pair();
-  }
-  tc_fence_before();
-  cluster_sync_all();
-  tc_fence_after();
-  const uint32_t tmem_base = *tmem_slot;
-  const uint32_t full0 = mapa_shared(smem_u32(full_bar), 0);
-  const uint32_t bfull0 = mapa_shared(smem_u32(bfull), 0);
-  const uint32_t tempty0 = mapa_shared(smem_u32(tempty_bar), 0);
-
-  if (warp == 0) {
-    // ---------------------------------------------------------- producer
-    if (lane == 0) {
-      tma_prefetch_desc(&mapA);
-      tma_prefetch_desc(&mapB);
-      tma_prefetch_desc(&mapR);
-      int stage = 0;
-      uint32_t phase = 0;
-      int cur = 0;
-      int64_t issued = 0;
-      int cur_l = -1;
-      uint32_t bempty_ph = 0;
-      int b_loads = 0;
-      I8Item it;
-      const uint32_t bbytes = (uint32_t)(p.KB * kI8P2TileBytes);
-      while (!*abort_flag && rot2_next_item(p, cl, rank, cur, it)) {
-        if (it.l != cur_l) {
-          // This CTA's half of B_l[tn] (all k blocks) for the next run of units.
-          if (cur_l >= 0) {
-            if (!mbar_wait(bempty, bempty_ph, p.err)) {
-              *abort_flag = 1;
-              break;
-            }
-            bempty_ph ^= 1;
-          }
-          uint64_t* bb = rank == 0 ? bfull : bown;
-          mbar_arrive_expect_tx(bb, bbytes);
-          for (int kb = 0; kb < p.KB; ++kb)
-            tma_load_3d(sB + kb * kI8P2TileBytes, &mapB, bb, kb * kI8BK,
-                        it.tn * kI8BN + 128 * rank, it.l);
-          if (rank == 1) {
-            // Relay: rank 0's MMAs may read this half once it has landed.
-            if (!mbar_wait(bown, (uint32_t)(b_loads & 1), p.err)) {
-              *abort_flag = 1;
-              break;
-            }
-            mbar_arrive_cluster(bfull0);
-          }
-          ++b_loads;
-          cur_l = it.l;
-        }
-        for (int kb = 0; kb < p.KB; ++kb) {
-          if (!mbar_wait(&empty_bar[stage], phase ^ 1, p.err)) {
-            *abort_flag = 1;
-            break;
-          }
-          ++issued;
-          if (rank == 0) mbar_arrive_expect_tx(&full_bar[stage], 2 * kI8P2TileBytes);
-          tma_load_3d_pair(sA + stage * kI8P2TileBytes, &mapA, full0 + stage * 8, kb * kI8BK,
-                           it.tm * kI8BM, it.l);
-          if (++stage == kI8R2Stages) {
-            stage = 0;
-            phase ^= 1;
-          }
-        }
-      }
-      // Drain: this CTA's last loads have landed before it may exit (rank 0
-      // on its full barriers, rank 1 once the MMAs released the stages; the
-      // B loads on each CTA's own barrier).
-      for (int j = 1; j <= kI8R2Stages && j <= issued; ++j) {
-        int s2 = stage - j;
-        uint32_t ph = phase;
-        if (s2 < 0) {
-          s2 += kI8R2Stages;
-          ph ^= 1;
-        }
-        if (rank == 0)
-          mbar_wait(&full_bar[s2], ph, p.err);
-        else
-          mbar_wait(&empty_bar[s2], ph, p.err);
-      }
-      if (b_loads > 0) mbar_wait(rank == 0 ? bfull : bown, (uint32_t)((b_loads - 1) & 1), p.err);
-    }
-  } else if (warp == 1) {
-    // --------------------------------------------------------- MMA issuer
-    if (lane == 0 && rank == 0) {
-      const uint32_t idesc = umma_idesc_i8(2 * kI8BM, kI8BN, 1);
-      const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
-      int stage = 0;
-      uint32_t phase = 0;
-      int acc = 0;
-      uint32_t acc_phase = 0;
-      int cur = 0;
-      int cur_l = -1;
-      uint32_t bfull_ph = 0;
-      I8Item it;
-      while (!*abort_flag && rot2_next_item(p, cl, rank, cur, it)) {
-        if (it.l != cur_l) {
-          // Every MMA issued so far read the old B: release both halves once
-          // they finish.
-          if (cur_l >= 0) umma_commit_pair(bempty, 0x3);
-          if (!mbar_wait(bfull, bfull_ph, p.err)) {
-            *abort_flag = 1;
-            break;
-          }
-          bfull_ph ^= 1;
-          cur_l = it.l;
-        }
-        if (!mbar_wait(&tempty_bar[acc], acc_phase ^ 1, p.err)) {
-          *abort_flag = 1;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t tmem_d = tmem_base + (uint32_t)(acc * kI8BN);
-        for (int kb = 0; kb < p.KB; ++kb) {
-          if (!mbar_wait(&full_bar[stage], phase, p.err)) {
-            *abort_flag = 1;
-            break;
-          }
-          tc_fence_after();
-          const uint64_t adesc = umma_desc_kmajor_sw128(a_base + stage * kI8P2TileBytes);
-          const uint64_t bdesc = umma_desc_kmajor_sw128(b_base + kb * kI8P2TileBytes);
-#pragma unroll
-          for (int kk = 0; kk < kI8BK / kI8UmmaK; ++kk)
-            umma_i8_pair(tmem_d, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2), idesc,
-                         (kb > 0 || kk > 0) ? 1u : 0u);
-          umma_commit_pair(&empty_bar[stage], 0x3);
-          if (++stage == kI8R2Stages) {
-            stage = 0;
-            phase ^= 1;
-          }
-        }
-        umma_commit_pair(&tfull_bar[acc], 0x3);
-        if (++acc == 2) {
-          acc = 0;
-          acc_phase ^= 1;
-        }
-      }
-    }
-  } else {
-    // ---------------------------------------------------------- epilogue
-    // As in i8_rot_kernel: warp w owns TMEM lanes 32 (w % 4) .. +31 (rows of
-    // this CTA's half) and columns 128 ((w - 2) / 4) .. +127, written as a
-    // 32 x 128-byte box in the 128-byte swizzle and stored by TMA.
-    const int quarter = warp & 3;
-    const int half = (warp - 2) >> 2;
-    uint8_t* box = sR + (warp - 2) * kI8RotBoxBytes;
-    uint8_t* my_row = box + lane * 128;
-    const int sw = lane & 7;
-    int acc = 0;
-    uint32_t acc_phase = 0;
-    int cur = 0;
-    I8Item it;
-    while (rot2_next_item(p, cl, rank, cur, it)) {
-      if (*abort_flag || !mbar_wait(&tfull_bar[acc], acc_phase, p.err)) {
-        *abort_flag = 1;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) +
-                             (uint32_t)(acc * kI8BN + half * 128);
-      if (lane == 0) bulk_wait_read_all();
-      __syncwarp();
-      const uint32_t m = c_i8mod.m[it.l], magic = c_i8mod.magic24[it.l];
-      const uint32_t off = c_i8mod.offset24[it.l];
-      const bool pow2 = (m == 256u);
-#pragma unroll 1
-      for (int c = 0; c < 4; c += 2) {
-        uint32_t v0[32], v1[32];
-        tmem_ld_32x32b_x32(taddr + c * 32, v0);
-        tmem_ld_32x32b_x32(taddr + c * 32 + 32, v1);
-        tmem_ld_wait();
-        if (!pow2) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            v0[j] = mod_exact24(v0[j] + off, m, magic);
-            v1[j] = mod_exact24(v1[j] + off, m, magic);
-          }
-        }
-        uint32_t w[16];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          w[j] = __byte_perm(__byte_perm(v0[4 * j], v0[4 * j + 1], 0x0040),
-                             __byte_perm(v0[4 * j + 2], v0[4 * j + 3], 0x0040), 0x5410);
-          w[8 + j] = __byte_perm(__byte_perm(v1[4 * j], v1[4 * j + 1], 0x0040),
-                                 __byte_perm(v1[4 * j + 2], v1[4 * j + 3], 0x0040), 0x5410);
-        }
-#pragma unroll
-        for (int h = 0; h < 4; ++h)
-          *reinterpret_cast<uint4*>(my_row + (((2 * c + h) ^ sw) << 4)) =
-              make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
-      }
-      tc_fence_before();
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) {
-        mbar_arrive_cluster(tempty0 + acc * 8);
-        const int x = it.tn * kI8BN + half * 128, y = it.tm * kI8BM + quarter * 32;
-        if (x < p.N && y < p.M) {
-          tma_store_3d(&mapR, box, x, y, it.l);
-          bulk_commit_group();
-        }
-      }
-      if (++acc == 2) {
-        acc = 0;
-        acc_phase ^= 1;
-      }
-    }
-    if (lane == 0) bulk_wait_all();
-  }
-
-  tc_fence_before();
-  cluster_sync_all();
-  tc_fence_after();
-  if (warp == 1) tmem_dealloc_pair(tmem_base, kI8TmemCols);
-}
 }  // namespace skg

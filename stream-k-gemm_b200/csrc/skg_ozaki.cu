@@ -1105,36 +1105,6 @@ int launch_i8_rot(DeviceState* dev, const CUtensorMap& mA, const CUtensorMap& mB
   return SKGEMM_OK;
 }
 
-// Co-resident clusters of the pair rotation kernel (0: one-CTA kernel).
-int rot_pair_clusters(DeviceState* dev) {
-  if (!lanes_pair_enabled()) return 0;
-  static int ncl[64] = {0};
-  if (!ncl[dev->device]) {
-    if (cudaFuncSetAttribute(i8_rot2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kI8R2SmemBytes) != cudaSuccess)
-      return 0;
-    cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = pair_config(2 * (dev->num_sms / 2), nullptr, attr);
-    cfg.dynamicSmemBytes = kI8R2SmemBytes;
-    int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, (const void*)i8_rot2_kernel, &cfg) != cudaSuccess ||
-        n < 1)
-      return 0;
-    ncl[dev->device] = n;
-  }
-  return ncl[dev->device];
-}
-
-int launch_i8_rot_pair(const CUtensorMap& mA, const CUtensorMap& mB, const CUtensorMap& mR,
-                       const I8RotParams& p, int clusters, cudaStream_t s) {
-  cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = pair_config(2 * clusters, s, attr);
-  cfg.dynamicSmemBytes = kI8R2SmemBytes;
-  KernelTimer kt_(s, "i8_rot2_kernel");
-  SKG_CUDA(cudaLaunchKernelEx(&cfg, i8_rot2_kernel, mA, mB, mR, p));
-  return SKGEMM_OK;
-}
-
 bool is_bf16(const skgemm_options_t* opts) {
   return opts && opts->precision == SKGEMM_PREC_OZAKI_BF16;
 }
@@ -1810,13 +1780,7 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
   if (!ws) return st;
   OzakiStream* os = ozaki_stream(dev, s);
   const int64_t KP = (nb + 127) / 128 * 128;
-  // The B-resident products run on CTA pairs (256-row units) unless the
-  // one-CTA kernel is selected; the A residue rows are then padded to 256.
-  const bool rot_resident = !bf && KP / 128 <= kI8RotKbMax && nb % 16 == 0 && nb >= 128 &&
-                            Nd >= 128;
-  const int rot_clusters = rot_resident ? rot_pair_clusters(dev) : 0;
-  const int64_t RA = (Nd + (rot_clusters ? 255 : kI8BM - 1)) / (rot_clusters ? 256 : kI8BM) *
-                     (rot_clusters ? 256 : kI8BM);
+  const int64_t RA = (Nd + kI8BM - 1) / kI8BM * kI8BM;
   const int64_t RB = (nb + kI8BN - 1) / kI8BN * kI8BN;
   const int64_t KPb = KP * (bf ? 2 : 1);
   if ((st = os->res_b.ensure((size_t)L * RB * KPb))) return st;
@@ -1832,8 +1796,8 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
     return st;
   CUtensorMap mA, mB;
   if ((st = make_res_map(&mA, os->res_a.ptr, KPb, RA, L, kI8BM))) return st;
-  if ((st = make_res_map(&mB, os->res_b.ptr, KPb, RB, L, rot_clusters ? 128 : kI8BN))) return st;
-  if (rot_resident) {
+  if ((st = make_res_map(&mB, os->res_b.ptr, KPb, RB, L, kI8BN))) return st;
+  if (!bf && KP / 128 <= kI8RotKbMax && nb % 16 == 0 && nb >= 128 && Nd >= 128) {
     // B_l[tn] fits in shared memory: the B-resident schedule, residue bytes
     // [L][Nd][nb] written by 32 x 128-byte TMA store boxes.
     CUtensorMap mR;
@@ -1851,19 +1815,12 @@ int ozaki_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, double* 
     p.KB = (int)(KP / 128);
     p.M = (int)Nd;
     p.N = (int)nb;
+    p.tiles_m = (int)(RA / kI8BM);
     p.tiles_n = (int)(RB / kI8BN);
+    const int64_t V = (int64_t)L * p.tiles_m;
+    p.groups = (int)std::max<int64_t>(1, std::min<int64_t>(dev->num_sms / p.tiles_n, V));
     p.err = ws->err;
-    if (rot_clusters) {
-      p.tiles_m = (int)(RA / 256);  // 256-row pair units
-      const int64_t V = (int64_t)L * p.tiles_m;
-      p.groups = (int)std::max<int64_t>(1, std::min<int64_t>(rot_clusters / p.tiles_n, V));
-      if ((st = launch_i8_rot_pair(mA, mB, mR, p, p.groups * p.tiles_n, s))) return st;
-    } else {
-      p.tiles_m = (int)(RA / kI8BM);
-      const int64_t V = (int64_t)L * p.tiles_m;
-      p.groups = (int)std::max<int64_t>(1, std::min<int64_t>(dev->num_sms / p.tiles_n, V));
-      if ((st = launch_i8_rot(dev, mA, mB, mR, p, p.groups * p.tiles_n, s))) return st;
-    }
+    if ((st = launch_i8_rot(dev, mA, mB, mR, p, p.groups * p.tiles_n, s))) return st;
   } else {
     I8Params p;
     memset(&p, 0, sizeof(p));

@@ -1,7 +1,8 @@
-"""The CTA-pair (tcgen05 .cta_group::2) INT8 kernels against the one-CTA
-kernels: the lanes kernels write the same int32 partial slabs and the
-rotation kernels the same residue bytes, so every Ozaki GEMM, SYRK, subspace
-pair, rotation and the exact int8 GEMM must agree bit for bit. The one-CTA
+"""The CTA-pair (tcgen05 .cta_group::2) lanes kernel against the one-CTA
+kernel: both write the same int32 partial slabs, so every Ozaki GEMM, SYRK,
+subspace pair and the exact int8 GEMM must agree bit for bit (the rotations,
+whose products run on the one-CTA B-resident kernel either way, are checked
+alongside). The one-CTA
 results come from a child process with SKGEMM_LANES_PAIR=0 (the switch is
 read once per process); this process runs the default (pair) kernel."""
 import os
@@ -47,8 +48,7 @@ def compute(prec):
             res += [S.cpu().numpy(), Hs.cpu().numpy()]
         skgemm.stream_status()
         out.append(res)
-    # Rotations (the B-resident products: CTA pairs of 256-row units), one of
-    # them with an odd number of 128-row tiles (the last pair half is padding).
+    # Rotations, one of them with an odd number of 128-row tiles.
     for j, (Nd, nb) in enumerate([(4096, 512), (12288, 256), (1040, 208), (110592, 512)]):
         g = torch.Generator(device="cuda").manual_seed(200 + j)
         Psi = torch.randn(Nd, nb, generator=g, dtype=torch.float64, device="cuda") / Nd ** 0.5
