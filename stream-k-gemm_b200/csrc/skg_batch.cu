@@ -968,6 +968,7 @@ struct skgemm_plan {
 SKG_EXPORT int skgemm_plan_create(const skgemm_batch_item_t* items, int n,
                                   skgemm_plan_options_t* opts, void* stream,
                                   skgemm_plan_t* plan_out) {
+  NvtxRange nvtx_(__func__);
   if (!plan_out) return fail(SKGEMM_ERR_INVALID_ARG, "null plan_out");
   *plan_out = nullptr;
   BatchPlan* P = nullptr;
@@ -978,11 +979,13 @@ SKG_EXPORT int skgemm_plan_create(const skgemm_batch_item_t* items, int n,
 }
 
 SKG_EXPORT int skgemm_plan_run(skgemm_plan_t plan, void* stream) {
+  NvtxRange nvtx_(__func__);
   if (!plan || !plan->impl) return fail(SKGEMM_ERR_INVALID_ARG, "null plan");
   return plan_run(plan->impl, reinterpret_cast<cudaStream_t>(stream));
 }
 
 SKG_EXPORT int skgemm_plan_status(skgemm_plan_t plan, void* stream) {
+  NvtxRange nvtx_(__func__);
   if (!plan || !plan->impl) return fail(SKGEMM_ERR_INVALID_ARG, "null plan");
   return plan_status(plan->impl, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -1003,6 +1006,7 @@ SKG_EXPORT void skgemm_plan_destroy(skgemm_plan_t plan) {
 }
 
 SKG_EXPORT int skgemm_batch_dev(const skgemm_batch_item_t* items, int n, void* stream) {
+  NvtxRange nvtx_(__func__);
   return batch_dev(items, n, reinterpret_cast<cudaStream_t>(stream));
 }
 

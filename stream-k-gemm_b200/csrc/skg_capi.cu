@@ -372,6 +372,7 @@ SKG_EXPORT const char* skgemm_version(void) { return "skgemm 0.1.0 (sm_100a)"; }
 SKG_EXPORT const char* skgemm_last_error(void) { return g_last_error.c_str(); }
 
 SKG_EXPORT int skgemm_stream_status(void* stream) {
+  NvtxRange nvtx_(__func__);
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -389,6 +390,7 @@ SKG_EXPORT int skgemm_stream_status(void* stream) {
 }
 
 SKG_EXPORT int skgemm_stream_release(void* stream) {
+  NvtxRange nvtx_(__func__);
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -460,6 +462,7 @@ SKG_EXPORT int skgemm_kernel_timing_report(char* buf, int64_t len) {
 }
 
 SKG_EXPORT int skgemm_diag_expire_wait(double budget_ms, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -467,6 +470,7 @@ SKG_EXPORT int skgemm_diag_expire_wait(double budget_ms, void* stream) {
 }
 
 SKG_EXPORT int skgemm_diag_expire_fixup_wait(double budget_ms, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -474,6 +478,7 @@ SKG_EXPORT int skgemm_diag_expire_fixup_wait(double budget_ms, void* stream) {
 }
 
 SKG_EXPORT int skgemm_probe_fp64_peak(double* tflops_out) {
+  NvtxRange nvtx_(__func__);
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -481,6 +486,7 @@ SKG_EXPORT int skgemm_probe_fp64_peak(double* tflops_out) {
 }
 
 SKG_EXPORT int skgemm_probe_i8_peak(double* tops_out) {
+  NvtxRange nvtx_(__func__);
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -491,6 +497,7 @@ SKG_EXPORT int skgemm_probe_i8_peak(double* tops_out) {
 SKG_EXPORT int skgemm_igemm_s8_dev(int64_t M, int64_t N, int64_t K, const int8_t* A,
                                    int64_t lda, const int8_t* B, int64_t ldb, int32_t* C,
                                    int64_t ldc, void* stream) {
+  NvtxRange nvtx_(__func__);
   return igemm_s8(M, N, K, A, lda, B, ldb, C, ldc, reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -498,6 +505,7 @@ SKG_EXPORT int skgemm_igemm_s8_dev(int64_t M, int64_t N, int64_t K, const int8_t
 SKG_EXPORT int skgemm_dgemm_packed_dev(int64_t M, int64_t N, int64_t K, const double* Ap,
                                        const double* Bp, double* D, int64_t ldd, double alpha,
                                        double gamma, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st = check_dims(M, N, K);
   if (st) return st;
   if (ldd < N) return fail(SKGEMM_ERR_INVALID_ARG, "ldd < N");
@@ -508,6 +516,7 @@ SKG_EXPORT int skgemm_dgemm_packed_dev(int64_t M, int64_t N, int64_t K, const do
 SKG_EXPORT int skgemm_dgemm_dev(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
                                 const double* B, int64_t ldb, double* D, int64_t ldd,
                                 double alpha, double gamma, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st = check_dims(M, N, K);
   if (st) return st;
   if (lda < M || ldb < N || ldd < N) return fail(SKGEMM_ERR_INVALID_ARG, "leading dimension too small");
@@ -541,6 +550,7 @@ SKG_EXPORT int skgemm_dgemm_packed_dev_opt(int64_t M, int64_t N, int64_t K, cons
                                            const double* Bp, double* D, int64_t ldd,
                                            double alpha, double gamma, skgemm_options_t* opts,
                                            void* stream) {
+  NvtxRange nvtx_(__func__);
   if (opts && opts->precision == SKGEMM_PREC_AUTO) {
     const int pr = auto_precision(
         ozaki_time_estimate(SKGEMM_OP_GEMM_PACKED, M, N, K, opts->slices),
@@ -618,6 +628,7 @@ struct HostPipe {
 
 SKG_EXPORT int skgemm_dgemm_packed(int64_t M, int64_t N, int64_t K, const double* Ap,
                                    const double* Bp, double* D, double alpha, double gamma) {
+  NvtxRange nvtx_(__func__);
   int st = check_dims(M, N, K);
   if (st) return st;
   if (M == 0 || N == 0) return SKGEMM_OK;
@@ -671,6 +682,7 @@ SKG_EXPORT int skgemm_dgemm_packed(int64_t M, int64_t N, int64_t K, const double
 
 SKG_EXPORT int skgemm_dgemm(int64_t M, int64_t N, int64_t K, const double* A, const double* B,
                             double* D, double alpha, double gamma) {
+  NvtxRange nvtx_(__func__);
   int st = check_dims(M, N, K);
   if (st) return st;
   if (M == 0 || N == 0) return SKGEMM_OK;
@@ -685,6 +697,7 @@ SKG_EXPORT int skgemm_dgemm(int64_t M, int64_t N, int64_t K, const double* A, co
 // ------------------------------------------------------------------- SYRK
 SKG_EXPORT int skgemm_dsyrk_packed_dev(int64_t K, int64_t M, const double* Ap, double* C,
                                        int64_t ldc, double alpha, double beta, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st = check_dims(K, M, 0);
   if (st) return st;
   if (ldc < M) return fail(SKGEMM_ERR_INVALID_ARG, "ldc < M");
@@ -695,6 +708,7 @@ SKG_EXPORT int skgemm_dsyrk_packed_dev(int64_t K, int64_t M, const double* Ap, d
 SKG_EXPORT int skgemm_dsyrk_packed_dev_opt(int64_t K, int64_t M, const double* Ap, double* C,
                                            int64_t ldc, double alpha, double beta,
                                            skgemm_options_t* opts, void* stream) {
+  NvtxRange nvtx_(__func__);
   if (opts && opts->precision == SKGEMM_PREC_AUTO) {
     const int pr = auto_precision(
         ozaki_time_estimate(SKGEMM_OP_SYRK_PACKED, M, M, K, opts->slices),
@@ -720,6 +734,7 @@ SKG_EXPORT int skgemm_dsyrk_packed_dev_opt(int64_t K, int64_t M, const double* A
 SKG_EXPORT int skgemm_dsubspace_packed_dev(int64_t K, int64_t M, const double* Psi,
                                            const double* HPsi, double* S, int64_t lds, double* Hs,
                                            int64_t ldh, skgemm_options_t* opts, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st = check_dims(K, M, 0);
   if (st) return st;
   if (lds < M || ldh < M) return fail(SKGEMM_ERR_INVALID_ARG, "lds or ldh < M");
@@ -747,6 +762,7 @@ SKG_EXPORT int skgemm_dsubspace_packed_dev(int64_t K, int64_t M, const double* P
 
 SKG_EXPORT int skgemm_dsyrk_packed(int64_t K, int64_t M, const double* Ap, double* C,
                                    double alpha, double beta) {
+  NvtxRange nvtx_(__func__);
   int st = check_dims(K, M, 0);
   if (st) return st;
   if (M == 0) return SKGEMM_OK;
@@ -806,6 +822,7 @@ static int check_rot(int64_t Nd, int64_t nb) {
 
 SKG_EXPORT int skgemm_drot_dev(int64_t Nd, int64_t nb, const double* A, const double* Q,
                                double* D, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st = check_rot(Nd, nb);
   if (st) return st;
   return run_native(rot_problem(Nd, nb, A, Q, D), reinterpret_cast<cudaStream_t>(stream));
@@ -813,6 +830,7 @@ SKG_EXPORT int skgemm_drot_dev(int64_t Nd, int64_t nb, const double* A, const do
 
 SKG_EXPORT int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A, const double* Q,
                                    double* D, skgemm_options_t* opts, void* stream) {
+  NvtxRange nvtx_(__func__);
   if (opts && opts->precision == SKGEMM_PREC_AUTO) {
     const int pr = auto_precision(ozaki_time_estimate(SKGEMM_OP_ROT, Nd, nb, nb, opts->slices),
                                   batch_native_estimate(rot_problem(Nd, nb, A, Q, D)));
@@ -840,6 +858,7 @@ SKG_EXPORT int skgemm_drot_dev_opt(int64_t Nd, int64_t nb, const double* A, cons
 // skgemm_drot_dev_opt on the grid-packed copy, bit for bit.
 SKG_EXPORT int skgemm_drot_band_dev(int64_t Nd, int64_t nb, const double* A_band,
                                     const double* Q, double* D, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st = check_rot(Nd, nb);
   if (st) return st;
   return run_native(rot_problem(Nd, nb, A_band, Q, D, true),
@@ -849,6 +868,7 @@ SKG_EXPORT int skgemm_drot_band_dev(int64_t Nd, int64_t nb, const double* A_band
 SKG_EXPORT int skgemm_drot_band_dev_opt(int64_t Nd, int64_t nb, const double* A_band,
                                         const double* Q, double* D, skgemm_options_t* opts,
                                         void* stream) {
+  NvtxRange nvtx_(__func__);
   if (opts && opts->precision == SKGEMM_PREC_AUTO) {
     const int pr = auto_precision(ozaki_time_estimate(SKGEMM_OP_ROT, Nd, nb, nb, opts->slices),
                                   batch_native_estimate(rot_problem(Nd, nb, A_band, Q, D)));
@@ -952,11 +972,13 @@ static int host_rot(int64_t Nd, int64_t nb, const double* A, const double* Q, do
 
 SKG_EXPORT int skgemm_drot(int64_t Nd, int64_t nb, const double* A, const double* Q,
                            double* D) {
+  NvtxRange nvtx_(__func__);
   return host_rot(Nd, nb, A, Q, D, nullptr);
 }
 
 SKG_EXPORT int skgemm_drot_opt(int64_t Nd, int64_t nb, const double* A, const double* Q,
                                double* D, skgemm_options_t* opts) {
+  NvtxRange nvtx_(__func__);
   return host_rot(Nd, nb, A, Q, D, opts);
 }
 
@@ -968,6 +990,7 @@ SKG_EXPORT int skgemm_drot_opt(int64_t Nd, int64_t nb, const double* A, const do
 SKG_EXPORT int skgemm_dgemm_packed_opt(int64_t M, int64_t N, int64_t K, const double* Ap,
                                        const double* Bp, double* D, double alpha, double gamma,
                                        skgemm_options_t* opts) {
+  NvtxRange nvtx_(__func__);
   if (opts && opts->precision == SKGEMM_PREC_AUTO) {
     const int pr = auto_precision(
         ozaki_time_estimate(SKGEMM_OP_GEMM_PACKED, M, N, K, opts->slices),
@@ -997,6 +1020,7 @@ SKG_EXPORT int skgemm_dgemm_packed_opt(int64_t M, int64_t N, int64_t K, const do
 
 SKG_EXPORT int skgemm_dsyrk_packed_opt(int64_t K, int64_t M, const double* Ap, double* C,
                                        double alpha, double beta, skgemm_options_t* opts) {
+  NvtxRange nvtx_(__func__);
   if (opts && opts->precision == SKGEMM_PREC_AUTO) {
     const int pr = auto_precision(
         ozaki_time_estimate(SKGEMM_OP_SYRK_PACKED, M, M, K, opts->slices),
@@ -1026,11 +1050,13 @@ SKG_EXPORT int skgemm_dsyrk_packed_opt(int64_t K, int64_t M, const double* Ap, d
 // ------------------------------------------------------ layout converters
 SKG_EXPORT int skgemm_pack_dev(int64_t R, int64_t K, const double* X, int64_t sr, int64_t sk,
                                int T, double* Xp, void* stream) {
+  NvtxRange nvtx_(__func__);
   return launch_pack(R, K, X, sr, sk, T, Xp, reinterpret_cast<cudaStream_t>(stream));
 }
 
 SKG_EXPORT int skgemm_unpack_dev(int64_t R, int64_t K, const double* X_packed, int T, double* X,
                                  int64_t sr, int64_t sk, void* stream) {
+  NvtxRange nvtx_(__func__);
   return launch_unpack(R, K, X_packed, T, X, sr, sk, reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -1047,23 +1073,27 @@ int c16_check(int64_t Nd, int64_t nb) {
 
 SKG_EXPORT int skgemm_pack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                    void* stream) {
+  NvtxRange nvtx_(__func__);
   if (int st = c16_check(Nd, nb)) return st;
   return launch_pack(Nd, nb, src, 1, Nd, 16, dst, reinterpret_cast<cudaStream_t>(stream));
 }
 
 SKG_EXPORT int skgemm_pack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                    void* stream) {
+  NvtxRange nvtx_(__func__);
   return skgemm_pack_c16_dev(Nd, nb, src, dst, stream);
 }
 
 SKG_EXPORT int skgemm_unpack_c16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                      void* stream) {
+  NvtxRange nvtx_(__func__);
   if (int st = c16_check(Nd, nb)) return st;
   return launch_unpack(Nd, nb, src, 16, dst, 1, Nd, reinterpret_cast<cudaStream_t>(stream));
 }
 
 SKG_EXPORT int skgemm_unpack_r16_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                      void* stream) {
+  NvtxRange nvtx_(__func__);
   return skgemm_unpack_c16_dev(Nd, nb, src, dst, stream);
 }
 
@@ -1100,22 +1130,26 @@ void linalg_convert(int Nd, int nb, const double* src, double* dst, bool pack) {
 
 SKG_EXPORT void linalg_pack_c16_f64(const int Nd, const int nb, const double* src,
                                     double* dst) {
+  NvtxRange nvtx_(__func__);
   linalg_convert(Nd, nb, src, dst, true);
 }
 
 // Row-major [nb, Nd] (src[b*Nd + g]) is the same bytes as column-major [Nd, nb].
 SKG_EXPORT void linalg_pack_r16_f64(const int Nd, const int nb, const double* src,
                                     double* dst) {
+  NvtxRange nvtx_(__func__);
   linalg_convert(Nd, nb, src, dst, true);
 }
 
 SKG_EXPORT void linalg_unpack_c16_f64(const int Nd, const int nb, const double* src,
                                       double* dst) {
+  NvtxRange nvtx_(__func__);
   linalg_convert(Nd, nb, src, dst, false);
 }
 
 SKG_EXPORT void linalg_unpack_r16_f64(const int Nd, const int nb, const double* src,
                                       double* dst) {
+  NvtxRange nvtx_(__func__);
   linalg_convert(Nd, nb, src, dst, false);
 }
 
@@ -1124,6 +1158,7 @@ SKG_EXPORT int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_
                                       const double* coef_x, const double* coef_y,
                                       const double* coef_z, double coef_0, double* out,
                                       int out_tile, void* stream) {
+  NvtxRange nvtx_(__func__);
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
@@ -1135,6 +1170,7 @@ SKG_EXPORT int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_
 SKG_EXPORT int skgemm_halo_periodic_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                                         const double* psi_local16, double* psi_ext16,
                                         void* stream) {
+  NvtxRange nvtx_(__func__);
   return launch_halo_periodic(ni, nj, nk, nb, FDn, psi_local16, psi_ext16,
                               reinterpret_cast<cudaStream_t>(stream));
 }
@@ -1143,12 +1179,14 @@ SKG_EXPORT int skgemm_nloc_create(int64_t P, const uint32_t* nrow, const uint32_
                                   const int32_t* atom, const uint32_t* offsets,
                                   const uint32_t* index, const double* chi, const double* gamma,
                                   int64_t K, skgemm_nloc_t* out) {
+  NvtxRange nvtx_(__func__);
   return nloc_create(P, nrow, ncol, atom, offsets, index, chi, gamma, K, out);
 }
 
 SKG_EXPORT int skgemm_nloc_apply_dev(skgemm_nloc_t h, int64_t nb, double dv,
                                      const double* psi16, double* out, int out_tile,
                                      void* stream) {
+  NvtxRange nvtx_(__func__);
   return nloc_apply(h, nb, dv, psi16, out, out_tile, reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -1156,10 +1194,12 @@ SKG_EXPORT void skgemm_nloc_destroy(skgemm_nloc_t h) { nloc_destroy(h); }
 
 SKG_EXPORT int skgemm_band_to_grid_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                        void* stream) {
+  NvtxRange nvtx_(__func__);
   return launch_band_to_grid(Nd, nb, src, dst, reinterpret_cast<cudaStream_t>(stream));
 }
 
 SKG_EXPORT int skgemm_grid_to_band_dev(int64_t Nd, int64_t nb, const double* src, double* dst,
                                        void* stream) {
+  NvtxRange nvtx_(__func__);
   return launch_grid_to_band(Nd, nb, src, dst, reinterpret_cast<cudaStream_t>(stream));
 }

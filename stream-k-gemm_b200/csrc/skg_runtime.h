@@ -11,9 +11,21 @@
 #include <mutex>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "skgemm.h"
 
 namespace skg {
+
+// NVTX range over one C-ABI call (named after the entry point), so that a
+// profiler's timeline shows the library's calls around their kernels; a push
+// and a pop through the NVTX injection hooks, nearly free without a tool.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Records a message for skgemm_last_error() and returns `code`.
 int fail(int code, const std::string& msg);

@@ -691,6 +691,7 @@ using namespace skg;
 
 SKG_EXPORT int skgemm_serve_run(skgemm_serve_request_t* reqs, int n,
                                 skgemm_serve_options_t* opts) {
+  NvtxRange nvtx_(__func__);
   return serve_run(reqs, n, opts, false);
 }
 
