@@ -439,6 +439,20 @@ int skgemm_batch_dev(const skgemm_batch_item_t* items, int n, void* stream);
  * issued MAC ratio. Items with a zero dimension get zero iterations. */
 int skgemm_batch_schedule(const skgemm_batch_item_t* items, int n, int tile, int order,
                           int* perm_out, int64_t* iter_begin_out, double* efficiency_out);
+/* The autotuner's choices persisted across processes: plans tuned in this
+ * process (per batch signature: device name, plan options, each item's op
+ * and shape) are written by skgemm_tune_cache_save as a JSON file (one entry
+ * per line: key, tile, order, grid, per-item Ozaki flags); a later process
+ * on the same device type loads them with skgemm_tune_cache_load and its
+ * skgemm_plan_create skips the timing runs of those batches (an entry is
+ * used only where it matches the plan's items and candidates). Both return
+ * the number of entries written / read, or a negative status (unreadable or
+ * malformed file: nothing is loaded). skgemm_tune_cache_clear forgets them.
+ * The reference has compile-time tiles only (gemm_opt.cpp:37-47); no
+ * counterpart. */
+int skgemm_tune_cache_save(const char* path);
+int skgemm_tune_cache_load(const char* path);
+int skgemm_tune_cache_clear(void);
 
 /* ------------------------------------------------------------- serving */
 /* A serving engine for subspace requests: each request is the sequence

@@ -32,6 +32,7 @@
 // plan and cannot be regrown by unrelated calls.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -132,9 +133,9 @@ struct Tuned {
 std::mutex g_tune_mu;
 std::map<std::string, Tuned> g_tune_cache;
 
-std::string signature(int device, const std::vector<skgemm_batch_item_t>& items,
+std::string signature(const char* device_name, const std::vector<skgemm_batch_item_t>& items,
                       const skgemm_plan_options_t& o) {
-  std::string s = std::to_string(device) + "|" + std::to_string(o.tile) + "," +
+  std::string s = std::string(device_name) + "|" + std::to_string(o.tile) + "," +
                   std::to_string(o.order) + "," + std::to_string(o.grid) + "," +
                   std::to_string(o.precision) + "," + std::to_string(o.slices) + "|";
   char buf[96];
@@ -658,12 +659,24 @@ int plan_create(const skgemm_batch_item_t* items, int n, skgemm_plan_options_t* 
   Tuned best{model_config(), assigns[0]};
   float best_ms = 0.f;
   int timed = 0;
-  const std::string sig = signature(P->device, P->items, o);
+  const std::string sig = signature(P->dev->name, P->items, o);
   bool cached = false;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto f = g_tune_cache.find(sig);
-    if (f != g_tune_cache.end() && !o.no_tune) {
+    // An entry (tuned here or loaded from a file) is used only if it is one
+    // of the choices this plan's own tuning would time: a candidate
+    // configuration and one of the precision assignments.
+    bool fits = f != g_tune_cache.end() && !o.no_tune;
+    if (fits) {
+      bool cfg_ok = false, oz_ok = false;
+      for (const auto& c : cands)
+        cfg_ok |= (c.tile == f->second.cfg.tile && c.order == f->second.cfg.order &&
+                   c.grid == f->second.cfg.grid);
+      for (const auto& asg : assigns) oz_ok |= (asg == f->second.oz);
+      fits = cfg_ok && oz_ok;
+    }
+    if (fits) {
       best = f->second;
       cached = true;
     }
@@ -1014,4 +1027,109 @@ SKG_EXPORT int skgemm_batch_schedule(const skgemm_batch_item_t* items, int n, in
                                      int order, int* perm_out, int64_t* iter_begin_out,
                                      double* efficiency_out) {
   return batch_schedule(items, n, tile, order, perm_out, iter_begin_out, efficiency_out);
+}
+
+// ------------------------------------------------------------ tuning cache
+// The autotuner's choices (per batch signature: device name, plan options,
+// each item's op and shape) as a JSON file, one entry per line:
+//   {"format": "skgemm-tune-cache/1", "entries": [
+//    {"key": "<signature>", "tile": 128, "order": 1, "grid": 0, "ozaki": "0101"},
+//    ...]}
+// so that a serving process or a solver restarted on the same device type
+// skips the timing runs of plans it has tuned before.
+namespace {
+const char* kTuneFormat = "skgemm-tune-cache/1";
+
+// The text after `"name": ` on `line` (its quoted string, or its integer).
+bool json_string(const std::string& line, const char* name, std::string* out) {
+  const std::string tag = std::string("\"") + name + "\": \"";
+  const size_t a = line.find(tag);
+  if (a == std::string::npos) return false;
+  const size_t b = line.find('"', a + tag.size());
+  if (b == std::string::npos) return false;
+  *out = line.substr(a + tag.size(), b - a - tag.size());
+  return true;
+}
+bool json_int(const std::string& line, const char* name, int* out) {
+  const std::string tag = std::string("\"") + name + "\": ";
+  const size_t a = line.find(tag);
+  if (a == std::string::npos) return false;
+  char* end = nullptr;
+  const long v = strtol(line.c_str() + a + tag.size(), &end, 10);
+  if (end == line.c_str() + a + tag.size()) return false;
+  *out = (int)v;
+  return true;
+}
+}  // namespace
+
+SKG_EXPORT int skgemm_tune_cache_save(const char* path) {
+  if (!path) return fail(SKGEMM_ERR_INVALID_ARG, "tune cache: null path");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  FILE* f = fopen(path, "w");
+  if (!f) return fail(SKGEMM_ERR_INVALID_ARG, std::string("tune cache: cannot write ") + path);
+  fprintf(f, "{\"format\": \"%s\", \"entries\": [\n", kTuneFormat);
+  size_t i = 0;
+  for (const auto& kv : g_tune_cache) {
+    std::string oz(kv.second.oz.size(), '0');
+    for (size_t j = 0; j < oz.size(); ++j) oz[j] = kv.second.oz[j] ? '1' : '0';
+    fprintf(f, "{\"key\": \"%s\", \"tile\": %d, \"order\": %d, \"grid\": %d, \"ozaki\": \"%s\"}%s\n",
+            kv.first.c_str(), kv.second.cfg.tile, kv.second.cfg.order, kv.second.cfg.grid,
+            oz.c_str(), ++i < g_tune_cache.size() ? "," : "");
+  }
+  fprintf(f, "]}\n");
+  const bool ok = fclose(f) == 0;
+  if (!ok) return fail(SKGEMM_ERR_INVALID_ARG, std::string("tune cache: write failed: ") + path);
+  return (int)g_tune_cache.size();
+}
+
+SKG_EXPORT int skgemm_tune_cache_load(const char* path) {
+  if (!path) return fail(SKGEMM_ERR_INVALID_ARG, "tune cache: null path");
+  FILE* f = fopen(path, "r");
+  if (!f) return fail(SKGEMM_ERR_INVALID_ARG, std::string("tune cache: cannot read ") + path);
+  std::vector<std::pair<std::string, Tuned>> got;
+  std::string line;
+  bool header = false, bad = false;
+  char buf[4096];
+  while (fgets(buf, sizeof(buf), f)) {
+    // One entry per line, of any length (a batch of many items has a long key).
+    line.assign(buf);
+    while (!line.empty() && line.back() != '\n' && fgets(buf, sizeof(buf), f)) line += buf;
+    if (!header) {
+      std::string fmt;
+      header = json_string(line, "format", &fmt) && fmt == kTuneFormat;
+      if (!header) {
+        bad = true;
+        break;
+      }
+      continue;
+    }
+    if (line.find("\"key\"") == std::string::npos) continue;
+    std::string key, oz;
+    Tuned t;
+    if (!json_string(line, "key", &key) || !json_int(line, "tile", &t.cfg.tile) ||
+        !json_int(line, "order", &t.cfg.order) || !json_int(line, "grid", &t.cfg.grid) ||
+        !json_string(line, "ozaki", &oz) || (t.cfg.tile != 64 && t.cfg.tile != 128) ||
+        t.cfg.grid < 0 || t.cfg.order < 0) {
+      bad = true;
+      break;
+    }
+    for (char c : oz) {
+      if (c != '0' && c != '1') bad = true;
+      t.oz.push_back(c == '1' ? 1 : 0);
+    }
+    if (bad) break;
+    got.emplace_back(key, t);
+  }
+  fclose(f);
+  if (bad || !header)
+    return fail(SKGEMM_ERR_INVALID_ARG, std::string("tune cache: not a skgemm tuning file: ") + path);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (auto& e : got) g_tune_cache[e.first] = e.second;
+  return (int)got.size();
+}
+
+SKG_EXPORT int skgemm_tune_cache_clear(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache.clear();
+  return SKGEMM_OK;
 }

@@ -92,6 +92,9 @@ DeviceState* current_device(int* status) {
       return nullptr;
     }
     dev->num_sms = prop.multiProcessorCount;
+    snprintf(dev->name, sizeof(dev->name), "%s", prop.name);
+    for (char* c = dev->name; *c; ++c)
+      if (*c == '"' || *c == '\\' || *c == '|') *c = '_';  // safe inside a JSON string and a key
     dev->cc_major = prop.major;
     dev->cc_minor = prop.minor;
     dev->device = d;

@@ -60,6 +60,7 @@ struct DeviceState {
   int device = -1;
   int num_sms = 0;
   int cc_major = 0, cc_minor = 0;
+  char name[96] = {0};  // the device's product name (keys of persisted tuning)
   std::mutex mu;
   std::map<cudaStream_t, StreamWorkspace*> ws;
   // Staging buffers of the blocking host-pointer entry points (guarded by

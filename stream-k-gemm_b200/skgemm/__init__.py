@@ -166,6 +166,9 @@ _SIGS = {
     "skgemm_serve_simulate": [ctypes.POINTER(ServeRequest), ctypes.c_int,
                               ctypes.POINTER(ServeOptions)],
     "skgemm_stream_release": [_vp],
+    "skgemm_tune_cache_save": [ctypes.c_char_p],
+    "skgemm_tune_cache_load": [ctypes.c_char_p],
+    "skgemm_tune_cache_clear": [],
     "skgemm_batch_schedule": [ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.c_int,
                               ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                               ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)],
@@ -644,6 +647,23 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def tune_cache_save(path) -> int:
+    """Write this process's tuned plan choices to `path` (JSON); returns the
+    entry count."""
+    n = lib().skgemm_tune_cache_save(os.fsencode(path))
+    return _check(n) if n < 0 else n
+
+
+def tune_cache_load(path) -> int:
+    """Load tuned plan choices from `path`; returns the entry count."""
+    n = lib().skgemm_tune_cache_load(os.fsencode(path))
+    return _check(n) if n < 0 else n
+
+
+def tune_cache_clear() -> None:
+    _check(lib().skgemm_tune_cache_clear())
 
 
 def batch_dev(items, stream=None) -> None:

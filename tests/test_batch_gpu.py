@@ -9,6 +9,11 @@ graph reads the current contents of the inputs; repeated runs bitwise equal;
 autotuning leaves SYRK outputs with beta != 0 as they were. Plans that run
 problems through the Ozaki split (precision Ozaki or auto) meet the same
 gates."""
+import json
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 import torch
@@ -164,6 +169,56 @@ def test_plan_autotune_keeps_syrk_beta_outputs(cuda):
     plan2 = skgemm.Plan([it.item() for it in items])
     assert plan2.config["candidates_timed"] == 0
     assert plan2.config["tile"] == cfg["tile"] and plan2.config["order"] == cfg["order"]
+
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_plan_tuning_persists_across_processes(cuda, tmp_path):
+    """A plan tuned in one process and saved (skgemm_tune_cache_save) is
+    reused by a plan over the same shapes in another process after
+    skgemm_tune_cache_load: no candidate is timed, the same configuration is
+    chosen and the results meet the oracle. An entry that this plan's tuning
+    could not have produced (Ozaki flags on a native plan) is ignored."""
+    path = str(tmp_path / "tune.json")
+    code = (f"import sys, json; sys.path[:0] = [{REPO!r}, "
+            f"{os.path.join(REPO, 'stream-k-gemm_b200')!r}]\n"
+            "import skgemm\n"
+            "from tests.test_batch_gpu import mixed_batch\n"
+            "items = mixed_batch(21)\n"
+            "plan = skgemm.Plan([it.item() for it in items])\n"
+            f"n = skgemm.tune_cache_save({path!r})\n"
+            "print(json.dumps(dict(plan.config, saved=n)))\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    first = json.loads(r.stdout.strip().splitlines()[-1])
+    assert first["candidates_timed"] == 4 and first["saved"] >= 1
+
+    skgemm.tune_cache_clear()
+    assert skgemm.tune_cache_load(path) == first["saved"]
+    items = mixed_batch(21)
+    plan = skgemm.Plan([it.item() for it in items])
+    cfg = plan.config
+    assert cfg["candidates_timed"] == 0
+    assert (cfg["tile"], cfg["order"]) == (first["tile"], first["order"])
+    plan.run()
+    plan.status()
+    for it in items:
+        it.check()
+    plan.close()
+
+    doc = json.load(open(path))
+    for e in doc["entries"]:
+        e["ozaki"] = "1" * len(e["ozaki"])
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"format": "%s", "entries": [\n' % doc["format"] +
+                   ",\n".join(json.dumps(e) for e in doc["entries"]) + "\n]}\n")
+    skgemm.tune_cache_clear()
+    assert skgemm.tune_cache_load(bad) == len(doc["entries"])
+    plan = skgemm.Plan([it.item() for it in mixed_batch(21)])
+    assert plan.config["candidates_timed"] == 4 and plan.config["ozaki_problems"] == 0
+    plan.close()
+    skgemm.tune_cache_clear()
 
 
 def test_plan_graph_replay_reads_current_inputs_and_is_deterministic(cuda):
