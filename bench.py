@@ -483,6 +483,7 @@ def kernel_rooflines(skgemm, step, torch, steps, peaks, band, grid, q, S, Pn):
         Ls, Lr = opts["syrk"].slices_used_out, opts["rot"].slices_used_out
         rb = 2 if step.prec == skgemm.PREC_OZAKI_BF16 else 1
         work = {"i8_gemm_kernel": (Ls * FLOP_SYRK, "TOP/s", i8_peak, "tensor"),
+                "i8_gemm2_kernel": (Ls * FLOP_SYRK, "TOP/s", i8_peak, "tensor"),
                 "i8_rot_kernel": (Lr * FLOP_ROT, "TOP/s", i8_peak, "tensor"),
                 "convert_tma_kernel": (E * (16 + rb * (Ls + Lr)), "GB/s", hbm, "hbm"),
                 "norm_partials_kernel": (2 * E * 8, "GB/s", hbm, "hbm"),
@@ -708,7 +709,8 @@ def run_op(args):
     """One standalone call per step (the reference's one-call-at-a-time use)
     on the subspace shapes: SYRK S = Psi^T Psi, GEMM Hs = Psi^T H Psi, the
     rotation Psi Q, or the S + Hs pair; for profiling a single op and timing
-    it alone. Prints {"op", "precision", "ms", "tflops"}."""
+    it alone. Prints {"op", "precision", "ms", "tflops"}, one line per
+    precision (two with --precision both)."""
     import torch
     import skgemm
     dev = torch.device("cuda", 0)
@@ -717,23 +719,24 @@ def run_op(args):
     S = torch.zeros(NB * NB, dtype=torch.float64, device=dev)
     Hs = torch.zeros_like(S)
     Pn = torch.empty_like(band)
-    name = "native" if args.precision == "both" else args.precision
-    p = _prec(skgemm, name)
     s = torch.cuda.current_stream()
-    calls = {
-        "syrk": (lambda: skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, stream=s, precision=p),
-                 FLOP_SYRK),
-        "gemm": (lambda: skgemm.dgemm_packed_dev(NB, NB, ND, band, h32, Hs, NB, stream=s,
-                                                 precision=p), FLOP_GEMM),
-        "rotation": (lambda: skgemm.drot_dev(ND, NB, grid, q, Pn, stream=s, precision=p),
-                     FLOP_ROT),
-        "pair": (lambda: skgemm.dsubspace_packed_dev(ND, NB, band, h32, S, Hs, stream=s,
-                                                     precision=p), FLOP_SYRK + FLOP_GEMM)}
-    fn, flop = calls[args.op]
-    ms = time_calls(fn, s, torch, reps=max(1, args.steps), warm=max(0, args.warmup))
-    skgemm.stream_status(s)
-    print(json.dumps({"workload": f"op_{args.op}_{WORKLOAD}", "op": args.op, "precision": name,
-                      "ms": round(ms, 4), "tflops": round(flop / ms / 1e9, 3)}), flush=True)
+    for name in (["native", "ozaki"] if args.precision == "both" else [args.precision]):
+        p = _prec(skgemm, name)
+        calls = {
+            "syrk": (lambda: skgemm.dsyrk_packed_dev(ND, NB, band, S, NB, stream=s, precision=p),
+                     FLOP_SYRK),
+            "gemm": (lambda: skgemm.dgemm_packed_dev(NB, NB, ND, band, h32, Hs, NB, stream=s,
+                                                     precision=p), FLOP_GEMM),
+            "rotation": (lambda: skgemm.drot_dev(ND, NB, grid, q, Pn, stream=s, precision=p),
+                         FLOP_ROT),
+            "pair": (lambda: skgemm.dsubspace_packed_dev(ND, NB, band, h32, S, Hs, stream=s,
+                                                         precision=p), FLOP_SYRK + FLOP_GEMM)}
+        fn, flop = calls[args.op]
+        ms = time_calls(fn, s, torch, reps=max(1, args.steps), warm=max(0, args.warmup))
+        skgemm.stream_status(s)
+        print(json.dumps({"workload": f"op_{args.op}_{WORKLOAD}", "op": args.op,
+                          "precision": name, "ms": round(ms, 4),
+                          "tflops": round(flop / ms / 1e9, 3)}), flush=True)
 
 
 # ------------------------------------------------------------ kernel tour
