@@ -77,7 +77,8 @@ def parse():
     ap.add_argument("--nd", type=int, default=ND,
                     help="grid points (default 110592 = 48^3; smaller values for profiling)")
     ap.add_argument("--nb", type=int, default=NB, help="states (default 512)")
-    ap.add_argument("--op", default="syrk", choices=["syrk", "gemm", "rotation", "pair"],
+    ap.add_argument("--op", default="syrk",
+                    choices=["syrk", "gemm", "rotation", "pair", "stencil", "halo"],
                     help="--workload op: which call (one per step, standalone)")
     ap.add_argument("--workload", default="subspace",
                     choices=["subspace", "batched", "serving", "tour", "op"],
@@ -720,6 +721,33 @@ def run_op(args):
     Hs = torch.zeros_like(S)
     Pn = torch.empty_like(band)
     s = torch.cuda.current_stream()
+    if args.op in ("stencil", "halo"):
+        # The H Psi producer on the same Psi (48^3 = 110592 grid points, 512
+        # bands): the periodic halo (band-packed Psi -> extended) or the
+        # 6th-order stencil (extended -> 32-band-packed H Psi), alone.
+        n = 48
+        ext = torch.empty((NB + 15) // 16 * (n + 12) ** 3 * 16, dtype=torch.float64, device=dev)
+        a_diag = torch.rand(ND, dtype=torch.float64, device=dev)
+        cx = [0.0, -1.0 / 12, 2.0 / 3, -2.5, 8.0 / 3, -1.0 / 4, 1.0 / 30]
+        hpsi = torch.empty_like(band)
+        skgemm.halo_periodic_dev(n, n, n, NB, band, ext, stream=s)
+        if args.op == "halo":
+            fn = lambda: skgemm.halo_periodic_dev(n, n, n, NB, band, ext, stream=s)
+            nbytes = band.numel() * 8 + ext.numel() * 8
+        else:
+            fn = lambda: skgemm.stencil_ext_dev(n, n, n, NB, ext, a_diag, cx, cx, cx, -0.5, hpsi,
+                                                32, stream=s)
+            nbytes = ext.numel() * 8 + a_diag.numel() * 8 + hpsi.numel() * 8
+        ms = time_calls(fn, s, torch, reps=max(1, args.steps), warm=max(0, args.warmup))
+        skgemm.stream_status(s)
+        hbm, src = measured_peaks()
+        gbs = nbytes / ms / 1e6
+        print(json.dumps({"workload": f"op_{args.op}_hpsi_48cubed_x{NB}", "op": args.op,
+                          "precision": "f64", "ms": round(ms, 4),
+                          "algorithmic_bytes": int(nbytes), "gbs": round(gbs, 1),
+                          "frac_of_hbm": round(gbs / hbm, 4), "hbm_peak_source": src}),
+              flush=True)
+        return
     for name in (["native", "ozaki"] if args.precision == "both" else [args.precision]):
         p = _prec(skgemm, name)
         calls = {
@@ -753,7 +781,7 @@ def run_tour(args=None) -> None:
       fp64_streamk_kernel64_ak,          the rotation on band-packed Psi, 110592 x 512,
       norm_partials / convert_tma (KM)   native and Ozaki (K-major operand reads)
       halo_periodic_kernel,              H Psi on the 48^3 grid (= 110592 points) x 512:
-      stencil_ext_kernel<32>             periodic halo, then the 6th-order stencil
+      stencil_staged_kernel<32>          periodic halo, then the 6th-order stencil
       nloc_forward / nloc_chi_c /        the nonlocal projector on the same Psi: 64 atoms
       nloc_backward<32>                  x 2 periodic images, 800 rows x 16 columns each
       k0_kernel                          GEMM with K = 0 (D = gamma), 4096 x 4096, through

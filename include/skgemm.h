@@ -321,7 +321,9 @@ int skgemm_grid_to_band_dev(int64_t Nd, int64_t nb, const double* src_grid,
  * coef_x/y/z: host arrays of FDn + 1 doubles (entry 0 unused); out:
  * [ceil(nb/T)][ni*nj*nk][T], T = out_tile, lanes b >= nb left untouched.
  * FDn must be 6 (the reference's kernels); other radii return
- * SKGEMM_ERR_UNSUPPORTED. */
+ * SKGEMM_ERR_UNSUPPORTED. psi_ext16, A_diag and out must be 16-byte aligned
+ * (the arrays are read by TMA), and ni*nj*nk < 2^31. Asynchronous on `stream`;
+ * a device-side wait that ran out is reported by skgemm_stream_status. */
 int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                            const double* psi_ext16, const double* A_diag,
                            const double* coef_x, const double* coef_y, const double* coef_z,

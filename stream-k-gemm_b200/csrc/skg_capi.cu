@@ -1165,9 +1165,11 @@ SKG_EXPORT int skgemm_stencil_ext_dev(int64_t ni, int64_t nj, int64_t nk, int64_
   int st;
   DeviceState* dev = current_device(&st);
   if (!dev) return st;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  StreamWorkspace* ws = stream_workspace(dev, s, 1, &st);
+  if (!ws) return st;
   return launch_stencil_ext(ni, nj, nk, nb, FDn, psi_ext16, A_diag, coef_x, coef_y, coef_z,
-                            coef_0, out, out_tile, dev->num_sms,
-                            reinterpret_cast<cudaStream_t>(stream));
+                            coef_0, out, out_tile, dev->num_sms, ws->err, s);
 }
 
 SKG_EXPORT int skgemm_halo_periodic_dev(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,

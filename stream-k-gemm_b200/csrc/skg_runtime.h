@@ -152,7 +152,7 @@ int launch_unpack(int64_t R, int64_t K, const double* Xp, int T, double* X, int6
 int launch_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                        const double* ext, const double* A, const double* cx, const double* cy,
                        const double* cz, double c0, double* out, int out_tile, int num_sms,
-                       cudaStream_t s);
+                       uint32_t* err, cudaStream_t s);
 int launch_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                          const double* local, double* ext, cudaStream_t s);
 // Nonlocal projector set on the device (skg_nloc.cu).

@@ -30,71 +30,203 @@ struct StencilCoef {
   double c0;
 };
 
-// Thread = (two band lanes 2h, 2h + 1, read as one 16-byte load; one (i, j)
-// column): 8 lane pairs x 8 i x 4 j per 256-thread CTA. It marches k through
-// [k0, k1) keeping the column's planes k - 6 .. k + 6 in a 13-slot register
-// queue (slot of plane k + d at step u of a 13-step period: (u + d + 6) mod
-// 13), so a step loads one new plane and the 24 x and y neighbours: 25 loads
-// per output pair instead of 74, and the CTA's own rows serve most y
-// neighbours from L1 (8 x 4 columns: 5.5 rows of the plane per output row
-// come from L2). Measured alternatives: one lane per thread on 4 x 4 columns
-// 0.73 ms, two i per thread on 16 x 2 columns 0.95 ms, against 0.66 ms here
-// (48^3 points x 512 bands).
+// CTA = one 4-band slab (bands 4 q ..
+// 4 q + 3: one 32-byte sector per point) of a 16 x 16 column tile, marching
+// k through [k0, k1). A producer warp streams, by TMA, one stage per k step
+// into a ring of kStRing shared-memory stages, kStRing - 1 steps ahead:
+//   the tile's plane k with its x / y halo, 28 x 28 points x 4 bands;
+//   the tile's 16 x 16 points of plane k + 6 (the z queue's new entry);
+//   A[g] of the tile's 16 x 16 points of plane k: one 2-D box when ni is
+//   even (A viewed as [nj nk][ni]: 16-byte row strides), else one 18-double
+//   box per row from an even index, in a 256-byte slot.
+// Consumer thread = two columns (i, j) and (i, j + 1) and a band pair: a
+// quarter-warp reads 4 consecutive points (128 contiguous bytes); the 14
+// staged values j - 6 .. j + 7 serve the y neighbours of both columns; the
+// 12 z neighbours come from the columns' 13-slot register queues (slot of
+// plane k + d at step u of a 13-step period: (u + d + 6) mod 13). No global
+// load waits inside the k loop. Same arithmetic in the same order as the
+// reference kernels: the output equals theirs bit for bit. Every wait is
+// bounded; on expiry the CTA records the error and skips the remaining waits.
+constexpr int kStI = 16;                 // columns per CTA along x
+constexpr int kStJ = 16;                 // columns per CTA along y
+constexpr int kSlab = 4;                 // bands per CTA
+constexpr int kStHI = kStI + 2 * kFDn;   // staged points along x
+constexpr int kStHJ = kStJ + 2 * kFDn;   // staged points along y
+constexpr int kStARow = 18;              // doubles per A box (from an even index)
+constexpr int kStAPitch = 32;            // doubles between staged A rows (TMA
+                                         // destinations are 128-byte aligned)
+constexpr int kStPlane = kStHI * kStHJ * kSlab;  // doubles: halo plane
+constexpr int kStCenter = kStI * kStJ * kSlab;   // doubles: plane k + 6
+constexpr int kStStage = kStPlane + kStCenter + kStJ * kStAPitch;  // doubles per stage
+constexpr int kStRing = 4;
+constexpr int kStConsumerWarps = kStJ / 2;
+constexpr int kStThreads = (kStConsumerWarps + 1) * 32;
+constexpr int kStTxBytes2d = (kStPlane + kStCenter + kStJ * kStI) * 8;
+constexpr int kStTxBytesRows = (kStPlane + kStCenter + kStJ * kStARow) * 8;
+constexpr int kStSmem = kStRing * kStStage * 8 + 2 * kStRing * 8 + 16 + 128;
+static_assert((kStPlane * 8) % 128 == 0 && (kStCenter * 8) % 128 == 0, "stage alignment");
+static_assert((kStStage * 8) % 128 == 0 && (kStAPitch * 8) % 128 == 0, "stage alignment");
+static_assert((kStARow * 8) % 16 == 0 && kStARow <= kStAPitch, "A box");
+static_assert(kStSmem <= 232448, "stencil stages exceed 227 KB of shared memory");
+
 template <int OT>
-__global__ void __launch_bounds__(256, 2) stencil_ext_kernel(
-    int ni, int nj, int nk, int nb, int kc, const double* __restrict__ ext,
-    const double* __restrict__ A, const __grid_constant__ StencilCoef cf,
-    double* __restrict__ out) {
-  const int h = threadIdx.x & 7;
-  const int it = (threadIdx.x >> 3) & 7;
-  const int jt = threadIdx.x >> 6;
-  const int itiles = (ni + 7) / 8;
-  const int i = (blockIdx.x % itiles) * 8 + it;
-  const int j = (blockIdx.x / itiles) * 4 + jt;
-  const int t = blockIdx.y;
-  const int b = t * 16 + 2 * h;
+__global__ void __launch_bounds__(kStThreads, 1) stencil_staged_kernel(
+    const __grid_constant__ CUtensorMap mapP, const __grid_constant__ CUtensorMap mapC,
+    const __grid_constant__ CUtensorMap mapA, bool a2d, int ni, int nj, int nk, int nb, int kc,
+    const double* __restrict__ ext, const __grid_constant__ StencilCoef cf,
+    double* __restrict__ out, uint32_t* __restrict__ err) {
+  extern __shared__ uint8_t sraw[];
+  double* stages =
+      reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sraw) + 127) & ~uintptr_t(127));
+  uint64_t* full = reinterpret_cast<uint64_t*>(stages + kStRing * kStStage);
+  uint64_t* empty = full + kStRing;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + kStRing);
+  const int itiles = (ni + kStI - 1) / kStI;
+  const int i0 = (int)(blockIdx.x % itiles) * kStI, j0 = (int)(blockIdx.x / itiles) * kStJ;
+  const int q = blockIdx.y;  // slab: bands 4 q .. 4 q + 3
+  const int t = q / (16 / kSlab), sl = q % (16 / kSlab);
   const int k0 = blockIdx.z * kc;
   const int k1 = min(nk, k0 + kc);
-  if (i >= ni || j >= nj || b >= nb) return;
+  if (q * kSlab >= nb || k0 >= k1) return;
+  const int nsteps = k1 - k0;
   const int64_t nix = ni + 2 * kFDn, njx = nj + 2 * kFDn, nkx = nk + 2 * kFDn;
-  const int64_t sj = nix * 8, sk = nix * njx * 8;  // y / z strides in lane pairs
-  const int64_t K = (int64_t)ni * nj * nk;
-  // Lane pair h of extended point (i, j, k): base + (k + F) * sk.
-  const double2* base = reinterpret_cast<const double2*>(ext) +
-                        ((int64_t)t * nix * njx * nkx + (i + kFDn) + (int64_t)(j + kFDn) * nix) * 8 +
-                        h;
-  double2 zq[kZq];
+  const int64_t plane_pts = (int64_t)ni * nj;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kStRing; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], kStConsumerWarps);
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == kStConsumerWarps) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      tma_prefetch_desc(&mapP);
+      tma_prefetch_desc(&mapC);
+      tma_prefetch_desc(&mapA);
+      int issued = 0;
+      for (int u = 0; u < nsteps; ++u) {
+        const int b = u % kStRing;
+        if (u >= kStRing) {
+          if (*abort_flag || !mbar_wait(&empty[b], ((u / kStRing) - 1) & 1, err)) {
+            *abort_flag = 1;
+            break;
+          }
+        }
+        const int k = k0 + u;
+        double* st = stages + b * kStStage;
+        mbar_arrive_expect_tx(&full[b], a2d ? kStTxBytes2d : kStTxBytesRows);
+        tma_load_4d(st, &mapP, &full[b], sl * kSlab, i0, j0, (int)(t * nkx + k + kFDn));
+        tma_load_4d(st + kStPlane, &mapC, &full[b], sl * kSlab, i0 + kFDn, j0 + kFDn,
+                    (int)(t * nkx + k + 2 * kFDn));
+        if (a2d) {
+          tma_load_2d(st + kStPlane + kStCenter, &mapA, &full[b], i0, j0 + k * nj);
+        } else {
+          for (int jj = 0; jj < kStJ; ++jj) {
+            const int64_t g = (int64_t)i0 + (int64_t)(j0 + jj) * ni + (int64_t)k * plane_pts;
+            tma_load_1d(st + kStPlane + kStCenter + jj * kStAPitch, &mapA, &full[b],
+                        (int)(g & ~1LL));
+          }
+        }
+        ++issued;
+      }
+      // The CTA leaves only after its last loads have landed (immediate on
+      // the normal path: the consumers waited for every one of them).
+      for (int u = issued - 1; u >= 0 && u >= issued - kStRing; --u)
+        mbar_wait(&full[u % kStRing], (u / kStRing) & 1, err);
+    }
+    return;
+  }
+
+  // -------------------------------------------------------------- consumers
+  const int bp = lane & 1;
+  const int il = lane >> 1;
+  const int jA = 2 * warp;  // tile rows jA, jA + 1
+  const int i = i0 + il, j = j0 + jA;
+  const int b = q * kSlab + 2 * bp;
+  const bool actA = i < ni && j < nj && b < nb;
+  const bool actB = i < ni && j + 1 < nj && b < nb;
+  const int64_t sk = nix * njx * 8;  // z stride in lane pairs
+  const int64_t K = plane_pts * nk;
+  const double2* baseA =
+      reinterpret_cast<const double2*>(ext) +
+      ((int64_t)t * nix * njx * nkx + (i + kFDn) + (int64_t)(j + kFDn) * nix) * 8 + sl * 2 + bp;
+  const double2* baseB = baseA + nix * 8;
+  double2 zqA[kZq], zqB[kZq];
 #pragma unroll
-  for (int d = -kFDn; d < kFDn; ++d)  // prologue: planes k0 - 6 .. k0 + 5
-    zq[d + kFDn] = __ldg(base + (int64_t)(k0 + d + kFDn) * sk);
+  for (int d = -kFDn; d < kFDn; ++d) {  // prologue: planes k0 - 6 .. k0 + 5
+    zqA[d + kFDn] = actA ? __ldg(baseA + (int64_t)(k0 + d + kFDn) * sk) : make_double2(0.0, 0.0);
+    zqB[d + kFDn] = actB ? __ldg(baseB + (int64_t)(k0 + d + kFDn) * sk) : make_double2(0.0, 0.0);
+  }
+  // Lane pair (il, row) offsets in a stage, in double2 units.
+  const int pA = ((jA + kFDn) * kStHI + il + kFDn) * 2 + bp;  // halo plane, row jA
+  const int yA = (jA * kStHI + il + kFDn) * 2 + bp;            // halo plane, row jA - 6
+  const int cA = ((jA * kStI) + il) * 2 + bp;                   // center box, row jA
   for (int kb = k0; kb < k1; kb += kZq) {
 #pragma unroll
     for (int u = 0; u < kZq; ++u) {
       const int k = kb + u;
       if (k >= k1) break;
-      const double2* pk = base + (int64_t)(k + kFDn) * sk;
-      zq[(u + 2 * kFDn) % kZq] = __ldg(pk + kFDn * sk);
-      const int64_t g = (int64_t)i + (int64_t)j * ni + (int64_t)k * ni * nj;
-      const double a = __ldg(A + g) + cf.c0;
-      const double2 c = zq[(u + kFDn) % kZq];
-      double r0 = c.x * a, r1 = c.y * a;
+      const int step = k - k0, buf = step % kStRing;
+      if (!*abort_flag && !mbar_wait(&full[buf], (step / kStRing) & 1, err)) *abort_flag = 1;
+      const double* st = stages + buf * kStStage;
+      const double2* P = reinterpret_cast<const double2*>(st);
+      const double2* C = reinterpret_cast<const double2*>(st + kStPlane);
+      const double* As = st + kStPlane + kStCenter;
+      zqA[(u + 2 * kFDn) % kZq] = C[cA];
+      zqB[(u + 2 * kFDn) % kZq] = C[cA + kStI * 2];
+      if (actA) {
+        const int64_t g = (int64_t)i + (int64_t)j * ni + (int64_t)k * plane_pts;
+        const int64_t gr = g - il;  // row start
+        const int64_t grB = gr + ni;
+        const double aA = (a2d ? As[jA * kStI + il] : As[jA * kStAPitch + (int)(gr & 1) + il]) +
+                          cf.c0;
+        const double aB = (a2d ? As[(jA + 1) * kStI + il]
+                               : As[(jA + 1) * kStAPitch + (int)(grB & 1) + il]) + cf.c0;
+        double2 Y[2 * kFDn + 2];  // rows jA - 6 .. jA + 7
 #pragma unroll
-      for (int r = 1; r <= kFDn; ++r) {
-        const double2 xp = __ldg(pk + r * 8), xm = __ldg(pk - r * 8);
-        r0 = fma(xp.x + xm.x, cf.cx[r], r0);
-        r1 = fma(xp.y + xm.y, cf.cx[r], r1);
-        const double2 yp = __ldg(pk + r * sj), ym = __ldg(pk - r * sj);
-        r0 = fma(yp.x + ym.x, cf.cy[r], r0);
-        r1 = fma(yp.y + ym.y, cf.cy[r], r1);
-        const double2 zp = zq[(u + kFDn + r) % kZq], zm = zq[(u + kFDn - r + kZq) % kZq];
-        r0 = fma(zp.x + zm.x, cf.cz[r], r0);
-        r1 = fma(zp.y + zm.y, cf.cz[r], r1);
+        for (int d = 0; d < 2 * kFDn + 2; ++d) Y[d] = P[yA + d * kStHI * 2];
+        const double2 ca = zqA[(u + kFDn) % kZq], cb = zqB[(u + kFDn) % kZq];
+        double a0 = ca.x * aA, a1 = ca.y * aA;
+        double b0 = cb.x * aB, b1 = cb.y * aB;
+#pragma unroll
+        for (int r = 1; r <= kFDn; ++r) {
+          const double2 xpA = P[pA + 2 * r], xmA = P[pA - 2 * r];
+          const double2 xpB = P[pA + 2 * kStHI + 2 * r], xmB = P[pA + 2 * kStHI - 2 * r];
+          a0 = fma(xpA.x + xmA.x, cf.cx[r], a0);
+          a1 = fma(xpA.y + xmA.y, cf.cx[r], a1);
+          b0 = fma(xpB.x + xmB.x, cf.cx[r], b0);
+          b1 = fma(xpB.y + xmB.y, cf.cx[r], b1);
+          a0 = fma(Y[kFDn + r].x + Y[kFDn - r].x, cf.cy[r], a0);
+          a1 = fma(Y[kFDn + r].y + Y[kFDn - r].y, cf.cy[r], a1);
+          b0 = fma(Y[kFDn + 1 + r].x + Y[kFDn + 1 - r].x, cf.cy[r], b0);
+          b1 = fma(Y[kFDn + 1 + r].y + Y[kFDn + 1 - r].y, cf.cy[r], b1);
+          const double2 zpA = zqA[(u + kFDn + r) % kZq], zmA = zqA[(u + kFDn - r + kZq) % kZq];
+          const double2 zpB = zqB[(u + kFDn + r) % kZq], zmB = zqB[(u + kFDn - r + kZq) % kZq];
+          a0 = fma(zpA.x + zmA.x, cf.cz[r], a0);
+          a1 = fma(zpA.y + zmA.y, cf.cz[r], a1);
+          b0 = fma(zpB.x + zmB.x, cf.cz[r], b0);
+          b1 = fma(zpB.y + zmB.y, cf.cz[r], b1);
+        }
+        double* o = out + ((int64_t)(b / OT) * K + g) * OT + b % OT;
+        if (b + 1 < nb)
+          *reinterpret_cast<double2*>(o) = make_double2(a0, a1);
+        else
+          o[0] = a0;  // lane b + 1 is padding: left untouched
+        if (actB) {
+          double* o2 = o + (int64_t)ni * OT;
+          if (b + 1 < nb)
+            *reinterpret_cast<double2*>(o2) = make_double2(b0, b1);
+          else
+            o2[0] = b0;
+        }
       }
-      double* o = out + ((int64_t)(b / OT) * K + g) * OT + b % OT;
-      if (b + 1 < nb)
-        *reinterpret_cast<double2*>(o) = make_double2(r0, r1);
-      else
-        o[0] = r0;  // lane b + 1 is padding: left untouched
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[buf]);
     }
   }
 }
@@ -124,10 +256,31 @@ __global__ void __launch_bounds__(256) halo_periodic_kernel(int ni, int nj, int 
 
 }  // namespace
 
+namespace {
+
+template <int OT>
+int launch_staged(const CUtensorMap& mapP, const CUtensorMap& mapC, const CUtensorMap& mapA,
+                  bool a2d, int ni, int nj, int nk, int nb, int kc, dim3 grid, const double* ext,
+                  const StencilCoef& cf, double* out, uint32_t* err, cudaStream_t s) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    SKG_CUDA(cudaFuncSetAttribute(stencil_staged_kernel<OT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kStSmem));
+    attr_set = true;
+  }
+  KernelTimer kt_(s, "stencil_staged_kernel");
+  stencil_staged_kernel<OT><<<grid, kStThreads, kStSmem, s>>>(mapP, mapC, mapA, a2d, ni, nj, nk,
+                                                              nb, kc, ext, cf, out, err);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
+}  // namespace
+
 int launch_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
                        const double* ext, const double* A, const double* cx, const double* cy,
                        const double* cz, double c0, double* out, int out_tile, int num_sms,
-                       cudaStream_t s) {
+                       uint32_t* err, cudaStream_t s) {
   if (ni < 0 || nj < 0 || nk < 0 || nb < 0) return fail(SKGEMM_ERR_INVALID_ARG, "negative extent");
   if (FDn != kFDn)
     return fail(SKGEMM_ERR_UNSUPPORTED, "stencil radius FDn must be 6 (the reference's kernels)");
@@ -145,23 +298,48 @@ int launch_stencil_ext(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
   cf.c0 = c0;
   if ((reinterpret_cast<uintptr_t>(ext) | reinterpret_cast<uintptr_t>(out)) & 15)
     return fail(SKGEMM_ERR_INVALID_ARG, "stencil arrays must be 16-byte aligned");
-  const int64_t cols = ((ni + 7) / 8) * ((nj + 3) / 4);
+  if ((reinterpret_cast<uintptr_t>(A) & 15) != 0)
+    return fail(SKGEMM_ERR_INVALID_ARG, "stencil A_diag must be 16-byte aligned");
+  const int64_t cols = ((ni + kStI - 1) / kStI) * ((nj + kStJ - 1) / kStJ);
   const int64_t tiles = (nb + 15) / 16;
-  if (cols > INT32_MAX || tiles > 65535) return fail(SKGEMM_ERR_INVALID_ARG, "grid too large");
-  // Split k only when the columns alone give fewer than two waves of CTAs
-  // (2 per SM); each chunk reloads 12 planes per column.
+  const int64_t slabs = tiles * (16 / kSlab);
+  if (cols > INT32_MAX || slabs > 65535) return fail(SKGEMM_ERR_INVALID_ARG, "grid too large");
+  const int64_t nix = ni + 2 * kFDn, njx = nj + 2 * kFDn, nkx = nk + 2 * kFDn;
+  if (tiles * nkx > INT32_MAX || ni * nj * nk + 2 >= INT32_MAX)
+    return fail(SKGEMM_ERR_INVALID_ARG, "grid too large");
+  // Extended Psi as a 4-D tensor [tiles * nkx][njx][nix][16 lanes]: boxes of
+  // 4 lanes x 28 x 28 points (halo planes) and 4 lanes x 16 x 16 points (z
+  // entries); A as a 1-D tensor, boxes of 18 doubles. Zero fill outside.
+  CUtensorMap mapP, mapC, mapA;
+  const uint64_t dims[4] = {16, (uint64_t)nix, (uint64_t)njx, (uint64_t)(tiles * nkx)};
+  const uint64_t strides[3] = {16 * 8, (uint64_t)nix * 16 * 8, (uint64_t)(nix * njx) * 16 * 8};
+  const uint32_t boxP[4] = {(uint32_t)kSlab, (uint32_t)kStHI, (uint32_t)kStHJ, 1};
+  const uint32_t boxC[4] = {(uint32_t)kSlab, (uint32_t)kStI, (uint32_t)kStJ, 1};
+  // A: [nj nk][ni] with 16 x 16 boxes when its rows are 16-byte strided,
+  // else 1-D with 18-double boxes.
+  const bool a2d = ni % 2 == 0;
+  const uint64_t dimsA[2] = {a2d ? (uint64_t)ni : (uint64_t)(ni * nj * nk), (uint64_t)(nj * nk)};
+  const uint64_t stridesA[1] = {(uint64_t)ni * 8};
+  const uint32_t boxA[2] = {a2d ? (uint32_t)kStI : (uint32_t)kStARow, (uint32_t)kStJ};
+  int st;
+  if ((st = encode_tiled(&mapP, 4, ext, dims, strides, boxP, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         CU_TENSOR_MAP_SWIZZLE_NONE)) ||
+      (st = encode_tiled(&mapC, 4, ext, dims, strides, boxC, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         CU_TENSOR_MAP_SWIZZLE_NONE)) ||
+      (st = encode_tiled(&mapA, a2d ? 2 : 1, A, dimsA, stridesA, boxA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         CU_TENSOR_MAP_SWIZZLE_NONE)))
+    return st;
+  // Split k only when the column tiles and slabs alone give fewer than four
+  // CTAs per SM; each chunk reloads 12 planes per column.
   int64_t chunks = 1;
-  while (cols * tiles * chunks < 4LL * num_sms && nk / (chunks * 2) >= 16) chunks *= 2;
+  while (cols * slabs * chunks < 4LL * num_sms && nk / (chunks * 2) >= 16) chunks *= 2;
   const int kc = (int)((nk + chunks - 1) / chunks);
-  dim3 grid((unsigned)cols, (unsigned)tiles, (unsigned)((nk + kc - 1) / kc));
+  const dim3 grid((unsigned)cols, (unsigned)slabs, (unsigned)((nk + kc - 1) / kc));
   if (out_tile == 32)
-    stencil_ext_kernel<32><<<grid, 256, 0, s>>>((int)ni, (int)nj, (int)nk, (int)nb, kc, ext, A, cf,
-                                                out);
-  else
-    stencil_ext_kernel<16><<<grid, 256, 0, s>>>((int)ni, (int)nj, (int)nk, (int)nb, kc, ext, A, cf,
-                                                out);
-  SKG_CUDA(cudaGetLastError());
-  return SKGEMM_OK;
+    return launch_staged<32>(mapP, mapC, mapA, a2d, (int)ni, (int)nj, (int)nk, (int)nb, kc, grid, ext,
+                             cf, out, err, s);
+  return launch_staged<16>(mapP, mapC, mapA, a2d, (int)ni, (int)nj, (int)nk, (int)nb, kc, grid, ext,
+                           cf, out, err, s);
 }
 
 int launch_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn,
