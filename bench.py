@@ -78,7 +78,7 @@ def parse():
                     help="grid points (default 110592 = 48^3; smaller values for profiling)")
     ap.add_argument("--nb", type=int, default=NB, help="states (default 512)")
     ap.add_argument("--op", default="syrk",
-                    choices=["syrk", "gemm", "rotation", "pair", "stencil", "halo"],
+                    choices=["syrk", "gemm", "rotation", "pair", "stencil", "halo", "nloc"],
                     help="--workload op: which call (one per step, standalone)")
     ap.add_argument("--workload", default="subspace",
                     choices=["subspace", "batched", "serving", "tour", "op"],
@@ -709,9 +709,11 @@ def run_e2e(args, band, h32, grid, q, dist, prec, name):
 def run_op(args):
     """One standalone call per step (the reference's one-call-at-a-time use)
     on the subspace shapes: SYRK S = Psi^T Psi, GEMM Hs = Psi^T H Psi, the
-    rotation Psi Q, or the S + Hs pair; for profiling a single op and timing
-    it alone. Prints {"op", "precision", "ms", "tflops"}, one line per
-    precision (two with --precision both)."""
+    rotation Psi Q, or the S + Hs pair (one line per precision, two with
+    --precision both); or the H Psi producer on the same Psi: the periodic
+    halo, the stencil, the nonlocal projector. For profiling a single op and
+    timing it alone. Prints {"op", "precision", "ms", ...}."""
+    import numpy as np
     import torch
     import skgemm
     dev = torch.device("cuda", 0)
@@ -721,6 +723,32 @@ def run_op(args):
     Hs = torch.zeros_like(S)
     Pn = torch.empty_like(band)
     s = torch.cuda.current_stream()
+    if args.op == "nloc":
+        # The nonlocal projector H Psi += V_nloc Psi on the same Psi (48^3
+        # grid points, 512 bands): 64 atoms x 2 periodic images, 800 random
+        # grid rows x 16 columns per projector (seeded).
+        rng = np.random.default_rng(8)
+        atoms, images, nrow, ncol = 64, 2, 800, 16
+        nproj = atoms * images
+        proj = skgemm.NlocProjector(
+            np.full(nproj, nrow), np.full(nproj, ncol),
+            np.repeat(np.arange(1, atoms + 1), images),
+            np.append(np.repeat(np.arange(atoms) * ncol, images), atoms * ncol),
+            np.concatenate([rng.permutation(ND)[:nrow] for _ in range(nproj)]),
+            rng.uniform(-1, 1, nproj * nrow * ncol), rng.uniform(-0.5, 0.5, nproj * ncol), ND)
+        hpsi = torch.zeros_like(band)
+        fn = lambda: proj.apply(NB, 0.01, band, hpsi, 32, stream=s)
+        ms = time_calls(fn, s, torch, reps=max(1, args.steps), warm=max(0, args.warmup))
+        rep = _timed_kernels(skgemm, fn, s, max(1, args.steps))
+        skgemm.stream_status(s)
+        proj.close()
+        flop = 2 * 2 * nproj * nrow * ncol * NB
+        print(json.dumps({"workload": f"op_nloc_48cubed_x{NB}_64atoms_x2", "op": "nloc",
+                          "precision": "f64", "ms": round(ms, 4),
+                          "tflops": round(flop / ms / 1e9, 3),
+                          "kernels_ms": {k: round(v[1] / v[0], 4) for k, v in rep.items()}}),
+              flush=True)
+        return
     if args.op in ("stencil", "halo"):
         # The H Psi producer on the same Psi (48^3 = 110592 grid points, 512
         # bands): the periodic halo (band-packed Psi -> extended) or the

@@ -189,6 +189,13 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, uint32_t s
                "r"(src_bytes)
                : "memory");
 }
+// 16-byte asynchronous global -> shared copy (L2 only); src_bytes = 0 writes
+// zeros. Both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
 }

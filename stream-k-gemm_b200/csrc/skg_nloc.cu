@@ -16,11 +16,12 @@
 //    memory, each (column, band) thread summing them in row order; then the
 //    block's gamma scalings in order;
 //  * nloc_chi_c_kernel: the back-projection rows chi_p C_p of every projector
-//    (64-row x 64-band tiles, C and chi staged in shared memory), into a
+//    (spans of 64-row tiles x 64 bands, C and chi staged in shared memory), into a
 //    scratch of total rows x nb;
-//  * nloc_backward_kernel: thread per (touched grid point, band) — walks the
-//    point's (projector, row) entries in projector order (an inverse index
-//    built at creation), so the scatter-adds keep the reference's order.
+//  * nloc_backward_kernel: thread per (touched grid point, band pair) — walks
+//    the point's (projector, row) entries in projector order (an inverse index
+//    built at creation, each entry stored as its scratch row), so the
+//    scatter-adds keep the reference's order.
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -45,8 +46,7 @@ struct skgemm_nloc {
   // touched points: grid index, entries (CSR of (projector, row))
   uint32_t* d_touch = nullptr;
   int64_t* d_touch_off = nullptr;
-  int32_t* d_ent_proj = nullptr;
-  uint32_t* d_ent_row = nullptr;
+  int64_t* d_ent_off = nullptr;  // per entry: its temp row (projector's row_off + row)
   // back-projection row tiles (projector, first row)
   int64_t ntiles = 0;
   int64_t *d_tile_proj = nullptr, *d_tile_r0 = nullptr;
@@ -65,13 +65,15 @@ namespace skg {
 namespace {
 
 // Forward CTA: (block q, 32 bands, 16 columns); thread (band bl = tid % 32,
-// columns 4 jq .. 4 jq + 3, jq = tid / 32). For each projector of the block,
-// in order, the CTA stages 64 gathered rows x 32 bands of psi and the
-// matching 64 rows x 16 columns of chi in shared memory (all 128 threads
-// loading: many gathers in flight), then every thread adds its four columns'
-// products over those rows in row order — the reference's order, so the
-// sums are exact to it — and folds each projector's sum into the block
-// coefficient with fma(dv, sum, C). Coefficients stored [column][band].
+// columns 4 jq .. 4 jq + 3, jq = tid / 32). The CTA walks the block's
+// projectors in order and each projector's rows in chunks of 64: per chunk,
+// 64 gathered rows x 32 bands of psi and the matching 64 rows x 16 columns
+// of chi land in shared memory by asynchronous copies, double-buffered (the
+// next chunk's gathers are in flight while the current one is summed). Every
+// thread adds its four columns' products over a chunk's rows in row order —
+// the reference's order, so the sums are exact to it — and folds each
+// projector's sum into the block coefficient with fma(dv, sum, C).
+// Coefficients stored [column][band].
 constexpr int kNlocBands = 32;
 constexpr int kNlocCols = 16;
 constexpr int kNlocRows = 64;
@@ -85,8 +87,8 @@ __global__ void __launch_bounds__(kNlocThreads) nloc_forward_kernel(
     const uint32_t* __restrict__ index, const double* __restrict__ chi,
     const double* __restrict__ gamma, const double* __restrict__ psi16,
     double* __restrict__ coef) {
-  __shared__ double rows[kNlocRows][kNlocBands];
-  __shared__ double xs[kNlocCols][kNlocRows];
+  __shared__ __align__(16) double rows[2][kNlocRows][kNlocBands];
+  __shared__ __align__(16) double xs[2][kNlocCols][kNlocRows];
   const int64_t q = blockIdx.x;
   const int64_t b0 = (int64_t)blockIdx.y * kNlocBands;
   const int64_t jb = (int64_t)blockIdx.z * kNlocCols;  // the CTA's first column
@@ -96,38 +98,87 @@ __global__ void __launch_bounds__(kNlocThreads) nloc_forward_kernel(
   if (jb >= nc) return;  // the whole CTA past the block
   const int ncc = (int)min((int64_t)kNlocCols, nc - jb);  // columns of this CTA
   const int64_t b = b0 + bl;
-  double acc[4] = {};
-  for (int64_t e = blk[4 * q + 2]; e < blk_end[2 * q]; ++e) {
+  const int64_t e_begin = blk[4 * q + 2], e_end = blk_end[2 * q];
+  // Issue the copies of chunk r0 of projector entry e into buffer buf.
+  auto issue = [&](int64_t e, int64_t r0, int buf) {
     const int p = blk_proj[e];
     const int64_t nr = nrow[p];
-    const double* x = chi + chi_off[p] + jb * nr;
+    const int nrr = (int)min((int64_t)kNlocRows, nr - r0);
     const uint32_t* idx = index + row_off[p];
-    double sum[4] = {};
-    for (int64_t r0 = 0; r0 < nr; r0 += kNlocRows) {
-      const int nrr = (int)min((int64_t)kNlocRows, nr - r0);
-      __syncthreads();  // the previous chunk is consumed
-      for (int i = threadIdx.x; i < kNlocRows * kNlocBands; i += blockDim.x) {
-        const int rr = i / kNlocBands, cb = i % kNlocBands;
-        const int64_t bb = b0 + cb;
-        double v = 0.0;
-        if (rr < nrr && bb < nb)
-          v = __ldg(psi16 + ((bb / 16) * K + (int64_t)__ldg(idx + r0 + rr)) * 16 + (bb % 16));
-        rows[rr][cb] = v;
-      }
-      for (int i = threadIdx.x; i < kNlocCols * kNlocRows; i += blockDim.x) {
-        const int jj = i / kNlocRows, rr = i % kNlocRows;
-        xs[jj][rr] = (jj < ncc && rr < nrr) ? __ldg(x + jj * nr + r0 + rr) : 0.0;
-      }
-      __syncthreads();
-      for (int rr = 0; rr < nrr; ++rr) {
-        const double v = rows[rr][bl];
+    // psi rows: 64 rows x 2 band tiles x 8 pieces of 16 bytes (two bands).
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-          sum[jj] = __dadd_rn(sum[jj], __dmul_rn(xs[4 * jq + jj][rr], v));
-      }
+    for (int i = threadIdx.x; i < kNlocRows * kNlocBands / 2; i += kNlocThreads) {
+      const int rr = i / (kNlocBands / 2), cb = 2 * (i % (kNlocBands / 2));
+      const int64_t bb = b0 + cb;
+      const bool ok = rr < nrr && bb < nb;
+      const double* src = psi16;
+      if (ok) src = psi16 + ((bb / 16) * K + (int64_t)__ldg(idx + r0 + rr)) * 16 + (bb % 16);
+      cp_async16(&rows[buf][rr][cb], src, ok ? 16u : 0u);
     }
+    const double* x = chi + chi_off[p] + jb * nr;
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) acc[jj] = fma(dv, sum[jj], acc[jj]);
+    for (int i = threadIdx.x; i < kNlocCols * kNlocRows; i += kNlocThreads) {
+      const int jj = i / kNlocRows, rr = i % kNlocRows;
+      const bool ok = jj < ncc && rr < nrr;
+      cp_async8(&xs[buf][jj][rr], ok ? x + jj * nr + r0 + rr : chi, ok ? 8u : 0u);
+    }
+  };
+  // Chunk cursor over (projector entry, first row); advance returns false at
+  // the block's end.
+  auto advance = [&](int64_t& e, int64_t& r0) -> bool {
+    r0 += kNlocRows;
+    while (e < e_end && r0 >= (int64_t)nrow[blk_proj[e]]) {
+      ++e;
+      r0 = 0;
+    }
+    return e < e_end;
+  };
+  int64_t e = e_begin, r0 = 0;
+  // Skip leading projectors without rows.
+  while (e < e_end && nrow[blk_proj[e]] == 0) ++e;
+  double acc[4] = {};
+  double sum[4] = {};
+  if (e < e_end) {
+    issue(e, r0, 0);
+    cp_async_commit();
+  }
+  int buf = 0;
+  int64_t done_e = e_begin;  // projectors before this one are folded into acc
+  while (e < e_end) {
+    int64_t ne = e, nr0 = r0;
+    const bool more = advance(ne, nr0);
+    if (more) issue(ne, nr0, buf ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int p = blk_proj[e];
+    const int nrr = (int)min((int64_t)kNlocRows, (int64_t)nrow[p] - r0);
+    for (int rr = 0; rr < nrr; ++rr) {
+      const double v = rows[buf][rr][bl];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+        sum[jj] = __dadd_rn(sum[jj], __dmul_rn(xs[buf][4 * jq + jj][rr], v));
+    }
+    // Projector e ends with this chunk: fold its sum; projectors without
+    // rows between e and the next chunk's contribute zero sums.
+    if (!more || ne != e) {
+      for (int64_t f = done_e; f <= e; ++f) {
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) acc[jj] = fma(dv, f == e ? sum[jj] : 0.0, acc[jj]);
+      }
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) sum[jj] = 0.0;
+      done_e = e + 1;
+    }
+    __syncthreads();  // buffer buf consumed before the next issue refills it
+    buf ^= 1;
+    e = ne;
+    r0 = nr0;
+  }
+  // Trailing projectors without rows.
+  for (int64_t f = done_e; f < e_end; ++f) {
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) acc[jj] = fma(dv, 0.0, acc[jj]);
   }
   if (b >= nb) return;
 #pragma unroll
@@ -135,20 +186,22 @@ __global__ void __launch_bounds__(kNlocThreads) nloc_forward_kernel(
     const int64_t j = jb + 4 * jq + jj;
     if (j >= nc) break;
     double a = acc[jj];
-    for (int64_t e = blk[4 * q + 3]; e < blk_end[2 * q + 1]; ++e)
-      a = __dmul_rn(a, __ldg(gamma + blk_scale[e] + j));
+    for (int64_t f = blk[4 * q + 3]; f < blk_end[2 * q + 1]; ++f)
+      a = __dmul_rn(a, __ldg(gamma + blk_scale[f] + j));
     coef[(col0 + j) * nb + b] = a;
   }
 }
 
 // Back-projection, step 1: temp_p[r, b] = sum_k chi_p[r, k] C_p[k, b] (fused,
 // k ascending: the reference's gemm_ab order) for every projector row, into
-// temp[(row_off_p + r) * nb + b]. CTA = (row tile of 64 of one projector,
-// 64 bands); chi's 64 rows and C's columns for the 64 bands are staged in
-// shared memory, so C comes from L2 once per row tile.
+// temp[(row_off_p + r) * nb + b]. CTA = (a span of up to kNlocSpan row tiles
+// of 64 rows of one projector, 64 bands): C's columns for the 64 bands are
+// staged in shared memory once, then each row tile's chi rows are staged and
+// its 64 x 64 outputs written.
 constexpr int kNlocTileR = 64;
 constexpr int kNlocTileB = 64;
 constexpr int kNlocMaxCols = 64;
+constexpr int kNlocSpan = 4;
 
 __global__ void __launch_bounds__(256) nloc_chi_c_kernel(
     int64_t nb, const int64_t* __restrict__ tile_proj, const int64_t* __restrict__ tile_r0,
@@ -161,66 +214,85 @@ __global__ void __launch_bounds__(256) nloc_chi_c_kernel(
   double* xs = nsm + kNlocMaxCols * kNlocTileB;  // [kNlocTileR][nc + 1]
   const int64_t tile = blockIdx.x;
   const int p = (int)tile_proj[tile];
-  const int64_t r0 = tile_r0[tile];
+  const int64_t span0 = tile_r0[tile];
   const int64_t nr = nrow[p], nc = ncol[p];
-  const int nrr = (int)min((int64_t)kNlocTileR, nr - r0);
   const int64_t b0 = (int64_t)blockIdx.y * kNlocTileB;
   const double* c = coef + proj_col[p] * nb;
   for (int i = threadIdx.x; i < nc * kNlocTileB; i += blockDim.x) {
     const int k = i / kNlocTileB, bb = i % kNlocTileB;
     cs[k * kNlocTileB + bb] = (b0 + bb < nb) ? c[k * nb + b0 + bb] : 0.0;
   }
-  const double* x = chi + chi_off[p] + r0;
-  for (int i = threadIdx.x; i < nc * kNlocTileR; i += blockDim.x) {
-    const int k = i / kNlocTileR, rr = i % kNlocTileR;
-    xs[rr * (nc + 1) + k] = rr < nrr ? x[k * nr + rr] : 0.0;
-  }
-  __syncthreads();
-  // Thread: bands 4 q4 .. 4 q4 + 3 of the tile (q4 = tid % 16) and rows
-  // rg, rg + 16, rg + 32, rg + 48 (rg = tid / 16): per column, four chi and
-  // four C values feed 16 multiply-adds, each output's sum over the columns
-  // in order.
+  // Thread: band pairs 2 q4, 2 q4 + 1 and 32 + 2 q4, 33 + 2 q4 of the tile
+  // (q4 = tid % 16; 16-byte loads and stores, consecutive lanes on
+  // consecutive pairs) and rows rg, rg + 16, rg + 32, rg + 48 (rg = tid / 16):
+  // per column, four chi and four C values feed 16 multiply-adds, each
+  // output's sum over the columns in order.
   const int q4 = threadIdx.x % 16, rg = threadIdx.x / 16;
-  double tt[4][4] = {};
-  for (int k = 0; k < nc; ++k) {
-    double cv[4], xv[4];
+  for (int t = 0; t < kNlocSpan; ++t) {
+    const int64_t r0 = span0 + (int64_t)t * kNlocTileR;
+    if (r0 >= nr) break;
+    const int nrr = (int)min((int64_t)kNlocTileR, nr - r0);
+    if (t > 0) __syncthreads();  // the previous tile's chi rows are consumed
+    const double* x = chi + chi_off[p] + r0;
+    for (int i = threadIdx.x; i < nc * kNlocTileR; i += blockDim.x) {
+      const int k = i / kNlocTileR, rr = i % kNlocTileR;
+      xs[rr * (nc + 1) + k] = rr < nrr ? x[k * nr + rr] : 0.0;
+    }
+    __syncthreads();
+    double tt[4][4] = {};
+    for (int k = 0; k < nc; ++k) {
+      double cv[4], xv[4];
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) cv[jj] = cs[k * kNlocTileB + 4 * q4 + jj];
+      for (int jj = 0; jj < 4; ++jj) cv[jj] = cs[k * kNlocTileB + 32 * (jj >> 1) + 2 * q4 + (jj & 1)];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) xv[i] = xs[(rg + 16 * i) * (nc + 1) + k];
+      for (int i = 0; i < 4; ++i) xv[i] = xs[(rg + 16 * i) * (nc + 1) + k];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) tt[i][jj] = fma(xv[i], cv[jj], tt[i][jj]);
-  }
-  double* out = temp + (row_off[p] + r0) * nb + b0 + 4 * q4;
+        for (int jj = 0; jj < 4; ++jj) tt[i][jj] = fma(xv[i], cv[jj], tt[i][jj]);
+    }
+    double* out = temp + (row_off[p] + r0) * nb + b0 + 2 * q4;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int rr = rg + 16 * i;
-    if (rr >= nrr) break;
+    for (int i = 0; i < 4; ++i) {
+      const int rr = rg + 16 * i;
+      if (rr >= nrr) break;
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj)
-      if (b0 + 4 * q4 + jj < nb) out[(int64_t)rr * nb + jj] = tt[i][jj];
+      for (int h = 0; h < 2; ++h) {
+        double* o = out + (int64_t)rr * nb + 32 * h;
+        const int64_t bb = b0 + 32 * h + 2 * q4;
+        if (bb + 1 < nb && ((reinterpret_cast<uintptr_t>(o) & 15) == 0)) {
+          *reinterpret_cast<double2*>(o) = make_double2(tt[i][2 * h], tt[i][2 * h + 1]);
+        } else {
+          if (bb < nb) o[0] = tt[i][2 * h];
+          if (bb + 1 < nb) o[1] = tt[i][2 * h + 1];
+        }
+      }
+    }
   }
 }
 
-// Back-projection, step 2: thread per (touched grid point, band): the point's
-// (projector, row) entries added to out in projector order.
+// Back-projection, step 2: thread per (touched grid point, band pair): the
+// point's (projector, row) entries added to out in projector order.
 template <int OT>
 __global__ void __launch_bounds__(256) nloc_backward_kernel(
     int64_t ntouch, int64_t nb, int64_t K, const uint32_t* __restrict__ touch,
-    const int64_t* __restrict__ touch_off, const int32_t* __restrict__ ent_proj,
-    const uint32_t* __restrict__ ent_row, const int64_t* __restrict__ row_off,
+    const int64_t* __restrict__ touch_off, const int64_t* __restrict__ ent_off,
     const double* __restrict__ temp, double* __restrict__ out) {
+  const int64_t nbp = (nb + 1) / 2;  // band pairs
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ntouch * nb) return;
-  const int64_t b = t % nb, s = t / nb;
+  if (t >= ntouch * nbp) return;
+  const int64_t b = 2 * (t % nbp), s = t / nbp;
+  const bool two = b + 1 < nb;
   const int64_t g = touch[s];
-  double* o = out + ((b / OT) * K + g) * OT + (b % OT);
-  double val = *o;
-  for (int64_t e = touch_off[s]; e < touch_off[s + 1]; ++e)
-    val = __dadd_rn(val, __ldg(temp + (row_off[ent_proj[e]] + ent_row[e]) * nb + b));
-  *o = val;
+  double* o = out + ((b / OT) * K + g) * OT + (b % OT);  // b + 1 in the same tile (OT even)
+  double v0 = o[0], v1 = two ? o[1] : 0.0;
+  for (int64_t e = touch_off[s]; e < touch_off[s + 1]; ++e) {
+    const double* tr = temp + __ldg(ent_off + e) * nb + b;
+    v0 = __dadd_rn(v0, __ldg(tr));
+    if (two) v1 = __dadd_rn(v1, __ldg(tr + 1));
+  }
+  o[0] = v0;
+  if (two) o[1] = v1;
 }
 
 template <typename T>
@@ -234,7 +306,7 @@ int upload(T** dst, const std::vector<T>& v) {
 void release(skgemm_nloc* h) {
   void* ptrs[] = {h->d_nrow, h->d_ncol, h->d_index, h->d_row_off, h->d_chi_off, h->d_chi,
                   h->d_gamma, h->d_blk, h->d_blk_end, h->d_blk_proj, h->d_blk_scale,
-                  h->d_proj_blk_col, h->d_touch, h->d_touch_off, h->d_ent_proj, h->d_ent_row,
+                  h->d_proj_blk_col, h->d_touch, h->d_touch_off, h->d_ent_off,
                   h->d_tile_proj, h->d_tile_r0, h->d_coef};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -345,15 +417,11 @@ int nloc_create(int64_t P, const uint32_t* nrow, const uint32_t* ncol, const int
   }
   std::vector<uint32_t> touch;
   std::vector<int64_t> touch_off{0};
-  std::vector<int32_t> ent_proj;
-  std::vector<uint32_t> ent_row;
+  std::vector<int64_t> ent_off;
   for (const auto& kv : inv) {
     touch.push_back(kv.first);
-    for (const auto& e : kv.second) {
-      ent_proj.push_back(e.first);
-      ent_row.push_back(e.second);
-    }
-    touch_off.push_back((int64_t)ent_proj.size());
+    for (const auto& e : kv.second) ent_off.push_back(row_off[e.first] + e.second);
+    touch_off.push_back((int64_t)ent_off.size());
   }
   h->ntouch = (int64_t)touch.size();
   h->total_rows = rows;
@@ -361,7 +429,7 @@ int nloc_create(int64_t P, const uint32_t* nrow, const uint32_t* ncol, const int
   for (int64_t p = 0; p < P; ++p) {
     if (nrow[p] == 0 || ncol[p] == 0) continue;
     h->max_cols = std::max<int64_t>(h->max_cols, ncol[p]);
-    for (int64_t r0 = 0; r0 < nrow[p]; r0 += kNlocTileR) {
+    for (int64_t r0 = 0; r0 < nrow[p]; r0 += kNlocTileR * kNlocSpan) {
       tile_proj.push_back(p);
       tile_r0.push_back(r0);
     }
@@ -377,7 +445,7 @@ int nloc_create(int64_t P, const uint32_t* nrow, const uint32_t* ncol, const int
       (st = upload(&h->d_blk_end, blk_end)) || (st = upload(&h->d_blk_proj, blk_proj)) ||
       (st = upload(&h->d_blk_scale, blk_scale)) || (st = upload(&h->d_proj_blk_col, proj_col)) ||
       (st = upload(&h->d_touch, touch)) || (st = upload(&h->d_touch_off, touch_off)) ||
-      (st = upload(&h->d_ent_proj, ent_proj)) || (st = upload(&h->d_ent_row, ent_row)) ||
+      (st = upload(&h->d_ent_off, ent_off)) ||
       (st = upload(&h->d_tile_proj, tile_proj)) || (st = upload(&h->d_tile_r0, tile_r0))) {
     release(h);
     delete h;
@@ -418,6 +486,7 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
               (unsigned)((maxw + kNlocCols - 1) / kNlocCols));
     if (grid.y > 65535u || grid.z > 65535u)
       return fail(SKGEMM_ERR_INVALID_ARG, "too many bands or projector columns");
+    KernelTimer kt_(s, "nloc_forward_kernel");
     nloc_forward_kernel<<<grid, kNlocThreads, 0, s>>>(
         nb, h->K, dv, h->d_blk, h->d_blk_end, h->d_blk_proj, h->d_blk_scale, h->d_nrow,
         h->d_row_off, h->d_chi_off, h->d_index, h->d_chi, h->d_gamma, psi16, h->d_coef);
@@ -434,23 +503,23 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       h->chi_c_smem_set = true;
     }
+    KernelTimer kt_(s, "nloc_chi_c_kernel");
     nloc_chi_c_kernel<<<grid, 256, smem, s>>>(nb, h->d_tile_proj, h->d_tile_r0, h->d_nrow,
                                               h->d_ncol, h->d_row_off, h->d_chi_off,
                                               h->d_proj_blk_col, h->d_chi, h->d_coef, temp);
     SKG_CUDA(cudaGetLastError());
   }
-  const int64_t nbk = h->ntouch * nb;
+  const int64_t nbk = h->ntouch * ((nb + 1) / 2);  // threads: (touched point, band pair)
   if (nbk > 0) {
     if ((nbk + 255) / 256 > INT32_MAX)
       return fail(SKGEMM_ERR_INVALID_ARG, "too many touched points x bands");
+    KernelTimer kt_(s, "nloc_backward_kernel");
     if (out_tile == 32)
       nloc_backward_kernel<32><<<(unsigned)((nbk + 255) / 256), 256, 0, s>>>(
-          h->ntouch, nb, h->K, h->d_touch, h->d_touch_off, h->d_ent_proj, h->d_ent_row,
-          h->d_row_off, temp, out);
+          h->ntouch, nb, h->K, h->d_touch, h->d_touch_off, h->d_ent_off, temp, out);
     else
       nloc_backward_kernel<16><<<(unsigned)((nbk + 255) / 256), 256, 0, s>>>(
-          h->ntouch, nb, h->K, h->d_touch, h->d_touch_off, h->d_ent_proj, h->d_ent_row,
-          h->d_row_off, temp, out);
+          h->ntouch, nb, h->K, h->d_touch, h->d_touch_off, h->d_ent_off, temp, out);
     SKG_CUDA(cudaGetLastError());
   }
   return SKGEMM_OK;

@@ -356,6 +356,7 @@ int launch_halo_periodic(int64_t ni, int64_t nj, int64_t nk, int64_t nb, int FDn
     return fail(SKGEMM_ERR_INVALID_ARG, "grid too large");
   const int64_t rows = ((nb + 15) / 16) * (nk + 2 * FDn) * (nj + 2 * FDn);
   if (rows > INT32_MAX) return fail(SKGEMM_ERR_INVALID_ARG, "grid too large");
+  KernelTimer kt_(s, "halo_periodic_kernel");
   halo_periodic_kernel<<<(unsigned)rows, 256, 0, s>>>((int)ni, (int)nj, (int)nk, FDn, local, ext);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
