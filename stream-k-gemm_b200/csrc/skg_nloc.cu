@@ -66,9 +66,10 @@ namespace {
 
 // Forward CTA: (block q, 32 bands, 16 columns); thread (band bl = tid % 32,
 // columns 4 jq .. 4 jq + 3, jq = tid / 32). The CTA walks the block's
-// projectors in order and each projector's rows in chunks of 64: per chunk,
-// 64 gathered rows x 32 bands of psi and the matching 64 rows x 16 columns
-// of chi land in shared memory by asynchronous copies, double-buffered (the
+// projectors in order and each projector's rows in chunks of 32: per chunk,
+// 32 gathered rows x 32 bands of psi and the matching 32 rows x 16 columns
+// of chi land in shared memory by asynchronous copies, double-buffered (24 KB
+// a CTA, so that all CTAs of the apply are resident at once; the
 // next chunk's gathers are in flight while the current one is summed). Every
 // thread adds its four columns' products over a chunk's rows in row order —
 // the reference's order, so the sums are exact to it — and folds each
@@ -76,7 +77,7 @@ namespace {
 // Coefficients stored [column][band].
 constexpr int kNlocBands = 32;
 constexpr int kNlocCols = 16;
-constexpr int kNlocRows = 64;
+constexpr int kNlocRows = 32;
 constexpr int kNlocThreads = kNlocBands * kNlocCols / 4;
 
 __global__ void __launch_bounds__(kNlocThreads) nloc_forward_kernel(
