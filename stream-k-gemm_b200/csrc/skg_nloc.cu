@@ -205,14 +205,15 @@ constexpr int kNlocMaxCols = 64;
 constexpr int kNlocSpan = 4;
 
 __global__ void __launch_bounds__(256) nloc_chi_c_kernel(
-    int64_t nb, const int64_t* __restrict__ tile_proj, const int64_t* __restrict__ tile_r0,
+    int64_t nb, int max_cols, const int64_t* __restrict__ tile_proj,
+    const int64_t* __restrict__ tile_r0,
     const uint32_t* __restrict__ nrow, const uint32_t* __restrict__ ncol,
     const int64_t* __restrict__ row_off, const int64_t* __restrict__ chi_off,
     const int64_t* __restrict__ proj_col, const double* __restrict__ chi,
     const double* __restrict__ coef, double* __restrict__ temp) {
   extern __shared__ double nsm[];
-  double* cs = nsm;                            // [kNlocMaxCols][kNlocTileB]
-  double* xs = nsm + kNlocMaxCols * kNlocTileB;  // [kNlocTileR][nc + 1]
+  double* cs = nsm;                     // [max_cols][kNlocTileB]
+  double* xs = nsm + max_cols * kNlocTileB;  // [kNlocTileR][nc + 1]
   const int64_t tile = blockIdx.x;
   const int p = (int)tile_proj[tile];
   const int64_t span0 = tile_r0[tile];
@@ -498,14 +499,17 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
     dim3 grid((unsigned)h->ntiles, (unsigned)((nb + kNlocTileB - 1) / kNlocTileB));
     if (h->ntiles > INT32_MAX || grid.y > 65535u)
       return fail(SKGEMM_ERR_INVALID_ARG, "too many projector rows or bands");
-    const size_t smem = (kNlocMaxCols * kNlocTileB + kNlocTileR * (kNlocMaxCols + 1)) * 8;
+    // Shared memory for the set's widest projector (C columns and chi rows).
+    const int mc = (int)h->max_cols;
+    const size_t smem = ((size_t)mc * kNlocTileB + kNlocTileR * (size_t)(mc + 1)) * 8;
     if (!h->chi_c_smem_set) {  // per handle: a handle belongs to one device
+      const size_t smem_max = (kNlocMaxCols * kNlocTileB + kNlocTileR * (kNlocMaxCols + 1)) * 8;
       SKG_CUDA(cudaFuncSetAttribute(nloc_chi_c_kernel,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       h->chi_c_smem_set = true;
     }
     KernelTimer kt_(s, "nloc_chi_c_kernel");
-    nloc_chi_c_kernel<<<grid, 256, smem, s>>>(nb, h->d_tile_proj, h->d_tile_r0, h->d_nrow,
+    nloc_chi_c_kernel<<<grid, 256, smem, s>>>(nb, mc, h->d_tile_proj, h->d_tile_r0, h->d_nrow,
                                               h->d_ncol, h->d_row_off, h->d_chi_off,
                                               h->d_proj_blk_col, h->d_chi, h->d_coef, temp);
     SKG_CUDA(cudaGetLastError());
