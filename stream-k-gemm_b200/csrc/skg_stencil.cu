@@ -262,11 +262,14 @@ template <int OT>
 int launch_staged(const CUtensorMap& mapP, const CUtensorMap& mapC, const CUtensorMap& mapA,
                   bool a2d, int ni, int nj, int nk, int nb, int kc, dim3 grid, const double* ext,
                   const StencilCoef& cf, double* out, uint32_t* err, cudaStream_t s) {
-  static bool attr_set = false;
-  if (!attr_set) {
+  static bool attr_set[64] = {};  // function attributes are per device
+  int d = 0;
+  SKG_CUDA(cudaGetDevice(&d));
+  if (d < 0 || d >= 64) return fail(SKGEMM_ERR_INVALID_ARG, "device index");
+  if (!attr_set[d]) {
     SKG_CUDA(cudaFuncSetAttribute(stencil_staged_kernel<OT>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kStSmem));
-    attr_set = true;
+    attr_set[d] = true;
   }
   KernelTimer kt_(s, "stencil_staged_kernel");
   stencil_staged_kernel<OT><<<grid, kStThreads, kStSmem, s>>>(mapP, mapC, mapA, a2d, ni, nj, nk,
