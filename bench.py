@@ -789,10 +789,13 @@ def run_op(args):
                                                          precision=p), FLOP_SYRK + FLOP_GEMM)}
         fn, flop = calls[args.op]
         ms = time_calls(fn, s, torch, reps=max(1, args.steps), warm=max(0, args.warmup))
+        rep = _timed_kernels(skgemm, fn, s, max(1, args.steps))  # a separate pass, timer on
         skgemm.stream_status(s)
         print(json.dumps({"workload": f"op_{args.op}_{WORKLOAD}", "op": args.op,
                           "precision": name, "ms": round(ms, 4),
-                          "tflops": round(flop / ms / 1e9, 3)}), flush=True)
+                          "tflops": round(flop / ms / 1e9, 3),
+                          "kernels_ms": {k: round(v[1] / v[0], 4) for k, v in rep.items()}}),
+              flush=True)
 
 
 # ------------------------------------------------------------ kernel tour
