@@ -115,6 +115,13 @@ int skgemm_diag_expire_fixup_wait(double budget_ms, void* stream);
  * counterpart in the reference. */
 int skgemm_kernel_timing(int enable);
 int skgemm_kernel_timing_report(char* buf, int64_t len);
+/* 1 when the process runs in debug fill mode (environment
+ * SKGEMM_DEBUG_FILL=1 at the first call): every scratch buffer of the library
+ * is filled with 0xFF bytes when allocated and again at the start of each
+ * call that uses it, so that a read of scratch not written first shows in
+ * the results (which are otherwise unchanged). Costs a fill per call. No
+ * counterpart in the reference. */
+int skgemm_debug_fill(void);
 /* Measured INT8 tensor-core (tcgen05.mma kind::i8, 128x256x32) throughput of
  * the current device, TOP/s; the roofline denominator of the Ozaki path. */
 int skgemm_probe_i8_peak(double* tops_out);

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -34,11 +35,26 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 // ----------------------------------------------------------------- buffers
+bool debug_fill_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("SKGEMM_DEBUG_FILL");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+int debug_poison(void* p, size_t bytes, cudaStream_t s) {
+  if (!debug_fill_enabled() || !p || !bytes) return SKGEMM_OK;
+  SKG_CUDA(cudaMemsetAsync(p, 0xFF, bytes, s));
+  return SKGEMM_OK;
+}
+
 int DeviceBuffer::ensure(size_t need) {
   if (need <= bytes) return SKGEMM_OK;
   release();
   SKG_CUDA(cudaMalloc(&ptr, need));
   bytes = need;
+  if (debug_fill_enabled()) SKG_CUDA(cudaMemset(ptr, 0xFF, need));
   return SKGEMM_OK;
 }
 
@@ -56,6 +72,8 @@ int StreamWorkspace::ensure(int slots) {
   flags = nullptr;
   partial_slots = 0;
   SKG_CUDA(cudaMalloc(&partials, (size_t)slots * kBM * kBN * sizeof(double)));
+  if (debug_fill_enabled())
+    SKG_CUDA(cudaMemset(partials, 0xFF, (size_t)slots * kBM * kBN * sizeof(double)));
   SKG_CUDA(cudaMalloc(&flags, (size_t)slots * sizeof(uint32_t)));
   SKG_CUDA(cudaMemset(flags, 0, (size_t)slots * sizeof(uint32_t)));
   if (!err) {
@@ -108,6 +126,8 @@ StreamWorkspace* stream_workspace(DeviceState* dev, cudaStream_t s, int slots, i
   StreamWorkspace*& ws = dev->ws[s];
   if (!ws) ws = new StreamWorkspace();
   *status = ws->ensure(slots);
+  if (*status == SKGEMM_OK)
+    *status = debug_poison(ws->partials, ws->partial_slots * kBM * kBN * sizeof(double), s);
   return *status == SKGEMM_OK ? ws : nullptr;
 }
 
@@ -413,6 +433,8 @@ SKG_EXPORT int skgemm_stream_release(void* stream) {
   }
   return ozaki_release_stream(dev, s);
 }
+
+SKG_EXPORT int skgemm_debug_fill(void) { return debug_fill_enabled() ? 1 : 0; }
 
 SKG_EXPORT int skgemm_kernel_timing(int enable) {
   std::lock_guard<std::mutex> lk(g_kt_mu);

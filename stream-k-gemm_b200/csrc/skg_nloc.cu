@@ -482,6 +482,8 @@ int nloc_apply(skgemm_nloc* h, int64_t nb, double dv, const double* psi16, doubl
     SKG_CUDA(cudaMalloc(&h->d_coef, need * sizeof(double)));
     h->coef_cap = need;
   }
+  // Debug mode: the coefficient and scratch rows start as 0xFF bytes.
+  if ((st = debug_poison(h->d_coef, (size_t)h->coef_cap * sizeof(double), s))) return st;
   const int64_t maxw = *std::max_element(h->blk_width.begin(), h->blk_width.end());
   if (maxw > 0) {
     dim3 grid((unsigned)h->nblk, (unsigned)((nb + kNlocBands - 1) / kNlocBands),

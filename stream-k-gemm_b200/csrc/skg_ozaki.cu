@@ -804,6 +804,10 @@ int ensure_consts(DeviceState* dev) {
 OzakiStream* ozaki_stream(DeviceState* dev, cudaStream_t s) {
   OzakiStream*& o = g_oz[dev->device].streams[s];
   if (!o) o = new OzakiStream();
+  if (debug_fill_enabled())  // the call's scratch starts as 0xFF bytes
+    for (DeviceBuffer* b : {&o->res_a, &o->res_b, &o->part_a, &o->part_b, &o->mu_a, &o->mu_b,
+                            &o->partials, &o->rbytes})
+      debug_poison(b->ptr, b->bytes, s);
   return o;
 }
 

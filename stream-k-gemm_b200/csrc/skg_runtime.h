@@ -38,6 +38,15 @@ int cuda_fail(cudaError_t e, const char* what);
   } while (0)
 
 // Grow-only device buffer.
+// Debug mode (environment SKGEMM_DEBUG_FILL=1, read once): every scratch
+// buffer is filled with 0xFF bytes when it is allocated and again, on the
+// call's stream, at the start of each call that uses it (an FP64 NaN, an
+// int8 residue of -1), so that a kernel reading scratch it did not write
+// first shows in its results. Results are unchanged when the kernels are
+// right (tests/test_debug_fill_gpu.py); the fills cost time.
+bool debug_fill_enabled();
+int debug_poison(void* p, size_t bytes, cudaStream_t s);
+
 struct DeviceBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;

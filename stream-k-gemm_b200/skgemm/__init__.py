@@ -166,6 +166,7 @@ _SIGS = {
     "skgemm_serve_simulate": [ctypes.POINTER(ServeRequest), ctypes.c_int,
                               ctypes.POINTER(ServeOptions)],
     "skgemm_stream_release": [_vp],
+    "skgemm_debug_fill": [],
     "skgemm_tune_cache_save": [ctypes.c_char_p],
     "skgemm_tune_cache_load": [ctypes.c_char_p],
     "skgemm_tune_cache_clear": [],
@@ -647,6 +648,11 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def debug_fill() -> bool:
+    """True when the library runs in debug fill mode (SKGEMM_DEBUG_FILL=1)."""
+    return bool(lib().skgemm_debug_fill())
 
 
 def tune_cache_save(path) -> int:
