@@ -460,9 +460,11 @@ def kernel_rooflines(skgemm, step, torch, steps, peaks, band, grid, q, S, Pn):
     INT8 peak, conversions / norms / the rotation's reconstruction against
     HBM. Algorithmic work per launch: SYRK M (M+1) K, rotation 2 Nd nb^2
     flop (INT8 ops: the same times the moduli count L); a conversion 8 + L
-    bytes per element (8 + 2 L for BF16 residues), a norm pass 8 bytes per
-    element, the rotation's reconstruction L + 8 bytes per element (element
-    = one of the Nd x nb operand's)."""
+    bytes per element (8 + 2 L for BF16 residues; the SYRK's operand by
+    convert_tma_kernel after a norm pass of 8 bytes per element, the
+    rotation's in one pass by convert_short_kernel), the rotation's
+    reconstruction L + 8 bytes per element (element = one of the Nd x nb
+    operand's)."""
     fp64_peak, i8_peak, hbm = peaks
     rep = _timed_kernels(skgemm, step, step.stream, steps)
     total = sum(ms for _, ms in rep.values()) or 1.0
@@ -486,8 +488,9 @@ def kernel_rooflines(skgemm, step, torch, steps, peaks, band, grid, q, S, Pn):
         work = {"i8_gemm_kernel": (Ls * FLOP_SYRK, "TOP/s", i8_peak, "tensor"),
                 "i8_gemm2_kernel": (Ls * FLOP_SYRK, "TOP/s", i8_peak, "tensor"),
                 "i8_rot_kernel": (Lr * FLOP_ROT, "TOP/s", i8_peak, "tensor"),
-                "convert_tma_kernel": (E * (16 + rb * (Ls + Lr)), "GB/s", hbm, "hbm"),
-                "norm_partials_kernel": (2 * E * 8, "GB/s", hbm, "hbm"),
+                "convert_tma_kernel": (E * (8 + rb * Ls), "GB/s", hbm, "hbm"),
+                "norm_partials_kernel": (E * 8, "GB/s", hbm, "hbm"),
+                "convert_short_kernel": (E * (8 + rb * Lr), "GB/s", hbm, "hbm"),
                 "crt_residues_band_kernel": (E * (rb * Lr + 8), "GB/s", hbm, "hbm")}
     if step.prec is None:
         # the GEMM's kernel from the step itself (one launch per step, serial)

@@ -334,6 +334,52 @@ constexpr int kConvWarps = 8;
 constexpr int kConvTile = 16 * 32;  // doubles per warp tile
 constexpr int kConvSmem = kConvWarps * (kConvStages * kConvTile * 8 + kConvStages * 8);
 
+// INT8 residues of one staged 16-row x 32-k tile (conversion kernels' stage
+// layout) for lane (r = lane / 2, h = lane % 2): k = 16 h .. 16 h + 15 of row
+// r, one 16-byte store per residue plane at dst + l lstride.
+template <int L, bool KM>
+__device__ __forceinline__ void convert_stage_i8(const double* stage, int r, int h, double s1,
+                                                 double s2, uint8_t* dst, int64_t lstride) {
+  // Swizzled stage: 16-byte chunk c of k-row k at c ^ (k % 8). At step j
+  // lane (r, h) reads k = 16 h + (j ^ 4 h), whose chunk (r / 2) ^ (j % 8)
+  // ^ 4 h differs from the other half-lane's in bit 2, so a half-warp
+  // touches 8 distinct chunks (all 32 banks once). d[j] then holds
+  // k = 16 h + (j ^ 4 h): for h = 1 the packed words are in the order
+  // 1, 0, 3, 2, and put() swaps them back.
+  // KM: lane h = 1 walks its k in the order j ^ 1 instead, so that the
+  // half-warp's two k-blocks read opposite halves of each 16-byte unit
+  // (conflict-free); its pairs come out swapped, which the byte-permute
+  // selector of pk() undoes, and put() keeps the word order.
+  const int z = KM ? 256 * h + 16 * r + ((r & 7) << 1) + h
+                   : 320 * h | (((r >> 1) ^ (4 * h)) << 1) | (r & 1);
+  Digits d[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j)
+    d[j] = digits_of<L>(stage[(KM ? j : ((j << 4) | ((j & 7) << 1))) ^ z], s1, s2);
+  const uint32_t sel = (KM && h) ? 0x0004u : 0x0040u;
+  auto pk = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t e) {
+    return __byte_perm(__byte_perm(a, b, sel), __byte_perm(c, e, sel), 0x5410);
+  };
+  auto put = [&](uint8_t* p, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3) {
+    *reinterpret_cast<uint4*>(p) =
+        (!KM && h) ? make_uint4(w1, w0, w3, w2) : make_uint4(w0, w1, w2, w3);
+  };
+  put(dst, pk(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pk(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
+      pk(d[8].lo, d[9].lo, d[10].lo, d[11].lo), pk(d[12].lo, d[13].lo, d[14].lo, d[15].lo));
+#pragma unroll
+  for (int l = 1; l < L; ++l) {
+    uint32_t b[16];
+#pragma unroll
+    for (int j = 0; j < 16; j += 2) {
+      const uint2 v = residue_byte2<L>(d[j], d[j + 1], l);
+      b[j] = v.x;
+      b[j + 1] = v.y;
+    }
+    put(dst + l * lstride, pk(b[0], b[1], b[2], b[3]), pk(b[4], b[5], b[6], b[7]),
+        pk(b[8], b[9], b[10], b[11]), pk(b[12], b[13], b[14], b[15]));
+  }
+}
+
 // KM: the operand is K-major, [K/16][R][16] (band-packed Psi as the
 // rotation's A: the band -> grid transposition happens here, in the reads).
 // Its box {16 k, 16 rows, 2 k-blocks} lands as [2][16 rows][16 k], 128B-
@@ -438,45 +484,7 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
         *reinterpret_cast<uint4*>(base + 32 + 16 * h) = make_uint4(w[4], w[5], w[6], w[7]);
       }
     } else if (ok) {
-      // Swizzled stage: 16-byte chunk c of k-row k at c ^ (k % 8). At step j
-      // lane (r, h) reads k = 16 h + (j ^ 4 h), whose chunk (r / 2) ^ (j % 8)
-      // ^ 4 h differs from the other half-lane's in bit 2, so a half-warp
-      // touches 8 distinct chunks (all 32 banks once). d[j] then holds
-      // k = 16 h + (j ^ 4 h): for h = 1 the packed words are in the order
-      // 1, 0, 3, 2, and put() swaps them back.
-      // KM: lane h = 1 walks its k in the order j ^ 1 instead, so that the
-      // half-warp's two k-blocks read opposite halves of each 16-byte unit
-      // (conflict-free); its pairs come out swapped, which the byte-permute
-      // selector of pk() undoes, and put() keeps the word order.
-      const double* stage = buf + s * kConvTile;
-      const int z = KM ? 256 * h + 16 * r + ((r & 7) << 1) + h
-                       : 320 * h | (((r >> 1) ^ (4 * h)) << 1) | (r & 1);
-      Digits d[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j)
-        d[j] = digits_of<L>(stage[(KM ? j : ((j << 4) | ((j & 7) << 1))) ^ z], s1, s2);
-      const uint32_t sel = (KM && h) ? 0x0004u : 0x0040u;
-      auto pk = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t e) {
-        return __byte_perm(__byte_perm(a, b, sel), __byte_perm(c, e, sel), 0x5410);
-      };
-      auto put = [&](uint8_t* p, uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3) {
-        *reinterpret_cast<uint4*>(p) =
-            (!KM && h) ? make_uint4(w1, w0, w3, w2) : make_uint4(w0, w1, w2, w3);
-      };
-      put(dst, pk(d[0].lo, d[1].lo, d[2].lo, d[3].lo), pk(d[4].lo, d[5].lo, d[6].lo, d[7].lo),
-          pk(d[8].lo, d[9].lo, d[10].lo, d[11].lo), pk(d[12].lo, d[13].lo, d[14].lo, d[15].lo));
-#pragma unroll
-      for (int l = 1; l < L; ++l) {
-        uint32_t b[16];
-#pragma unroll
-        for (int j = 0; j < 16; j += 2) {
-          const uint2 v = residue_byte2<L>(d[j], d[j + 1], l);
-          b[j] = v.x;
-          b[j + 1] = v.y;
-        }
-        put(dst + l * lstride, pk(b[0], b[1], b[2], b[3]), pk(b[4], b[5], b[6], b[7]),
-            pk(b[8], b[9], b[10], b[11]), pk(b[12], b[13], b[14], b[15]));
-      }
+      convert_stage_i8<L, KM>(buf + s * kConvTile, r, h, s1, s2, dst, lstride);
     } else {
 #pragma unroll
       for (int l = 0; l < L; ++l)
@@ -487,6 +495,90 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     __syncwarp();  // stage s consumed by every lane before it is refilled
     s = (s + 1) % kConvStages;
     advance(g, kb);
+  }
+}
+
+// One pass for packed16 operands with short rows (K <= 512: grid-packed Psi
+// as the rotation's A, rows = grid points, k = bands). A persistent CTA (two
+// per SM, so that one loads while the other converts) takes one 16-row group
+// at a time: its KP/32 boxes of 16 rows x 32 k (the conversion kernels' stage
+// layout) land in shared memory by TMA together; the rows' sums of squares
+// are taken there, then each warp converts its boxes with the conversion
+// kernels' tile code. HBM reads the operand once instead of twice. The sums follow the two-pass path exactly when that path
+// uses one k-chunk (ceil(R/16) >= 600): thread (r = tid % 16, kl = tid / 16)
+// adds v*v by fma over k = kl, kl + 16, ..., and row r adds the 16 partials in
+// kl order. So the exponents, and the residues, equal that path's bit for bit
+// (and the K-major path's, which reproduces the same sums).
+constexpr int kShortKbMax = 16;  // KP <= 512
+constexpr int kShortSmem = kShortKbMax * kConvTile * 8 + 256 * 8 + 32 * 8 + 64 + 1024;
+
+template <int L>
+__global__ void __launch_bounds__(256, 2) convert_short_kernel(
+    const __grid_constant__ CUtensorMap map, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
+    int gamma_bits, int* __restrict__ mu, uint8_t* __restrict__ res, uint32_t* __restrict__ err) {
+  extern __shared__ uint8_t ssm[];
+  double* tiles =  // [16 boxes][32 k][16 rows]
+      reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(ssm) + 1023) & ~uintptr_t(1023));
+  double* red = tiles + kShortKbMax * kConvTile;  // [16 kl][16 rows]
+  double* sc = red + 256;                         // s1 [16], s2 [16]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sc + 32);
+  const int KB = (int)(KP / 32);
+  const int64_t G = Rpad / 16;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    tma_prefetch_desc(&map);
+  }
+  __syncthreads();
+  uint32_t phase = 0;
+  for (int64_t g = blockIdx.x; g < G; g += gridDim.x) {
+    if (threadIdx.x == 0) {
+      fence_proxy_async_smem();  // the previous group's reads of the tiles are done
+      mbar_arrive_expect_tx(bar, (uint32_t)(KB * kConvTile * 8));
+      for (int kb = 0; kb < KB; ++kb)
+        tma_load_3d(tiles + kb * kConvTile, &map, bar, 0, kb * 32, (int)g);
+    }
+    const bool ok = mbar_wait(bar, phase, err);
+    phase ^= 1;
+    {
+      const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
+      double acc = 0.0;
+      for (int64_t k = kl; k < K; k += 16) {
+        const double v = tiles[(k >> 5) * kConvTile + (k & 31) * 16 +
+                               ((((r >> 1) ^ (int)(k & 7))) << 1) + (r & 1)];
+        acc = fma(v, v, acc);
+      }
+      red[kl * 16 + r] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) {
+      double part = 0.0;
+      for (int j = 0; j < 16; ++j) part += red[j * 16 + threadIdx.x];
+      const int64_t row = g * 16 + threadIdx.x;
+      double sq = 0.0;
+      sq += row < R ? part : 0.0;
+      const int m = row < R ? row_exponent(sq, gamma_bits) : 0;
+      mu[row] = m;
+      double s1v, s2v;
+      pow2_pair(m, s1v, s2v);
+      sc[threadIdx.x] = s1v;
+      sc[16 + threadIdx.x] = s2v;
+    }
+    __syncthreads();
+    const int r = lane >> 1, h = lane & 1;
+    const double s1 = sc[r], s2 = sc[16 + r];
+    const int64_t lstride = Rpad * KP;
+    for (int kb = warp; kb < KB; kb += kConvWarps) {
+      uint8_t* dst = res + ((g * 16 + r) * KP + kb * 32 + 16 * h);
+      if (ok) {
+        convert_stage_i8<L, false>(tiles + kb * kConvTile, r, h, s1, s2, dst, lstride);
+      } else {
+        for (int l = 0; l < L; ++l)
+          *reinterpret_cast<uint4*>(dst + l * lstride) = make_uint4(0, 0, 0, 0);
+      }
+    }
+    __syncthreads();  // the tiles (and sc, red) are consumed before the next group
   }
 }
 
@@ -1184,6 +1276,24 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
 // plus row exponents, in two steps: prep_norms (norm partials, then the row
 // exponents) and prep_convert (the TMA-fed conversion). The steps may run on
 // different streams with an event between them.
+template <int L>
+int launch_short_L(DeviceState* dev, const CUtensorMap& map, int64_t R, int64_t K, int64_t KP,
+                   int64_t Rpad, int* mu, uint8_t* res, uint32_t* err, cudaStream_t s) {
+  static bool attr_done[64] = {false};
+  if (!attr_done[dev->device]) {
+    SKG_CUDA(cudaFuncSetAttribute(convert_short_kernel<L>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kShortSmem));
+    attr_done[dev->device] = true;
+  }
+  const int64_t G = Rpad / 16;
+  const int64_t grid = std::min<int64_t>(G, 2 * (int64_t)dev->num_sms);  // two CTAs per SM
+  KernelTimer kt_(s, "convert_short_kernel");
+  convert_short_kernel<L><<<(unsigned)grid, 256, kShortSmem, s>>>(map, R, K, KP, Rpad,
+                                                                  gamma_for(L), mu, res, err);
+  SKG_CUDA(cudaGetLastError());
+  return SKGEMM_OK;
+}
+
 template <int T>
 int prep_norms(int64_t R, int64_t K, int64_t KP, int64_t Rpad, const double* X, int L,
                DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu, cudaStream_t s,
@@ -1258,6 +1368,24 @@ int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad
                 const double* X, int L, DeviceBuffer& res, DeviceBuffer& part, DeviceBuffer& mu,
                 uint32_t* err, cudaStream_t s, bool bf = false, bool km = false) {
   int st;
+  // Short rows (K <= 512) and a one-chunk norm pass (ceil(R/16) >= 600): one
+  // pass, convert_short_kernel (same exponents and residues bit for bit).
+  if (T == 16 && !bf && !km && KP <= 32 * kShortKbMax && (R + 15) / 16 >= 600) {
+    if ((reinterpret_cast<uintptr_t>(X) & 15) != 0)
+      return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
+    if ((st = res.ensure((size_t)L * Rpad * KP))) return st;
+    if ((st = mu.ensure((size_t)Rpad * sizeof(int)))) return st;
+    const int64_t P_in = (R + 15) / 16;
+    const uint64_t dims[3] = {16, (uint64_t)K, (uint64_t)P_in};
+    const uint64_t strides[2] = {16 * 8, (uint64_t)K * 16 * 8};
+    const uint32_t box[3] = {16, 32, 1};
+    CUtensorMap map;
+    if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                           CU_TENSOR_MAP_SWIZZLE_128B)))
+      return st;
+    SKG_DISPATCH_L(L, (launch_short_L<LL>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
+                                          (uint8_t*)res.ptr, err, s)))
+  }
   if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s, bf, km))) return st;
   return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s, bf, km);
 }
