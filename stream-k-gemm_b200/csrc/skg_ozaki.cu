@@ -501,21 +501,23 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
 }
 
 // One pass for packed16 operands with short rows (K <= 512: grid-packed Psi
-// as the rotation's A, rows = grid points, k = bands). A persistent CTA (two
-// per SM, so that one loads while the other converts) takes one 16-row group
+// as the rotation's A, rows = grid points, k = bands). A persistent CTA of
+// four warps (three per SM, so that some load while others convert) takes
+// one 16-row group
 // at a time: its KP/32 boxes of 16 rows x 32 k (the conversion kernels' stage
 // layout) land in shared memory by TMA together; the rows' sums of squares
 // are taken there, then each warp converts its boxes with the conversion
 // kernels' tile code. HBM reads the operand once instead of twice. The sums follow the two-pass path exactly when that path
-// uses one k-chunk (ceil(R/16) >= 600): thread (r = tid % 16, kl = tid / 16)
-// adds v*v by fma over k = kl, kl + 16, ..., and row r adds the 16 partials in
+// uses one k-chunk (ceil(R/16) >= 600): partial (r, kl) of 256 (two per
+// thread) adds v*v by fma over k = kl, kl + 16, ..., and row r adds the 16 partials in
 // kl order. So the exponents, and the residues, equal that path's bit for bit
 // (and the K-major path's, which reproduces the same sums).
-constexpr int kShortKbMax = 16;  // KP <= 512
+constexpr int kShortKbMax = 16;   // KP <= 512
+constexpr int kShortThreads = 128;  // 4 warps; three CTAs per SM
 constexpr int kShortSmem = kShortKbMax * kConvTile * 8 + 256 * 8 + 32 * 8 + 64 + 1024;
 
 template <int L>
-__global__ void __launch_bounds__(256, 2) convert_short_kernel(
+__global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
     const __grid_constant__ CUtensorMap map, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
     int gamma_bits, int* __restrict__ mu, uint8_t* __restrict__ res, uint32_t* __restrict__ err) {
   extern __shared__ uint8_t ssm[];
@@ -543,8 +545,8 @@ __global__ void __launch_bounds__(256, 2) convert_short_kernel(
     }
     const bool ok = mbar_wait(bar, phase, err);
     phase ^= 1;
-    {
-      const int r = threadIdx.x & 15, kl = threadIdx.x >> 4;
+    for (int t = threadIdx.x; t < 256; t += kShortThreads) {  // partial (r, kl) = t
+      const int r = t & 15, kl = t >> 4;
       double acc = 0.0;
       for (int64_t k = kl; k < K; k += 16) {
         const double v = tiles[(k >> 5) * kConvTile + (k & 31) * 16 +
@@ -571,7 +573,7 @@ __global__ void __launch_bounds__(256, 2) convert_short_kernel(
     const int r = lane >> 1, h = lane & 1;
     const double s1 = sc[r], s2 = sc[16 + r];
     const int64_t lstride = Rpad * KP;
-    for (int kb = warp; kb < KB; kb += kConvWarps) {
+    for (int kb = warp; kb < KB; kb += kShortThreads / 32) {
       uint8_t* dst = res + ((g * 16 + r) * KP + kb * 32 + 16 * h);
       if (ok) {
         convert_stage_i8<L, false>(tiles + kb * kConvTile, r, h, s1, s2, dst, lstride);
@@ -1288,9 +1290,9 @@ int launch_short_L(DeviceState* dev, const CUtensorMap& map, int64_t R, int64_t 
     attr_done[dev->device] = true;
   }
   const int64_t G = Rpad / 16;
-  const int64_t grid = std::min<int64_t>(G, 2 * (int64_t)dev->num_sms);  // two CTAs per SM
+  const int64_t grid = std::min<int64_t>(G, 3 * (int64_t)dev->num_sms);  // three CTAs per SM
   KernelTimer kt_(s, "convert_short_kernel");
-  convert_short_kernel<L><<<(unsigned)grid, 256, kShortSmem, s>>>(map, R, K, KP, Rpad,
+  convert_short_kernel<L><<<(unsigned)grid, kShortThreads, kShortSmem, s>>>(map, R, K, KP, Rpad,
                                                                   gamma_for(L), mu, res, err);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
