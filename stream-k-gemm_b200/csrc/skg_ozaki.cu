@@ -503,15 +503,16 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
 // One pass for packed16 operands with short rows (K <= 512: grid-packed Psi
 // as the rotation's A, rows = grid points, k = bands). A persistent CTA of
 // four warps (three per SM, so that some load while others convert) takes
-// one 16-row group
-// at a time: its KP/32 boxes of 16 rows x 32 k (the conversion kernels' stage
-// layout) land in shared memory by TMA together; the rows' sums of squares
-// are taken there, then each warp converts its boxes with the conversion
-// kernels' tile code. HBM reads the operand once instead of twice. The sums follow the two-pass path exactly when that path
+// one 16-row group at a time: its KP/32 boxes of 16 rows x 32 k (the
+// conversion kernels' stage layout) land in shared memory by TMA together;
+// the rows' sums of squares are taken there, then each warp converts its
+// boxes with the conversion kernels' tile code. HBM reads the operand once
+// instead of twice. The sums follow the two-pass path exactly when that path
 // uses one k-chunk (ceil(R/16) >= 600): partial (r, kl) of 256 (two per
-// thread) adds v*v by fma over k = kl, kl + 16, ..., and row r adds the 16 partials in
-// kl order. So the exponents, and the residues, equal that path's bit for bit
-// (and the K-major path's, which reproduces the same sums).
+// thread) adds v*v by fma over k = kl, kl + 16, ..., and row r adds its 16
+// partials in kl order. So the exponents, and the residues, equal that
+// path's bit for bit (and the K-major path's, which reproduces the same
+// sums).
 constexpr int kShortKbMax = 16;   // KP <= 512
 constexpr int kShortThreads = 128;  // 4 warps; three CTAs per SM
 constexpr int kShortSmem = kShortKbMax * kConvTile * 8 + 256 * 8 + 32 * 8 + 64 + 1024;
