@@ -500,6 +500,18 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
   }
 }
 
+// Element (k, r) (k < 32) of a conversion stage: packed16 stages are
+// [32 k][16 rows] with 16-byte chunk c of k-row k at c ^ (k % 8); K-major
+// stages are [2][16 rows][16 k], 128-byte row 16 (k / 16) + r with chunk c
+// at c ^ (r % 8).
+template <bool KM>
+__device__ __forceinline__ double stage_elem(const double* st, int k, int r) {
+  if constexpr (KM)
+    return st[(16 * (k >> 4) + r) * 16 + ((((k & 15) >> 1) ^ (r & 7)) << 1) + (k & 1)];
+  else
+    return st[k * 16 + (((r >> 1) ^ (k & 7)) << 1) + (r & 1)];
+}
+
 // One pass for packed16 operands with short rows (K <= 512: grid-packed Psi
 // as the rotation's A, rows = grid points, k = bands). A persistent CTA of
 // four warps (three per SM, so that some load while others convert) takes
@@ -511,13 +523,13 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
 // uses one k-chunk (ceil(R/16) >= 600): partial (r, kl) of 256 (two per
 // thread) adds v*v by fma over k = kl, kl + 16, ..., and row r adds its 16
 // partials in kl order. So the exponents, and the residues, equal that
-// path's bit for bit (and the K-major path's, which reproduces the same
-// sums).
+// path's bit for bit. KM: the K-major form [K/16][R][16] (band-packed Psi),
+// staged as the conversion kernel's K-major boxes; same sums, same bits.
 constexpr int kShortKbMax = 16;   // KP <= 512
 constexpr int kShortThreads = 128;  // 4 warps; three CTAs per SM
 constexpr int kShortSmem = kShortKbMax * kConvTile * 8 + 256 * 8 + 32 * 8 + 64 + 1024;
 
-template <int L>
+template <int L, bool KM>
 __global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
     const __grid_constant__ CUtensorMap map, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
     int gamma_bits, int* __restrict__ mu, uint8_t* __restrict__ res, uint32_t* __restrict__ err) {
@@ -541,8 +553,12 @@ __global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
     if (threadIdx.x == 0) {
       fence_proxy_async_smem();  // the previous group's reads of the tiles are done
       mbar_arrive_expect_tx(bar, (uint32_t)(KB * kConvTile * 8));
-      for (int kb = 0; kb < KB; ++kb)
-        tma_load_3d(tiles + kb * kConvTile, &map, bar, 0, kb * 32, (int)g);
+      for (int kb = 0; kb < KB; ++kb) {
+        if constexpr (KM)
+          tma_load_3d(tiles + kb * kConvTile, &map, bar, 0, (int)(16 * g), 2 * kb);
+        else
+          tma_load_3d(tiles + kb * kConvTile, &map, bar, 0, kb * 32, (int)g);
+      }
     }
     const bool ok = mbar_wait(bar, phase, err);
     phase ^= 1;
@@ -550,8 +566,7 @@ __global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
       const int r = t & 15, kl = t >> 4;
       double acc = 0.0;
       for (int64_t k = kl; k < K; k += 16) {
-        const double v = tiles[(k >> 5) * kConvTile + (k & 31) * 16 +
-                               ((((r >> 1) ^ (int)(k & 7))) << 1) + (r & 1)];
+        const double v = stage_elem<KM>(tiles + (k >> 5) * kConvTile, (int)(k & 31), r);
         acc = fma(v, v, acc);
       }
       red[kl * 16 + r] = acc;
@@ -577,7 +592,7 @@ __global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
     for (int kb = warp; kb < KB; kb += kShortThreads / 32) {
       uint8_t* dst = res + ((g * 16 + r) * KP + kb * 32 + 16 * h);
       if (ok) {
-        convert_stage_i8<L, false>(tiles + kb * kConvTile, r, h, s1, s2, dst, lstride);
+        convert_stage_i8<L, KM>(tiles + kb * kConvTile, r, h, s1, s2, dst, lstride);
       } else {
         for (int l = 0; l < L; ++l)
           *reinterpret_cast<uint4*>(dst + l * lstride) = make_uint4(0, 0, 0, 0);
@@ -1281,19 +1296,19 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
 // plus row exponents, in two steps: prep_norms (norm partials, then the row
 // exponents) and prep_convert (the TMA-fed conversion). The steps may run on
 // different streams with an event between them.
-template <int L>
+template <int L, bool KM>
 int launch_short_L(DeviceState* dev, const CUtensorMap& map, int64_t R, int64_t K, int64_t KP,
                    int64_t Rpad, int* mu, uint8_t* res, uint32_t* err, cudaStream_t s) {
   static bool attr_done[64] = {false};
   if (!attr_done[dev->device]) {
-    SKG_CUDA(cudaFuncSetAttribute(convert_short_kernel<L>,
+    SKG_CUDA(cudaFuncSetAttribute(convert_short_kernel<L, KM>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kShortSmem));
     attr_done[dev->device] = true;
   }
   const int64_t G = Rpad / 16;
   const int64_t grid = std::min<int64_t>(G, 3 * (int64_t)dev->num_sms);  // three CTAs per SM
   KernelTimer kt_(s, "convert_short_kernel");
-  convert_short_kernel<L><<<(unsigned)grid, kShortThreads, kShortSmem, s>>>(map, R, K, KP, Rpad,
+  convert_short_kernel<L, KM><<<(unsigned)grid, kShortThreads, kShortSmem, s>>>(map, R, K, KP, Rpad,
                                                                   gamma_for(L), mu, res, err);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
@@ -1374,22 +1389,35 @@ int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad
                 uint32_t* err, cudaStream_t s, bool bf = false, bool km = false) {
   int st;
   // Short rows (K <= 512) and a one-chunk norm pass (ceil(R/16) >= 600): one
-  // pass, convert_short_kernel (same exponents and residues bit for bit).
-  if (T == 16 && !bf && !km && KP <= 32 * kShortKbMax && (R + 15) / 16 >= 600) {
+  // pass, convert_short_kernel (same exponents and residues bit for bit),
+  // for the packed16 layout and its K-major form.
+  if (T == 16 && !bf && KP <= 32 * kShortKbMax && (R + 15) / 16 >= 600 && (!km || K % 16 == 0)) {
     if ((reinterpret_cast<uintptr_t>(X) & 15) != 0)
       return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
     if ((st = res.ensure((size_t)L * Rpad * KP))) return st;
     if ((st = mu.ensure((size_t)Rpad * sizeof(int)))) return st;
+    CUtensorMap map;
+    if (km) {
+      // [K/16][R][16]: boxes {16 k, 16 rows, 2 k-blocks} (the conversion
+      // kernel's K-major stage).
+      const uint64_t dims[3] = {16, (uint64_t)R, (uint64_t)(K / 16)};
+      const uint64_t strides[2] = {16 * 8, (uint64_t)R * 16 * 8};
+      const uint32_t box[3] = {16, 16, 2};
+      if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                             CU_TENSOR_MAP_SWIZZLE_128B)))
+        return st;
+      SKG_DISPATCH_L(L, (launch_short_L<LL, true>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
+                                                  (uint8_t*)res.ptr, err, s)))
+    }
     const int64_t P_in = (R + 15) / 16;
     const uint64_t dims[3] = {16, (uint64_t)K, (uint64_t)P_in};
     const uint64_t strides[2] = {16 * 8, (uint64_t)K * 16 * 8};
     const uint32_t box[3] = {16, 32, 1};
-    CUtensorMap map;
     if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                            CU_TENSOR_MAP_SWIZZLE_128B)))
       return st;
-    SKG_DISPATCH_L(L, (launch_short_L<LL>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
-                                          (uint8_t*)res.ptr, err, s)))
+    SKG_DISPATCH_L(L, (launch_short_L<LL, false>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
+                                                 (uint8_t*)res.ptr, err, s)))
   }
   if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s, bf, km))) return st;
   return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s, bf, km);
