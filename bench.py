@@ -813,7 +813,7 @@ def run_tour(args=None) -> None:
       fp64_streamk_kernel_ak             the rotation on band-packed Psi, 8192 x 1024
                                          (512 tiles of 128 x 128: the 128-row kernel)
       fp64_streamk_kernel64_ak,          the rotation on band-packed Psi, 110592 x 512,
-      norm_partials / convert_tma (KM)   native and Ozaki (K-major operand reads)
+      convert_short_kernel (KM)          native and Ozaki (K-major operand reads)
       halo_periodic_kernel,              H Psi on the 48^3 grid (= 110592 points) x 512:
       stencil_staged_kernel<32>          periodic halo, then the 6th-order stencil
       nloc_forward / nloc_chi_c /        the nonlocal projector on the same Psi: 64 atoms
