@@ -123,12 +123,12 @@ def test_ozaki_rot_accuracy(cuda, Nd, nb, kind):
 
 @pytest.mark.parametrize("Nd,nb,prec", [(4096, 512, "i8"), (2000, 400, "i8"), (48, 80, "i8"),
                                         (1024, 576, "i8"), (4096, 256, "bf"), (144, 496, "bf"),
-                                        (12296, 256, "i8")])
+                                        (12288, 256, "i8")])
 def test_ozaki_rot_band_equals_grid(cuda, Nd, nb, prec):
     """The Ozaki rotation on band-packed Psi (norms and residues read K-major)
     equals the grid-packed call bit for bit: same exponents, same residues.
-    Nd >= 9600 with nb <= 512 takes the one-pass operand prep in both layouts
-    (12296 grid points: a partial last 16-row group)."""
+    Nd >= 9600 with nb <= 512 takes the one-pass operand prep in both
+    layouts."""
     precision = OZ if prec == "i8" else skgemm.PREC_OZAKI_BF16
     Psi = gaussian((Nd, nb), 5 * Nd + nb, 1 / np.sqrt(Nd))
     Psi[::7, 3] *= 2.0 ** 30  # rows of very different scale
