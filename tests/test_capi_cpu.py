@@ -5,6 +5,7 @@ import ctypes
 import os
 import re
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -87,3 +88,16 @@ def test_no_silent_cpu_fallback():
     with pytest.raises(skgemm.SkgemmError) as e:
         skgemm.gemm.compute_test(2, 2, 2, np.ones(4), np.ones(4), np.zeros(4))
     assert e.value.code in (skgemm.ERR_NO_DEVICE, skgemm.ERR_CUDA)
+
+
+def test_debug_fill_switch_read_from_environment():
+    """SKGEMM_DEBUG_FILL=1 turns the debug fill mode on for the process
+    (read once); it is off otherwise. No device is needed to ask."""
+    assert skgemm.debug_fill() is False
+    code = ("import sys; sys.path.insert(0, %r); import skgemm; "
+            "print(int(skgemm.debug_fill()))" % os.path.join(REPO, "stream-k-gemm_b200"))
+    for val, want in (("1", "1"), ("0", "0")):
+        env = dict(os.environ, SKGEMM_DEBUG_FILL=val)
+        out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True,
+                             text=True, check=True).stdout.strip()
+        assert out == want, (val, out)
