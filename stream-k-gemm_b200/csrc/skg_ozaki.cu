@@ -336,6 +336,40 @@ constexpr int kConvWarps = 8;
 constexpr int kConvTile = 16 * 32;  // doubles per warp tile
 constexpr int kConvSmem = kConvWarps * (kConvStages * kConvTile * 8 + kConvStages * 8);
 
+// BF16 residues of one staged 16-row x 32-k tile (BF16 stages: packed16
+// [32 k][16 rows] unswizzled, K-major as for INT8) for lane (r = lane % 16,
+// h = lane / 16). BF16 rows take 64 bytes per 32-k block: lane h converts
+// k = 8 h .. 8 h + 7 and 16 + 8 h .. 16 + 8 h + 7, so that each of its two
+// 16-byte stores and the other half-lane's together fill one whole 32-byte
+// sector. row: the residue row's first byte of this k-block (plane 0).
+template <int L, bool KM>
+__device__ __forceinline__ void convert_stage_bf16(const double* stage, int r, int h, double s1,
+                                                   double s2, uint8_t* row, int64_t lstride) {
+  auto at = [&](int k) {  // element (k, r) of the stage
+    if constexpr (KM)
+      return stage[(16 * (k >> 4) + r) * 16 + (((((k & 15) >> 1) ^ (r & 7))) << 1) + (k & 1)];
+    else
+      return stage[k * 16 + r];
+  };
+  Digits d[16];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    d[j] = digits_of<L>(at(8 * h + j), s1, s2);
+    d[8 + j] = digits_of<L>(at(16 + 8 * h + j), s1, s2);
+  }
+#pragma unroll
+  for (int l = 0; l < L; ++l) {
+    uint32_t w[8];  // w[i]: elements 2i, 2i + 1
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      w[i] = l == 0 ? pack2(low_byte_bf16(d[2 * i]), low_byte_bf16(d[2 * i + 1]))
+                    : residue_bf16x2<L>(d[2 * i], d[2 * i + 1], l);
+    uint8_t* base = row + l * lstride;
+    *reinterpret_cast<uint4*>(base + 16 * h) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(base + 32 + 16 * h) = make_uint4(w[4], w[5], w[6], w[7]);
+  }
+}
+
 // INT8 residues of one staged 16-row x 32-k tile (conversion kernels' stage
 // layout) for lane (r = lane / 2, h = lane % 2): k = 16 h .. 16 h + 15 of row
 // r, one 16-byte store per residue plane at dst + l lstride.
@@ -456,35 +490,8 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
     uint8_t* dst = res + ((g * 16 + r) * KP + kb * 32 + 16 * h) * ES;
     const int64_t lstride = Rpad * KP * ES;
     if (ok && BF) {
-      // BF16 rows take 64 bytes per 32-k block: lane h converts k = 8h .. 8h+7
-      // and 16+8h .. 16+8h+7, so that each of its two 16-byte stores and the
-      // other half-lane's together fill one whole 32-byte sector.
-      const double* col = buf + s * kConvTile + r;
-      auto at = [&](int k) {  // element (k, r) of the stage
-        if constexpr (KM)
-          return buf[s * kConvTile + (16 * (k >> 4) + r) * 16 +
-                     (((((k & 15) >> 1) ^ (r & 7))) << 1) + (k & 1)];
-        else
-          return col[k * 16];
-      };
-      Digits d[16];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        d[j] = digits_of<L>(at(8 * h + j), s1, s2);
-        d[8 + j] = digits_of<L>(at(16 + 8 * h + j), s1, s2);
-      }
       uint8_t* row = res + ((g * 16 + r) * KP + kb * 32) * 2;
-#pragma unroll
-      for (int l = 0; l < L; ++l) {
-        uint32_t w[8];  // w[i]: elements 2i, 2i + 1
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-          w[i] = l == 0 ? pack2(low_byte_bf16(d[2 * i]), low_byte_bf16(d[2 * i + 1]))
-                        : residue_bf16x2<L>(d[2 * i], d[2 * i + 1], l);
-        uint8_t* base = row + l * lstride;
-        *reinterpret_cast<uint4*>(base + 16 * h) = make_uint4(w[0], w[1], w[2], w[3]);
-        *reinterpret_cast<uint4*>(base + 32 + 16 * h) = make_uint4(w[4], w[5], w[6], w[7]);
-      }
+      convert_stage_bf16<L, KM>(buf + s * kConvTile, r, h, s1, s2, row, lstride);
     } else if (ok) {
       convert_stage_i8<L, KM>(buf + s * kConvTile, r, h, s1, s2, dst, lstride);
     } else {
@@ -504,10 +511,12 @@ __global__ void __launch_bounds__(256, 2) convert_tma_kernel(
 // [32 k][16 rows] with 16-byte chunk c of k-row k at c ^ (k % 8); K-major
 // stages are [2][16 rows][16 k], 128-byte row 16 (k / 16) + r with chunk c
 // at c ^ (r % 8).
-template <bool KM>
+template <bool KM, bool BF = false>
 __device__ __forceinline__ double stage_elem(const double* st, int k, int r) {
   if constexpr (KM)
     return st[(16 * (k >> 4) + r) * 16 + ((((k & 15) >> 1) ^ (r & 7)) << 1) + (k & 1)];
+  else if constexpr (BF)
+    return st[k * 16 + r];  // BF16 packed16 stages are not swizzled
   else
     return st[k * 16 + (((r >> 1) ^ (k & 7)) << 1) + (r & 1)];
 }
@@ -529,7 +538,7 @@ constexpr int kShortKbMax = 16;   // KP <= 512
 constexpr int kShortThreads = 128;  // 4 warps; three CTAs per SM
 constexpr int kShortSmem = kShortKbMax * kConvTile * 8 + 256 * 8 + 32 * 8 + 64 + 1024;
 
-template <int L, bool KM>
+template <int L, bool KM, bool BF>
 __global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
     const __grid_constant__ CUtensorMap map, int64_t R, int64_t K, int64_t KP, int64_t Rpad,
     int gamma_bits, int* __restrict__ mu, uint8_t* __restrict__ res, uint32_t* __restrict__ err) {
@@ -566,7 +575,7 @@ __global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
       const int r = t & 15, kl = t >> 4;
       double acc = 0.0;
       for (int64_t k = kl; k < K; k += 16) {
-        const double v = stage_elem<KM>(tiles + (k >> 5) * kConvTile, (int)(k & 31), r);
+        const double v = stage_elem<KM, BF>(tiles + (k >> 5) * kConvTile, (int)(k & 31), r);
         acc = fma(v, v, acc);
       }
       red[kl * 16 + r] = acc;
@@ -586,16 +595,20 @@ __global__ void __launch_bounds__(kShortThreads, 3) convert_short_kernel(
       sc[16 + threadIdx.x] = s2v;
     }
     __syncthreads();
-    const int r = lane >> 1, h = lane & 1;
+    const int r = BF ? (lane & 15) : (lane >> 1), h = BF ? (lane >> 4) : (lane & 1);
     const double s1 = sc[r], s2 = sc[16 + r];
-    const int64_t lstride = Rpad * KP;
+    constexpr int ES = BF ? 2 : 1;  // bytes per residue
+    const int64_t lstride = Rpad * KP * ES;
     for (int kb = warp; kb < KB; kb += kShortThreads / 32) {
-      uint8_t* dst = res + ((g * 16 + r) * KP + kb * 32 + 16 * h);
-      if (ok) {
-        convert_stage_i8<L, KM>(tiles + kb * kConvTile, r, h, s1, s2, dst, lstride);
+      uint8_t* row = res + ((g * 16 + r) * KP + kb * 32) * ES;
+      if (ok && BF) {
+        convert_stage_bf16<L, KM>(tiles + kb * kConvTile, r, h, s1, s2, row, lstride);
+      } else if (ok) {
+        convert_stage_i8<L, KM>(tiles + kb * kConvTile, r, h, s1, s2, row + 16 * h, lstride);
       } else {
         for (int l = 0; l < L; ++l)
-          *reinterpret_cast<uint4*>(dst + l * lstride) = make_uint4(0, 0, 0, 0);
+          for (int e = 0; e < ES; ++e)
+            reinterpret_cast<uint4*>(row + 16 * h * ES + l * lstride)[e] = make_uint4(0, 0, 0, 0);
       }
     }
     __syncthreads();  // the tiles (and sc, red) are consumed before the next group
@@ -1296,19 +1309,19 @@ int launch_convert(DeviceState* dev, const CUtensorMap& map, int64_t KP, int64_t
 // plus row exponents, in two steps: prep_norms (norm partials, then the row
 // exponents) and prep_convert (the TMA-fed conversion). The steps may run on
 // different streams with an event between them.
-template <int L, bool KM>
+template <int L, bool KM, bool BF>
 int launch_short_L(DeviceState* dev, const CUtensorMap& map, int64_t R, int64_t K, int64_t KP,
                    int64_t Rpad, int* mu, uint8_t* res, uint32_t* err, cudaStream_t s) {
   static bool attr_done[64] = {false};
   if (!attr_done[dev->device]) {
-    SKG_CUDA(cudaFuncSetAttribute(convert_short_kernel<L, KM>,
+    SKG_CUDA(cudaFuncSetAttribute(convert_short_kernel<L, KM, BF>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kShortSmem));
     attr_done[dev->device] = true;
   }
   const int64_t G = Rpad / 16;
   const int64_t grid = std::min<int64_t>(G, 3 * (int64_t)dev->num_sms);  // three CTAs per SM
   KernelTimer kt_(s, "convert_short_kernel");
-  convert_short_kernel<L, KM><<<(unsigned)grid, kShortThreads, kShortSmem, s>>>(map, R, K, KP, Rpad,
+  convert_short_kernel<L, KM, BF><<<(unsigned)grid, kShortThreads, kShortSmem, s>>>(map, R, K, KP, Rpad,
                                                                   gamma_for(L), mu, res, err);
   SKG_CUDA(cudaGetLastError());
   return SKGEMM_OK;
@@ -1391,10 +1404,10 @@ int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad
   // Short rows (K <= 512) and a one-chunk norm pass (ceil(R/16) >= 600): one
   // pass, convert_short_kernel (same exponents and residues bit for bit),
   // for the packed16 layout and its K-major form.
-  if (T == 16 && !bf && KP <= 32 * kShortKbMax && (R + 15) / 16 >= 600 && (!km || K % 16 == 0)) {
+  if (T == 16 && KP <= 32 * kShortKbMax && (R + 15) / 16 >= 600 && (!km || K % 16 == 0)) {
     if ((reinterpret_cast<uintptr_t>(X) & 15) != 0)
       return fail(SKGEMM_ERR_INVALID_ARG, "operand base must be 16-byte aligned");
-    if ((st = res.ensure((size_t)L * Rpad * KP))) return st;
+    if ((st = res.ensure((size_t)L * Rpad * KP * (bf ? 2 : 1)))) return st;
     if ((st = mu.ensure((size_t)Rpad * sizeof(int)))) return st;
     CUtensorMap map;
     if (km) {
@@ -1406,18 +1419,26 @@ int prep_packed(DeviceState* dev, int64_t R, int64_t K, int64_t KP, int64_t Rpad
       if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                              CU_TENSOR_MAP_SWIZZLE_128B)))
         return st;
-      SKG_DISPATCH_L(L, (launch_short_L<LL, true>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
-                                                  (uint8_t*)res.ptr, err, s)))
+      if (bf) {
+        SKG_DISPATCH_L(L, (launch_short_L<LL, true, true>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
+                                                          (uint8_t*)res.ptr, err, s)))
+      }
+      SKG_DISPATCH_L(L, (launch_short_L<LL, true, false>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
+                                                         (uint8_t*)res.ptr, err, s)))
     }
     const int64_t P_in = (R + 15) / 16;
     const uint64_t dims[3] = {16, (uint64_t)K, (uint64_t)P_in};
     const uint64_t strides[2] = {16 * 8, (uint64_t)K * 16 * 8};
     const uint32_t box[3] = {16, 32, 1};
     if ((st = encode_tiled(&map, 3, X, dims, strides, box, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                           CU_TENSOR_MAP_SWIZZLE_128B)))
+                           bf ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B)))
       return st;
-    SKG_DISPATCH_L(L, (launch_short_L<LL, false>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
-                                                 (uint8_t*)res.ptr, err, s)))
+    if (bf) {
+      SKG_DISPATCH_L(L, (launch_short_L<LL, false, true>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
+                                                         (uint8_t*)res.ptr, err, s)))
+    }
+    SKG_DISPATCH_L(L, (launch_short_L<LL, false, false>(dev, map, R, K, KP, Rpad, (int*)mu.ptr,
+                                                        (uint8_t*)res.ptr, err, s)))
   }
   if ((st = prep_norms<T>(R, K, KP, Rpad, X, L, res, part, mu, s, bf, km))) return st;
   return prep_convert<T>(dev, R, K, KP, Rpad, X, L, res, mu, err, s, bf, km);

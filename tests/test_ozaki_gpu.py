@@ -123,7 +123,7 @@ def test_ozaki_rot_accuracy(cuda, Nd, nb, kind):
 
 @pytest.mark.parametrize("Nd,nb,prec", [(4096, 512, "i8"), (2000, 400, "i8"), (48, 80, "i8"),
                                         (1024, 576, "i8"), (4096, 256, "bf"), (144, 496, "bf"),
-                                        (12288, 256, "i8")])
+                                        (12288, 256, "i8"), (12288, 256, "bf")])
 def test_ozaki_rot_band_equals_grid(cuda, Nd, nb, prec):
     """The Ozaki rotation on band-packed Psi (norms and residues read K-major)
     equals the grid-packed call bit for bit: same exponents, same residues.
@@ -310,7 +310,7 @@ def test_ozaki_bf16_syrk_and_pair_equal_int8(cuda, K, M):
     assert oracle.rel_frobenius(s[iu], oracle.dot2_matmul(Psi.T, Psi)[iu]) <= TOL
 
 
-@pytest.mark.parametrize("Nd,nb", [(2048, 512), (1040, 208), (512, 1024)])
+@pytest.mark.parametrize("Nd,nb", [(2048, 512), (1040, 208), (512, 1024), (12288, 256)])
 def test_ozaki_bf16_rot_equals_int8(cuda, Nd, nb):
     Psi = gaussian((Nd, nb), 51)
     Q = uniform((nb, nb), 52)
