@@ -8,16 +8,16 @@
 //   out[index_p[r], b] += sum_j chi_p[r, j] C_p[j, b]             (chi C + scatter)
 // The single-rank all-reduce of the coefficients is the identity here.
 //
-// Two kernels, no atomics, the reference's loop and rounding order (as its
+// Three kernels, no atomics, the reference's loop and rounding order (as its
 // C++ compiles: the forward dot products unfused, the block update fused, the
 // back-projection sums fused), so results equal it bit for bit:
 //  * nloc_forward_kernel: CTA per (block, 32 bands, 16 columns) — for each of
 //    the block's projectors in order, gathered psi rows staged in shared
-//    memory, each (column, band) thread summing them in row order; then the
-//    block's gamma scalings in order;
+//    memory (double-buffered asynchronous copies), each (column, band) thread
+//    summing them in row order; then the block's gamma scalings in order;
 //  * nloc_chi_c_kernel: the back-projection rows chi_p C_p of every projector
-//    (spans of 64-row tiles x 64 bands, C and chi staged in shared memory), into a
-//    scratch of total rows x nb;
+//    (spans of 64-row tiles x 64 bands, C and chi staged in shared memory),
+//    into a scratch of total rows x nb;
 //  * nloc_backward_kernel: thread per (touched grid point, band pair) — walks
 //    the point's (projector, row) entries in projector order (an inverse index
 //    built at creation, each entry stored as its scratch row), so the
