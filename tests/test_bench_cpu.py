@@ -48,3 +48,19 @@ def test_subspace_errors_index_maps():
         assert e["S"] > 1e-10 and e["Psi_Q"] > 1e-10 and e["Hs"] <= 1e-14
     finally:
         bench.set_shape(bench.ND0, bench.NB0)
+
+
+def test_profile_traffic_lines_parse():
+    """The bench's `roofline.traffic` comes from the committed ncu summaries'
+    `traffic_bytes_per_launch <kernel>:` lines: each kernel the headline
+    roofline can name has one, and it parses to bytes per launch."""
+    for kernel, lo, hi in [("convert_tma_kernel", 1e9, 2e9),
+                           ("i8_gemm2_kernel", 5e8, 2e9),
+                           ("i8_rot_kernel", 1e9, 2e9),
+                           ("fp64_streamk_kernel", 1e9, 4e9),
+                           ("fp64_streamk_kernel64", 1e9, 4e9),
+                           ("stencil_staged_kernel", 1e9, 2e9),
+                           ("nloc_backward_kernel", 5e8, 2e9)]:
+        t = bench.read_profile_traffic(kernel)
+        assert t is not None and lo <= t <= hi, (kernel, t)
+    assert bench.read_profile_traffic("no_such_kernel") is None
